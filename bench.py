@@ -1,0 +1,359 @@
+"""UVLM time-stepper benchmark on B200 (one JSON line on rank 0).
+
+Workload (the metric's configuration): one flat-plate wing, aspect ratio 8
+(chord 1, span 8), 32 x 128 = 4096 bound vortex rings, heave
+h = 0.2 sin(wt) and pitch 10 deg sin(wt + 90 deg) about the leading-edge root,
+reduced frequency k = wc/2U = 0.5 (w = 1), U = 1, dt = 2 pi / w / 40, RK2 wake
+advection.  The run is advanced 400 steps so that the wake holds 400 ring rows
+(51,200 rings); --erase_wake_after 400 (EraseOldestWake) then keeps it at that
+size while steps are timed.  A "step" is one full MainLoop: kinematics, shed,
+influence matrix, RHS, solve, Joukowski loads and RK2 roll-up.
+
+value       steps/s of the mixed-precision form (FP32 N-body and assembly,
+            stale-LU-preconditioned GMRES with FP64 residuals), device-timed
+            with CUDA events on the library's stream, L2 flushed between steps
+plain_fp64  steps/s of the plain FP64 form (fresh FP64 LU every step)
+cl_rel_err  max |CL_mixed - CL_fp64| / max |CL_fp64| over the 400-step run
+e2e         the same metric through the C-ABI, wall-clock, with the load row
+            and the circulation vector copied to host memory every step
+roofline    the N-body advection kernel: 59 FLOP per (target, unique segment)
+            pair over the measured FP32 FMA peak of this GPU
+cpu_baseline the FP64 CPU oracle (restated reference) on a bounded sample
+
+--impl reference times that CPU oracle alone (the reference cannot be built
+here) on a synthetic state of the same shapes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "UVLM steps/s (4096 panels, 50k wake) mixed+learned vs plain FP64, CL err<=1e-6"
+ROWS, COLS, CHORD, SPAN = 32, 128, 1.0, 8.0
+OMEGA = 1.0  # k = 0.5, c = 1, U = 1
+DT = 2 * math.pi / OMEGA / 40
+WAKE_ROWS = 400
+FLOP_PER_PAIR = 59
+
+
+def workload_config():
+    return {"workload": "single flapping wing 32x128 (4096 rings), heave 0.2 sin(wt) + pitch 10deg sin(wt+90deg), "
+                        "k=0.5, RK2, wake held at 400 rows (51,200 rings) by erase_wake_after=400",
+            "rows": ROWS, "cols": COLS, "wake_rings": WAKE_ROWS * COLS, "dt": DT, "advection": "RK2",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def make_sim(precision, **kw):
+    import uvlm_b200 as U
+
+    sim = U.SimpleSimulator(precision=precision, erase_wake_after=WAKE_ROWS, max_wake_rows=WAKE_ROWS + 8, **kw)
+    m = U.Morphing().set_plug(0.2, OMEGA).set_twist(math.radians(10), OMEGA, math.pi / 2)
+    sim.AddWing(U.RectGenerator(), m, CHORD, SPAN, ROWS, COLS, (0.0, 0.0, 0.0))
+    sim.set_forward_flight([-1.0, 0.0, 0.0])
+    sim.set_advection("RK2")
+    return sim
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[2 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def oracle_sample(state, stride, lu_n, threads):
+    """Time one MainLoop of the FP64 CPU oracle on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as o
+
+    sim = o.Simulator()
+    kin = o.kinematics(plug_amp=0.2, plug_omega=OMEGA, twist_amp=math.radians(10), twist_omega=OMEGA,
+                       twist_phase=math.pi / 2)
+    sim.add_wing(CHORD, SPAN, ROWS, COLS, kin=kin)
+    sim.set_forward_flight([-1.0, 0.0, 0.0])
+    sim.set_advection("RK2")
+    sim.set_threads(threads)
+    sim.begin()
+    wr = state["wake_gamma"].shape[1]
+    sim.set_state(wr, state["wing_pos"], state["wake_pos"], state["wing_gamma"], state["wing_gamma_prev"],
+                  state["wake_gamma"])
+    sec = sim.time_step_sampled(WAKE_ROWS + 1, DT, stride, lu_n)
+    return float(np.sum(sec)), sec
+
+
+def synthetic_state():
+    """Wake of the metric's shape from pure convection of the shed trailing edge
+    (no roll-up), for runs that cannot advance the GPU solver."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as o
+
+    kin = o.kinematics(plug_amp=0.2, plug_omega=OMEGA, twist_amp=math.radians(10), twist_omega=OMEGA,
+                       twist_phase=math.pi / 2)
+    half = o.rect_generate(CHORD, SPAN / 2, ROWS, COLS // 2)
+    nodes = o.whole_wing(half, ROWS, COLS // 2).reshape(ROWS + 1, COLS + 1, 3)
+    t_now = WAKE_ROWS * DT
+    wing = np.array([o.perfome(kin, p, t_now) for p in nodes.reshape(-1, 3)]).reshape(1, ROWS + 1, COLS + 1, 3)
+    te0 = nodes[ROWS]
+    wake = np.zeros((1, WAKE_ROWS + 1, COLS + 1, 3))
+    for i in range(WAKE_ROWS + 1):
+        t = t_now - i * DT
+        wake[0, i] = np.array([o.perfome(kin, p, t) for p in te0]) + np.array([i * DT, 0, 0])
+    y = np.linspace(-1, 1, COLS)
+    g = np.sqrt(np.clip(1 - y ** 2, 0, None)) * 0.1
+    wing_gamma = np.tile(g, (ROWS, 1))[None] * np.linspace(1, 0.2, ROWS)[None, :, None]
+    wake_gamma = np.stack([g * 0.1 * math.sin(OMEGA * (t_now - i * DT)) for i in range(WAKE_ROWS)])[None]
+    return dict(wing_pos=wing, wake_pos=wake, wing_gamma=wing_gamma, wing_gamma_prev=wing_gamma * 0.99,
+                wake_gamma=wake_gamma)
+
+
+def cpu_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def run_reference(args, rank, world):
+    threads = cpu_threads()
+    if rank != 0:
+        return
+    state = synthetic_state()
+    stride, lu_n = 1024, 512
+    for _ in range(args.warmup):
+        oracle_sample(state, stride, lu_n, threads)
+    times = []
+    for _ in range(args.steps):
+        t, _ = oracle_sample(state, stride, lu_n, threads)
+        times.append(t)
+    value = args.steps / float(np.sum(times))
+    sample = (f"one MainLoop per step at the 51,200-ring state: N-body stages (assembly, RHS, loads, RK2 advection) on "
+              f"every {stride}th target scaled x{stride}, FullPivLU on the leading {lu_n}x{lu_n} block scaled by "
+              f"(4096/{lu_n})^3; OpenMP {threads} threads; synthetic convected wake")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def timed_steps(sim, first_step, k, flush_buf, torch, stream):
+    """Per-step CUDA-event times on the library's stream, L2 flushed between."""
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+    rows = []
+    with torch.cuda.stream(stream):
+        for i in range(k):
+            flush_buf.fill_(float(i))
+            ev0[i].record(stream)
+            rows.append(sim.step(first_step + i, DT))
+            ev1[i].record(stream)
+    torch.cuda.synchronize()
+    return np.array([a.elapsed_time(b) for a, b in zip(ev0, ev1)]), rows
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import uvlm_b200 as U
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+
+    # --- accuracy run: both forms from step 0 to the 400-row wake ------------
+    sim64 = make_sim("fp64", device=dev)
+    simmx = make_sim("mixed", device=dev, solver="gmres_stale", warm_start="extrapolate")
+    sim64.begin()
+    simmx.begin()
+    cl64, clmx = [], []
+    t0 = time.time()
+    for s in range(WAKE_ROWS + 1):
+        cl64.append(sim64.step(s, DT))
+        clmx.append(simmx.step(s, DT))
+    preroll_s = time.time() - t0
+    cl64, clmx = np.array(cl64), np.array(clmx)
+    cl_err = float(np.max(np.abs(clmx[:, 2] - cl64[:, 2])) / np.max(np.abs(cl64[:, 2])))
+    cd_err = float(np.max(np.abs(clmx[:, 1] - cl64[:, 1])) / np.max(np.abs(cl64[:, 1])))
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
+    step0 = WAKE_ROWS + 1
+    # --- warm-up and timed steps ---------------------------------------------
+    s_mx = torch.cuda.ExternalStream(simmx.stream(), device=dev)
+    s_64 = torch.cuda.ExternalStream(sim64.stream(), device=dev)
+    for i in range(args.warmup):
+        simmx.step(step0 + i, DT)
+        sim64.step(step0 + i, DT)
+    step0 += args.warmup
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    launches0 = U.lib().uvlm_kernel_launch_count()
+    t_mx, _ = timed_steps(simmx, step0, args.steps, flush, torch, s_mx)
+    launches = U.lib().uvlm_kernel_launch_count() - launches0
+    clk = clocks.stop()
+    t_64, _ = timed_steps(sim64, step0, args.steps, flush, torch, s_64)
+    st = simmx.stats()
+    total_mx = float(np.sum(t_mx))
+    if world > 1:
+        tt = torch.tensor([total_mx], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_mx = float(tt.item())
+        dist.barrier()
+    value = world * args.steps / (total_mx * 1e-3)
+    plain = args.steps / (float(np.sum(t_64)) * 1e-3)
+    step0 += args.steps
+
+    # --- stage timing + roofline of the N-body advection kernel --------------
+    simmx.set_stage_timing(True)
+    simmx.step(step0, DT)
+    stmx = simmx.stats()
+    simmx.set_stage_timing(False)
+    step0 += 1
+    stage_ms = [float(x) for x in stmx.stage_ms]
+    C1 = COLS + 1
+    W = WAKE_ROWS + 1  # ring rows during the advect stage (before the erase)
+    segs_bound = (ROWS + 1) * COLS + ROWS * C1
+    segs_wake = (W + 1) * COLS + W * C1
+    pairs_advect = 2 * W * C1 * (segs_bound + segs_wake)
+    adv_ms = stage_ms[5]
+    achieved = FLOP_PER_PAIR * pairs_advect / (adv_ms * 1e-3) / 1e12
+    peak = U._capi.c_double() if False else None
+    import ctypes as C
+
+    pk = C.c_double()
+    U._capi.check(U.lib().uvlm_measure_fp32_peak(dev, C.byref(pk)))
+    peak = pk.value
+
+    # --- end-to-end through the C-ABI with host buffers ------------------------
+    e2e_t = []
+    gam = np.zeros((1, ROWS, COLS))
+    for i in range(args.steps):
+        t1 = time.perf_counter()
+        simmx.step(step0 + i, DT)
+        U.lib().uvlm_get_state(simmx._h, None, None, None, gam.ctypes.data_as(C.POINTER(C.c_double)), None, None)
+        e2e_t.append(time.perf_counter() - t1)
+    step0 += args.steps
+    e2e_value = world * args.steps / float(np.sum(e2e_t))
+
+    # --- CPU baseline (rank 0 only) --------------------------------------------
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        state = simmx.state()
+        threads = cpu_threads()
+        stride, lu_n = 128, 1024
+        tcpu, secs = oracle_sample(state, stride, lu_n, threads)
+        cpu = {"value": 1.0 / tcpu, "unit": "steps/s", "cores": threads, "kind": "port",
+               "sample": (f"FP64 CPU oracle, one MainLoop at the 51,200-ring state: N-body stages on every "
+                          f"{stride}th target scaled x{stride}, FullPivLU on the leading {lu_n}^2 block scaled by "
+                          f"(4096/{lu_n})^3; stage seconds {[round(float(x), 3) for x in secs]}")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_mx / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": dict(workload_config(), parallelism=f"replicas x{world}",
+                           form="mixed: FP32 N-body+assembly, stale-LU GMRES (FP64 residual), warm start "
+                                "2*g_n-g_{n-1}"),
+            "plain_fp64_steps_per_s": plain, "speedup_vs_plain_fp64": value / world / plain,
+            "cl_rel_err": cl_err, "cd_rel_err": cd_err, "cl_err_reference": "plain FP64 GPU form, same 400 steps",
+            "gmres_iters_last": int(st.gmres_iters), "solve_path_last": int(st.solve_path),
+            "stage_ms": {"kin_shed": stage_ms[0], "assembly": stage_ms[1], "rhs": stage_ms[2], "solve": stage_ms[3],
+                         "loads": stage_ms[4], "advect": stage_ms[5], "total": stage_ms[7]},
+            "roofline": {"bound": "fp32_simt", "kernel": "nbody_kernel (RK2 advection stage)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": "FP32 FMA probe on this GPU (uvlm_measure_fp32_peak)",
+                         "per_unit": f"{FLOP_PER_PAIR} FLOP per (target, unique segment) pair",
+                         "units_per_step": pairs_advect, "traffic": None},
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * (3 + ROWS * COLS),
+                    "note": "wall clock per uvlm_step + circulation download; per-step inputs are scalars"},
+            "gpu_launches": int(launches), "clocks": clk, "preroll_s": preroll_s,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim64.close()
+    simmx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,229 @@
+/*
+ * uvlm_b200.h -- C-ABI of the B200 (sm_100a) UVLM time-stepper.
+ *
+ * Drop-in boundary for the per-step hot path of xeno14/UVLM: plain pointers
+ * and sizes, no C++ or torch types.  Host arrays are borrowed only for the
+ * duration of a call (copied in or out); all simulation state lives in HBM
+ * inside an opaque context.  Every function returns a status code (0 = OK);
+ * uvlm_last_error() gives the message of the last failure on a context, and
+ * uvlm_global_last_error() that of the context-free entry points.
+ *
+ * Layouts (the reference's MultipleSheet, whose element K sits at
+ * j + cols*(i + rows*n), with Eigen::Vector3d = 3 packed doubles):
+ *   node sheet  (num, rows+1, cols+1) x 3 doubles  [n][i][j][xyz]
+ *   gamma sheet (num, rows,   cols)       doubles  [n][i][j]
+ *   AoS ring    4 nodes x 3 doubles (VortexRing::nodes())
+ *
+ * Reference interfaces replaced (paths inside xeno14/UVLM):
+ *   SimpleSimulator::{AddWing,Run,MainLoop,set_forward_flight,set_advection}
+ *       src/simulator/simple_simulator.h:50-63, simple_simulator.cpp:126-313
+ *   advect::Advection::Advect + AdvectFactory
+ *       src/advect.h:48-59, src/advect_factory.cpp:43-60
+ *   UVLM::InducedVelocity(x, pos, gamma)          src/velocity.h:14-24
+ *   UVLM::InducedVelocity / ChordwiseInducedVelocity / Advect /
+ *       AdvectParallel / ConnectTrailingEdge (AoS) src/shed.h:14-46
+ *   UVLM::SolveLinearProblem (AoS)                src/linear.h:104-119
+ *   Eigen::FullPivLU<MatrixXd>(A).solve(b)        src/simulator/simple_simulator.cpp:264-268
+ */
+#ifndef UVLM_B200_H_
+#define UVLM_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define UVLM_OK 0
+#define UVLM_ERR_INVALID 1     /* bad argument, shape or name */
+#define UVLM_ERR_CUDA 2        /* CUDA runtime error */
+#define UVLM_ERR_SINGULAR 3    /* zero pivot in the LU factorisation */
+#define UVLM_ERR_NONFINITE 4   /* non-finite circulation after the solve */
+#define UVLM_ERR_STATE 5       /* call out of order (e.g. step before begin) */
+#define UVLM_ERR_CAPACITY 6    /* wake longer than max_wake_rows */
+#define UVLM_ERR_TIMEOUT 7     /* a bounded device-side wait gave up */
+#define UVLM_ERR_UNSUPPORTED 8 /* size or option outside what is built */
+
+/* Advection schemes: AdvectFactory names "euler", "RK2", "RK4", "AB2". */
+#define UVLM_ADVECT_EULER 0
+#define UVLM_ADVECT_RK2 1
+#define UVLM_ADVECT_RK4 2
+#define UVLM_ADVECT_AB2 3
+
+/* Arithmetic of the N-body, assembly and factorisation stages. */
+#define UVLM_PRECISION_FP64 0  /* plain form: FP64 everywhere, fresh LU each step */
+#define UVLM_PRECISION_MIXED 1 /* FP32 N-body/assembly, TF32/BF16 LU, FP64 residual */
+
+/* Dense solve strategy. */
+#define UVLM_SOLVER_LU 0          /* factor + solve every step (the reference's method) */
+#define UVLM_SOLVER_GMRES_STALE 1 /* GMRES, FP64 residual, preconditioned by stale LU */
+
+/* Initial guess of the GMRES solve. */
+#define UVLM_WARM_PREVIOUS 0    /* previous step's circulation */
+#define UVLM_WARM_EXTRAPOLATE 1 /* 2*Gamma_n - Gamma_{n-1} */
+#define UVLM_WARM_MLP 2         /* learned warm start (uvlm_set_mlp) */
+
+/* Factor precision of the mixed form (trailing updates on tcgen05). */
+#define UVLM_LU_TF32 0
+#define UVLM_LU_BF16 1
+
+typedef struct uvlm_ctx uvlm_ctx;
+
+typedef struct {
+  int32_t precision;        /* UVLM_PRECISION_* */
+  int32_t solver;           /* UVLM_SOLVER_* */
+  int32_t warm_start;       /* UVLM_WARM_* */
+  int32_t lu_precision;     /* UVLM_LU_* (mixed form) */
+  int32_t advection;        /* UVLM_ADVECT_* */
+  int32_t rk_ignore_rows;   /* RK2/RK4 use Euler for wake rows i <= this (5, src/advect.h:77) */
+  int64_t max_wake_rows;    /* capacity in ring rows */
+  int64_t erase_wake_after; /* --erase_wake_after (0 = never) */
+  int32_t gmres_restart;    /* Krylov dimension before a restart */
+  int32_t gmres_max_iter;   /* above this a fresh LU is factored (the fallback) */
+  double gmres_tol;         /* relative residual ||b - A g|| / ||b|| */
+  int32_t device;           /* CUDA device ordinal */
+  int32_t compute_loads;    /* 1: Joukowski loads every step (CalcLoad) */
+  int32_t assembly_fp64;    /* mixed form: assemble the residual matrix in FP64 */
+  int32_t nbody_variant;    /* -1: autotune; else a tile variant index */
+} uvlm_config;
+
+/* Closed-form kinematics of one wing (Morphing, src/morphing.h:70-92, with the
+ * std::function arguments replaced by sinusoids):
+ *   plug(t)     = plug_amp * sin(plug_omega * t + plug_phase)
+ *   flap(t)     = flap_amp * sin(flap_omega * t + flap_phase)
+ *   twist(x0,t) = (twist_amp + twist_span_slope*|y|) * sin(twist_omega*t + twist_phase)
+ *   bend(x0,t)  = (bend_cx*x*(1-x) + bend_cy*y*y) * sin(bend_omega*t + bend_phase)
+ * with (x, y) taken from x_ref = x0 - origin mirrored to y >= 0.  The velocity
+ * is the reference's FP64 central difference with h = 1e-6. */
+typedef struct {
+  double alpha;
+  double plug_amp, plug_omega, plug_phase;
+  double flap_amp, flap_omega, flap_phase;
+  double twist_amp, twist_span_slope, twist_omega, twist_phase;
+  double bend_cx, bend_cy, bend_omega, bend_phase;
+  double origin[3];
+} uvlm_kinematics;
+
+/* One rectangular wing: RectGenerator + WholeWing of AddWing/BuildWing
+ * (src/simulator/simple_simulator.cpp:126-169, src/wing/rect.cpp:18-45,
+ * src/wing/wing.cpp:12-52).  cols must be even. */
+typedef struct {
+  double chord, span;
+  int64_t rows, cols;
+  double origin[3];
+  int32_t chebyshev_chord, chebyshev_span;
+} uvlm_wing_desc;
+
+typedef struct {
+  int64_t step;
+  double t;
+  int32_t solve_path;   /* 0 fresh LU, 1 GMRES with stale LU, 2 GMRES then fresh-LU fallback */
+  int32_t gmres_iters;
+  double residual;      /* final ||b - A g|| / ||b|| (FP64), 0 for the plain LU path */
+  int32_t refactored;   /* a factorisation ran in this step */
+  int32_t wake_rows;    /* ring rows of the wake after the step */
+  double stage_ms[8];   /* kinematics+shed, assembly, rhs, solve, loads, advect, warm start, total */
+} uvlm_step_stats;
+
+/* ------------------------------------------------------- time-stepper */
+void uvlm_config_default(uvlm_config* cfg);
+int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out);
+int uvlm_destroy(uvlm_ctx* ctx);
+const char* uvlm_last_error(const uvlm_ctx* ctx);
+const char* uvlm_global_last_error(void);
+const char* uvlm_status_string(int status);
+
+/* SimpleSimulator::AddWing (simple_simulator.cpp:126-140): all wings must
+ * share rows and cols, cols even. */
+int uvlm_add_wing(uvlm_ctx* ctx, const uvlm_wing_desc* wing, const uvlm_kinematics* kin);
+/* SimpleSimulator::set_forward_flight (simple_simulator.h:57). */
+int uvlm_set_forward_flight(uvlm_ctx* ctx, const double ff[3]);
+/* SimpleSimulator::set_advection + AdvectFactory(name). */
+int uvlm_set_advection(uvlm_ctx* ctx, const char* name);
+/* Prologue of SimpleSimulator::Run (simple_simulator.cpp:288-303): builds
+ * the wings and an empty wake; resets AB2 history. */
+int uvlm_begin(uvlm_ctx* ctx);
+/* SimpleSimulator::MainLoop(step, dt) plus the optional erase
+ * (simple_simulator.cpp:240-286, 307-311).  load_row (host, may be NULL)
+ * receives t, CD0, CL0, CD1, CL1, ... (1 + 2*num doubles, CalcLoad :226-232). */
+int uvlm_step(uvlm_ctx* ctx, int64_t step, double dt, double* load_row);
+/* SimpleSimulator::Run(steps, dt): begin + steps+1 MainLoops; loads (host,
+ * may be NULL) receives (steps+1) rows of 1 + 2*num doubles. */
+int uvlm_run(uvlm_ctx* ctx, int64_t steps, double dt, double* loads);
+/* SimpleSimulator::EraseOldestWake (simple_simulator.cpp:235-238). */
+int uvlm_erase_oldest_wake(uvlm_ctx* ctx);
+int uvlm_get_sizes(const uvlm_ctx* ctx, int64_t* num, int64_t* rows, int64_t* cols, int64_t* wake_rows,
+                   int64_t* wake_node_rows);
+/* Copies of the state (host arrays in the MultipleSheet layouts above; any
+ * pointer may be NULL).  wake_pos has wake_node_rows rows. */
+int uvlm_get_state(uvlm_ctx* ctx, double* wing_pos, double* wing_pos_init, double* wake_pos, double* wing_gamma,
+                   double* wing_gamma_prev, double* wake_gamma);
+/* Replaces positions and circulations with a wake of wake_rows ring rows
+ * (wake_rows + 1 node rows); clears AB2 history and the stale factors. */
+int uvlm_set_state(uvlm_ctx* ctx, int64_t wake_rows, const double* wing_pos, const double* wake_pos,
+                   const double* wing_gamma, const double* wing_gamma_prev, const double* wake_gamma);
+int uvlm_get_last_stats(const uvlm_ctx* ctx, uvlm_step_stats* stats);
+/* 1: record per-stage times with CUDA events (adds synchronisation). */
+int uvlm_set_stage_timing(uvlm_ctx* ctx, int32_t enable);
+int uvlm_synchronize(uvlm_ctx* ctx);
+/* The CUDA stream the context launches on (cudaStream_t), for callers that
+ * time or order work around uvlm_step. */
+void* uvlm_stream(uvlm_ctx* ctx);
+/* Number of CUDA kernels this library has launched in this process (all
+ * contexts and entry points); differences bracket a region of interest. */
+int64_t uvlm_kernel_launch_count(void);
+/* Measured FP32 FMA throughput of the device (TFLOP/s): the denominator of
+ * the N-body roofline.  No counterpart in the reference (measurement aid). */
+int uvlm_measure_fp32_peak(int32_t device, double* tflops);
+/* Algorithmic work of the last step: unique-segment interactions of every
+ * N-body stage and the assembly (target x segment pairs). */
+int uvlm_get_last_work(const uvlm_ctx* ctx, double* nbody_pairs, double* assembly_pairs, double* lu_flops);
+
+/* ------------------------------------------- context-free reference API */
+/* UVLM::InducedVelocity(x, pos, gamma) for n_targets points
+ * (src/velocity.h:14-24).  pos: (num, grows+1, gcols+1) nodes; gamma:
+ * (num, grows, gcols); targets/out: n_targets x 3.  precision: UVLM_PRECISION_*. */
+int uvlm_sheet_induced_velocity(const double* pos, const double* gamma, int64_t num, int64_t grows, int64_t gcols,
+                                const double* targets, int64_t n_targets, double* out, int32_t precision);
+
+/* advect::Advection strategy object (src/advect.h:48-59) from
+ * AdvectFactory(name) (src/advect_factory.cpp:43-60): "euler", "RK2",
+ * "RK4", "AB2".  AB2 keeps its velocity history between calls. */
+typedef struct uvlm_advection uvlm_advection;
+int uvlm_advection_create(const char* name, int32_t precision, uvlm_advection** out);
+int uvlm_advection_destroy(uvlm_advection* adv);
+/* Advection::Advect(next, wing_pos, wing_gamma, wake_pos, wake_gamma,
+ * forward_flight, dt).  Shapes: wing (num, rows, cols) rings, wake
+ * (num, wake_rows, cols) rings with wake_rows + 1 node rows.  `next` may alias
+ * `wake_pos` (simple_simulator.cpp:190-193). */
+int uvlm_advection_advect(uvlm_advection* adv, double* next, const double* wing_pos, const double* wing_gamma,
+                          int64_t num, int64_t rows, int64_t cols, const double* wake_pos, const double* wake_gamma,
+                          int64_t wake_rows, const double forward_flight[3], double dt);
+
+/* UVLM::InducedVelocity / ChordwiseInducedVelocity over AoS rings
+ * (src/shed.inl:22-33, 66-77) for n_targets points. */
+int uvlm_rings_induced_velocity(const double* rings, const double* gammas, int64_t n_rings, const double* targets,
+                                int64_t n_targets, int32_t chordwise_only, double* out);
+/* UVLM::AdvectParallel (src/shed.inl:52-64): every node of every wake ring
+ * moves by (induced + freestream) * dt, velocities taken before any move. */
+int uvlm_rings_advect(const double* vortex_rings, const double* vortex_gamma, int64_t n_vortex, double* wake_rings,
+                      int64_t n_wake, const double freestream[3], double dt);
+/* UVLM::ConnectTrailingEdge (src/shed.inl:79-86). */
+int uvlm_rings_connect_trailing_edge(const double* edge_rings, int64_t n_edge, double* wake_rings);
+/* UVLM::SolveLinearProblem (src/linear.inl:113-130).  drop_wake_term = 1
+ * reproduces the reference, whose wake RHS term is a discarded statement
+ * (src/linear.inl:123-124); 0 subtracts the wake normal wash. */
+int uvlm_rings_solve_linear_problem(const double* bound_rings, const double* bound_rings0, int64_t n_bound,
+                                    const double* wake_rings, const double* wake_gamma, int64_t n_wake,
+                                    const double freestream[3], const uvlm_kinematics* kin, double t,
+                                    int32_t drop_wake_term, double* gamma_out);
+/* Dense solve A x = b, A row-major n x n (FullPivLU replacement).  method:
+ * 0 FP64 LU; 1 TF32 LU + FP64-residual GMRES; 2 BF16 LU + GMRES.
+ * iters (may be NULL) receives the GMRES iteration count. */
+int uvlm_dense_solve(const double* A, int64_t n, const double* b, double* x, int32_t method, int32_t* iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UVLM_B200_H_ */

@@ -1,0 +1,90 @@
+"""Parity cases shared by the fixture generator and the tests.
+
+Each case is a SimpleSimulator set-up in the reference's own terms (wings from
+RectGenerator + WholeWing, Morphing kinematics, forward flight, advection
+scheme, dt, steps).  ``cfg1`` is the reference's CPU-runnable configuration:
+one 8 x 16 flat-plate wing (chord 1, span 4), plunge 0.1 sin(2 pi 0.25 t) at
+5 degrees, U = 1, dt = 1/8, 200 explicit-Euler steps; its lattice is shifted
+1/4 panel downstream so that the ring centroids (the reference's collocation
+points) sit at 3/4 of each geometric panel chord.
+"""
+import math
+
+DEG = math.pi / 180.0
+
+CASES = {
+    "cfg1_euler_200": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=8, cols=16, origin=(1.0 / 8 / 4, 0.0, 0.0),
+                    kin=dict(alpha=5 * DEG, plug_amp=0.1, plug_omega=2 * math.pi * 0.25))],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=0.125, steps=200),
+    "rk2_heave_pitch_4x8": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
+                    kin=dict(plug_amp=0.2, plug_omega=1.0, twist_amp=10 * DEG, twist_omega=1.0,
+                             twist_phase=math.pi / 2))],
+        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / 40, steps=14),
+    "rk4_flap_4x8": dict(
+        wings=[dict(chord=1.0, span=6.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
+                    kin=dict(alpha=4 * DEG, flap_amp=15 * DEG, flap_omega=0.2, flap_phase=math.pi / 2,
+                             twist_span_slope=4 * DEG / 6.0, twist_omega=0.2, twist_phase=math.pi))],
+        ff=(-1.0, 0.0, 0.0), advection="RK4", dt=0.25, steps=10),
+    "ab2_plunge_4x8": dict(
+        wings=[dict(chord=1.0, span=6.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
+                    kin=dict(alpha=5 * DEG, plug_amp=0.175, plug_omega=1.0, plug_phase=math.pi / 2))],
+        ff=(-1.0, 0.0, 0.0), advection="AB2", dt=2 * math.pi / 40, steps=12),
+    "two_wings_euler_3x6": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=3, cols=6, origin=(0.0, 0.0, 0.0),
+                    kin=dict(alpha=5 * DEG, plug_amp=0.15, plug_omega=0.8)),
+               dict(chord=1.0, span=4.0, rows=3, cols=6, origin=(1.5, 0.0, 0.5),
+                    kin=dict(alpha=5 * DEG, plug_amp=0.15, plug_omega=0.8, plug_phase=math.pi / 2))],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=0.2, steps=10),
+    "morph_bend_rk2_4x8": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
+                    kin=dict(alpha=3 * DEG, bend_cx=0.05, bend_cy=0.1, bend_omega=0.6))],
+        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=0.2, steps=10),
+    "erase_euler_4x8": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
+                    kin=dict(alpha=5 * DEG, plug_amp=0.1, plug_omega=1.0))],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=0.2, steps=14, erase_wake_after=8),
+    "chebyshev_euler_4x8": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0), cheb_chord=True, cheb_span=True,
+                    kin=dict(alpha=6 * DEG, plug_amp=0.05, plug_omega=1.5))],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=0.2, steps=8),
+}
+
+
+def run_oracle(case: dict):
+    """Runs a case on the CPU oracle; returns (loads, final state)."""
+    import numpy as np
+    import pyoracle as o
+
+    sim = o.Simulator()
+    for w in case["wings"]:
+        sim.add_wing(w["chord"], w["span"], w["rows"], w["cols"], origin=w["origin"], kin=o.kinematics(**w["kin"]),
+                     cheb_chord=w.get("cheb_chord", False), cheb_span=w.get("cheb_span", False))
+    sim.set_forward_flight(case["ff"])
+    sim.set_advection(case["advection"])
+    if case.get("erase_wake_after"):
+        sim.set_erase_wake_after(case["erase_wake_after"])
+    loads = sim.run(case["steps"], case["dt"])
+    return np.asarray(loads), sim.state()
+
+
+def make_gpu_sim(case: dict, **kw):
+    """The same case on the CUDA library (uvlm_b200.SimpleSimulator)."""
+    import uvlm_b200 as U
+
+    sim = U.SimpleSimulator(erase_wake_after=case.get("erase_wake_after", 0), **kw)
+    for w in case["wings"]:
+        m = U.Morphing()
+        k = w["kin"]
+        m.set_alpha(k.get("alpha", 0.0))
+        m.set_plug(k.get("plug_amp", 0.0), k.get("plug_omega", 0.0), k.get("plug_phase", 0.0))
+        m.set_flap(k.get("flap_amp", 0.0), k.get("flap_omega", 0.0), k.get("flap_phase", 0.0))
+        m.set_twist(k.get("twist_amp", 0.0), k.get("twist_omega", 0.0), k.get("twist_phase", 0.0),
+                    k.get("twist_span_slope", 0.0))
+        m.set_bend(k.get("bend_cx", 0.0), k.get("bend_cy", 0.0), k.get("bend_omega", 0.0), k.get("bend_phase", 0.0))
+        sim.AddWing(U.RectGenerator(w.get("cheb_chord", False), w.get("cheb_span", False)), m, w["chord"], w["span"],
+                    w["rows"], w["cols"], w["origin"])
+    sim.set_forward_flight(case["ff"])
+    sim.set_advection(case["advection"])
+    return sim

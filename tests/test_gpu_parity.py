@@ -1,0 +1,308 @@
+"""CUDA path vs the CPU oracle and the golden fixtures (needs a B200).
+
+Every call goes through the C-ABI (include/uvlm_b200.h) via uvlm_b200.
+Tolerances: the plain FP64 form must match the FP64 oracle to rounding
+(1e-10 relative on short runs; 1e-7 relative to max|C| over the 200-step
+config 1 run, where wake roll-up amplifies rounding); the mixed form is held
+to the north-star bound on the load coefficients, 1e-6 relative to max|C|.
+"""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+from cases import CASES, make_gpu_sim, run_oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+SQ2 = math.sqrt(2.0)
+RING_2 = np.array([[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]], float)
+
+
+def U():
+    import uvlm_b200
+
+    return uvlm_b200
+
+
+def square_ring(l, x0, y0):
+    x0 -= l / 2
+    y0 -= l / 2
+    return np.array([[x0, y0, 0], [x0 + l, y0, 0], [x0 + l, y0 + l, 0], [x0, y0 + l, 0]], float)
+
+
+def rel_to_max(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+# --------------------------------------------- reference KATs through the C-ABI
+def test_kat_ring_velocity():  # test/vortex_test.cpp:104-130
+    R = U().rings
+    np.testing.assert_allclose(R.InducedVelocity([0, 0, 0], RING_2[None], [4 * math.pi]), [0, 0, -4 * SQ2],
+                               atol=1e-13)
+    np.testing.assert_allclose(R.InducedVelocity([0, 0, 0], RING_2[None], [4 * math.pi], chordwise=True),
+                               [0, 0, -2 * SQ2], atol=1e-13)
+
+
+def test_kat_many_rings():  # test/shed_test.cpp:21-50
+    R = U().rings
+    ring = np.array([[1, 1, 0], [-1, 1, 0], [-1, -1, 0], [1, -1, 0]], float)
+    rings = np.stack([ring] * 20)
+    g = np.full(20, 4 * math.pi)
+    np.testing.assert_allclose(R.InducedVelocity([0, 0, 0], rings, g), [0, 0, -4 * SQ2 * 20], rtol=1e-14)
+    np.testing.assert_allclose(R.InducedVelocity([0, 0, 0], rings, g, chordwise=True), [0, 0, -2 * SQ2 * 20],
+                               rtol=1e-14)
+
+
+def test_kat_connect_trailing_edge_and_advect():  # test/shed_test.cpp:52-91
+    R = U().rings
+    edge = np.stack([square_ring(2, 1, 1), square_ring(2, 1, 3)])
+    wake = np.stack([square_ring(2, 99, 1), square_ring(2, 99, 3)])
+    w = R.ConnectTrailingEdge(edge, wake)
+    np.testing.assert_array_equal(w[0], [[2, 0, 0], [100, 0, 0], [100, 2, 0], [2, 2, 0]])
+    np.testing.assert_array_equal(w[1], [[2, 2, 0], [100, 2, 0], [100, 4, 0], [2, 4, 0]])
+    moved = R.AdvectParallel(np.zeros((0, 4, 3)), np.zeros(0), square_ring(2, 0, 0)[None], [1, 0, 0], 0.1)
+    np.testing.assert_allclose(moved[0], [[-0.9, -1, 0], [1.1, -1, 0], [1.1, 1, 0], [-0.9, 1, 0]], rtol=0,
+                               atol=1e-15)
+
+
+def test_kat_solve_linear_problem():  # test/linear_test.cpp:61-116
+    M = U()
+    alpha, Uinf, a = math.pi / 6, 2.0, 0.1
+    v = np.array([[0, 0, 0], [a * math.cos(alpha), 0, -a * math.sin(alpha)],
+                  [a * math.cos(alpha), a, -a * math.sin(alpha)], [0, a, 0]])
+    g = M.rings.SolveLinearProblem(v[None], np.zeros((0, 4, 3)), [], [Uinf, 0, 0], M.Morphing(), 0.0)
+    assert abs(g[0] - SQ2 * math.pi * a * Uinf * math.sin(alpha) / 4) < 1e-10
+    vs = np.stack([square_ring(2, -1, 0), square_ring(2, 1, 0)])
+    g = M.rings.SolveLinearProblem(vs, np.zeros((0, 4, 3)), [], [0, 0, 1], M.Morphing(), 0.0)
+    for x in ([-1, 0, 0], [1, 0, 0]):
+        np.testing.assert_allclose(M.rings.InducedVelocity(x, vs, g), [0, 0, -1], atol=1e-14)
+    m = M.Morphing().set_plug(0.1, 1.0)
+    g = M.rings.SolveLinearProblem(vs, np.zeros((0, 4, 3)), [], [0, 0, 1], m, 0.0)
+    for x in ([-1, 0, 0], [1, 0, 0]):
+        np.testing.assert_allclose(M.rings.InducedVelocity(x, vs, g), [0, 0, -0.9], atol=1e-10)
+
+
+def test_legacy_solve_matches_oracle_with_wake():
+    import pyoracle as o
+
+    vs = np.stack([square_ring(2, -1, 0), square_ring(2, 1, 0)])
+    wake = square_ring(2, 2, 0)[None]
+    for drop in (True, False):
+        ref = o.solve_linear_problem(vs, wake, [1.3], [0, 0, 1], o.kinematics(plug_amp=0.1, plug_omega=1.0), 0.0,
+                                     drop_wake_term=drop)
+        got = U().rings.SolveLinearProblem(vs, wake, [1.3], [0, 0, 1], U().Morphing().set_plug(0.1, 1.0), 0.0,
+                                           drop_wake_term=drop)
+        np.testing.assert_allclose(got, ref, rtol=1e-12)
+
+
+# ------------------------------------------------------------- N-body vs oracle
+def _random_sheet(rng, num, rows, cols):
+    base = np.stack(np.meshgrid(np.linspace(0, 1, rows + 1), np.linspace(-2, 2, cols + 1), indexing="ij"), -1)
+    pos = np.zeros((num, rows + 1, cols + 1, 3))
+    for n in range(num):
+        pos[n, ..., :2] = base + 0.02 * rng.standard_normal(base.shape)
+        pos[n, ..., 0] += 1.3 * n
+        pos[n, ..., 2] = 0.05 * rng.standard_normal(base.shape[:2]) + 0.2 * n
+    gamma = rng.standard_normal((num, rows, cols))
+    return pos, gamma
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 5, 7), (2, 9, 130), (3, 4, 6)])
+def test_sheet_induced_velocity_fp64(shape):
+    import pyoracle as o
+
+    rng = np.random.default_rng(sum(shape))
+    pos, gamma = _random_sheet(rng, *shape)
+    # targets: random points, every node (self cut-off), segment midpoints (colinear cut-off)
+    tg = [rng.uniform(-1, 3, size=(64, 3)), pos.reshape(-1, 3),
+          0.5 * (pos[:, :, 1:] + pos[:, :, :-1]).reshape(-1, 3)]
+    targets = np.concatenate(tg)
+    ref = o.sheet_induced_velocity(pos, gamma, targets)
+    got = U().InducedVelocity(targets, pos, gamma)
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) <= 1e-12 * scale
+
+
+def test_sheet_induced_velocity_mixed():
+    import pyoracle as o
+
+    rng = np.random.default_rng(7)
+    pos, gamma = _random_sheet(rng, 2, 12, 40)
+    targets = np.concatenate([rng.uniform(-1, 3, size=(500, 3)), pos[:, 1:-1, 1:-1].reshape(-1, 3) + 1e-3])
+    ref = o.sheet_induced_velocity(pos, gamma, targets)
+    got = U().InducedVelocity(targets, pos, gamma, precision="mixed")
+    err = np.abs(got - ref).max(axis=1)
+    mag = np.linalg.norm(ref, axis=1)
+    # FP32 arithmetic on FP64-exact relative vectors: ~1e-6 of the local velocity
+    assert np.all(err <= 2e-5 * mag + 1e-6 * np.max(mag))
+
+
+# -------------------------------------------------------- advection strategies
+def _oracle_velocity(x, wing_pos, wing_gamma, wake_pos, wake_gamma, ff):
+    import pyoracle as o
+
+    v = -np.asarray(ff) + o.sheet_induced_velocity(wing_pos, wing_gamma, x)
+    if wake_gamma.size:
+        v = v + o.sheet_induced_velocity(wake_pos, wake_gamma, x)
+    return v
+
+
+@pytest.mark.parametrize("name", ["euler", "RK2"])
+def test_advection_object_matches_restated_scheme(name):
+    fx = np.load(os.path.join(HERE, "golden", "rk2_heave_pitch_4x8.npz"))
+    wing_pos, wing_gamma = fx["wing_pos"], fx["wing_gamma"]
+    wake_pos, wake_gamma = fx["wake_pos"], fx["wake_gamma"]
+    ff, dt = np.array([-1.0, 0, 0]), 0.1
+    adv = U().AdvectFactory(name)
+    got = adv.Advect(wing_pos, wing_gamma, wake_pos, wake_gamma, ff, dt)
+    x = wake_pos.reshape(-1, 3)
+
+    def vel(p):
+        v = _oracle_velocity(p.reshape(-1, 3), wing_pos, wing_gamma, p.reshape(wake_pos.shape), wake_gamma, ff)
+        v = v.reshape(wake_pos.shape)
+        v[:, 0] = -ff  # trailing-edge row (src/advect.h:41-45)
+        return v.reshape(-1, 3)
+
+    k1 = vel(x)
+    if name == "euler":
+        ref = x + k1 * dt
+    else:
+        k2 = vel(x + k1 * dt)
+        rows = np.repeat(np.arange(wake_pos.shape[1]), wake_pos.shape[2])
+        rows = np.tile(rows, wake_pos.shape[0])
+        ref = np.where((rows > 5)[:, None], x + (k1 + k2) * dt / 2, x + k1 * dt)
+    np.testing.assert_allclose(got.reshape(-1, 3), ref, rtol=0, atol=1e-12)
+
+
+def test_advection_ab2_history():
+    fx = np.load(os.path.join(HERE, "golden", "ab2_plunge_4x8.npz"))
+    wing_pos, wing_gamma, wake_pos, wake_gamma = fx["wing_pos"], fx["wing_gamma"], fx["wake_pos"], fx["wake_gamma"]
+    ff, dt = np.array([-1.0, 0, 0]), 0.1
+    adv = U().AdvectFactory("AB2")
+    # first call: Euler (src/advect.cpp:192-196)
+    small_pos, small_g = wake_pos[:, :-1].copy(), wake_gamma[:, :-1].copy()
+    first = adv.Advect(wing_pos, wing_gamma, small_pos, small_g, ff, dt)
+    v1 = _oracle_velocity(small_pos.reshape(-1, 3), wing_pos, wing_gamma, small_pos, small_g, ff).reshape(small_pos.shape)
+    v1[:, 0] = -ff
+    np.testing.assert_allclose(first, small_pos + v1 * dt, atol=1e-12, rtol=0)
+    # second call with one more row: v(i) pairs with v_prev(i-1)
+    second = adv.Advect(wing_pos, wing_gamma, wake_pos, wake_gamma, ff, dt)
+    v2 = _oracle_velocity(wake_pos.reshape(-1, 3), wing_pos, wing_gamma, wake_pos, wake_gamma, ff).reshape(wake_pos.shape)
+    v2[:, 0] = -ff
+    ref = wake_pos + v2 * dt
+    ref[:, 1:] = wake_pos[:, 1:] + (v2[:, 1:] * 3 - v1[:, :]) * dt / 2
+    np.testing.assert_allclose(second, ref, atol=1e-12, rtol=0)
+
+
+# --------------------------------------------------------- whole time-stepper
+@pytest.mark.parametrize("name", [n for n in CASES if n != "cfg1_euler_200"])
+def test_simulator_fp64_matches_golden(name):
+    fx = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    case = CASES[name]
+    sim = make_gpu_sim(case)
+    loads = sim.Run(case["steps"], case["dt"])
+    st = sim.state()
+    assert rel_to_max(loads[:, 1:], fx["loads"][:, 1:]) < 1e-10
+    np.testing.assert_allclose(loads[:, 0], fx["loads"][:, 0], rtol=0, atol=0)
+    assert rel_to_max(st["wing_gamma"], fx["wing_gamma"]) < 1e-10
+    assert st["wake_pos"].shape == fx["wake_pos"].shape
+    assert np.max(np.abs(st["wake_pos"] - fx["wake_pos"])) < 1e-10
+    assert rel_to_max(st["wake_gamma"], fx["wake_gamma"]) < 1e-10
+
+
+def test_simulator_fp64_cfg1_full_run():
+    fx = np.load(os.path.join(HERE, "golden", "cfg1_euler_200.npz"))
+    case = CASES["cfg1_euler_200"]
+    sim = make_gpu_sim(case)
+    loads = sim.Run(case["steps"], case["dt"])
+    assert rel_to_max(loads[:, 2], fx["loads"][:, 2]) < 1e-7  # CL
+    assert rel_to_max(loads[:, 1], fx["loads"][:, 1]) < 1e-7  # CD
+    st = sim.state()
+    assert rel_to_max(st["wing_gamma"], fx["wing_gamma"]) < 1e-7
+
+
+def test_simulator_mixed_cfg1_within_north_star_bound():
+    fx = np.load(os.path.join(HERE, "golden", "cfg1_euler_200.npz"))
+    case = CASES["cfg1_euler_200"]
+    sim = make_gpu_sim(case, precision="mixed")
+    loads = sim.Run(case["steps"], case["dt"])
+    err_cl = rel_to_max(loads[:, 2], fx["loads"][:, 2])
+    err_cd = rel_to_max(loads[:, 1], fx["loads"][:, 1])
+    print(f"mixed vs FP64 oracle, config 1: CL {err_cl:.3e}  CD {err_cd:.3e}")
+    assert err_cl <= 1e-6
+    assert err_cd <= 1e-6
+
+
+def test_state_round_trip_continues_identically():
+    case = CASES["rk2_heave_pitch_4x8"]
+    a = make_gpu_sim(case)
+    a.begin()
+    for s in range(6):
+        a.step(s, case["dt"])
+    st = a.state()
+    rows_a = [a.step(s, case["dt"]) for s in range(6, 10)]
+    b = make_gpu_sim(case)
+    b.begin()
+    b.set_state(st["wake_gamma"].shape[1], st["wing_pos"], st["wake_pos"], st["wing_gamma"], st["wing_gamma_prev"],
+                st["wake_gamma"])
+    rows_b = [b.step(s, case["dt"]) for s in range(6, 10)]
+    np.testing.assert_array_equal(np.array(rows_a), np.array(rows_b))
+
+
+def test_error_paths():
+    M = U()
+    sim = M.SimpleSimulator()
+    with pytest.raises(M.UVLMError) as ei:
+        sim.step(0, 0.1)
+    assert ei.value.code == 5
+    with pytest.raises(M.UVLMError) as ei:
+        sim.AddWing(M.RectGenerator(), M.Morphing(), 1.0, 4.0, 4, 7)
+    assert ei.value.code == 1
+    small = M.SimpleSimulator(max_wake_rows=3)
+    small.AddWing(M.RectGenerator(), M.Morphing().set_alpha(0.1), 1.0, 4.0, 2, 4)
+    small.set_forward_flight([-1, 0, 0])
+    small.begin()
+    with pytest.raises(M.UVLMError) as ei:
+        for s in range(200):
+            small.step(s, 0.1)
+    assert ei.value.code == 6
+
+
+# ---------------------------------------------------------------- dense solve
+def _influence_like(n, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n, n)) / np.sqrt(n)
+    A += np.diag(2.0 + rng.random(n))
+    return A
+
+
+@pytest.mark.parametrize("n", [5, 64, 200, 700])
+def test_dense_solve_fp64(n):
+    A = _influence_like(n, n)
+    b = np.random.default_rng(1).standard_normal(n)
+    x, _ = U().dense_solve(A, b, "fp64")
+    np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("method", ["tf32", "bf16"])
+@pytest.mark.parametrize("n", [64, 640])
+def test_dense_solve_mixed_gmres(method, n):
+    A = _influence_like(n, n + 3)
+    b = np.random.default_rng(2).standard_normal(n)
+    x, it = U().dense_solve(A, b, method)
+    np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=1e-10, atol=1e-11)
+    assert it <= 20
+
+
+def test_dense_solve_singular_reports():
+    M = U()
+    A = np.ones((4, 4))
+    with pytest.raises(M.UVLMError) as ei:
+        M.dense_solve(A, np.ones(4), "fp64")
+    assert ei.value.code == 3

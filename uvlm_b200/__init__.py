@@ -1,0 +1,335 @@
+"""uvlm_b200 -- B200-native UVLM time-stepper behind xeno14/UVLM's interface.
+
+The Python classes mirror the reference's C++ API for the per-step hot path
+(names, argument meaning and error behaviour):
+
+  SimpleSimulator  src/simulator/simple_simulator.h:36-108
+  Morphing         src/morphing.h:25-108 (closed-form sinusoids instead of
+                   std::function; see ``Morphing``)
+  RectGenerator    src/wing/rect.h:28-35
+  AdvectFactory    src/advect_factory.cpp:43-60 -> ``Advection`` objects
+                   whose ``Advect`` matches src/advect.h:48-59
+  InducedVelocity  src/velocity.h:14-24
+  rings.*          the legacy AoS API of src/shed.h and src/linear.h
+
+Every call goes through the C-ABI of include/uvlm_b200.h into the CUDA
+library built in-tree for sm_100a; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._capi import (ADVECT, LU_PREC, PRECISION, SOLVER, WARM, Config, Kinematics, StepStats, UVLMError, WingDesc,
+                    check, lib)
+
+__all__ = ["SimpleSimulator", "Morphing", "RectGenerator", "AdvectFactory", "Advection", "InducedVelocity",
+           "UVLMError", "dense_solve", "rings", "lib"]
+
+_P = C.POINTER(C.c_double)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+@dataclass
+class Sinusoid:
+    """f(t) = amp * sin(omega * t + phase)."""
+
+    amp: float = 0.0
+    omega: float = 0.0
+    phase: float = 0.0
+
+
+class Morphing:
+    """Wing kinematics (src/morphing.h:25-108).
+
+    The reference takes arbitrary std::function objects; here each motion is a
+    closed-form sinusoid so that it can be evaluated on the device:
+      plug(t)     = A sin(w t + p)                          set_plug
+      flap(t)     = A sin(w t + p)                          set_flap
+      twist(x0,t) = (A + slope*|y|) sin(w t + p)            set_twist
+      bend(x0,t)  = (cx x(1-x) + cy y^2) sin(w t + p)       set_bend
+    The velocity is the reference's FP64 central difference (h = 1e-6).
+    """
+
+    def __init__(self):
+        self.k = Kinematics()
+
+    def set_alpha(self, alpha: float) -> "Morphing":
+        self.k.alpha = float(alpha)
+        return self
+
+    def set_plug(self, amp: float, omega: float, phase: float = 0.0) -> "Morphing":
+        self.k.plug_amp, self.k.plug_omega, self.k.plug_phase = float(amp), float(omega), float(phase)
+        return self
+
+    def set_flap(self, amp: float, omega: float, phase: float = 0.0) -> "Morphing":
+        self.k.flap_amp, self.k.flap_omega, self.k.flap_phase = float(amp), float(omega), float(phase)
+        return self
+
+    def set_twist(self, amp: float, omega: float, phase: float = 0.0, span_slope: float = 0.0) -> "Morphing":
+        self.k.twist_amp, self.k.twist_omega, self.k.twist_phase = float(amp), float(omega), float(phase)
+        self.k.twist_span_slope = float(span_slope)
+        return self
+
+    def set_bend(self, cx: float, cy: float, omega: float, phase: float = 0.0) -> "Morphing":
+        self.k.bend_cx, self.k.bend_cy = float(cx), float(cy)
+        self.k.bend_omega, self.k.bend_phase = float(omega), float(phase)
+        return self
+
+    def set_origin(self, origin) -> None:
+        for i in range(3):
+            self.k.origin[i] = float(origin[i])
+
+    def Clear(self) -> None:  # noqa: N802 (reference name)
+        alpha = self.k.alpha
+        origin = tuple(self.k.origin)
+        self.k = Kinematics()
+        self.k.alpha = alpha
+        self.set_origin(origin)
+
+
+class RectGenerator:
+    """Flat rectangular half-wing lattice (src/wing/rect.cpp:18-45)."""
+
+    def __init__(self, chebyshev_chord: bool = False, chebyshev_span: bool = False):
+        self.chebyshev_chord = bool(chebyshev_chord)
+        self.chebyshev_span = bool(chebyshev_span)
+
+
+class SimpleSimulator:
+    """The UVLM time-stepper (src/simulator/simple_simulator.{h,cpp}) on a B200.
+
+    Extra keyword arguments select the B200 arithmetic:
+      precision   "fp64" (plain form) or "mixed" (FP32 N-body/assembly,
+                  tensor-core LU, FP64 residuals)
+      solver      "lu" (factor every step) or "gmres_stale" (GMRES
+                  preconditioned by stale LU factors, fresh-LU fallback)
+      warm_start  "previous", "extrapolate" or "mlp"
+    """
+
+    def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
+                 lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
+                 gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
+                 assembly_fp64: bool = False, nbody_variant: int = -1, compute_loads: bool = True):
+        cfg = Config()
+        lib().uvlm_config_default(C.byref(cfg))
+        cfg.precision = PRECISION[precision]
+        if solver is None:
+            solver = "lu" if precision == "fp64" else "gmres_stale"
+        cfg.solver = SOLVER[solver]
+        cfg.warm_start = WARM[warm_start]
+        cfg.lu_precision = LU_PREC[lu_precision]
+        cfg.max_wake_rows = int(max_wake_rows)
+        cfg.erase_wake_after = int(erase_wake_after)
+        cfg.gmres_tol = float(gmres_tol)
+        cfg.gmres_max_iter = int(gmres_max_iter)
+        cfg.gmres_restart = int(gmres_restart)
+        cfg.device = int(device)
+        cfg.assembly_fp64 = int(bool(assembly_fp64))
+        cfg.nbody_variant = int(nbody_variant)
+        cfg.compute_loads = int(bool(compute_loads))
+        self._cfg = cfg
+        h = C.c_void_p()
+        check(lib().uvlm_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._num = 0
+        self._wings = []
+        self._load_path = None
+        self._built = False
+
+    # -- reference API ------------------------------------------------------
+    def AddWing(self, generator: RectGenerator, morphing: Morphing, chord: float, span: float, rows: int,  # noqa: N802
+                cols: int, origin=(0.0, 0.0, 0.0)) -> None:
+        w = WingDesc()
+        w.chord, w.span, w.rows, w.cols = float(chord), float(span), int(rows), int(cols)
+        for i in range(3):
+            w.origin[i] = float(origin[i])
+        gen = generator or RectGenerator()
+        w.chebyshev_chord, w.chebyshev_span = int(gen.chebyshev_chord), int(gen.chebyshev_span)
+        check(lib().uvlm_add_wing(self._h, C.byref(w), C.byref(morphing.k)), self._h)
+        self._num += 1
+        self._wings.append((chord, span, rows, cols))
+
+    add_wing = AddWing
+
+    def set_forward_flight(self, v) -> None:
+        check(lib().uvlm_set_forward_flight(self._h, _p(_f64(v))), self._h)
+
+    def set_advection(self, advection) -> None:
+        name = advection.name if isinstance(advection, Advection) else str(advection)
+        check(lib().uvlm_set_advection(self._h, name.encode()), self._h)
+
+    def set_load_path(self, path: str) -> None:
+        self._load_path = path or None
+
+    def set_erase_wake_after(self, step: int) -> None:
+        self._cfg.erase_wake_after = int(step)
+
+    def Run(self, steps: int, dt: float) -> np.ndarray:  # noqa: N802
+        """Run(steps, dt): steps+1 MainLoops; returns the load rows."""
+        self.begin()
+        rows = np.zeros((steps + 1, 1 + 2 * self._num))
+        for s in range(steps + 1):
+            rows[s] = self.step(s, dt)
+        if self._load_path:
+            self._write_loads(rows)
+        return rows
+
+    run = Run
+
+    # -- stepping and state -------------------------------------------------
+    def begin(self) -> None:
+        check(lib().uvlm_begin(self._h), self._h)
+        self._built = True
+
+    def step(self, step: int, dt: float) -> np.ndarray:
+        row = np.zeros(1 + 2 * self._num)
+        check(lib().uvlm_step(self._h, int(step), float(dt), _p(row)), self._h)
+        return row
+
+    def erase_oldest_wake(self) -> None:
+        check(lib().uvlm_erase_oldest_wake(self._h), self._h)
+
+    def sizes(self):
+        v = [C.c_int64() for _ in range(5)]
+        check(lib().uvlm_get_sizes(self._h, *[C.byref(x) for x in v]), self._h)
+        return tuple(x.value for x in v)
+
+    def state(self) -> dict:
+        num, rows, cols, wr, wn = self.sizes()
+        s = dict(wing_pos=np.zeros((num, rows + 1, cols + 1, 3)), wing_pos_init=np.zeros((num, rows + 1, cols + 1, 3)),
+                 wake_pos=np.zeros((num, wn, cols + 1, 3)), wing_gamma=np.zeros((num, rows, cols)),
+                 wing_gamma_prev=np.zeros((num, rows, cols)), wake_gamma=np.zeros((num, wr, cols)))
+        check(lib().uvlm_get_state(self._h, _p(s["wing_pos"]), _p(s["wing_pos_init"]), _p(s["wake_pos"]),
+                                   _p(s["wing_gamma"]), _p(s["wing_gamma_prev"]), _p(s["wake_gamma"])), self._h)
+        return s
+
+    def set_state(self, wake_rows, wing_pos, wake_pos, wing_gamma, wing_gamma_prev, wake_gamma) -> None:
+        check(lib().uvlm_set_state(self._h, int(wake_rows), _p(_f64(wing_pos)), _p(_f64(wake_pos)),
+                                   _p(_f64(wing_gamma)), _p(_f64(wing_gamma_prev)), _p(_f64(wake_gamma))), self._h)
+
+    def stats(self) -> StepStats:
+        s = StepStats()
+        check(lib().uvlm_get_last_stats(self._h, C.byref(s)), self._h)
+        return s
+
+    def last_work(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        check(lib().uvlm_get_last_work(self._h, C.byref(a), C.byref(b), C.byref(c)), self._h)
+        return a.value, b.value, c.value
+
+    def set_stage_timing(self, enable: bool) -> None:
+        check(lib().uvlm_set_stage_timing(self._h, int(bool(enable))), self._h)
+
+    def synchronize(self) -> None:
+        check(lib().uvlm_synchronize(self._h), self._h)
+
+    def stream(self) -> int:
+        return lib().uvlm_stream(self._h) or 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().uvlm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _write_loads(self, rows: np.ndarray) -> None:
+        # PrepareOutputLoad + CalcLoad's TSV rows (simple_simulator.cpp:226-232, 334-346)
+        names = ["t"] + [f"{k}{n}" for n in range(self._num) for k in ("CD", "CL")]
+        with open(self._load_path, "w") as f:
+            f.write("\t".join(names) + "\n")
+            for r in rows:
+                f.write("\t".join("%g" % v for v in r) + "\n")
+
+
+class Advection:
+    """advect::Advection (src/advect.h:48-59) created by ``AdvectFactory``."""
+
+    def __init__(self, name: str, precision: str = "fp64"):
+        if name not in ADVECT:
+            raise UVLMError(1, "Invalid advection name! Please choose from following: [AB2, RK2, RK4, euler]")
+        self.name = name
+        h = C.c_void_p()
+        check(lib().uvlm_advection_create(name.encode(), PRECISION[precision], C.byref(h)))
+        self._h = h
+
+    def Advect(self, wing_pos, wing_gamma, wake_pos, wake_gamma, forward_flight, dt, next=None):  # noqa: N802,A002
+        """Returns the advected wake nodes (``next``, which may be wake_pos)."""
+        wp = _f64(wing_pos)
+        wg = _f64(wing_gamma)
+        kp = _f64(wake_pos)
+        kg = _f64(wake_gamma)
+        num, rows, cols = wg.shape
+        wake_rows = kp.shape[1] - 1
+        out = next if next is not None else np.empty_like(kp)
+        if out is kp or not out.flags.c_contiguous:
+            out = np.empty_like(kp)
+        check(lib().uvlm_advection_advect(self._h, _p(out), _p(wp), _p(wg), num, rows, cols, _p(kp),
+                                          _p(kg) if kg.size else None, wake_rows, _p(_f64(forward_flight)),
+                                          float(dt)))
+        if next is not None and out is not next:
+            next[...] = out
+            return next
+        return out
+
+    advect = Advect
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                lib().uvlm_advection_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def AdvectFactory(name: str, precision: str = "fp64") -> Advection:  # noqa: N802
+    """src/advect_factory.cpp:43-60."""
+    return Advection(name, precision)
+
+
+def InducedVelocity(x, pos, gamma, precision: str = "fp64") -> np.ndarray:  # noqa: N802
+    """UVLM::InducedVelocity(x, pos, gamma) (src/velocity.h:14-24).
+
+    x: (3,) or (T, 3); pos: (num, rows+1, cols+1, 3); gamma: (num, rows, cols)."""
+    pos = _f64(pos)
+    gamma = _f64(gamma)
+    xs = _f64(x)
+    single = xs.ndim == 1
+    xs = xs.reshape(-1, 3)
+    out = np.zeros_like(xs)
+    num, gr, gc = gamma.shape
+    check(lib().uvlm_sheet_induced_velocity(_p(pos), _p(gamma) if gamma.size else None, num, gr, gc, _p(xs),
+                                            xs.shape[0], _p(out), PRECISION[precision]))
+    return out[0] if single else out
+
+
+def dense_solve(A, b, method: str = "fp64"):
+    """x = A^-1 b on the GPU; method "fp64" (LU), "tf32" or "bf16" (LU + GMRES).
+
+    Returns (x, gmres_iterations)."""
+    A = _f64(A)
+    b = _f64(b)
+    x = np.zeros_like(b)
+    it = C.c_int32(0)
+    m = {"fp64": 0, "tf32": 1, "bf16": 2}[method]
+    check(lib().uvlm_dense_solve(_p(A), A.shape[0], _p(b), _p(x), m, C.byref(it)))
+    return x, it.value
+
+
+from . import rings  # noqa: E402  (legacy AoS API)

@@ -1,0 +1,765 @@
+// capi.cu -- the C-ABI: context, SimpleSimulator::MainLoop orchestration on
+// the device, and the context-free replacements of the reference API.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/uvlm_b200.h"
+#include "gmres.cuh"
+#include "lu.cuh"
+#include "nbody.cuh"
+#include "step.cuh"
+
+using namespace uvlm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+}  // namespace
+
+void uvlm::set_global_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<long long> g_launches{0};
+void uvlm::note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+int set_global(const Error& e) {
+  if (e.code) g_last_error = e.msg;
+  return e.code;
+}
+
+// RectGenerator (src/wing/rect.cpp:18-45) with linspace (src/util.h:36-43)
+// and TransformChebyshev (src/wing/rect.h:16-25); host set-up, once per case.
+std::vector<double> linspace(double a, double b, size_t N) {
+  const double dx = (b - a) / (N - 1);
+  std::vector<double> r;
+  for (size_t i = 0; i < N; i++) r.push_back(a + i * dx);
+  return r;
+}
+std::vector<double> chebyshev(size_t N, double xmin, double xmax) {
+  auto th = linspace(-M_PI_2, 0, N);
+  std::vector<double> r;
+  for (double t : th) r.push_back(xmin + (xmax - xmin) * std::cos(t));
+  r.front() = xmin;
+  r.back() = xmax;
+  return r;
+}
+// WholeWing (src/wing/wing.cpp:12-52) of the half wing (chord, span/2,
+// rows, cols/2), shifted by the wing origin (simple_simulator.cpp:159-166).
+std::vector<double> whole_wing_nodes(const uvlm_wing_desc& w) {
+  const size_t rows = (size_t)w.rows, hc = (size_t)w.cols / 2;
+  auto xs = w.chebyshev_chord ? chebyshev(rows + 1, 0, w.chord) : linspace(0, w.chord, rows + 1);
+  auto ys = w.chebyshev_span ? chebyshev(hc + 1, 0, w.span / 2) : linspace(0, w.span / 2, hc + 1);
+  std::vector<double> out;
+  out.reserve((rows + 1) * (2 * hc + 1) * 3);
+  for (size_t i = 0; i <= rows; i++) {
+    for (size_t q = 0; q <= hc; q++) {  // mirrored half, reversed
+      const size_t jj = hc - q;
+      out.push_back(xs[i] + 0.0 + w.origin[0]);
+      out.push_back(ys[jj] * -1 + w.origin[1]);
+      out.push_back(0.0 + w.origin[2]);
+    }
+    for (size_t jj = 1; jj <= hc; jj++) {
+      out.push_back(xs[i] + w.origin[0]);
+      out.push_back(ys[jj] + w.origin[1]);
+      out.push_back(0.0 + w.origin[2]);
+    }
+  }
+  return out;
+}
+
+template <class T>
+Error dalloc(T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (count == 0) return ok();
+  UVLM_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count));
+  return ok();
+}
+
+int device_sms(int dev) {
+  int v = 148;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  return v;
+}
+
+}  // namespace
+
+struct uvlm_ctx {
+  uvlm_config cfg{};
+  std::vector<uvlm_wing_desc> wings;
+  std::vector<uvlm_kinematics> kins;
+  double ff[3] = {0, 0, 0};
+  std::string err;
+  cudaStream_t st = nullptr;
+  int num_sms = 148;
+  bool built = false;
+  bool timing = false;
+
+  int num = 0, R = 0, C = 0, N = 0;
+  int PR = 0;            // physical node rows per wake sheet
+  int wake_start = 0;    // physical row of logical node row 0
+  int wake_nodes = 0;    // logical node rows (0 before the first shed)
+  bool has_vprev = false;
+  long long tcap = 0;
+
+  uvlm_kinematics* d_kin = nullptr;
+  double* d_chord_span = nullptr;
+  double *d_pos_init = nullptr, *d_pos = nullptr;
+  double *d_gamma = nullptr, *d_gamma_prev = nullptr, *d_gamma_hist = nullptr;
+  double *d_wpos = nullptr, *d_wpos2 = nullptr, *d_wgamma = nullptr;
+  double *d_k1 = nullptr, *d_k2 = nullptr, *d_k3 = nullptr, *d_vprev = nullptr;
+  double *d_cx = nullptr, *d_cy = nullptr, *d_cz = nullptr, *d_normal = nullptr, *d_area = nullptr, *d_uls = nullptr;
+  double* d_rhs = nullptr;
+  double* d_line_uls = nullptr;
+  double *d_tx = nullptr, *d_ty = nullptr, *d_tz = nullptr, *d_vx = nullptr, *d_vy = nullptr, *d_vz = nullptr;
+  double* d_A64 = nullptr;   // FP64 matrix (plain: factored in place; mixed: residual matrix if assembly_fp64)
+  float* d_A32 = nullptr;    // FP32 matrix of the mixed form
+  float* d_F32 = nullptr;    // FP32 factors of the mixed form
+  double* d_tmp = nullptr;   // [N] scratch
+  double* d_row = nullptr;   // [1+2num] load row
+  int* d_flags = nullptr;    // [4] non-finite etc.
+  double* h_row = nullptr;   // pinned
+  int* h_flags = nullptr;    // pinned
+  NBodyWork nb;
+  LuWork lu;
+  GmresWork gm;
+  bool have_factors = false;
+  int variant_fp64 = 0, variant_fp32 = 3;
+  uvlm_step_stats last{};
+  double work_nbody = 0, work_asm = 0, work_lu = 0;
+  cudaEvent_t ev[8] = {};
+
+  WingShape ws() const { return WingShape{num, R, C}; }
+  WakeLayout wl() const { return WakeLayout{num, C, PR, wake_start, wake_nodes}; }
+  int wake_rings() const { return wake_nodes > 0 ? wake_nodes - 1 : 0; }
+  bool mixed() const { return cfg.precision == UVLM_PRECISION_MIXED; }
+
+  int fail_with(const Error& e) {
+    if (e.code) err = e.msg;
+    return e.code;
+  }
+  void free_all();
+  Error alloc_all();
+  Error build_sources(bool with_bound, const double* wake_pos_buf, SourceBlock* blocks, int* nb_out);
+  Error eval(const SourceBlock* blocks, int nblocks, long long nt);
+  Error shed(long long step);
+  Error solve(long long step);
+  Error advect(double dt);
+  Error step(long long step, double dt, double* row);
+  void mark(int i) {
+    if (timing) cudaEventRecord(ev[i], st);
+  }
+};
+
+void uvlm_ctx::free_all() {
+  double** dd[] = {&d_pos_init, &d_pos, &d_gamma, &d_gamma_prev, &d_gamma_hist, &d_wpos, &d_wpos2, &d_wgamma, &d_k1, &d_k2,
+                   &d_k3, &d_vprev, &d_cx, &d_cy, &d_cz, &d_normal, &d_area, &d_uls, &d_rhs, &d_line_uls,
+                   &d_tx, &d_ty, &d_tz, &d_vx, &d_vy, &d_vz, &d_A64, &d_tmp, &d_row, &d_chord_span};
+  for (auto p : dd) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  cudaFree(d_A32);
+  cudaFree(d_F32);
+  cudaFree(d_kin);
+  cudaFree(d_flags);
+  cudaFree(nb.records);
+  cudaFree(nb.partial);
+  d_A32 = d_F32 = nullptr;
+  d_kin = nullptr;
+  d_flags = nullptr;
+  nb = NBodyWork{};
+  if (h_row) cudaFreeHost(h_row);
+  if (h_flags) cudaFreeHost(h_flags);
+  h_row = nullptr;
+  h_flags = nullptr;
+  lu_work_free(&lu);
+  gmres_work_free(&gm);
+  have_factors = false;
+}
+
+Error uvlm_ctx::alloc_all() {
+  free_all();
+  const size_t nn = (size_t)num * (R + 1) * (C + 1);
+  const size_t wn = (size_t)num * PR * (C + 1);
+  UVLM_TRY(dalloc(&d_kin, (size_t)num));
+  UVLM_TRY(dalloc(&d_chord_span, (size_t)2 * num));
+  UVLM_TRY(dalloc(&d_pos_init, 3 * nn));
+  UVLM_TRY(dalloc(&d_pos, 3 * nn));
+  UVLM_TRY(dalloc(&d_gamma, (size_t)N));
+  UVLM_TRY(dalloc(&d_gamma_prev, (size_t)N));
+  UVLM_TRY(dalloc(&d_gamma_hist, (size_t)N));
+  for (double** p : {&d_wpos, &d_wpos2, &d_k1, &d_k2, &d_k3, &d_vprev}) UVLM_TRY(dalloc(p, 3 * wn));
+  UVLM_TRY(dalloc(&d_wgamma, (size_t)num * PR * C));
+  for (double** p : {&d_cx, &d_cy, &d_cz, &d_area, &d_rhs, &d_tmp}) UVLM_TRY(dalloc(p, (size_t)N));
+  UVLM_TRY(dalloc(&d_normal, 3 * (size_t)N));
+  UVLM_TRY(dalloc(&d_uls, 3 * (size_t)N));
+  const long long lines = (long long)num * R * (2 * C + 1);
+  tcap = std::max<long long>({(long long)N, lines, (long long)wn});
+  UVLM_TRY(dalloc(&d_line_uls, 3 * (size_t)lines));
+  for (double** p : {&d_tx, &d_ty, &d_tz, &d_vx, &d_vy, &d_vz}) UVLM_TRY(dalloc(p, (size_t)tcap));
+  UVLM_TRY(dalloc(&d_row, (size_t)(1 + 2 * num)));
+  UVLM_TRY(dalloc(&d_flags, 4));
+  UVLM_CUDA_TRY(cudaMallocHost(&h_row, sizeof(double) * (1 + 2 * num)));
+  UVLM_CUDA_TRY(cudaMallocHost(&h_flags, sizeof(int) * 8));
+  // N-body scratch: records for bound + wake sheets, per-split partial sums
+  nb.records_cap = (long long)(nn + wn) * (long long)sizeof(RecD);
+  UVLM_CUDA_TRY(cudaMalloc(&nb.records, nb.records_cap));
+  nb.partial_cap = 3LL * std::max<long long>(64LL * N, 16LL * tcap);
+  UVLM_CUDA_TRY(cudaMalloc(&nb.partial, sizeof(double) * nb.partial_cap));
+  // dense matrices
+  if (!mixed() || cfg.assembly_fp64) UVLM_TRY(dalloc(&d_A64, (size_t)N * N));
+  if (mixed()) {
+    UVLM_CUDA_TRY(cudaMalloc(&d_A32, sizeof(float) * (size_t)N * N));
+    UVLM_CUDA_TRY(cudaMalloc(&d_F32, sizeof(float) * (size_t)N * N));
+    UVLM_TRY(lu_work_alloc(&lu, N, 4, num_sms));
+    UVLM_TRY(gmres_work_alloc(&gm, N, std::max(2, cfg.gmres_restart)));
+  } else {
+    UVLM_TRY(lu_work_alloc(&lu, N, 8, num_sms));
+  }
+  std::vector<double> cs;
+  for (auto& w : wings) {
+    cs.push_back(w.chord);
+    cs.push_back(w.span);
+  }
+  UVLM_CUDA_TRY(cudaMemcpy(d_chord_span, cs.data(), sizeof(double) * cs.size(), cudaMemcpyHostToDevice));
+  return ok();
+}
+
+// Source records: [bound sheets][wake sheets (positions from wake_pos_buf)].
+Error uvlm_ctx::build_sources(bool with_bound, const double* wake_pos_buf, SourceBlock* blocks, int* nb_out) {
+  SheetView views[2];
+  int nv = 0;
+  if (with_bound) views[nv++] = SheetView{d_pos, R + 1, 0, d_gamma, R, 0, num, R + 1, C};
+  if (wake_rings() > 0)
+    views[nv++] = SheetView{wake_pos_buf, PR, wake_start, d_wgamma, PR, wake_start, num, wake_nodes, C};
+  *nb_out = nv;
+  if (nv == 0) return ok();
+  return nbody_build_sources(views, nv, mixed() ? kNBodyFP32 : kNBodyFP64, &nb, blocks, st);
+}
+
+Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt) {
+  work_nbody += (double)nt * (double)nbody_unique_segments(blocks, nblocks);
+  if (nblocks == 0) {
+    UVLM_CUDA_TRY(cudaMemsetAsync(d_vx, 0, sizeof(double) * nt, st));
+    UVLM_CUDA_TRY(cudaMemsetAsync(d_vy, 0, sizeof(double) * nt, st));
+    UVLM_CUDA_TRY(cudaMemsetAsync(d_vz, 0, sizeof(double) * nt, st));
+    return ok();
+  }
+  return nbody_eval(blocks, nblocks, mixed() ? kNBodyFP32 : kNBodyFP64, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb,
+                    mixed() ? variant_fp32 : variant_fp64, num_sms, st);
+}
+
+Error uvlm_ctx::shed(long long step) {
+  if (wake_start == 0) {
+    // compact the prepend buffer: move the live rows to the end
+    const int to = PR - wake_nodes;
+    if (to <= 0) return fail(kErrCapacity, "wake longer than max_wake_rows");
+    UVLM_TRY(launch_move_rows(d_wpos, num, PR, 3 * (C + 1), wake_start, to, wake_nodes, d_k3, st));
+    UVLM_TRY(launch_move_rows(d_wgamma, num, PR, C, wake_start, to, wake_nodes, d_k3, st));
+    if (has_vprev) UVLM_TRY(launch_move_rows(d_vprev, num, PR, 3 * (C + 1), wake_start, to, wake_nodes, d_k3, st));
+    wake_start = to;
+  }
+  wake_start -= 1;
+  wake_nodes += 1;
+  return launch_shed(ws(), d_pos, d_gamma, wl(), d_wpos, d_wgamma, step > 0, st);
+}
+
+Error uvlm_ctx::solve(long long step) {
+  last.refactored = 0;
+  last.gmres_iters = 0;
+  last.residual = 0;
+  if (!mixed()) {
+    // plain form: FP64 assembly, fresh FP64 LU, FP64 triangular solves
+    UVLM_TRY(lu_factor_f64(d_A64, N, &lu, st));
+    UVLM_TRY(lu_solve_f64(d_A64, N, &lu, d_rhs, d_gamma, d_tmp, st));
+    last.solve_path = 0;
+    last.refactored = 1;
+    work_lu += 2.0 / 3.0 * (double)N * N * N;
+    return ok();
+  }
+  const LuUpdate upd = cfg.lu_precision == UVLM_LU_BF16 ? kLuUpdateBF16 : kLuUpdateTF32;
+  const LuUpdate use = gemm_tc_available() ? upd : kLuUpdateSimt;
+  auto factor = [&]() -> Error {
+    UVLM_CUDA_TRY(cudaMemcpyAsync(d_F32, d_A32, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToDevice, st));
+    UVLM_TRY(lu_factor_f32(d_F32, N, use, &lu, st));
+    UVLM_TRY(lu_check(&lu, st));
+    have_factors = true;
+    last.refactored = 1;
+    work_lu += 2.0 / 3.0 * (double)N * N * N;
+    return ok();
+  };
+  const bool fresh = cfg.solver == UVLM_SOLVER_LU || !have_factors;
+  if (fresh) UVLM_TRY(factor());
+  // initial guess: d_gamma holds g_n (the previous solution); the linear
+  // extrapolation 2 g_n - g_{n-1} uses the history kept in d_gamma_hist
+  if (cfg.warm_start == UVLM_WARM_EXTRAPOLATE && step >= 2)
+    UVLM_TRY(launch_extrapolate(d_gamma, d_gamma_prev, d_gamma_hist, N, st));
+  const float* A32 = cfg.assembly_fp64 ? nullptr : d_A32;
+  const double* A64 = cfg.assembly_fp64 ? d_A64 : nullptr;
+  GmresResult r;
+  UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_rhs, d_gamma, cfg.gmres_tol, cfg.gmres_max_iter, &gm, &r, st));
+  last.solve_path = fresh ? 0 : 1;
+  if (!r.converged && !fresh) {
+    // fresh-LU fallback: factor the current matrix and solve again
+    UVLM_TRY(factor());
+    UVLM_CUDA_TRY(cudaMemcpyAsync(d_gamma, d_gamma_prev, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    GmresResult r2;
+    UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_rhs, d_gamma, cfg.gmres_tol, 4 * cfg.gmres_max_iter, &gm, &r2,
+                         st));
+    r2.iters += r.iters;
+    r = r2;
+    last.solve_path = 2;
+  }
+  last.gmres_iters = r.iters;
+  last.residual = r.relres;
+  if (!r.converged) return fail(kErrNonFinite, "GMRES did not converge after a fresh factorisation");
+  return ok();
+}
+
+Error uvlm_ctx::advect(double dt) {
+  const WakeLayout L = wl();
+  const long long nt = (long long)num * (wake_nodes - 1) * (C + 1);
+  SourceBlock blocks[2];
+  int nbk = 0;
+  auto velocity_at = [&](const double* pos_buf, bool rebuild) -> Error {
+    if (rebuild) UVLM_TRY(build_sources(true, pos_buf, blocks, &nbk));
+    if (nt > 0) {
+      UVLM_TRY(launch_gather_wake(L, pos_buf, d_tx, d_ty, d_tz, st));
+      UVLM_TRY(eval(blocks, nbk, nt));
+    }
+    return ok();
+  };
+  const int ign = cfg.rk_ignore_rows;
+  const bool loads_built = cfg.compute_loads != 0;
+  switch (cfg.advection) {
+    case UVLM_ADVECT_EULER:
+      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(launch_advect(kAdvEuler, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
+                             ign, st));
+      break;
+    case UVLM_ADVECT_RK2:
+      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(launch_advect(kAdvRK2K1, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
+                             ign, st));
+      UVLM_TRY(velocity_at(d_wpos2, true));
+      UVLM_TRY(launch_advect(kAdvRK2Upd, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff,
+                             dt, ign, st));
+      break;
+    case UVLM_ADVECT_RK4:
+      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(launch_advect(kAdvRK4K1, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
+                             ign, st));
+      UVLM_TRY(velocity_at(d_wpos2, true));
+      UVLM_TRY(launch_advect(kAdvRK4K2, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
+                             ign, st));
+      UVLM_TRY(velocity_at(d_wpos2, true));
+      UVLM_TRY(launch_advect(kAdvRK4Upd, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff,
+                             dt, ign, st));
+      break;
+    case UVLM_ADVECT_AB2:
+      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(launch_advect(kAdvAB2, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, has_vprev, d_vx, d_vy, d_vz, ff,
+                             dt, ign, st));
+      has_vprev = true;
+      break;
+    default:
+      return fail(kErrInvalid, "unknown advection scheme");
+  }
+  (void)loads_built;
+  return ok();
+}
+
+Error uvlm_ctx::step(long long step, double dt, double* row) {
+  if (!built) return fail(kErrState, "uvlm_begin has not been called");
+  const double t = step * dt;
+  work_nbody = work_asm = work_lu = 0;
+  mark(0);
+  UVLM_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, st));
+  UVLM_CUDA_TRY(cudaMemcpyAsync(d_gamma_hist, d_gamma_prev, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+  UVLM_CUDA_TRY(cudaMemcpyAsync(d_gamma_prev, d_gamma, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+  UVLM_TRY(launch_kinematics(d_kin, ws(), d_pos_init, d_pos, t, st));
+  if (wake_nodes + 1 > PR) return fail(kErrCapacity, "wake longer than max_wake_rows");
+  UVLM_TRY(shed(step));
+  UVLM_TRY(launch_panel_geometry(d_kin, ws(), d_pos, d_pos_init, t, d_cx, d_cy, d_cz, d_normal, d_area, d_uls, st));
+  mark(1);
+  // influence matrix (simple_simulator.cpp:76-101)
+  if (mixed()) {
+    UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, true, d_A32, true, st));
+    if (cfg.assembly_fp64) UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, false, d_A64, false, st));
+  } else {
+    UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, false, d_A64, false, st));
+  }
+  work_asm = (double)N * (double)N * 4.0;
+  mark(2);
+  // RHS: wake normal wash at the collocation points (:103-124)
+  {
+    SourceBlock blocks[2];
+    int nbk = 0;
+    UVLM_TRY(build_sources(false, d_wpos, blocks, &nbk));
+    UVLM_CUDA_TRY(cudaMemcpyAsync(d_tx, d_cx, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    UVLM_CUDA_TRY(cudaMemcpyAsync(d_ty, d_cy, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    UVLM_CUDA_TRY(cudaMemcpyAsync(d_tz, d_cz, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    UVLM_TRY(eval(blocks, nbk, N));
+    UVLM_TRY(launch_rhs(N, d_vx, d_vy, d_vz, d_uls, d_normal, ff, d_rhs, st));
+  }
+  mark(3);
+  UVLM_TRY(solve(step));
+  UVLM_TRY(launch_check_finite(d_gamma, N, d_flags, st));
+  mark(4);
+  if (cfg.compute_loads) {
+    const long long lines = (long long)num * R * (2 * C + 1);
+    UVLM_TRY(launch_line_prep(d_kin, ws(), d_pos, d_pos_init, t, d_tx, d_ty, d_tz, d_line_uls, st));
+    SourceBlock blocks[2];
+    int nbk = 0;
+    UVLM_TRY(build_sources(true, d_wpos, blocks, &nbk));
+    UVLM_TRY(eval(blocks, nbk, lines));
+    UVLM_TRY(launch_loads(ws(), d_pos, d_gamma, d_gamma_prev, d_normal, d_area, d_vx, d_vy, d_vz, d_line_uls, ff,
+                          d_chord_span, t, dt, d_row, st));
+  }
+  mark(5);
+  UVLM_TRY(advect(dt));
+  mark(6);
+  if (cfg.erase_wake_after > 0 && step >= cfg.erase_wake_after && wake_nodes > 0) wake_nodes -= 1;
+  // end of step: load row and error words back to the host
+  UVLM_CUDA_TRY(cudaMemcpyAsync(h_row, d_row, sizeof(double) * (1 + 2 * num), cudaMemcpyDeviceToHost, st));
+  UVLM_CUDA_TRY(cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  UVLM_CUDA_TRY(cudaMemcpyAsync(h_flags + 4, lu.err, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  mark(7);
+  UVLM_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h_flags[4]) return fail(kErrTimeout, "a bounded device wait in the dense solve gave up");
+  if (h_flags[5]) return fail(kErrSingular, "zero pivot in the LU factorisation");
+  if (h_flags[0]) return fail(kErrNonFinite, "non-finite circulation after the solve");
+  if (!cfg.compute_loads) {
+    h_row[0] = t;
+    for (int i = 1; i < 1 + 2 * num; ++i) h_row[i] = 0;
+  }
+  if (row) std::memcpy(row, h_row, sizeof(double) * (1 + 2 * num));
+  last.step = step;
+  last.t = t;
+  last.wake_rows = wake_rings();
+  if (timing) {
+    float ms[8] = {0};
+    const int map[7][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {0, 7}};
+    for (int q = 0; q < 7; ++q) cudaEventElapsedTime(&ms[q], ev[map[q][0]], ev[map[q][1]]);
+    last.stage_ms[0] = ms[0];
+    last.stage_ms[1] = ms[1];
+    last.stage_ms[2] = ms[2];
+    last.stage_ms[3] = ms[3];
+    last.stage_ms[4] = ms[4];
+    last.stage_ms[5] = ms[5];
+    last.stage_ms[6] = 0;
+    last.stage_ms[7] = ms[6];
+  }
+  return ok();
+}
+
+// =================================================================== C-ABI
+extern "C" {
+
+void uvlm_config_default(uvlm_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->precision = UVLM_PRECISION_FP64;
+  c->solver = UVLM_SOLVER_LU;
+  c->warm_start = UVLM_WARM_PREVIOUS;
+  c->lu_precision = UVLM_LU_TF32;
+  c->advection = UVLM_ADVECT_EULER;
+  c->rk_ignore_rows = 5;
+  c->max_wake_rows = 1024;
+  c->erase_wake_after = 0;
+  c->gmres_restart = 20;
+  c->gmres_max_iter = 20;
+  c->gmres_tol = 1e-12;
+  c->device = 0;
+  c->compute_loads = 1;
+  c->assembly_fp64 = 0;
+  c->nbody_variant = -1;
+}
+
+const char* uvlm_status_string(int s) {
+  switch (s) {
+    case UVLM_OK: return "ok";
+    case UVLM_ERR_INVALID: return "invalid argument";
+    case UVLM_ERR_CUDA: return "CUDA error";
+    case UVLM_ERR_SINGULAR: return "singular matrix";
+    case UVLM_ERR_NONFINITE: return "non-finite value";
+    case UVLM_ERR_STATE: return "call out of order";
+    case UVLM_ERR_CAPACITY: return "capacity exceeded";
+    case UVLM_ERR_TIMEOUT: return "device wait timed out";
+    case UVLM_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+const char* uvlm_global_last_error(void) { return g_last_error.c_str(); }
+
+int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
+  if (!out) return set_global(fail(kErrInvalid, "out is NULL"));
+  *out = nullptr;
+  uvlm_ctx* c = new uvlm_ctx();
+  if (cfg)
+    c->cfg = *cfg;
+  else
+    uvlm_config_default(&c->cfg);
+  const uvlm_config& k = c->cfg;
+  if (k.precision != UVLM_PRECISION_FP64 && k.precision != UVLM_PRECISION_MIXED) {
+    delete c;
+    return set_global(fail(kErrInvalid, "unknown precision"));
+  }
+  if (k.advection < 0 || k.advection > 3 || k.max_wake_rows < 1 || k.gmres_restart < 1 || k.gmres_max_iter < 1 ||
+      !(k.gmres_tol > 0)) {
+    delete c;
+    return set_global(fail(kErrInvalid, "invalid configuration"));
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    delete c;
+    cudaGetLastError();
+    return set_global(fail(kErrCuda, "no CUDA device"));
+  }
+  if (cudaSetDevice(k.device) != cudaSuccess) {
+    delete c;
+    return set_global(fail(kErrCuda, "cudaSetDevice failed"));
+  }
+  c->num_sms = device_sms(k.device);
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return set_global(fail(kErrCuda, "cudaStreamCreate failed"));
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  if (k.nbody_variant >= 0) {
+    if (k.nbody_variant >= nbody_num_variants()) {
+      uvlm_destroy(c);
+      return set_global(fail(kErrInvalid, "nbody_variant out of range"));
+    }
+    if (k.precision == UVLM_PRECISION_MIXED)
+      c->variant_fp32 = k.nbody_variant;
+    else
+      c->variant_fp64 = k.nbody_variant;
+  }
+  *out = c;
+  return UVLM_OK;
+}
+
+int uvlm_destroy(uvlm_ctx* c) {
+  if (!c) return UVLM_OK;
+  if (c->st) cudaStreamSynchronize(c->st);
+  c->free_all();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return UVLM_OK;
+}
+
+const char* uvlm_last_error(const uvlm_ctx* c) { return c ? c->err.c_str() : g_last_error.c_str(); }
+
+int uvlm_add_wing(uvlm_ctx* c, const uvlm_wing_desc* w, const uvlm_kinematics* kin) {
+  if (!c || !w) return set_global(fail(kErrInvalid, "NULL argument"));
+  if (c->built) return c->fail_with(fail(kErrState, "wings are added before uvlm_begin"));
+  if (w->rows < 1 || w->cols < 2 || (w->cols & 1) || !(w->chord > 0) || !(w->span > 0))
+    return c->fail_with(fail(kErrInvalid, "rows >= 1, even cols >= 2 and positive chord/span are required"));
+  if (!c->wings.empty() && (c->wings.back().rows != w->rows || c->wings.back().cols != w->cols))
+    return c->fail_with(fail(kErrInvalid, "all wings must have the same rows and cols"));
+  c->wings.push_back(*w);
+  uvlm_kinematics k{};
+  if (kin) k = *kin;
+  // BuildWing sets the morphing origin to the wing origin (simple_simulator.cpp:157)
+  for (int d = 0; d < 3; ++d) k.origin[d] = w->origin[d];
+  c->kins.push_back(k);
+  return UVLM_OK;
+}
+
+int uvlm_set_forward_flight(uvlm_ctx* c, const double ff[3]) {
+  if (!c || !ff) return set_global(fail(kErrInvalid, "NULL argument"));
+  for (int d = 0; d < 3; ++d) c->ff[d] = ff[d];
+  return UVLM_OK;
+}
+
+int uvlm_set_advection(uvlm_ctx* c, const char* name) {
+  if (!c || !name) return set_global(fail(kErrInvalid, "NULL argument"));
+  const std::string s(name);
+  int a = -1;
+  if (s == "euler") a = UVLM_ADVECT_EULER;
+  if (s == "RK2") a = UVLM_ADVECT_RK2;
+  if (s == "RK4") a = UVLM_ADVECT_RK4;
+  if (s == "AB2") a = UVLM_ADVECT_AB2;
+  if (a < 0) return c->fail_with(fail(kErrInvalid, "Invalid advection name! Please choose from following: [AB2, RK2, RK4, euler]"));
+  c->cfg.advection = a;
+  c->has_vprev = false;
+  return UVLM_OK;
+}
+
+int uvlm_begin(uvlm_ctx* c) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (c->wings.empty()) return c->fail_with(fail(kErrState, "call uvlm_add_wing at least once"));
+  cudaSetDevice(c->cfg.device);
+  c->num = (int)c->wings.size();
+  c->R = (int)c->wings[0].rows;
+  c->C = (int)c->wings[0].cols;
+  c->N = c->num * c->R * c->C;
+  c->PR = (int)c->cfg.max_wake_rows + 2 + 64;
+  Error e = c->alloc_all();
+  if (e.code) return c->fail_with(e);
+  std::vector<double> nodes;
+  for (auto& w : c->wings) {
+    auto v = whole_wing_nodes(w);
+    nodes.insert(nodes.end(), v.begin(), v.end());
+  }
+  if (cudaMemcpy(c->d_pos_init, nodes.data(), sizeof(double) * nodes.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_pos, nodes.data(), sizeof(double) * nodes.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_kin, c->kins.data(), sizeof(uvlm_kinematics) * c->kins.size(), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemset(c->d_gamma, 0, sizeof(double) * c->N) != cudaSuccess ||
+      cudaMemset(c->d_gamma_prev, 0, sizeof(double) * c->N) != cudaSuccess ||
+      cudaMemset(c->d_row, 0, sizeof(double) * (1 + 2 * c->num)) != cudaSuccess)
+    return c->fail_with(fail(kErrCuda, "initial upload failed"));
+  c->wake_start = c->PR;
+  c->wake_nodes = 0;
+  c->has_vprev = false;
+  c->have_factors = false;
+  c->built = true;
+  return UVLM_OK;
+}
+
+int uvlm_step(uvlm_ctx* c, int64_t step, double dt, double* row) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (!(dt > 0)) return c->fail_with(fail(kErrInvalid, "dt must be positive"));
+  return c->fail_with(c->step(step, dt, row));
+}
+
+int uvlm_run(uvlm_ctx* c, int64_t steps, double dt, double* loads) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  int rc = uvlm_begin(c);
+  if (rc) return rc;
+  for (int64_t s = 0; s <= steps; ++s) {
+    rc = uvlm_step(c, s, dt, loads ? loads + s * (1 + 2 * c->num) : nullptr);
+    if (rc) return rc;
+  }
+  return UVLM_OK;
+}
+
+int uvlm_erase_oldest_wake(uvlm_ctx* c) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));
+  if (c->wake_nodes > 0) c->wake_nodes -= 1;
+  return UVLM_OK;
+}
+
+int uvlm_get_sizes(const uvlm_ctx* c, int64_t* num, int64_t* rows, int64_t* cols, int64_t* wake_rows,
+                   int64_t* wake_node_rows) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (num) *num = c->built ? c->num : (int64_t)c->wings.size();
+  if (rows) *rows = c->built ? c->R : (c->wings.empty() ? 0 : c->wings[0].rows);
+  if (cols) *cols = c->built ? c->C : (c->wings.empty() ? 0 : c->wings[0].cols);
+  if (wake_rows) *wake_rows = c->wake_rings();
+  if (wake_node_rows) *wake_node_rows = c->wake_nodes;
+  return UVLM_OK;
+}
+
+static Error copy_wake_out(uvlm_ctx* c, const double* src, double* dst, int row_elems, int rows) {
+  for (int n = 0; n < c->num; ++n) {
+    const double* s = src + ((size_t)n * c->PR + c->wake_start) * row_elems;
+    UVLM_CUDA_TRY(cudaMemcpy(dst + (size_t)n * rows * row_elems, s, sizeof(double) * rows * row_elems,
+                             cudaMemcpyDeviceToHost));
+  }
+  return ok();
+}
+
+int uvlm_get_state(uvlm_ctx* c, double* wing_pos, double* wing_pos_init, double* wake_pos, double* wing_gamma,
+                   double* wing_gamma_prev, double* wake_gamma) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail_with(fail(kErrCuda, "stream sync failed"));
+  const size_t nn = (size_t)c->num * (c->R + 1) * (c->C + 1) * 3;
+  Error e;
+  auto cp = [&](double* dst, const double* src, size_t cnt) {
+    if (dst && !e.code && cudaMemcpy(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess)
+      e = fail(kErrCuda, "state copy failed");
+  };
+  cp(wing_pos, c->d_pos, nn);
+  cp(wing_pos_init, c->d_pos_init, nn);
+  cp(wing_gamma, c->d_gamma, (size_t)c->N);
+  cp(wing_gamma_prev, c->d_gamma_prev, (size_t)c->N);
+  if (!e.code && wake_pos && c->wake_nodes > 0) e = copy_wake_out(c, c->d_wpos, wake_pos, 3 * (c->C + 1), c->wake_nodes);
+  if (!e.code && wake_gamma && c->wake_rings() > 0) e = copy_wake_out(c, c->d_wgamma, wake_gamma, c->C, c->wake_rings());
+  return c->fail_with(e);
+}
+
+int uvlm_set_state(uvlm_ctx* c, int64_t wake_rows, const double* wing_pos, const double* wake_pos,
+                   const double* wing_gamma, const double* wing_gamma_prev, const double* wake_gamma) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));
+  if (wake_rows < 0 || wake_rows + 2 > c->PR) return c->fail_with(fail(kErrCapacity, "wake_rows exceeds capacity"));
+  if (!wing_pos || !wake_pos || !wing_gamma || !wing_gamma_prev || (wake_rows > 0 && !wake_gamma))
+    return c->fail_with(fail(kErrInvalid, "NULL state array"));
+  cudaStreamSynchronize(c->st);
+  const size_t nn = (size_t)c->num * (c->R + 1) * (c->C + 1) * 3;
+  const int nodes = (int)wake_rows + 1;
+  c->wake_start = c->PR - nodes - 1;
+  c->wake_nodes = nodes;
+  Error e;
+  auto up = [&](double* dst, const double* src, size_t cnt) {
+    if (!e.code && cudaMemcpy(dst, src, sizeof(double) * cnt, cudaMemcpyHostToDevice) != cudaSuccess)
+      e = fail(kErrCuda, "state upload failed");
+  };
+  up(c->d_pos, wing_pos, nn);
+  up(c->d_gamma, wing_gamma, (size_t)c->N);
+  up(c->d_gamma_prev, wing_gamma_prev, (size_t)c->N);
+  for (int n = 0; n < c->num && !e.code; ++n) {
+    up(c->d_wpos + ((size_t)n * c->PR + c->wake_start) * 3 * (c->C + 1), wake_pos + (size_t)n * nodes * 3 * (c->C + 1),
+       (size_t)nodes * 3 * (c->C + 1));
+    if (wake_rows > 0)
+      up(c->d_wgamma + ((size_t)n * c->PR + c->wake_start) * c->C, wake_gamma + (size_t)n * wake_rows * c->C,
+         (size_t)wake_rows * c->C);
+  }
+  c->has_vprev = false;
+  c->have_factors = false;
+  return c->fail_with(e);
+}
+
+int uvlm_get_last_stats(const uvlm_ctx* c, uvlm_step_stats* s) {
+  if (!c || !s) return set_global(fail(kErrInvalid, "NULL argument"));
+  *s = c->last;
+  return UVLM_OK;
+}
+
+int uvlm_set_stage_timing(uvlm_ctx* c, int32_t enable) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  c->timing = enable != 0;
+  return UVLM_OK;
+}
+
+int uvlm_synchronize(uvlm_ctx* c) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail_with(fail(kErrCuda, "stream sync failed"));
+  return UVLM_OK;
+}
+
+void* uvlm_stream(uvlm_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int64_t uvlm_kernel_launch_count(void) { return g_launches.load(); }
+
+int uvlm_measure_fp32_peak(int32_t device, double* tflops) {
+  if (!tflops) return set_global(fail(kErrInvalid, "NULL argument"));
+  if (cudaSetDevice(device) != cudaSuccess) return set_global(fail(kErrCuda, "cudaSetDevice failed"));
+  return set_global(measure_fp32_fma_peak(device_sms(device), tflops));
+}
+
+int uvlm_get_last_work(const uvlm_ctx* c, double* nbody_pairs, double* assembly_pairs, double* lu_flops) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (nbody_pairs) *nbody_pairs = c->work_nbody;
+  if (assembly_pairs) *assembly_pairs = c->work_asm;
+  if (lu_flops) *lu_flops = c->work_lu;
+  return UVLM_OK;
+}
+
+}  // extern "C"

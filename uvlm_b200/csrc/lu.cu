@@ -1,0 +1,586 @@
+// lu.cu -- blocked LU with partial pivoting, FP64 and FP32 factor types.
+#include <climits>
+
+#include "lu.cuh"
+
+namespace uvlm {
+namespace {
+
+// Grid-wide barrier for cooperative launches.  bar[0] = arrival count,
+// bar[1] = generation.  The wait is bounded: after kSpinLimitCycles the
+// waiter sets err[0] (abort) and every CTA leaves at its next barrier.
+__device__ bool grid_sync(unsigned* bar, unsigned nblocks, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    volatile int* verr = err;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+    int okv = 1;
+    if (arrived == nblocks) {
+      bar[0] = 0u;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*vgen == g) {
+        if (verr[0]) { okv = 0; break; }
+        if (clock64() - t0 > kSpinLimitCycles) { atomicExch(err, 1); okv = 0; break; }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    if (verr[0]) okv = 0;
+    s_ok = okv;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__device__ inline void argmax_merge(double& v, int& r, double ov, int orow) {
+  if (ov > v || (ov == v && orow < r)) { v = ov; r = orow; }
+}
+
+// Block-wide argmax of (|value|, row) with ties to the lower row.
+__device__ void block_argmax(double& v, int& r) {
+  __shared__ double sv[32];
+  __shared__ int sr[32];
+  for (int off = 16; off; off >>= 1) {
+    const double ov = __shfl_down_sync(0xffffffffu, v, off);
+    const int orow = __shfl_down_sync(0xffffffffu, r, off);
+    argmax_merge(v, r, ov, orow);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sv[wid] = v; sr[wid] = r; }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = lane < nw ? sv[lane] : -1.0;
+    r = lane < nw ? sr[lane] : INT_MAX;
+    for (int off = 16; off; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, v, off);
+      const int orow = __shfl_down_sync(0xffffffffu, r, off);
+      argmax_merge(v, r, ov, orow);
+    }
+    if (lane == 0) { sv[0] = v; sr[0] = r; }
+  }
+  __syncthreads();
+  v = sv[0];
+  r = sr[0];
+  __syncthreads();
+}
+
+// One panel (columns k0..k0+kb-1, rows k0..n-1) of the factorisation.
+template <class T>
+__global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int lda, int n, int k0, int kb, int* ipiv,
+                                                        double* cand_val, int* cand_row, T* cand_data,
+                                                        T* diag_data, unsigned* bar, int* err, int rows_per_cta) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* rows = reinterpret_cast<T*>(smraw);     // [rows_per_cta][kLuNB]
+  T* urow = rows + rows_per_cta * kLuNB;     // [kLuNB]
+  __shared__ int s_piv, s_owner;
+  const int P = gridDim.x, bid = blockIdx.x, tid = threadIdx.x;
+  const int m = n - k0;
+  const int rb = bid * rows_per_cta;
+  const int re = min(rb + rows_per_cta, m);
+  const int nloc = max(0, re - rb);
+  for (int q = tid; q < nloc * kb; q += blockDim.x) {
+    const int r = q / kb, c = q % kb;
+    rows[r * kLuNB + c] = A[(long long)(k0 + rb + r) * lda + k0 + c];
+  }
+  __syncthreads();
+  for (int c = 0; c < kb; ++c) {
+    const int par = c & 1;
+    double bv = -1.0;
+    int br = INT_MAX;
+    for (int r = tid; r < nloc; r += blockDim.x) {
+      const int pr = rb + r;
+      if (pr < c) continue;
+      argmax_merge(bv, br, fabs((double)rows[r * kLuNB + c]), pr);
+    }
+    block_argmax(bv, br);
+    if (tid == 0) {
+      cand_val[par * kLuMaxCtas + bid] = bv;
+      cand_row[par * kLuMaxCtas + bid] = (bv >= 0.0) ? br : -1;
+    }
+    if (bv >= 0.0)
+      for (int q = tid; q < kb; q += blockDim.x)
+        cand_data[((long long)par * kLuMaxCtas + bid) * kLuNB + q] = rows[(br - rb) * kLuNB + q];
+    if (c >= rb && c < re)
+      for (int q = tid; q < kb; q += blockDim.x) diag_data[par * kLuNB + q] = rows[(c - rb) * kLuNB + q];
+    __threadfence();
+    if (!grid_sync(bar, (unsigned)P, err)) return;
+    if (tid < 32) {
+      double v = -1.0;
+      int r = INT_MAX, ow = -1;
+      for (int q = tid; q < P; q += 32) {
+        const double cv = ((volatile double*)cand_val)[par * kLuMaxCtas + q];
+        const int cr = ((volatile int*)cand_row)[par * kLuMaxCtas + q];
+        if (cr >= 0 && (cv > v || (cv == v && cr < r))) { v = cv; r = cr; ow = q; }
+      }
+      for (int off = 16; off; off >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, v, off);
+        const int orow = __shfl_down_sync(0xffffffffu, r, off);
+        const int oow = __shfl_down_sync(0xffffffffu, ow, off);
+        if (oow >= 0 && (ov > v || (ov == v && orow < r))) { v = ov; r = orow; ow = oow; }
+      }
+      if (tid == 0) {
+        if (!(v > 0.0)) {  // zero column: record, do not swap
+          atomicExch(err + 1, 1);
+          r = c;
+          ow = -1;
+        }
+        s_piv = r;
+        s_owner = ow;
+        if (bid == 0) ipiv[k0 + c] = k0 + r;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv, ow = s_owner;
+    const T* src = (ow >= 0) ? cand_data + ((long long)par * kLuMaxCtas + ow) * kLuNB : diag_data + par * kLuNB;
+    for (int q = tid; q < kb; q += blockDim.x) urow[q] = ((volatile T*)src)[q];
+    __syncthreads();
+    if (p != c && p >= rb && p < re)
+      for (int q = tid; q < kb; q += blockDim.x) rows[(p - rb) * kLuNB + q] = ((volatile T*)diag_data)[par * kLuNB + q];
+    if (c >= rb && c < re)
+      for (int q = tid; q < kb; q += blockDim.x) rows[(c - rb) * kLuNB + q] = urow[q];
+    __syncthreads();
+    const T piv = urow[c];
+    for (int r = tid; r < nloc; r += blockDim.x) {
+      if (rb + r > c) {
+        const T a = rows[r * kLuNB + c];
+        rows[r * kLuNB + c] = (piv != (T)0) ? a / piv : (T)0;
+      }
+    }
+    __syncthreads();
+    const int w = kb - c - 1;
+    if (w > 0) {
+      for (int q = tid; q < nloc * w; q += blockDim.x) {
+        const int r = q / w, cc = c + 1 + q % w;
+        if (rb + r > c) rows[r * kLuNB + cc] -= rows[r * kLuNB + c] * urow[cc];
+      }
+    }
+    __syncthreads();
+  }
+  for (int q = tid; q < nloc * kb; q += blockDim.x) {
+    const int r = q / kb, c = q % kb;
+    A[(long long)(k0 + rb + r) * lda + k0 + c] = rows[r * kLuNB + c];
+  }
+}
+
+// Row swaps of one panel applied to the columns outside the panel.
+template <class T>
+__global__ void laswp_kernel(T* A, int lda, int n, int k0, int kb, const int* __restrict__ ipiv) {
+  const int other = n - kb;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < other; q += gridDim.x * blockDim.x) {
+    const int col = q < k0 ? q : q + kb;
+    for (int c = 0; c < kb; ++c) {
+      const int p = ipiv[k0 + c];
+      if (p != k0 + c) {
+        T* a = A + (long long)(k0 + c) * lda + col;
+        T* b = A + (long long)p * lda + col;
+        const T t = *a;
+        *a = *b;
+        *b = t;
+      }
+    }
+  }
+}
+
+// U12 = L11^-1 A12 (unit lower L11), one thread per column.  Optionally also
+// writes U12 transposed into ut ([col - (k0+kb)][k], leading dim ldut).
+template <class T>
+__global__ void __launch_bounds__(128) trsm_kernel(T* A, int lda, int n, int k0, int kb, T* ut, int ldut) {
+  __shared__ T L[kLuNB][kLuNB + 1];
+  for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+    const int r = q / kb, c = q % kb;
+    L[r][c] = A[(long long)(k0 + r) * lda + k0 + c];
+  }
+  __syncthreads();
+  const int col = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  T x[kLuNB];
+#pragma unroll
+  for (int r = 0; r < kLuNB; ++r) x[r] = (r < kb) ? A[(long long)(k0 + r) * lda + col] : (T)0;
+#pragma unroll
+  for (int s = 0; s < kLuNB; ++s) {
+#pragma unroll
+    for (int r = s + 1; r < kLuNB; ++r) x[r] -= L[r][s] * x[s];
+  }
+#pragma unroll
+  for (int r = 0; r < kLuNB; ++r)
+    if (r < kb) A[(long long)(k0 + r) * lda + col] = x[r];
+  if (ut) {
+    T* o = ut + (long long)(col - k0 - kb) * ldut;
+#pragma unroll
+    for (int r = 0; r < kLuNB; ++r)
+      if (r < kb) o[r] = x[r];
+  }
+}
+
+// C -= A B with A [m x k] row-major (lda), B [k x nc] row-major (ldb).
+template <class T>
+__global__ void __launch_bounds__(256) gemm_update_kernel(T* C, int ldc, const T* __restrict__ A, int lda,
+                                                          const T* __restrict__ B, int ldb, int m, int nc, int k) {
+  constexpr int BM = 64, BN = 64, BK = 32;
+  __shared__ __align__(16) T As[BK][BM];
+  __shared__ __align__(16) T Bs[BK][BN];
+  const int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
+  for (int kk0 = 0; kk0 < k; kk0 += BK) {
+    const int kc = min(BK, k - kk0);
+    for (int q = tid; q < BM * BK; q += 256) {
+      const int r = q / BK, kk = q % BK;
+      As[kk][r] = (row0 + r < m && kk < kc) ? A[(long long)(row0 + r) * lda + kk0 + kk] : (T)0;
+    }
+    for (int q = tid; q < BK * BN; q += 256) {
+      const int kk = q / BN, c = q % BN;
+      Bs[kk][c] = (col0 + c < nc && kk < kc) ? B[(long long)(kk0 + kk) * ldb + col0 + c] : (T)0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < BK; ++kk) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = row0 + ty * 4 + i;
+    if (r >= m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = col0 + tx * 4 + j;
+      if (c < nc) C[(long long)r * ldc + c] -= acc[i][j];
+    }
+  }
+}
+
+// Inverses of the diagonal blocks: thread j < 64 forms column j of L_II^-1
+// (unit lower), thread 64 + j column j of U_II^-1.
+template <class T>
+__global__ void diag_inverse_kernel(const T* LU, int n, T* dinv_l, T* dinv_u) {
+  const int I = blockIdx.x;
+  const int r0 = I * kTriB;
+  const int nb = min(kTriB, n - r0);
+  T* Li = dinv_l + (long long)I * kTriB * kTriB;
+  T* Ui = dinv_u + (long long)I * kTriB * kTriB;
+  const int j = threadIdx.x & (kTriB - 1);
+  const bool upper = threadIdx.x >= kTriB;
+  if (!upper) {
+    for (int i = 0; i < kTriB; ++i) {
+      T x = (i == j) ? (T)1 : (T)0;
+      if (i < nb && j < nb && i > j) {
+        for (int s = j; s < i; ++s) x -= LU[(long long)(r0 + i) * n + r0 + s] * Li[s * kTriB + j];
+      }
+      if (i >= nb || j >= nb) x = (i == j) ? (T)1 : (T)0;
+      Li[i * kTriB + j] = (i < j) ? (T)0 : x;
+    }
+  } else {
+    for (int i = kTriB - 1; i >= 0; --i) {
+      T x = (T)0;
+      if (i < nb && j < nb && i <= j) {
+        x = (i == j) ? (T)1 : (T)0;
+        for (int s = i + 1; s <= j; ++s) x -= LU[(long long)(r0 + i) * n + r0 + s] * Ui[s * kTriB + j];
+        x = x / LU[(long long)(r0 + i) * n + r0 + i];
+      } else if (i == j) {
+        x = (T)1;
+      }
+      Ui[i * kTriB + j] = x;
+    }
+  }
+}
+
+// perm[k] = row of b that lands in row k after the LAPACK-style swap sequence.
+__global__ void ipiv_to_perm_kernel(const int* ipiv, int n, int* perm) {
+  extern __shared__ int sp[];
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < n; ++k) sp[k] = k;
+  for (int k = 0; k < n; ++k) {
+    const int p = ipiv[k];
+    const int t = sp[k];
+    sp[k] = sp[p];
+    sp[p] = t;
+  }
+  for (int k = 0; k < n; ++k) perm[k] = sp[k];
+}
+
+__device__ bool wait_flag(const unsigned* flag, unsigned epoch, int* err) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    const long long t0 = clock64();
+    int okv = 1;
+    while (((volatile const unsigned*)flag)[0] != epoch) {
+      if (((volatile int*)err)[0]) { okv = 0; break; }
+      if (clock64() - t0 > kSpinLimitCycles) { atomicExch(err + 2, 1); atomicExch(err, 1); okv = 0; break; }
+      __nanosleep(32);
+    }
+    __threadfence();
+    s_ok = okv;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Sync-free blocked triangular solve.  lower: y = L^-1 (P v); upper: z = U^-1 y.
+// CTA I owns block row I; for the lower solve it applies the block rows
+// J < I in order as their flags appear, for the upper solve J > I.
+template <class T, class V, bool kLower>
+__global__ void __launch_bounds__(256) trsv_kernel(const T* __restrict__ LU, int n, const int* __restrict__ perm,
+                                                   const double* __restrict__ vin, const V* yin, V* yout,
+                                                   const T* __restrict__ dinv, unsigned* flags, unsigned epoch,
+                                                   int* err, double* dout) {
+  __shared__ V acc[kTriB];
+  __shared__ V xs[kTriB];
+  const int nblk = gridDim.x;
+  const int I = kLower ? blockIdx.x : nblk - 1 - blockIdx.x;
+  const int r0 = I * kTriB;
+  const int nb = min(kTriB, n - r0);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid < kTriB) {
+    V v = 0;
+    if (tid < nb) v = kLower ? (V)vin[perm[r0 + tid]] : yin[r0 + tid];
+    acc[tid] = v;
+  }
+  __syncthreads();
+  for (int step = 0; step < nblk - 1 - (kLower ? nblk - 1 - I : I); ++step) {
+    const int J = kLower ? step : nblk - 1 - step;
+    if (!wait_flag(flags + J, epoch, err)) return;
+    const int c0 = J * kTriB;
+    const int nbj = min(kTriB, n - c0);
+    if (tid < kTriB) xs[tid] = (tid < nbj) ? ((volatile V*)yout)[c0 + tid] : (V)0;
+    __syncthreads();
+    // 8 warps x 8 rows each; lanes split the 64 columns
+    for (int rr = 0; rr < 8; ++rr) {
+      const int r = wid * 8 + rr;
+      V s = 0;
+      if (r < nb) {
+        const T* row = LU + (long long)(r0 + r) * n + c0;
+        for (int c = lane; c < nbj; c += 32) s += (V)row[c] * xs[c];
+      }
+      for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+      if (lane == 0 && r < nb) acc[r] -= s;
+    }
+    __syncthreads();
+  }
+  // x_I = dinv_I * acc
+  const T* D = dinv + (long long)I * kTriB * kTriB;
+  for (int rr = 0; rr < 8; ++rr) {
+    const int r = wid * 8 + rr;
+    V s = 0;
+    for (int c = lane; c < kTriB; c += 32) s += (V)D[r * kTriB + c] * acc[c];
+    for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (lane == 0) xs[r] = s;
+  }
+  __syncthreads();
+  if (tid < nb) {
+    yout[r0 + tid] = xs[tid];
+    if (dout) dout[r0 + tid] = (double)xs[tid];
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) atomicExch(flags + I, epoch);
+}
+
+template <class T>
+Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
+  if (n <= 0) return ok();
+  if (n > kLuMaxCtas * kTriB) return fail(kErrUnsupported, "matrix larger than the cooperative solve supports");
+  UVLM_CUDA_TRY(cudaMemsetAsync(w->err, 0, 4 * sizeof(int), st));
+  UVLM_CUDA_TRY(cudaMemsetAsync(w->bar, 0, 2 * sizeof(unsigned), st));
+  auto panel = lu_panel_kernel<T>;
+  for (int k0 = 0; k0 < n; k0 += kLuNB) {
+    const int kb = std::min(kLuNB, n - k0);
+    const int m = n - k0;
+    int P = std::min(std::min(w->num_sms, kLuMaxCtas), std::max(1, ceil_div(m, 16)));
+    const int rpc = ceil_div(m, P);
+    P = ceil_div(m, rpc);
+    size_t smem = sizeof(T) * ((size_t)rpc * kLuNB + kLuNB);
+    if (smem > 48 * 1024) UVLM_CUDA_TRY(cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int lda = n;
+    int* ipiv = w->ipiv;
+    double* cv = w->cand_val;
+    int* cr = w->cand_row;
+    T* cd = reinterpret_cast<T*>(w->cand_data);
+    T* dd = reinterpret_cast<T*>(w->diag_data);
+    unsigned* bar = w->bar;
+    int* err = w->err;
+    int nn = n, kk0 = k0, kkb = kb, rr = rpc;
+    void* args[] = {&A, &lda, &nn, &kk0, &kkb, &ipiv, &cv, &cr, &cd, &dd, &bar, &err, &rr};
+    UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(256), args, smem, st));
+    note_launch();
+    if (n - kb > 0) {
+      const int other = n - kb;
+      laswp_kernel<T><<<std::min(ceil_div(other, 256), 1024), 256, 0, st>>>(A, n, n, k0, kb, w->ipiv);
+      UVLM_LAUNCH_CHECK();
+    }
+    const int rest = n - k0 - kb;
+    if (rest > 0) {
+      T* ut = (upd != kLuUpdateSimt) ? reinterpret_cast<T*>(w->ut) : nullptr;
+      trsm_kernel<T><<<ceil_div(rest, 128), 128, 0, st>>>(A, n, n, k0, kb, ut, kLuNB);
+      UVLM_LAUNCH_CHECK();
+      T* C = A + (long long)(k0 + kb) * n + (k0 + kb);
+      const T* L21 = A + (long long)(k0 + kb) * n + k0;
+      const T* U12 = A + (long long)k0 * n + (k0 + kb);
+      if constexpr (sizeof(T) == 8) {
+        UVLM_TRY(gemm_update_f64(reinterpret_cast<double*>(C), n, reinterpret_cast<const double*>(L21), n,
+                                 reinterpret_cast<const double*>(U12), n, rest, rest, kb, st));
+      } else {
+        if (upd == kLuUpdateSimt || kb % 32 != 0) {
+          UVLM_TRY(gemm_update_f32_simt(reinterpret_cast<float*>(C), n, reinterpret_cast<const float*>(L21), n,
+                                        reinterpret_cast<const float*>(U12), n, rest, rest, kb, st));
+        } else {
+          UVLM_TRY(gemm_update_tc(reinterpret_cast<float*>(C), n, reinterpret_cast<const float*>(L21), n,
+                                  reinterpret_cast<const float*>(w->ut), kLuNB, rest, rest, kb, upd, w, st));
+        }
+      }
+    }
+  }
+  const int nblk = ceil_div(n, kTriB);
+  diag_inverse_kernel<T><<<nblk, 2 * kTriB, 0, st>>>(A, n, reinterpret_cast<T*>(w->dinv_l),
+                                                     reinterpret_cast<T*>(w->dinv_u));
+  UVLM_LAUNCH_CHECK();
+  // permutation vector stored after ipiv
+  ipiv_to_perm_kernel<<<1, 32, sizeof(int) * n, st>>>(w->ipiv, n, w->ipiv + n);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+template <class T, class V>
+Error tri_solve(const T* LU, int n, LuWork* w, const double* vin, V* y, V* z, double* dout, cudaStream_t st) {
+  const int nblk = ceil_div(n, kTriB);
+  const unsigned epoch = ++w->epoch;
+  const int* perm = w->ipiv + n;
+  const T* dl = reinterpret_cast<const T*>(w->dinv_l);
+  const T* du = reinterpret_cast<const T*>(w->dinv_u);
+  unsigned* fl = w->flags;
+  unsigned* fu = w->flags + kLuMaxCtas;
+  int* err = w->err;
+  double* nod = nullptr;
+  const V* noy = nullptr;
+  {
+    auto k = trsv_kernel<T, V, true>;
+    int nn = n;
+    unsigned ep = epoch;
+    void* args[] = {(void*)&LU, &nn, (void*)&perm, (void*)&vin, (void*)&noy, (void*)&y, (void*)&dl, &fl, &ep, &err, &nod};
+    UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k, dim3(nblk), dim3(256), args, 0, st));
+    note_launch();
+  }
+  {
+    auto k = trsv_kernel<T, V, false>;
+    int nn = n;
+    unsigned ep = epoch;
+    const V* yc = y;
+    const double* nov = nullptr;
+    void* args[] = {(void*)&LU, &nn, (void*)&perm, (void*)&nov, (void*)&yc, (void*)&z, (void*)&du, &fu, &ep, &err, &dout};
+    UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k, dim3(nblk), dim3(256), args, 0, st));
+    note_launch();
+  }
+  return ok();
+}
+
+}  // namespace
+
+Error lu_work_alloc(LuWork* w, int n, int elem_size, int num_sms) {
+  lu_work_free(w);
+  w->n = n;
+  w->elem_size = elem_size;
+  w->num_sms = num_sms;
+  const int nblk = ceil_div(n, kTriB);
+  UVLM_CUDA_TRY(cudaMalloc(&w->ipiv, sizeof(int) * 2 * n));
+  UVLM_CUDA_TRY(cudaMalloc(&w->err, sizeof(int) * 4));
+  UVLM_CUDA_TRY(cudaMalloc(&w->bar, sizeof(unsigned) * 2));
+  UVLM_CUDA_TRY(cudaMalloc(&w->cand_val, sizeof(double) * 2 * kLuMaxCtas));
+  UVLM_CUDA_TRY(cudaMalloc(&w->cand_row, sizeof(int) * 2 * kLuMaxCtas));
+  UVLM_CUDA_TRY(cudaMalloc(&w->cand_data, (size_t)elem_size * 2 * kLuMaxCtas * kLuNB));
+  UVLM_CUDA_TRY(cudaMalloc(&w->diag_data, (size_t)elem_size * 2 * kLuNB));
+  UVLM_CUDA_TRY(cudaMalloc(&w->dinv_l, (size_t)elem_size * nblk * kTriB * kTriB));
+  UVLM_CUDA_TRY(cudaMalloc(&w->dinv_u, (size_t)elem_size * nblk * kTriB * kTriB));
+  UVLM_CUDA_TRY(cudaMalloc(&w->flags, sizeof(unsigned) * 2 * kLuMaxCtas));
+  UVLM_CUDA_TRY(cudaMemset(w->flags, 0, sizeof(unsigned) * 2 * kLuMaxCtas));
+  UVLM_CUDA_TRY(cudaMemset(w->err, 0, sizeof(int) * 4));
+  if (elem_size == 4) {
+    UVLM_CUDA_TRY(cudaMalloc(&w->ut, sizeof(float) * (size_t)n * kLuNB));
+    UVLM_CUDA_TRY(cudaMalloc(&w->opA, 2 * (size_t)n * kLuNB));
+    UVLM_CUDA_TRY(cudaMalloc(&w->opB, 2 * (size_t)n * kLuNB));
+  }
+  w->epoch = 0;
+  return ok();
+}
+
+void lu_work_free(LuWork* w) {
+  cudaFree(w->ipiv);
+  cudaFree(w->err);
+  cudaFree(w->bar);
+  cudaFree(w->cand_val);
+  cudaFree(w->cand_row);
+  cudaFree(w->cand_data);
+  cudaFree(w->diag_data);
+  cudaFree(w->dinv_l);
+  cudaFree(w->dinv_u);
+  cudaFree(w->flags);
+  cudaFree(w->ut);
+  cudaFree(w->opA);
+  cudaFree(w->opB);
+  *w = LuWork{};
+}
+
+Error lu_factor_f64(double* A, int n, LuWork* w, cudaStream_t st) {
+  return lu_factor_impl<double>(A, n, kLuUpdateSimt, w, st);
+}
+
+Error lu_factor_f32(float* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
+  return lu_factor_impl<float>(A, n, upd, w, st);
+}
+
+Error lu_check(LuWork* w, cudaStream_t st) {
+  int h[4] = {0, 0, 0, 0};
+  UVLM_CUDA_TRY(cudaMemcpyAsync(h, w->err, sizeof(h), cudaMemcpyDeviceToHost, st));
+  UVLM_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h[0]) return fail(kErrTimeout, h[2] ? "triangular solve wait timed out" : "LU panel barrier timed out");
+  if (h[1]) return fail(kErrSingular, "zero pivot in LU factorisation");
+  return ok();
+}
+
+Error lu_solve_f64(const double* LU, int n, LuWork* w, const double* b, double* x, double* tmp, cudaStream_t st) {
+  return tri_solve<double, double>(LU, n, w, b, tmp, x, nullptr, st);
+}
+
+Error lu_solve_f32(const float* LU, int n, LuWork* w, const double* v, double* z, float* tmp, cudaStream_t st) {
+  return tri_solve<float, float>(LU, n, w, v, tmp, tmp + n, z, st);
+}
+
+Error gemm_update_f64(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int m, int nc, int k,
+                      cudaStream_t st) {
+  if (m <= 0 || nc <= 0 || k <= 0) return ok();
+  dim3 grid(ceil_div(nc, 64), ceil_div(m, 64));
+  gemm_update_kernel<double><<<grid, 256, 0, st>>>(C, ldc, A, lda, B, ldb, m, nc, k);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error gemm_update_f32_simt(float* C, int ldc, const float* A, int lda, const float* B, int ldb, int m, int nc, int k,
+                           cudaStream_t st) {
+  if (m <= 0 || nc <= 0 || k <= 0) return ok();
+  dim3 grid(ceil_div(nc, 64), ceil_div(m, 64));
+  gemm_update_kernel<float><<<grid, 256, 0, st>>>(C, ldc, A, lda, B, ldb, m, nc, k);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+}  // namespace uvlm

@@ -1,0 +1,569 @@
+// step.cu -- kinematics, shedding, geometry, assembly, RHS, loads, advection.
+#include "bs_math.cuh"
+#include "step.cuh"
+
+namespace uvlm {
+namespace {
+
+// ------------------------------------------------------------ kinematics
+// Morphing::Perfome (src/morphing.cpp:23-43) with PrepareMatrix (:54-76):
+// x = plug(t) z + (attack * flap * twist) (x_ref + bend z), y<0 mirrored.
+__device__ d3 perfome(const uvlm_kinematics& k, d3 x0, double t) {
+  const d3 o = mk(k.origin[0], k.origin[1], k.origin[2]);
+  d3 xr = sub(x0, o);
+  const bool neg = xr.y < 0;
+  if (neg) xr.y *= -1;
+  const double phi = k.flap_amp * sin(k.flap_omega * t + k.flap_phase);
+  const double alpha = k.alpha;
+  const double beta = (k.twist_amp + k.twist_span_slope * fabs(xr.y)) * sin(k.twist_omega * t + k.twist_phase);
+  const double F[3][3] = {{1, 0, 0}, {0, cos(phi), -sin(phi)}, {0, sin(phi), cos(phi)}};
+  const double A[3][3] = {{cos(alpha), 0, sin(alpha)}, {0, 1, 0}, {-sin(alpha), 0, cos(alpha)}};
+  const double T[3][3] = {{cos(beta), 0, sin(beta)}, {0, 1, 0}, {-sin(beta), 0, cos(beta)}};
+  double AF[3][3], M[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) AF[i][j] = A[i][0] * F[0][j] + A[i][1] * F[1][j] + A[i][2] * F[2][j];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) M[i][j] = AF[i][0] * T[0][j] + AF[i][1] * T[1][j] + AF[i][2] * T[2][j];
+  const double gz = k.plug_amp * sin(k.plug_omega * t + k.plug_phase);
+  const double gb = (k.bend_cx * xr.x * (1 - xr.x) + k.bend_cy * xr.y * xr.y) * sin(k.bend_omega * t + k.bend_phase);
+  const d3 v = mk(xr.x, xr.y, xr.z + gb);
+  d3 x = mk(M[0][0] * v.x + M[0][1] * v.y + M[0][2] * v.z, M[1][0] * v.x + M[1][1] * v.y + M[1][2] * v.z,
+            M[2][0] * v.x + M[2][1] * v.y + M[2][2] * v.z);
+  x = add(mk(0, 0, gz), x);
+  if (xr.y == 0) x.y = 0;
+  if (neg) x.y *= -1;
+  return add(x, o);
+}
+
+// Morphing::Velocity (src/morphing.cpp:45-52): central difference, h = 1e-6.
+__device__ d3 morph_velocity(const uvlm_kinematics& k, d3 x0, double t) {
+  const double h = 1e-6;
+  const d3 x1 = perfome(k, x0, t - h);
+  const d3 x2 = perfome(k, x0, t + h);
+  return dvs(sub(x2, x1), 2 * h);
+}
+
+__global__ void kinematics_kernel(const uvlm_kinematics* __restrict__ kin, WingShape ws, const double* pos_init,
+                                  double* pos, double t) {
+  const long long per = (long long)(ws.R + 1) * (ws.C + 1);
+  const long long total = per * ws.num;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int n = (int)(k / per);
+    st3(pos + 3 * k, perfome(kin[n], ld3(pos_init + 3 * k), t));
+  }
+}
+
+// SimpleSimulator::Shed (simple_simulator.cpp:171-188): prepend the TE node
+// row; from step 1 on also the TE circulation row of the previous solve.
+__global__ void shed_kernel(WingShape ws, const double* wing_pos, const double* wing_gamma, WakeLayout wl,
+                            double* wake_pos, double* wake_gamma, int shed_gamma) {
+  const int C1 = ws.C + 1;
+  const int total = ws.num * C1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const int n = k / C1, j = k % C1;
+    const double* p = wing_pos + 3 * ws.node(n, ws.R, j);
+    double* q = wake_pos + 3 * wl.node(n, 0, j);
+    q[0] = p[0];
+    q[1] = p[1];
+    q[2] = p[2];
+    if (shed_gamma && j < ws.C) wake_gamma[wl.ring(n, 0, j)] = wing_gamma[ws.ring(n, ws.R - 1, j)];
+  }
+}
+
+__global__ void panel_geometry_kernel(const uvlm_kinematics* __restrict__ kin, WingShape ws, const double* pos,
+                                      const double* pos_init, double t, double* cx, double* cy, double* cz,
+                                      double* normal, double* area, double* uls) {
+  const int per = ws.R * ws.C;
+  const int total = per * ws.num;
+  for (int K = blockIdx.x * blockDim.x + threadIdx.x; K < total; K += gridDim.x * blockDim.x) {
+    const int n = K / per, i = (K % per) / ws.C, j = K % ws.C;
+    const d3 p00 = ld3(pos + 3 * ws.node(n, i, j)), p10 = ld3(pos + 3 * ws.node(n, i + 1, j));
+    const d3 p11 = ld3(pos + 3 * ws.node(n, i + 1, j + 1)), p01 = ld3(pos + 3 * ws.node(n, i, j + 1));
+    // CollocationPoints (simple_simulator.cpp:19-32)
+    const d3 c = dvs(add(add(add(p00, p10), p11), p01), 4);
+    cx[K] = c.x;
+    cy[K] = c.y;
+    cz[K] = c.z;
+    // Normals (:34-50)
+    st3(normal + 3 * K, normalized(cross(sub(p11, p00), sub(p01, p10))));
+    // CalcPanelArea (src/calc_load/joukowski.cpp:55-67)
+    area[K] = norm(cross(sub(p10, p00), sub(p01, p00)));
+    const d3 q00 = ld3(pos_init + 3 * ws.node(n, i, j)), q10 = ld3(pos_init + 3 * ws.node(n, i + 1, j));
+    const d3 q11 = ld3(pos_init + 3 * ws.node(n, i + 1, j + 1)), q01 = ld3(pos_init + 3 * ws.node(n, i, j + 1));
+    const d3 c0 = dvs(add(add(add(q00, q10), q11), q01), 4);
+    st3(uls + 3 * K, morph_velocity(kin[n], c0, t));
+  }
+}
+
+// ---------------------------------------------------------------- assembly
+// CTA: 128 rings (threads) x a chunk of collocation points staged in shared
+// memory; each thread evaluates its ring's four segments p0->p1->p2->p3->p0
+// (VORING, src/vortex.cpp:145-160) at every staged point.
+constexpr int kAsmRings = 128;
+constexpr int kAsmTargets = 128;
+
+template <class T>
+struct AsmPt {
+  T hx, hy, hz, lx, ly, lz, nx, ny, nz;
+};
+
+template <class T, class OutT>
+__global__ void __launch_bounds__(kAsmRings) assemble_kernel(WingShape ws, const double* __restrict__ pos,
+                                                              const double* __restrict__ cx, const double* __restrict__ cy,
+                                                              const double* __restrict__ cz,
+                                                              const double* __restrict__ normal, int chunk, OutT* A) {
+  __shared__ AsmPt<T> pts[kAsmTargets];
+  const int N = ws.num * ws.R * ws.C;
+  const int L = blockIdx.x * kAsmRings + threadIdx.x;
+  const bool valid = L < N;
+  const int Lc = valid ? L : N - 1;
+  const int per = ws.R * ws.C;
+  const int n = Lc / per, i = (Lc % per) / ws.C, j = Lc % ws.C;
+  const long long idx[4] = {ws.node(n, i, j), ws.node(n, i, j + 1), ws.node(n, i + 1, j + 1), ws.node(n, i + 1, j)};
+  T ph[4][3], pl[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double v = pos[3 * idx[q] + d];
+      ph[q][d] = (T)v;
+      pl[q][d] = (T)(v - (double)ph[q][d]);
+    }
+  const T g = (T)(1.0 / (4.0 * kPi));
+  const int K0 = blockIdx.y * chunk;
+  const int K1 = min(N, K0 + chunk);
+  for (int kb = K0; kb < K1; kb += kAsmTargets) {
+    const int cnt = min(kAsmTargets, K1 - kb);
+    __syncthreads();
+    if (threadIdx.x < cnt) {
+      const int K = kb + threadIdx.x;
+      AsmPt<T> p;
+      const double x = cx[K], y = cy[K], z = cz[K];
+      p.hx = (T)x; p.hy = (T)y; p.hz = (T)z;
+      p.lx = (T)(x - (double)p.hx); p.ly = (T)(y - (double)p.hy); p.lz = (T)(z - (double)p.hz);
+      p.nx = (T)normal[3 * K]; p.ny = (T)normal[3 * K + 1]; p.nz = (T)normal[3 * K + 2];
+      pts[threadIdx.x] = p;
+    }
+    __syncthreads();
+    for (int t = 0; t < cnt; ++t) {
+      const AsmPt<T> p = pts[t];
+      Node<T> nd[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const T x = (p.hx - ph[q][0]) + (p.lx - pl[q][0]);
+        const T y = (p.hy - ph[q][1]) + (p.ly - pl[q][1]);
+        const T z = (p.hz - ph[q][2]) + (p.lz - pl[q][2]);
+        nd[q] = make_node<T>(x, y, z);
+      }
+      T vx = 0, vy = 0, vz = 0;
+      segment<T>(nd[0], nd[1], g, vx, vy, vz);
+      segment<T>(nd[1], nd[2], g, vx, vy, vz);
+      segment<T>(nd[2], nd[3], g, vx, vy, vz);
+      segment<T>(nd[3], nd[0], g, vx, vy, vz);
+      if (valid) A[(long long)(kb + t) * N + L] = (OutT)(vx * p.nx + vy * p.ny + vz * p.nz);
+    }
+  }
+}
+
+// Legacy AoS assembly (src/linear.inl:14-32): A[i][j] = ring_j.BiotSavartLaw(
+// centroid_i, 1).Normal_i with ForEachSegment order nodes[k+1] -> nodes[k].
+__global__ void ring_geometry_kernel(const double* rings, int n, double* centroid, double* normal) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double* r = rings + 12 * i;
+    const d3 a = ld3(r), b = ld3(r + 3), c = ld3(r + 6), d = ld3(r + 9);
+    st3(centroid + 3 * i, dvs(add(add(add(a, b), c), d), 4));                 // vortex.cpp:98-100
+    st3(normal + 3 * i, normalized(cross(sub(b, d), sub(c, a))));               // vortex.cpp:82-87
+  }
+}
+
+__global__ void assemble_rings_kernel(const double* rings, int n, const double* centroid, const double* normal,
+                                      double* A) {
+  const long long total = (long long)n * n;
+  const double g = 1.0 / (4.0 * kPi);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / n), j = (int)(q % n);
+    const d3 x = ld3(centroid + 3 * i);
+    const double* r = rings + 12 * j;
+    Node<double> nd[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) nd[k] = make_node<double>(x.x - r[3 * k], x.y - r[3 * k + 1], x.z - r[3 * k + 2]);
+    double vx = 0, vy = 0, vz = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) segment<double>(nd[(k + 1) & 3], nd[k], g, vx, vy, vz);
+    A[q] = vx * normal[3 * i] + vy * normal[3 * i + 1] + vz * normal[3 * i + 2];
+  }
+}
+
+__global__ void legacy_rhs_kernel(const uvlm_kinematics* __restrict__ kin, const double* rings0, int n,
+                                  const double* normal, d3 fs, double t, const double* wake_vel, double* b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double* r = rings0 + 12 * i;
+    const d3 c0 = dvs(add(add(add(ld3(r), ld3(r + 3)), ld3(r + 6)), ld3(r + 9)), 4);  // ReferenceCentroid
+    const d3 nl = ld3(normal + 3 * i);
+    double v = dot(morph_velocity(kin[0], c0, t), nl) - dot(fs, nl);
+    if (wake_vel) v -= dot(ld3(wake_vel + 3 * i), nl);
+    b[i] = v;
+  }
+}
+
+__global__ void rhs_kernel(int N, const double* uwx, const double* uwy, const double* uwz, const double* uls,
+                           const double* normal, d3 ff, double* b) {
+  for (int K = blockIdx.x * blockDim.x + threadIdx.x; K < N; K += gridDim.x * blockDim.x) {
+    const d3 uw = mk(uwx ? uwx[K] : 0.0, uwy ? uwy[K] : 0.0, uwz ? uwz[K] : 0.0);
+    const d3 u = sub(uw, add(ld3(uls + 3 * K), ff));
+    b[K] = -dot(u, ld3(normal + 3 * K));
+  }
+}
+
+// Unique load lines of wing n: q < R*C spanwise S(i,j) (i < R, the TE row is
+// skipped, joukowski.cpp:26), then R*(C+1) chordwise H(i,j).
+__device__ inline void line_nodes(const WingShape& ws, int n, int q, long long& a, long long& b) {
+  if (q < ws.R * ws.C) {
+    const int i = q / ws.C, j = q % ws.C;
+    a = ws.node(n, i, j);
+    b = ws.node(n, i, j + 1);
+  } else {
+    q -= ws.R * ws.C;
+    const int i = q / (ws.C + 1), j = q % (ws.C + 1);
+    a = ws.node(n, i, j);
+    b = ws.node(n, i + 1, j);
+  }
+}
+
+__device__ inline double gam(const WingShape& ws, const double* g, int n, int i, int j) {
+  if (i < 0 || i >= ws.R || j < 0 || j >= ws.C) return 0.0;
+  return g[ws.ring(n, i, j)];
+}
+
+__device__ inline double line_strength(const WingShape& ws, const double* g, int n, int q) {
+  if (q < ws.R * ws.C) {
+    const int i = q / ws.C, j = q % ws.C;
+    return gam(ws, g, n, i, j) - gam(ws, g, n, i - 1, j);
+  }
+  q -= ws.R * ws.C;
+  const int i = q / (ws.C + 1), j = q % (ws.C + 1);
+  return gam(ws, g, n, i, j - 1) - gam(ws, g, n, i, j);
+}
+
+__global__ void line_prep_kernel(const uvlm_kinematics* __restrict__ kin, WingShape ws, const double* pos,
+                                 const double* pos_init, double t, double* tx, double* ty, double* tz,
+                                 double* line_uls) {
+  const int Lw = ws.lines_per_wing();
+  const int total = Lw * ws.num;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const int n = k / Lw, q = k % Lw;
+    long long a, b;
+    line_nodes(ws, n, q, a, b);
+    const d3 mp = dvs(add(ld3(pos + 3 * a), ld3(pos + 3 * b)), 2);
+    const d3 mp0 = dvs(add(ld3(pos_init + 3 * a), ld3(pos_init + 3 * b)), 2);
+    tx[k] = mp.x;
+    ty[k] = mp.y;
+    tz[k] = mp.z;
+    st3(line_uls + 3 * k, morph_velocity(kin[n], mp0, t));
+  }
+}
+
+template <int BS>
+__device__ inline double block_sum(double v, double* sh) {
+  for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  v = (threadIdx.x < BS / 32) ? sh[threadIdx.x] : 0.0;
+  if (wid == 0)
+    for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  return v;  // valid in thread 0
+}
+
+// CalcLoad (simple_simulator.cpp:195-233): JoukowskiSteady over the lines
+// (U x dl) * Gamma with U = (-ff + Ub + Uw)(mid) - Uls(mid0), plus
+// JoukowskiUnsteady n * dGamma/dt * A; C = F / (0.5 |ff|^2 chord span).
+template <int BS>
+__global__ void __launch_bounds__(BS) loads_kernel(WingShape ws, const double* pos, const double* gamma,
+                                                    const double* gamma_prev, const double* normal,
+                                                    const double* area, const double* vx, const double* vy,
+                                                    const double* vz, const double* line_uls, d3 ff,
+                                                    const double* chord_span, double t, double dt, double* row) {
+  __shared__ double sh[32];
+  const int n = blockIdx.x;
+  const int Lw = ws.lines_per_wing();
+  double f[3] = {0, 0, 0}, u[3] = {0, 0, 0};
+  for (int q = threadIdx.x; q < Lw; q += BS) {
+    const int k = n * Lw + q;
+    long long a, b;
+    line_nodes(ws, n, q, a, b);
+    const d3 dl = sub(ld3(pos + 3 * b), ld3(pos + 3 * a));
+    const d3 U = sub(add(mk(-ff.x, -ff.y, -ff.z), mk(vx[k], vy[k], vz[k])), ld3(line_uls + 3 * k));
+    const d3 df = scl(cross(U, dl), line_strength(ws, gamma, n, q));
+    f[0] += df.x;
+    f[1] += df.y;
+    f[2] += df.z;
+  }
+  const int per = ws.R * ws.C;
+  for (int p = threadIdx.x; p < per; p += BS) {
+    const int K = n * per + p;
+    const double dgdt = (gamma[K] - gamma_prev[K]) / dt;
+    const d3 df = scl(scl(ld3(normal + 3 * K), dgdt), area[K]);
+    u[0] += df.x;
+    u[1] += df.y;
+    u[2] += df.z;
+  }
+  double F[3];
+  for (int d = 0; d < 3; ++d) {
+    const double fs = block_sum<BS>(f[d], sh);
+    const double fu = block_sum<BS>(u[d], sh);
+    F[d] = fs + fu;
+  }
+  if (threadIdx.x == 0) {
+    const double Q = norm(ff);
+    const double S = chord_span[2 * n] * chord_span[2 * n + 1];
+    const double den = 0.5 * Q * Q * S;
+    if (n == 0) row[0] = t;
+    row[1 + 2 * n] = F[0] / den;
+    row[2 + 2 * n] = F[2] / den;
+  }
+}
+
+__global__ void gather_wake_kernel(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz) {
+  const int C1 = wl.C + 1;
+  const int rows = wl.node_rows - 1;
+  const long long total = (long long)wl.num * rows * C1;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(k % C1);
+    const long long nr = k / C1;
+    const int i = (int)(nr % rows) + 1, n = (int)(nr / rows);
+    const double* p = pos + 3 * wl.node(n, i, j);
+    tx[k] = p[0];
+    ty[k] = p[1];
+    tz[k] = p[2];
+  }
+}
+
+__global__ void advect_kernel(int mode, WakeLayout wl, double* x, double* pos2, double* k1, double* k2, double* k3,
+                              double* vprev, int has_vprev, const double* vx, const double* vy, const double* vz,
+                              d3 ff, double dt, int ignore) {
+  const int C1 = wl.C + 1;
+  const long long total = (long long)wl.num * wl.node_rows * C1;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(k % C1);
+    const long long nr = k / C1;
+    const int i = (int)(nr % wl.node_rows), n = (int)(nr / wl.node_rows);
+    const long long P = 3 * wl.node(n, i, j);
+    const d3 mff = mk(-ff.x, -ff.y, -ff.z);
+    d3 u = mff;
+    if (i >= 1) {
+      const long long ti = ((long long)n * (wl.node_rows - 1) + (i - 1)) * C1 + j;
+      u = add(mff, mk(vx[ti], vy[ti], vz[ti]));
+    }
+    const d3 xp = ld3(x + P);
+    switch (mode) {
+      case kAdvEuler:  // src/advect.cpp:11-22
+        st3(x + P, add(xp, scl(u, dt)));
+        break;
+      case kAdvRK2K1:  // src/advect.cpp:40-57
+        st3(k1 + P, u);
+        st3(pos2 + P, add(xp, scl(u, dt)));
+        break;
+      case kAdvRK2Upd: {  // src/advect.cpp:71-79
+        const d3 a = ld3(k1 + P);
+        st3(x + P, i > ignore ? add(xp, dvs(scl(add(a, u), dt), 2)) : add(xp, scl(a, dt)));
+        break;
+      }
+      case kAdvRK4K1:  // src/advect.cpp:98-118
+        st3(k1 + P, u);
+        st3(pos2 + P, add(xp, dvs(scl(u, dt), 2)));
+        break;
+      case kAdvRK4K2:  // :118-135
+        st3(k2 + P, u);
+        st3(pos2 + P, add(xp, dvs(scl(u, dt), 2)));
+        break;
+      case kAdvRK4Upd: {  // :167-178, k3 used twice and k4 never (:173)
+        const d3 a = ld3(k1 + P), b = ld3(k2 + P);
+        const d3 s = add(add(add(a, scl(b, 2)), scl(u, 2)), u);
+        st3(x + P, i > ignore ? add(xp, dvs(scl(s, dt), 6)) : add(xp, scl(a, dt)));
+        break;
+      }
+      case kAdvAB2: {  // src/advect.cpp:181-217
+        if (has_vprev && i >= 1) {
+          const d3 vp = ld3(vprev + P);
+          st3(x + P, add(xp, dvs(scl(sub(scl(u, 3), vp), dt), 2)));
+        } else {
+          st3(x + P, add(xp, scl(u, dt)));
+        }
+        st3(vprev + P, u);
+        break;
+      }
+      default:
+        break;
+    }
+  }
+}
+
+__global__ void copy_rows_kernel(const double* src, double* dst, int num, int PR, int row_elems, int from, int to,
+                                 int rows) {
+  const long long per = (long long)rows * row_elems;
+  const long long total = per * num;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int n = (int)(k / per);
+    const long long r = k % per;
+    dst[((long long)n * PR + to) * row_elems + r] = src[((long long)n * PR + from) * row_elems + r];
+  }
+}
+
+__global__ void extrapolate_kernel(double* x, const double* a, const double* b, int n) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 2.0 * a[k] - b[k];
+}
+
+__global__ void check_finite_kernel(const double* x, long long n, int* flag) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    if (!isfinite(x[k])) atomicOr(flag, 1);
+}
+
+inline int grid_for(long long n, int bs = 256) {
+  long long g = (n + bs - 1) / bs;
+  if (g < 1) g = 1;
+  if (g > 65535) g = 65535;
+  return (int)g;
+}
+
+}  // namespace
+
+Error launch_kinematics(const uvlm_kinematics* d_kin, WingShape ws, const double* pos_init, double* pos, double t,
+                        cudaStream_t st) {
+  const long long total = (long long)ws.num * (ws.R + 1) * (ws.C + 1);
+  kinematics_kernel<<<grid_for(total), 256, 0, st>>>(d_kin, ws, pos_init, pos, t);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_shed(WingShape ws, const double* wing_pos, const double* wing_gamma, WakeLayout wl, double* wake_pos,
+                  double* wake_gamma, bool shed_gamma, cudaStream_t st) {
+  shed_kernel<<<grid_for(ws.num * (ws.C + 1)), 256, 0, st>>>(ws, wing_pos, wing_gamma, wl, wake_pos, wake_gamma,
+                                                             shed_gamma ? 1 : 0);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_panel_geometry(const uvlm_kinematics* d_kin, WingShape ws, const double* pos, const double* pos_init,
+                            double t, double* cx, double* cy, double* cz, double* normal, double* area, double* uls,
+                            cudaStream_t st) {
+  panel_geometry_kernel<<<grid_for((long long)ws.num * ws.R * ws.C), 256, 0, st>>>(d_kin, ws, pos, pos_init, t, cx, cy,
+                                                                                   cz, normal, area, uls);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_assemble(WingShape ws, const double* pos, const double* cx, const double* cy, const double* cz,
+                      const double* normal, bool fp32, void* A, bool out_f32, cudaStream_t st) {
+  const int N = ws.num * ws.R * ws.C;
+  const int gx = ceil_div(N, kAsmRings);
+  // split the collocation points so that the grid has a few waves
+  int chunk = kAsmTargets * std::max(1, ceil_div(N, kAsmTargets * std::max(1, 1184 / std::max(gx, 1))));
+  const int gy = ceil_div(N, chunk);
+  dim3 grid(gx, gy);
+  if (fp32) {
+    if (out_f32)
+      assemble_kernel<float, float><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (float*)A);
+    else
+      assemble_kernel<float, double><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (double*)A);
+  } else {
+    if (out_f32)
+      assemble_kernel<double, float><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (float*)A);
+    else
+      assemble_kernel<double, double><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (double*)A);
+  }
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_assemble_rings(const double* rings, int n, double* A, double* centroid, double* normal,
+                            cudaStream_t st) {
+  ring_geometry_kernel<<<grid_for(n), 256, 0, st>>>(rings, n, centroid, normal);
+  UVLM_LAUNCH_CHECK();
+  assemble_rings_kernel<<<grid_for((long long)n * n), 256, 0, st>>>(rings, n, centroid, normal, A);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_legacy_rhs(const uvlm_kinematics* d_kin, const double* rings0, int n, const double* centroid,
+                        const double* normal, const double fs[3], double t, const double* wake_vel, double* b,
+                        cudaStream_t st) {
+  (void)centroid;
+  legacy_rhs_kernel<<<grid_for(n), 256, 0, st>>>(d_kin, rings0, n, normal, mk(fs[0], fs[1], fs[2]), t, wake_vel, b);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_rhs(int N, const double* uw_x, const double* uw_y, const double* uw_z, const double* uls,
+                 const double* normal, const double ff[3], double* b, cudaStream_t st) {
+  rhs_kernel<<<grid_for(N), 256, 0, st>>>(N, uw_x, uw_y, uw_z, uls, normal, mk(ff[0], ff[1], ff[2]), b);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_line_prep(const uvlm_kinematics* d_kin, WingShape ws, const double* pos, const double* pos_init,
+                       double t, double* tx, double* ty, double* tz, double* line_uls, cudaStream_t st) {
+  line_prep_kernel<<<grid_for((long long)ws.num * ws.lines_per_wing()), 256, 0, st>>>(d_kin, ws, pos, pos_init, t, tx,
+                                                                                      ty, tz, line_uls);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_loads(WingShape ws, const double* pos, const double* gamma, const double* gamma_prev,
+                   const double* normal, const double* area, const double* vx, const double* vy, const double* vz,
+                   const double* line_uls, const double ff[3], const double* chord_span, double t, double dt,
+                   double* row, cudaStream_t st) {
+  loads_kernel<512><<<ws.num, 512, 0, st>>>(ws, pos, gamma, gamma_prev, normal, area, vx, vy, vz, line_uls,
+                                            mk(ff[0], ff[1], ff[2]), chord_span, t, dt, row);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_gather_wake(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz, cudaStream_t st) {
+  if (wl.node_rows < 2) return ok();
+  gather_wake_kernel<<<grid_for((long long)wl.num * (wl.node_rows - 1) * (wl.C + 1)), 256, 0, st>>>(wl, pos, tx, ty,
+                                                                                                   tz);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_advect(AdvectMode mode, WakeLayout wl, double* x, double* pos2, double* k1, double* k2, double* k3,
+                    double* vprev, bool has_vprev, const double* vx, const double* vy, const double* vz,
+                    const double ff[3], double dt, int ignore_rows, cudaStream_t st) {
+  if (wl.node_rows < 1) return ok();
+  advect_kernel<<<grid_for((long long)wl.num * wl.node_rows * (wl.C + 1)), 256, 0, st>>>(
+      (int)mode, wl, x, pos2, k1, k2, k3, vprev, has_vprev ? 1 : 0, vx, vy, vz, mk(ff[0], ff[1], ff[2]), dt,
+      ignore_rows);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_move_rows(double* buf, int num, int PR, int row_elems, int from, int to, int rows, double* tmp,
+                       cudaStream_t st) {
+  if (rows <= 0 || from == to) return ok();
+  const long long total = (long long)num * rows * row_elems;
+  copy_rows_kernel<<<grid_for(total), 256, 0, st>>>(buf, tmp, num, PR, row_elems, from, 0, rows);
+  UVLM_LAUNCH_CHECK();
+  copy_rows_kernel<<<grid_for(total), 256, 0, st>>>(tmp, buf, num, PR, row_elems, 0, to, rows);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_extrapolate(double* x, const double* a, const double* b, int n, cudaStream_t st) {
+  extrapolate_kernel<<<grid_for(n), 256, 0, st>>>(x, a, b, n);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error launch_check_finite(const double* x, long long n, int* flag, cudaStream_t st) {
+  check_finite_kernel<<<grid_for(n), 256, 0, st>>>(x, n, flag);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+}  // namespace uvlm

@@ -1,0 +1,72 @@
+"""Legacy AoS vortex-ring API (src/shed.h:14-46, src/linear.h:104-119).
+
+Rings are arrays of shape (n, 4, 3): VortexRing::nodes() of each ring.  The
+segments of a ring run nodes[k+1] -> nodes[k] (ForEachSegment,
+src/vortex.h:132-140).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._capi import check, lib
+
+_P = C.POINTER(C.c_double)
+
+
+def _p(a):
+    return None if a is None or a.size == 0 else a.ctypes.data_as(_P)
+
+
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def InducedVelocity(pos, rings, gammas, chordwise: bool = False) -> np.ndarray:  # noqa: N802
+    """UVLM::InducedVelocity / ChordwiseInducedVelocity (src/shed.inl:22-33, 66-77)."""
+    r = _f64(rings).reshape(-1, 4, 3)
+    g = _f64(gammas).reshape(-1)
+    x = _f64(pos)
+    single = x.ndim == 1
+    x = x.reshape(-1, 3)
+    out = np.zeros_like(x)
+    check(lib().uvlm_rings_induced_velocity(_p(r), _p(g), r.shape[0], _p(x), x.shape[0], int(chordwise), _p(out)))
+    return out[0] if single else out
+
+
+def AdvectParallel(vortex_rings, vortex_gammas, wake_rings, freestream, dt) -> np.ndarray:  # noqa: N802
+    """UVLM::AdvectParallel (src/shed.inl:52-64); returns the moved wake rings."""
+    v = _f64(vortex_rings).reshape(-1, 4, 3)
+    g = _f64(vortex_gammas).reshape(-1)
+    w = _f64(wake_rings).reshape(-1, 4, 3).copy()
+    check(lib().uvlm_rings_advect(_p(v), _p(g), v.shape[0], _p(w), w.shape[0], _p(_f64(freestream)), float(dt)))
+    return w
+
+
+Advect = AdvectParallel
+
+
+def ConnectTrailingEdge(edge_rings, wake_rings) -> np.ndarray:  # noqa: N802
+    """UVLM::ConnectTrailingEdge (src/shed.inl:79-86)."""
+    e = _f64(edge_rings).reshape(-1, 4, 3)
+    w = _f64(wake_rings).reshape(-1, 4, 3).copy()
+    check(lib().uvlm_rings_connect_trailing_edge(_p(e), e.shape[0], _p(w)))
+    return w
+
+
+def SolveLinearProblem(bound_rings, wake_rings, wake_gammas, freestream, morphing, t,  # noqa: N802
+                       drop_wake_term: bool = True, bound_rings0=None) -> np.ndarray:
+    """UVLM::SolveLinearProblem (src/linear.inl:113-130).
+
+    drop_wake_term=True reproduces the reference, whose wake RHS term is a
+    discarded statement (src/linear.inl:123-124)."""
+    b = _f64(bound_rings).reshape(-1, 4, 3)
+    b0 = None if bound_rings0 is None else _f64(bound_rings0).reshape(-1, 4, 3)
+    w = _f64(wake_rings).reshape(-1, 4, 3)
+    wg = _f64(wake_gammas).reshape(-1)
+    out = np.zeros(b.shape[0])
+    check(lib().uvlm_rings_solve_linear_problem(_p(b), _p(b0), b.shape[0], _p(w), _p(wg), w.shape[0],
+                                                _p(_f64(freestream)), C.byref(morphing.k), float(t),
+                                                int(drop_wake_term), _p(out)))
+    return out
