@@ -101,7 +101,7 @@ class Clocks:
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[2 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
@@ -126,29 +126,47 @@ def oracle_sample(state, stride, lu_n, threads):
     return float(np.sum(sec)), sec
 
 
-def synthetic_state():
-    """Wake of the metric's shape from pure convection of the shed trailing edge
-    (no roll-up), for runs that cannot advance the GPU solver."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as o
+def synthetic_state_np():
+    """The metric's shapes without the solver or the oracle: the whole-wing
+    lattice moved by the heave/pitch kinematics, its trailing edge convected at
+    U (no roll-up) to form 400 wake rows, smooth circulations."""
+    xs = np.linspace(0, CHORD, ROWS + 1)
+    ys = np.concatenate([-np.linspace(0, SPAN / 2, COLS // 2 + 1)[::-1], np.linspace(0, SPAN / 2, COLS // 2 + 1)[1:]])
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
 
-    kin = o.kinematics(plug_amp=0.2, plug_omega=OMEGA, twist_amp=math.radians(10), twist_omega=OMEGA,
-                       twist_phase=math.pi / 2)
-    half = o.rect_generate(CHORD, SPAN / 2, ROWS, COLS // 2)
-    nodes = o.whole_wing(half, ROWS, COLS // 2).reshape(ROWS + 1, COLS + 1, 3)
+    def move(x, y, t):
+        th = math.radians(10) * math.sin(OMEGA * t + math.pi / 2)
+        z = 0.2 * math.sin(OMEGA * t)
+        return np.stack([math.cos(th) * x, y, -math.sin(th) * x + z], -1)
+
     t_now = WAKE_ROWS * DT
-    wing = np.array([o.perfome(kin, p, t_now) for p in nodes.reshape(-1, 3)]).reshape(1, ROWS + 1, COLS + 1, 3)
-    te0 = nodes[ROWS]
-    wake = np.zeros((1, WAKE_ROWS + 1, COLS + 1, 3))
-    for i in range(WAKE_ROWS + 1):
-        t = t_now - i * DT
-        wake[0, i] = np.array([o.perfome(kin, p, t) for p in te0]) + np.array([i * DT, 0, 0])
-    y = np.linspace(-1, 1, COLS)
-    g = np.sqrt(np.clip(1 - y ** 2, 0, None)) * 0.1
-    wing_gamma = np.tile(g, (ROWS, 1))[None] * np.linspace(1, 0.2, ROWS)[None, :, None]
+    wing = move(X, Y, t_now)[None]
+    wake = np.stack([move(np.full(COLS + 1, CHORD), ys, t_now - i * DT) + np.array([i * DT, 0, 0])
+                     for i in range(WAKE_ROWS + 1)])[None]
+    g = np.sqrt(np.clip(1 - np.linspace(-1, 1, COLS) ** 2, 0, None)) * 0.1
+    wing_gamma = (np.tile(g, (ROWS, 1)) * np.linspace(1, 0.2, ROWS)[:, None])[None]
     wake_gamma = np.stack([g * 0.1 * math.sin(OMEGA * (t_now - i * DT)) for i in range(WAKE_ROWS)])[None]
     return dict(wing_pos=wing, wake_pos=wake, wing_gamma=wing_gamma, wing_gamma_prev=wing_gamma * 0.99,
                 wake_gamma=wake_gamma)
+
+
+def run_profile(args):
+    """Mixed form only, from a synthesized full-size state: the small,
+    quick workload used for ncu captures of the per-step kernels."""
+    import uvlm_b200 as U
+
+    sim = make_sim("mixed", solver="gmres_stale", warm_start="extrapolate")
+    sim.begin()
+    sim.step(0, DT)
+    st = synthetic_state_np()
+    sim.set_state(WAKE_ROWS, st["wing_pos"], st["wake_pos"], st["wing_gamma"], st["wing_gamma_prev"],
+                  st["wake_gamma"])
+    for i in range(args.warmup + args.steps):
+        sim.step(WAKE_ROWS + 1 + i, DT)
+    sim.synchronize()
+    print(json.dumps({"profile": "ok", "steps": args.steps, "warmup": args.warmup,
+                      "launches": int(U.lib().uvlm_kernel_launch_count())}), flush=True)
+    sim.close()
 
 
 def cpu_threads():
@@ -159,7 +177,7 @@ def run_reference(args, rank, world):
     threads = cpu_threads()
     if rank != 0:
         return
-    state = synthetic_state()
+    state = synthetic_state_np()
     stride, lu_n = 1024, 512
     for _ in range(args.warmup):
         oracle_sample(state, stride, lu_n, threads)
@@ -330,6 +348,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="mixed form on a synthesized state, for ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -337,6 +356,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile:
+        run_profile(args)
         return
     if world > 1:
         import datetime
