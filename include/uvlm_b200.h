@@ -187,6 +187,21 @@ int uvlm_get_last_work(const uvlm_ctx* ctx, double* nbody_pairs, double* assembl
 int uvlm_sheet_induced_velocity(const double* pos, const double* gamma, int64_t num, int64_t grows, int64_t gcols,
                                 const double* targets, int64_t n_targets, double* out, int32_t precision);
 
+/* No counterpart in the reference.  The same velocities as
+ * uvlm_sheet_induced_velocity for callers that cannot allocate device memory
+ * (inside a stream capture, in loops where cudaMalloc/cudaFree would
+ * synchronise the device, or under a host framework that owns the device
+ * memory budget).  pos, gamma, targets and out are DEVICE pointers owned by the
+ * caller; nothing is allocated.  All scratch lives in one 32 MiB device array
+ * inside the library (held by every GPU that loads it until exit); a request
+ * that needs more returns UVLM_ERR_CAPACITY.  The first call on a device looks
+ * up that array's address, so make it before any stream capture.  Work is
+ * queued on `stream` (a cudaStream_t, NULL = legacy default stream) and is not
+ * synchronised.  Calls share the array: calls that overlap on the GPU race. */
+int uvlm_sheet_induced_velocity_noalloc(const double* pos, const double* gamma, int64_t num, int64_t grows,
+                                        int64_t gcols, const double* targets, int64_t n_targets, double* out,
+                                        int32_t precision, void* stream);
+
 /* advect::Advection strategy object (src/advect.h:48-59) from
  * AdvectFactory(name) (src/advect_factory.cpp:43-60): "euler", "RK2",
  * "RK4", "AB2".  AB2 keeps its velocity history between calls. */

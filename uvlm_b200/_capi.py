@@ -93,6 +93,7 @@ SIGNATURES = [
     ("uvlm_kernel_launch_count", C.c_int64, []),
     ("uvlm_measure_fp32_peak", C.c_int, [C.c_int32, _P]),
     ("uvlm_sheet_induced_velocity", C.c_int, [_P, _P, _I, _I, _I, _P, _I, _P, C.c_int32]),
+    ("uvlm_sheet_induced_velocity_noalloc", C.c_int, [_P, _P, _I, _I, _I, _P, _I, _P, C.c_int32, _V]),
     ("uvlm_advection_create", C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_V)]),
     ("uvlm_advection_destroy", C.c_int, [_V]),
     ("uvlm_advection_advect", C.c_int, [_V, _P, _P, _P, _I, _I, _I, _P, _P, _I, _P, C.c_double]),

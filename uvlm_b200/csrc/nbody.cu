@@ -301,6 +301,7 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   long long splits = (want + tiles - 1) / tiles;
   if (splits > n_strips) splits = n_strips;
   if (splits > 64) splits = 64;
+  if (work->max_splits > 0 && splits > work->max_splits) splits = work->max_splits;
   if (splits < 1) splits = 1;
   const long long sps = (n_strips + splits - 1) / splits;
   splits = (n_strips + sps - 1) / sps;

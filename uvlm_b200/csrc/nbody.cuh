@@ -75,6 +75,7 @@ struct NBodyWork {
   long long records_cap = 0;
   double* partial = nullptr;  // [splits][3][targets]
   long long partial_cap = 0;  // doubles
+  long long max_splits = 0;   // > 0: at most this many source splits (bounded scratch)
 };
 
 int nbody_num_variants();
