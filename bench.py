@@ -323,6 +323,7 @@ def run_ours(args, rank, world, local_rank):
             "plain_fp64_steps_per_s": plain, "speedup_vs_plain_fp64": value / world / plain,
             "cl_rel_err": cl_err, "cd_rel_err": cd_err, "cl_err_reference": "plain FP64 GPU form, same 400 steps",
             "gmres_iters_last": int(st.gmres_iters), "solve_path_last": int(st.solve_path),
+            "nbody_variant": U.lib().uvlm_nbody_variant_name(int(st.nbody_variant)).decode(),
             "stage_ms": {"kin_shed": stage_ms[0], "assembly": stage_ms[1], "rhs": stage_ms[2], "solve": stage_ms[3],
                          "loads": stage_ms[4], "advect": stage_ms[5], "total": stage_ms[7]},
             "roofline": {"bound": "fp32_simt", "kernel": "nbody_kernel (RK2 advection stage)",

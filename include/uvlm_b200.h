@@ -124,6 +124,8 @@ typedef struct {
   int32_t refactored;   /* a factorisation ran in this step */
   int32_t wake_rows;    /* ring rows of the wake after the step */
   double stage_ms[8];   /* kinematics+shed, assembly, rhs, solve, loads, advect, warm start, total */
+  int32_t nbody_variant; /* N-body tile variant in use (see uvlm_nbody_variant_name) */
+  int32_t pad_;
 } uvlm_step_stats;
 
 /* ------------------------------------------------------- time-stepper */
@@ -176,6 +178,8 @@ int64_t uvlm_kernel_launch_count(void);
 /* Measured FP32 FMA throughput of the device (TFLOP/s): the denominator of
  * the N-body roofline.  No counterpart in the reference (measurement aid). */
 int uvlm_measure_fp32_peak(int32_t device, double* tflops);
+/* Name of an N-body tile variant (e.g. "fp32_h4_t2_b128"), "?" if out of range. */
+const char* uvlm_nbody_variant_name(int32_t variant);
 /* Algorithmic work of the last step: unique-segment interactions of every
  * N-body stage and the assembly (target x segment pairs). */
 int uvlm_get_last_work(const uvlm_ctx* ctx, double* nbody_pairs, double* assembly_pairs, double* lu_flops);

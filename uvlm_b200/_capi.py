@@ -59,7 +59,7 @@ class StepStats(C.Structure):
     _fields_ = [
         ("step", C.c_int64), ("t", C.c_double), ("solve_path", C.c_int32), ("gmres_iters", C.c_int32),
         ("residual", C.c_double), ("refactored", C.c_int32), ("wake_rows", C.c_int32),
-        ("stage_ms", C.c_double * 8),
+        ("stage_ms", C.c_double * 8), ("nbody_variant", C.c_int32), ("pad_", C.c_int32),
     ]
 
 
@@ -92,6 +92,7 @@ SIGNATURES = [
     ("uvlm_get_last_work", C.c_int, [_V, _P, _P, _P]),
     ("uvlm_kernel_launch_count", C.c_int64, []),
     ("uvlm_measure_fp32_peak", C.c_int, [C.c_int32, _P]),
+    ("uvlm_nbody_variant_name", C.c_char_p, [C.c_int32]),
     ("uvlm_sheet_induced_velocity", C.c_int, [_P, _P, _I, _I, _I, _P, _I, _P, C.c_int32]),
     ("uvlm_sheet_induced_velocity_noalloc", C.c_int, [_P, _P, _I, _I, _I, _P, _I, _P, C.c_int32, _V]),
     ("uvlm_advection_create", C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_V)]),

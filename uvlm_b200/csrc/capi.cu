@@ -132,6 +132,7 @@ struct uvlm_ctx {
   GmresWork gm;
   bool have_factors = false;
   int variant_fp64 = 0, variant_fp32 = 3;
+  bool tuned = false;  // N-body tile variant chosen (autotune or config)
   uvlm_step_stats last{};
   double work_nbody = 0, work_asm = 0, work_lu = 0;
   cudaEvent_t ev[8] = {};
@@ -246,7 +247,36 @@ Error uvlm_ctx::build_sources(bool with_bound, const double* wake_pos_buf, Sourc
 }
 
 Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt) {
-  work_nbody += (double)nt * (double)nbody_unique_segments(blocks, nblocks);
+  const double pairs = (double)nt * (double)nbody_unique_segments(blocks, nblocks);
+  work_nbody += pairs;
+  if (!tuned && nblocks > 0 && pairs >= 2e9) {
+    // Tile autotune on the first large evaluation: time every compiled variant
+    // of this precision on the real sources and targets, keep the fastest
+    // (the default unless another is more than 3% faster).
+    const NBodyPrec prec = mixed() ? kNBodyFP32 : kNBodyFP64;
+    int& chosen = mixed() ? variant_fp32 : variant_fp64;
+    float best_ms = 1e30f;
+    int best = chosen;
+    for (int v = 0; v < nbody_num_variants(); ++v) {
+      if (nbody_variant_prec(v) != prec) continue;
+      float ms = 0;
+      for (int rep = 0; rep < 2; ++rep) {
+        UVLM_CUDA_TRY(cudaEventRecord(ev[0], st));
+        UVLM_TRY(nbody_eval(blocks, nblocks, prec, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb, v, num_sms, st));
+        UVLM_CUDA_TRY(cudaEventRecord(ev[1], st));
+        UVLM_CUDA_TRY(cudaEventSynchronize(ev[1]));
+        UVLM_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      }
+      const bool is_default = v == chosen;
+      const float score = is_default ? ms / 1.03f : ms;
+      if (score < best_ms) {
+        best_ms = score;
+        best = v;
+      }
+    }
+    chosen = best;
+    tuned = true;
+  }
   if (nblocks == 0) {
     UVLM_CUDA_TRY(cudaMemsetAsync(d_vx, 0, sizeof(double) * nt, st));
     UVLM_CUDA_TRY(cudaMemsetAsync(d_vy, 0, sizeof(double) * nt, st));
@@ -445,6 +475,7 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   last.step = step;
   last.t = t;
   last.wake_rows = wake_rings();
+  last.nbody_variant = mixed() ? variant_fp32 : variant_fp64;
   if (timing) {
     float ms[8] = {0};
     const int map[7][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {0, 7}};
@@ -536,6 +567,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
   if (k.nbody_variant >= 0) {
+    c->tuned = true;
     if (k.nbody_variant >= nbody_num_variants()) {
       uvlm_destroy(c);
       return set_global(fail(kErrInvalid, "nbody_variant out of range"));
@@ -747,6 +779,8 @@ int uvlm_synchronize(uvlm_ctx* c) {
 void* uvlm_stream(uvlm_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 int64_t uvlm_kernel_launch_count(void) { return g_launches.load(); }
+
+const char* uvlm_nbody_variant_name(int32_t v) { return nbody_variant_name(v); }
 
 int uvlm_measure_fp32_peak(int32_t device, double* tflops) {
   if (!tflops) return set_global(fail(kErrInvalid, "NULL argument"));

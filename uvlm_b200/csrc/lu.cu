@@ -320,73 +320,103 @@ __global__ void ipiv_to_perm_kernel(const int* ipiv, int n, int* perm) {
   for (int k = 0; k < n; ++k) perm[k] = sp[k];
 }
 
-__device__ bool wait_flag(const unsigned* flag, unsigned epoch, int* err) {
-  __shared__ int s_ok;
+constexpr int kTriBatch = 8;  // block rows a CTA can consume in one pass
+
+// Thread 0 waits (bounded) until the block row of solve-order position
+// `first` is published, then counts how many of the following positions are
+// published too (up to kTriBatch).  Returns that count, or 0 on abort.
+__device__ int wait_ready(const unsigned* flags, int first, int left, bool lower, int nblk, unsigned epoch,
+                          int* err) {
+  __shared__ int s_cnt;
   if (threadIdx.x == 0) {
+    const volatile unsigned* vf = flags;
+    const int b0 = lower ? first : nblk - 1 - first;
     const long long t0 = clock64();
-    int okv = 1;
-    while (((volatile const unsigned*)flag)[0] != epoch) {
-      if (((volatile int*)err)[0]) { okv = 0; break; }
-      if (clock64() - t0 > kSpinLimitCycles) { atomicExch(err + 2, 1); atomicExch(err, 1); okv = 0; break; }
+    int cnt = 1;
+    while (vf[b0] != epoch) {
+      if (((volatile int*)err)[0]) { cnt = 0; break; }
+      if (clock64() - t0 > kSpinLimitCycles) { atomicExch(err + 2, 1); atomicExch(err, 1); cnt = 0; break; }
       __nanosleep(32);
     }
+    if (cnt) {
+      while (cnt < left && cnt < kTriBatch) {
+        const int b = lower ? first + cnt : nblk - 1 - (first + cnt);
+        if (vf[b] != epoch) break;
+        ++cnt;
+      }
+    }
     __threadfence();
-    s_ok = okv;
+    s_cnt = cnt;
   }
   __syncthreads();
-  return s_ok != 0;
+  return s_cnt;
 }
 
 // Sync-free blocked triangular solve.  lower: y = L^-1 (P v); upper: z = U^-1 y.
-// CTA I owns block row I; for the lower solve it applies the block rows
-// J < I in order as their flags appear, for the upper solve J > I.
+// CTA I owns block row I.  It consumes the block rows it depends on (J < I for
+// the lower solve, J > I for the upper one) in solve order, taking in one pass
+// every consecutive block row already published, so that once its last
+// dependency appears only one 64x64 GEMV and the diagonal-inverse product
+// remain on the critical path.  Each GEMV runs 4 threads per row with 16
+// independent loads each.
 template <class T, class V, bool kLower>
 __global__ void __launch_bounds__(256) trsv_kernel(const T* __restrict__ LU, int n, const int* __restrict__ perm,
                                                    const double* __restrict__ vin, const V* yin, V* yout,
                                                    const T* __restrict__ dinv, unsigned* flags, unsigned epoch,
                                                    int* err, double* dout) {
   __shared__ V acc[kTriB];
-  __shared__ V xs[kTriB];
+  __shared__ V xs[kTriBatch * kTriB];
   const int nblk = gridDim.x;
   const int I = kLower ? blockIdx.x : nblk - 1 - blockIdx.x;
   const int r0 = I * kTriB;
   const int nb = min(kTriB, n - r0);
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x;
+  const int row = tid >> 2, quarter = tid & 3;
   if (tid < kTriB) {
     V v = 0;
     if (tid < nb) v = kLower ? (V)vin[perm[r0 + tid]] : yin[r0 + tid];
     acc[tid] = v;
   }
   __syncthreads();
-  for (int step = 0; step < nblk - 1 - (kLower ? nblk - 1 - I : I); ++step) {
-    const int J = kLower ? step : nblk - 1 - step;
-    if (!wait_flag(flags + J, epoch, err)) return;
-    const int c0 = J * kTriB;
-    const int nbj = min(kTriB, n - c0);
-    if (tid < kTriB) xs[tid] = (tid < nbj) ? ((volatile V*)yout)[c0 + tid] : (V)0;
-    __syncthreads();
-    // 8 warps x 8 rows each; lanes split the 64 columns
-    for (int rr = 0; rr < 8; ++rr) {
-      const int r = wid * 8 + rr;
-      V s = 0;
-      if (r < nb) {
-        const T* row = LU + (long long)(r0 + r) * n + c0;
-        for (int c = lane; c < nbj; c += 32) s += (V)row[c] * xs[c];
-      }
-      for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-      if (lane == 0 && r < nb) acc[r] -= s;
+  const int deps = kLower ? I : nblk - 1 - I;
+  int done = 0;
+  while (done < deps) {
+    const int cnt = wait_ready(flags, done, deps - done, kLower, nblk, epoch, err);
+    if (cnt == 0) return;
+    for (int q = tid; q < cnt * kTriB; q += blockDim.x) {
+      const int b = q / kTriB, c = q % kTriB;
+      const int J = kLower ? done + b : nblk - 1 - (done + b);
+      const int col = J * kTriB + c;
+      xs[q] = (col < n) ? ((volatile V*)yout)[col] : (V)0;
     }
     __syncthreads();
-  }
-  // x_I = dinv_I * acc
-  const T* D = dinv + (long long)I * kTriB * kTriB;
-  for (int rr = 0; rr < 8; ++rr) {
-    const int r = wid * 8 + rr;
     V s = 0;
-    for (int c = lane; c < kTriB; c += 32) s += (V)D[r * kTriB + c] * acc[c];
-    for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-    if (lane == 0) xs[r] = s;
+    if (row < nb) {
+      const T* rp = LU + (long long)(r0 + row) * n;
+      for (int b = 0; b < cnt; ++b) {
+        const int J = kLower ? done + b : nblk - 1 - (done + b);
+        const int c0 = J * kTriB + quarter * 16;
+        T a[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) a[c] = (c0 + c < n) ? rp[c0 + c] : (T)0;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) s += (V)a[c] * xs[b * kTriB + quarter * 16 + c];
+      }
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (quarter == 0 && row < nb) acc[row] -= s;
+    __syncthreads();
+    done += cnt;
   }
+  // x_I = dinv_I * acc (4 threads per row)
+  const T* D = dinv + (long long)I * kTriB * kTriB + (long long)row * kTriB + quarter * 16;
+  V s = 0;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) s += (V)D[c] * acc[quarter * 16 + c];
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  if (quarter == 0) xs[row] = s;
   __syncthreads();
   if (tid < nb) {
     yout[r0 + tid] = xs[tid];

@@ -1,6 +1,5 @@
 // nbody.cu -- strip-tiled Biot-Savart N-body (FP32 hi/lo and FP64 forms).
 #include "nbody.cuh"
-#include "bs_math.cuh"
 
 namespace uvlm {
 namespace {
@@ -28,15 +27,24 @@ __global__ void build_records_kernel(SheetView v, Rec* out) {
     // strengths: spanwise S(i,j) and chordwise H(i,j) (nbody.cuh)
     const double gS = (j < v.cols) ? ring_gamma(v, n, i, j) - ring_gamma(v, n, i - 1, j) : 0.0;
     const double gH = (i < R && !v.spanwise_only) ? ring_gamma(v, n, i, j - 1) - ring_gamma(v, n, i, j) : 0.0;
+    // segment vectors s0 = p(i,j+1) - p(i,j), h0 = p(i+1,j) - p(i,j)
+    double s0[3] = {0, 0, 0}, h0[3] = {0, 0, 0};
+    if (j < v.cols)
+      for (int d = 0; d < 3; ++d) s0[d] = p[3 + d] - p[d];
+    if (i < R)
+      for (int d = 0; d < 3; ++d) h0[d] = p[3 * C1 + d] - p[d];
     Rec r;
     if constexpr (sizeof(Rec) == sizeof(RecF)) {
       const float hx = (float)p[0], hy = (float)p[1], hz = (float)p[2];
       r.hi = make_float4(hx, hy, hz, (float)(gS * s));
       r.lo = make_float4((float)(p[0] - (double)hx), (float)(p[1] - (double)hy),
                          (float)(p[2] - (double)hz), (float)(gH * s));
+      r.sv = make_float4((float)s0[0], (float)s0[1], (float)s0[2], (float)h0[0]);
+      r.hv = make_float4((float)h0[1], (float)h0[2], 0.f, 0.f);
     } else {
       r.a = make_double4(p[0], p[1], p[2], gS * s);
-      r.b = make_double2(gH * s, 0.0);
+      r.b = make_double4(gH * s, s0[0], s0[1], s0[2]);
+      r.c = make_double4(h0[0], h0[1], h0[2], 0.0);
     }
     out[k] = r;
   }
@@ -105,45 +113,110 @@ struct Tgt {
   T lx, ly, lz;  // FP32: lo part; FP64: unused
 };
 
-template <class T, class Rec>
-__device__ __forceinline__ Node<T> node_from(const Rec& r, const Tgt<T>& t) {
-  if constexpr (sizeof(T) == 4) {
-    const float x = (t.hx - r.hi.x) + (t.lx - r.lo.x);
-    const float y = (t.hy - r.hi.y) + (t.ly - r.lo.y);
-    const float z = (t.hz - r.hi.z) + (t.lz - r.lo.z);
-    return make_node<float>(x, y, z);
-  } else {
-    return make_node<double>(t.hx - r.a.x, t.hy - r.a.y, t.hz - r.a.z);
-  }
+template <class T>
+struct NodeV {
+  T rx, ry, rz;  // x - p
+  T ux, uy, uz;  // (x - p)/|x - p|  (NaN/inf lanes when x == p are cut by |d|^2)
+};
+
+__device__ __forceinline__ float nb_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
+__device__ __forceinline__ float nb_rcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 template <class T, class Rec>
-__device__ __forceinline__ void strengths(const Rec& r, T& gS, T& gH) {
+__device__ __forceinline__ NodeV<T> node_from(const Rec& r, const Tgt<T>& t) {
+  NodeV<T> n;
+  if constexpr (sizeof(T) == 4) {
+    n.rx = (t.hx - r.hi.x) + (t.lx - r.lo.x);
+    n.ry = (t.hy - r.hi.y) + (t.ly - r.lo.y);
+    n.rz = (t.hz - r.hi.z) + (t.lz - r.lo.z);
+    const float inv = nb_rsqrt(n.rx * n.rx + n.ry * n.ry + n.rz * n.rz);
+    n.ux = n.rx * inv;
+    n.uy = n.ry * inv;
+    n.uz = n.rz * inv;
+  } else {
+    n.rx = t.hx - r.a.x;
+    n.ry = t.hy - r.a.y;
+    n.rz = t.hz - r.a.z;
+    const double inv = rsqrt(n.rx * n.rx + n.ry * n.ry + n.rz * n.rz);
+    n.ux = n.rx * inv;
+    n.uy = n.ry * inv;
+    n.uz = n.rz * inv;
+  }
+  return n;
+}
+
+template <class T>
+struct SegV {
+  T x, y, z;
+};
+
+template <class T, class Rec>
+__device__ __forceinline__ void rec_fields(const Rec& r, T& gS, T& gH, SegV<T>& s0, SegV<T>& h0) {
   if constexpr (sizeof(T) == 4) {
     gS = r.hi.w;
     gH = r.lo.w;
+    s0 = SegV<T>{r.sv.x, r.sv.y, r.sv.z};
+    h0 = SegV<T>{r.sv.w, r.hv.x, r.hv.y};
   } else {
     gS = r.a.w;
     gH = r.b.x;
+    s0 = SegV<T>{r.b.y, r.b.z, r.b.w};
+    h0 = SegV<T>{r.c.x, r.c.y, r.c.z};
   }
 }
 
-// Walk one staged strip for TPT targets.
+// Segment start=A -> end=B at x (src/vortex.cpp:24-38): r0 = B - A, r1 = x - A,
+// d = r0 x r1 (= r1 x r2), K = g r0.(u1 - u2) / |d|^2, cut when |d|^2 < 1e-10.
+// |x - A| < 1e-10 or |x - B| < 1e-10 implies |d|^2 < 1e-10 for |x - p| < 1e5,
+// so the reference's node cut-off is contained in the |d|^2 test (and the
+// select also discards the NaN that rsqrt(0) produces in u).
+template <class T>
+__device__ __forceinline__ void seg(const SegV<T>& r0, const NodeV<T>& a, const NodeV<T>& b, T g, T& vx, T& vy,
+                                    T& vz) {
+  const T dx = r0.y * a.rz - r0.z * a.ry;
+  const T dy = r0.z * a.rx - r0.x * a.rz;
+  const T dz = r0.x * a.ry - r0.y * a.rx;
+  const T d2 = dx * dx + dy * dy + dz * dz;
+  const T dot = r0.x * (a.ux - b.ux) + r0.y * (a.uy - b.uy) + r0.z * (a.uz - b.uz);
+  T k;
+  if constexpr (sizeof(T) == 4) {
+    k = g * dot * nb_rcp(d2);
+  } else {
+    k = g * dot * __drcp_rn(d2);
+  }
+  k = (d2 < (T)kCutD2) ? (T)0 : k;
+  vx += k * dx;
+  vy += k * dy;
+  vz += k * dz;
+}
+
+// Walk one staged strip for TPT targets: per node column, the H+1 node
+// quantities, then the H chordwise segments of the column and the H spanwise
+// segments that end in it.
 template <class T, class Rec, int H, int TPT>
 __device__ __forceinline__ void walk_strip(const Rec* sm, const StripInfo& si, const Tgt<T> (&tg)[TPT],
                                            T (&acc)[TPT][3]) {
-  Node<T> prev[TPT][H];
+  NodeV<T> prev[TPT][H];
+  SegV<T> ps0[H];
   T pgS[H];
-#pragma unroll
-  for (int r = 0; r < H; ++r) pgS[r] = (T)0;
   const int nr = si.nr, n_rows = si.n_rows, n_cols = si.n_cols;
   for (int j = 0; j < n_cols; ++j) {
-    Node<T> cur[TPT][H + 1];
+    NodeV<T> cur[TPT][H + 1];
     T gS[H], gH[H];
+    SegV<T> s0[H], h0[H];
 #pragma unroll
     for (int r = 0; r <= H; ++r) {
       if (r < nr) {
         const Rec rec = sm[r * n_cols + j];
-        if (r < H) strengths<T, Rec>(rec, gS[r], gH[r]);
+        if (r < H) rec_fields<T, Rec>(rec, gS[r], gH[r], s0[r], h0[r]);
 #pragma unroll
         for (int q = 0; q < TPT; ++q) cur[q][r] = node_from<T, Rec>(rec, tg[q]);
       }
@@ -153,7 +226,7 @@ __device__ __forceinline__ void walk_strip(const Rec* sm, const StripInfo& si, c
     for (int r = 0; r < H; ++r) {
       if (r < n_rows && r + 1 < nr && col_h) {
 #pragma unroll
-        for (int q = 0; q < TPT; ++q) segment<T>(cur[q][r], cur[q][r + 1], gH[r], acc[q][0], acc[q][1], acc[q][2]);
+        for (int q = 0; q < TPT; ++q) seg<T>(h0[r], cur[q][r], cur[q][r + 1], gH[r], acc[q][0], acc[q][1], acc[q][2]);
       }
     }
     if (j > 0) {
@@ -161,7 +234,7 @@ __device__ __forceinline__ void walk_strip(const Rec* sm, const StripInfo& si, c
       for (int r = 0; r < H; ++r) {
         if (r < n_rows) {
 #pragma unroll
-          for (int q = 0; q < TPT; ++q) segment<T>(prev[q][r], cur[q][r], pgS[r], acc[q][0], acc[q][1], acc[q][2]);
+          for (int q = 0; q < TPT; ++q) seg<T>(ps0[r], prev[q][r], cur[q][r], pgS[r], acc[q][0], acc[q][1], acc[q][2]);
         }
       }
     }
@@ -169,6 +242,7 @@ __device__ __forceinline__ void walk_strip(const Rec* sm, const StripInfo& si, c
     for (int r = 0; r < H; ++r) {
       if (r < n_rows) {
         pgS[r] = gS[r];
+        ps0[r] = s0[r];
 #pragma unroll
         for (int q = 0; q < TPT; ++q) prev[q][r] = cur[q][r];
       }
@@ -176,8 +250,8 @@ __device__ __forceinline__ void walk_strip(const Rec* sm, const StripInfo& si, c
   }
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
                                                        const double* __restrict__ tx, const double* __restrict__ ty,
                                                        const double* __restrict__ tz, long long n_targets,
                                                        const Rec* __restrict__ rec, double* __restrict__ partial) {
@@ -269,23 +343,31 @@ __global__ void reduce_partials_kernel(const double* __restrict__ partial, int s
 struct Variant {
   const char* name;
   int prec;  // NBodyPrec
-  int H, TPT, BLOCK;
+  int H, TPT, BLOCK, MINB;
 };
 
+// Tile shapes: H owned node rows per strip, TPT targets per thread, BLOCK
+// threads, MINB resident CTAs per SM requested from the register allocator.
 constexpr Variant kVariants[] = {
-    {"fp64_h4_t1_b128", kNBodyFP64, 4, 1, 128},
-    {"fp64_h2_t1_b256", kNBodyFP64, 2, 1, 256},
-    {"fp32_h4_t1_b256", kNBodyFP32, 4, 1, 256},
-    {"fp32_h4_t2_b128", kNBodyFP32, 4, 2, 128},
-    {"fp32_h2_t2_b128", kNBodyFP32, 2, 2, 128},
+    {"fp64_h4_t1_b128", kNBodyFP64, 4, 1, 128, 1},
+    {"fp64_h2_t1_b256", kNBodyFP64, 2, 1, 256, 1},
+    {"fp32_h4_t1_b256", kNBodyFP32, 4, 1, 256, 2},
+    {"fp32_h4_t2_b128", kNBodyFP32, 4, 2, 128, 3},
+    {"fp32_h2_t2_b128", kNBodyFP32, 2, 2, 128, 3},
+    {"fp32_h4_t1_b128_m4", kNBodyFP32, 4, 1, 128, 4},
+    {"fp32_h3_t2_b128_m4", kNBodyFP32, 3, 2, 128, 4},
+    {"fp32_h2_t1_b256_m3", kNBodyFP32, 2, 1, 256, 3},
+    {"fp64_h2_t2_b128", kNBodyFP64, 2, 2, 128, 1},
+    {"fp64_h2_t1_b128_m3", kNBodyFP64, 2, 1, 128, 3},
+    {"fp64_h2_t1_b256_m2", kNBodyFP64, 2, 1, 256, 2},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-template <class T, class Rec, int H, int TPT, int BLOCK>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
 Error launch_variant(const Blocks& B, long long n_strips, const double* tx, const double* ty, const double* tz,
                      long long n_targets, const Rec* rec, NBodyWork* work, double* vx, double* vy, double* vz,
                      int num_sms, cudaStream_t st) {
-  auto kern = nbody_kernel<T, Rec, H, TPT, BLOCK>;
+  auto kern = nbody_kernel<T, Rec, H, TPT, BLOCK, MINB>;
   const size_t smem = 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
   static bool attr_done = false;
   if (!attr_done) {
@@ -320,6 +402,7 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
 }  // namespace
 
 int nbody_num_variants() { return kNumVariants; }
+int nbody_variant_prec(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].prec : -1; }
 const char* nbody_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
 
 long long nbody_unique_segments(const SourceBlock* blocks, int n_blocks) {
@@ -386,14 +469,22 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
   }
   const RecF* rf = reinterpret_cast<const RecF*>(work->records);
   const RecD* rd = reinterpret_cast<const RecD*>(work->records);
+  const Blocks& B_ = B;
   switch (variant) {
-    case 0: return launch_variant<double, RecD, 4, 1, 128>(B, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
-    case 1: return launch_variant<double, RecD, 2, 1, 256>(B, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
-    case 2: return launch_variant<float, RecF, 4, 1, 256>(B, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
-    case 3: return launch_variant<float, RecF, 4, 2, 128>(B, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
-    case 4: return launch_variant<float, RecF, 2, 2, 128>(B, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 0: return launch_variant<double, RecD, 4, 1, 128, 1>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 1: return launch_variant<double, RecD, 2, 1, 256, 1>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 2: return launch_variant<float, RecF, 4, 1, 256, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 3: return launch_variant<float, RecF, 4, 2, 128, 3>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 4: return launch_variant<float, RecF, 2, 2, 128, 3>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 5: return launch_variant<float, RecF, 4, 1, 128, 4>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 6: return launch_variant<float, RecF, 3, 2, 128, 4>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 7: return launch_variant<float, RecF, 2, 1, 256, 3>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 8: return launch_variant<double, RecD, 2, 2, 128, 1>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 9: return launch_variant<double, RecD, 2, 1, 128, 3>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 10: return launch_variant<double, RecD, 2, 1, 256, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     default: return fail(kErrInvalid, "bad nbody variant");
   }
+
 }
 
 }  // namespace uvlm

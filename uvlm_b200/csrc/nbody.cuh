@@ -19,29 +19,36 @@
 // 1/|x - p|) are shared by the segments meeting at that node.
 //
 // Data layout in HBM: per evaluation a "record" array holds, for every node of
-// every source sheet, its position and the strengths of the spanwise segment
-// to its right and the chordwise segment below it (pre-scaled by 1/4pi):
-//   FP32 form: {float4(x_hi,y_hi,z_hi,gS), float4(x_lo,y_lo,z_lo,gH)} (32 B),
-//              x = x_hi + x_lo exactly enough that x - p keeps ~FP64 accuracy
-//              for near pairs (hi/lo split of the FP64 positions);
-//   FP64 form: {double4(x,y,z,gS), double2(gH,0)} (48 B).
-// Sources are walked in "strips" of H owned node rows x up to kStripCols
-// node columns, staged through shared memory by cp.async double buffering.
+// every source sheet, its position, the vectors s0 = p(i,j+1) - p(i,j) and
+// h0 = p(i+1,j) - p(i,j) of the spanwise segment to its right and the
+// chordwise segment below it (FP64 differences rounded once), and their
+// strengths (pre-scaled by 1/4pi):
+//   FP32 form (64 B): position as a hi/lo float pair (x = x_hi + x_lo), so that
+//              x - p keeps near-FP64 accuracy for near pairs;
+//   FP64 form (96 B).
+// With the segment vector r0 at hand the cross product is d = r0 x r1
+// (= r1 x r2 of src/vortex.cpp:24-28) without the cancellation of two long,
+// nearly parallel vectors.  Sources are walked in "strips" of H owned node
+// rows x up to kStripCols node columns, staged through shared memory by
+// cp.async double buffering.
 #pragma once
 
 #include "common.cuh"
 
 namespace uvlm {
 
-constexpr int kStripCols = 128;  // segments per strip row (nodes = +1)
+constexpr int kStripCols = 64;  // segments per strip row (nodes = +1)
 
 struct alignas(16) RecF {
   float4 hi;  // x_hi, y_hi, z_hi, gS/(4 pi)
   float4 lo;  // x_lo, y_lo, z_lo, gH/(4 pi)
+  float4 sv;  // s0.x, s0.y, s0.z, h0.x
+  float4 hv;  // h0.y, h0.z, 0, 0
 };
 struct alignas(16) RecD {
   double4 a;  // x, y, z, gS/(4 pi)
-  double2 b;  // gH/(4 pi), 0
+  double4 b;  // gH/(4 pi), s0.x, s0.y, s0.z
+  double4 c;  // h0.x, h0.y, h0.z, 0
 };
 
 // One contiguous block of sheets in the record array: num sheets of
@@ -79,6 +86,7 @@ struct NBodyWork {
 };
 
 int nbody_num_variants();
+int nbody_variant_prec(int v);
 const char* nbody_variant_name(int v);
 
 // Build the source records of `n_views` sheets into work.records (blocks are
