@@ -155,7 +155,10 @@ def run_profile(args):
     quick workload used for ncu captures of the per-step kernels."""
     import uvlm_b200 as U
 
-    sim = make_sim("mixed", solver="gmres_stale", warm_start="extrapolate")
+    if args.form == "mixed":
+        sim = make_sim("mixed", solver="gmres_stale", warm_start="extrapolate")
+    else:
+        sim = make_sim("fp64")
     sim.begin()
     sim.step(0, DT)
     st = synthetic_state_np()
@@ -237,6 +240,23 @@ def run_ours(args, rank, world, local_rank):
     cl64, clmx = np.array(cl64), np.array(clmx)
     cl_err = float(np.max(np.abs(clmx[:, 2] - cl64[:, 2])) / np.max(np.abs(cl64[:, 2])))
     cd_err = float(np.max(np.abs(clmx[:, 1] - cl64[:, 1])) / np.max(np.abs(cl64[:, 1])))
+    # rounding floor of the FP64 form itself: the same run with the forward
+    # flight perturbed by one ulp (the wake roll-up amplifies any rounding)
+    accuracy = {}
+    if not args.no_floor:
+        simf = make_sim("fp64", device=dev)
+        simf.set_forward_flight([-(1.0 + 2.0 ** -52), 0.0, 0.0])
+        simf.begin()
+        clf = np.array([simf.step(s, DT) for s in range(WAKE_ROWS + 1)])
+        simf.close()
+        accuracy["fp64_one_ulp_cl_rel_err"] = {}
+    accuracy["mixed_cl_rel_err"] = {}
+    scale = np.max(np.abs(cl64[:, 2]))
+    for end in (50, 100, 200, 300, WAKE_ROWS + 1):
+        accuracy["mixed_cl_rel_err"][f"steps_0_{end - 1}"] = float(np.max(np.abs(clmx[:end, 2] - cl64[:end, 2])) / scale)
+        if not args.no_floor:
+            accuracy["fp64_one_ulp_cl_rel_err"][f"steps_0_{end - 1}"] = float(
+                np.max(np.abs(clf[:end, 2] - cl64[:end, 2])) / scale)
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
     step0 = WAKE_ROWS + 1
@@ -322,6 +342,7 @@ def run_ours(args, rank, world, local_rank):
                                 "2*g_n-g_{n-1}"),
             "plain_fp64_steps_per_s": plain, "speedup_vs_plain_fp64": value / world / plain,
             "cl_rel_err": cl_err, "cd_rel_err": cd_err, "cl_err_reference": "plain FP64 GPU form, same 400 steps",
+            "accuracy": accuracy,
             "gmres_iters_last": int(st.gmres_iters), "solve_path_last": int(st.solve_path),
             "nbody_variant": U.lib().uvlm_nbody_variant_name(int(st.nbody_variant)).decode(),
             "stage_ms": {"kin_shed": stage_ms[0], "assembly": stage_ms[1], "rhs": stage_ms[2], "solve": stage_ms[3],
@@ -349,7 +370,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--profile", action="store_true", help="mixed form on a synthesized state, for ncu")
+    ap.add_argument("--no-floor", action="store_true", help="skip the one-ulp FP64 rounding-floor run")
+    ap.add_argument("--profile", action="store_true", help="one form on a synthesized state, for ncu")
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"], help="form run by --profile")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

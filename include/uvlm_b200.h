@@ -84,7 +84,9 @@ typedef struct {
   double gmres_tol;         /* relative residual ||b - A g|| / ||b|| */
   int32_t device;           /* CUDA device ordinal */
   int32_t compute_loads;    /* 1: Joukowski loads every step (CalcLoad) */
-  int32_t assembly_fp64;    /* mixed form: assemble the residual matrix in FP64 */
+  int32_t assembly_fp64;    /* mixed form: residual matrix assembled in FP64 each step
+                               (the FP32 kernel then assembles only the matrix that is
+                               factored); 0: FP32 assembly serves both */
   int32_t nbody_variant;    /* -1: autotune; else a tile variant index */
 } uvlm_config;
 
@@ -126,6 +128,7 @@ typedef struct {
   double stage_ms[8];   /* kinematics+shed, assembly, rhs, solve, loads, advect, warm start, total */
   int32_t nbody_variant; /* N-body tile variant in use (see uvlm_nbody_variant_name) */
   int32_t pad_;
+  double initial_residual; /* ||b - A g0|| / ||b|| of the GMRES initial guess */
 } uvlm_step_stats;
 
 /* ------------------------------------------------------- time-stepper */
@@ -237,6 +240,38 @@ int uvlm_rings_solve_linear_problem(const double* bound_rings, const double* bou
                                     const double* wake_rings, const double* wake_gamma, int64_t n_wake,
                                     const double freestream[3], const uvlm_kinematics* kin, double t,
                                     int32_t drop_wake_term, double* gamma_out);
+/* ---------------------------------------------- learned warm start (MLP) */
+/* No counterpart in the reference.  A per-panel MLP (8 features -> 3 x 256
+ * GELU -> 1, BF16 weights, FP32 accumulation) predicts the correction of the
+ * extrapolation 2*G_n - G_{n-1} of each panel's circulation from
+ * (G_n, G_n - G_{n-1}, b_{n+1}, b_{n+1} - b_n, sin/cos of the dominant
+ * kinematic phase, chordwise/spanwise position); the result seeds the GMRES
+ * solve when cfg.warm_start == UVLM_WARM_MLP. */
+typedef struct uvlm_mlp uvlm_mlp;
+int uvlm_mlp_create(uint64_t seed, uvlm_mlp** out);
+int uvlm_mlp_destroy(uvlm_mlp* mlp);
+int64_t uvlm_mlp_num_params(const uvlm_mlp* mlp);
+/* FP32 master parameters: per layer W [in][out] then b [out]. */
+int uvlm_mlp_get_params(const uvlm_mlp* mlp, float* params);
+int uvlm_mlp_set_params(uvlm_mlp* mlp, const float* params);
+/* x' = (x - mean) / stdev per feature; prediction = out_scale * network(x'). */
+int uvlm_mlp_set_normalization(uvlm_mlp* mlp, const float* mean, const float* stdev, float out_scale);
+/* Host arrays: x [n][8], y [n]. */
+int uvlm_mlp_forward(uvlm_mlp* mlp, const float* x, int64_t n, float* y);
+/* Mean-square loss on (prediction - target)/out_scale and its gradient with
+ * respect to every parameter (same layout as the parameters). */
+int uvlm_mlp_gradients(uvlm_mlp* mlp, const float* x, const float* target, int64_t n, float* grads, double* loss);
+/* Adam on shuffled minibatches; final_loss = mean loss of the last epoch. */
+int uvlm_mlp_train(uvlm_mlp* mlp, const float* x, const float* target, int64_t n, int32_t epochs, int32_t batch,
+                   double lr, uint64_t seed, double* final_loss);
+/* The context uses (borrows) this network for UVLM_WARM_MLP. */
+int uvlm_set_mlp(uvlm_ctx* ctx, uvlm_mlp* mlp);
+/* Record (features, target) pairs of every solve from step 2 on, up to
+ * max_samples panels (enable = 0 frees the buffer). */
+int uvlm_collect_training_data(uvlm_ctx* ctx, int32_t enable, int64_t max_samples);
+/* n = samples recorded; X [n][8] and T [n] (either may be NULL). */
+int uvlm_get_training_data(uvlm_ctx* ctx, float* X, float* T, int64_t* n);
+
 /* Dense solve A x = b, A row-major n x n (FullPivLU replacement).  method:
  * 0 FP64 LU; 1 TF32 LU + FP64-residual GMRES; 2 BF16 LU + GMRES.
  * iters (may be NULL) receives the GMRES iteration count. */

@@ -120,7 +120,7 @@ class SimpleSimulator:
     def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
                  lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
                  gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
-                 assembly_fp64: bool = False, nbody_variant: int = -1, compute_loads: bool = True):
+                 assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True):
         cfg = Config()
         lib().uvlm_config_default(C.byref(cfg))
         cfg.precision = PRECISION[precision]
@@ -135,7 +135,8 @@ class SimpleSimulator:
         cfg.gmres_max_iter = int(gmres_max_iter)
         cfg.gmres_restart = int(gmres_restart)
         cfg.device = int(device)
-        cfg.assembly_fp64 = int(bool(assembly_fp64))
+        # the mixed form forms its FP64 residual matrix in FP64 unless told otherwise
+        cfg.assembly_fp64 = int(precision == "mixed" if assembly_fp64 is None else bool(assembly_fp64))
         cfg.nbody_variant = int(nbody_variant)
         cfg.compute_loads = int(bool(compute_loads))
         self._cfg = cfg
@@ -171,9 +172,6 @@ class SimpleSimulator:
 
     def set_load_path(self, path: str) -> None:
         self._load_path = path or None
-
-    def set_erase_wake_after(self, step: int) -> None:
-        self._cfg.erase_wake_after = int(step)
 
     def Run(self, steps: int, dt: float) -> np.ndarray:  # noqa: N802
         """Run(steps, dt): steps+1 MainLoops; returns the load rows."""
@@ -227,6 +225,24 @@ class SimpleSimulator:
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         check(lib().uvlm_get_last_work(self._h, C.byref(a), C.byref(b), C.byref(c)), self._h)
         return a.value, b.value, c.value
+
+    def set_mlp(self, mlp) -> None:
+        """Network of the learned warm start (keep it alive while in use)."""
+        self._mlp = mlp
+        check(lib().uvlm_set_mlp(self._h, mlp.handle if mlp is not None else None), self._h)
+
+    def collect_training_data(self, enable: bool, max_samples: int = 0) -> None:
+        check(lib().uvlm_collect_training_data(self._h, int(bool(enable)), int(max_samples)), self._h)
+
+    def training_data(self):
+        n = C.c_int64()
+        check(lib().uvlm_get_training_data(self._h, None, None, C.byref(n)), self._h)
+        X = np.zeros((n.value, 8), np.float32)
+        T = np.zeros(n.value, np.float32)
+        FP = C.POINTER(C.c_float)
+        check(lib().uvlm_get_training_data(self._h, X.ctypes.data_as(FP), T.ctypes.data_as(FP), C.byref(n)),
+              self._h)
+        return X, T
 
     def set_stage_timing(self, enable: bool) -> None:
         check(lib().uvlm_set_stage_timing(self._h, int(bool(enable))), self._h)
@@ -333,3 +349,4 @@ def dense_solve(A, b, method: str = "fp64"):
 
 
 from . import rings  # noqa: E402  (legacy AoS API)
+from . import warmstart  # noqa: E402  (learned warm start)

@@ -60,6 +60,7 @@ class StepStats(C.Structure):
         ("step", C.c_int64), ("t", C.c_double), ("solve_path", C.c_int32), ("gmres_iters", C.c_int32),
         ("residual", C.c_double), ("refactored", C.c_int32), ("wake_rows", C.c_int32),
         ("stage_ms", C.c_double * 8), ("nbody_variant", C.c_int32), ("pad_", C.c_int32),
+        ("initial_residual", C.c_double),
     ]
 
 
@@ -103,6 +104,20 @@ SIGNATURES = [
     ("uvlm_rings_connect_trailing_edge", C.c_int, [_P, _I, _P]),
     ("uvlm_rings_solve_linear_problem", C.c_int, [_P, _P, _I, _P, _P, _I, _P, C.POINTER(Kinematics),
                                                   C.c_double, C.c_int32, _P]),
+    ("uvlm_mlp_create", C.c_int, [C.c_uint64, C.POINTER(_V)]),
+    ("uvlm_mlp_destroy", C.c_int, [_V]),
+    ("uvlm_mlp_num_params", C.c_int64, [_V]),
+    ("uvlm_mlp_get_params", C.c_int, [_V, C.POINTER(C.c_float)]),
+    ("uvlm_mlp_set_params", C.c_int, [_V, C.POINTER(C.c_float)]),
+    ("uvlm_mlp_set_normalization", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float]),
+    ("uvlm_mlp_forward", C.c_int, [_V, C.POINTER(C.c_float), _I, C.POINTER(C.c_float)]),
+    ("uvlm_mlp_gradients", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.POINTER(C.c_float),
+                                     _P]),
+    ("uvlm_mlp_train", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.c_int32, C.c_int32,
+                                 C.c_double, C.c_uint64, _P]),
+    ("uvlm_set_mlp", C.c_int, [_V, _V]),
+    ("uvlm_collect_training_data", C.c_int, [_V, C.c_int32, _I]),
+    ("uvlm_get_training_data", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(_I)]),
     ("uvlm_dense_solve", C.c_int, [_P, _I, _P, _P, C.c_int32, C.POINTER(C.c_int32)]),
 ]
 

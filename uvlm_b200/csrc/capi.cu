@@ -10,6 +10,7 @@
 
 #include "../../include/uvlm_b200.h"
 #include "gmres.cuh"
+#include "mlp.cuh"
 #include "lu.cuh"
 #include "nbody.cuh"
 #include "step.cuh"
@@ -91,6 +92,10 @@ int device_sms(int dev) {
 
 }  // namespace
 
+namespace uvlm {
+Mlp* mlp_of(uvlm_mlp* h);
+}
+
 struct uvlm_ctx {
   uvlm_config cfg{};
   std::vector<uvlm_wing_desc> wings;
@@ -133,6 +138,18 @@ struct uvlm_ctx {
   bool have_factors = false;
   int variant_fp64 = 0, variant_fp32 = 3;
   bool tuned = false;  // N-body tile variant chosen (autotune or config)
+  // learned warm start: network (borrowed), per-step features, collected data
+  uvlm_mlp* mlp = nullptr;
+  double* d_rhs_prev = nullptr;
+  double* d_phase = nullptr;
+  double* h_phase = nullptr;
+  float* d_feat = nullptr;
+  float* d_mlp_y = nullptr;
+  bool collect = false;
+  long long collect_cap = 0, collect_n = 0;
+  float* d_collect_x = nullptr;
+  float* d_collect_t = nullptr;
+  Error warm_features(double t);
   uvlm_step_stats last{};
   double work_nbody = 0, work_asm = 0, work_lu = 0;
   cudaEvent_t ev[8] = {};
@@ -154,6 +171,7 @@ struct uvlm_ctx {
   Error solve(long long step);
   Error advect(double dt);
   Error step(long long step, double dt, double* row);
+  double cur_dt = 0;
   void mark(int i) {
     if (timing) cudaEventRecord(ev[i], st);
   }
@@ -169,6 +187,14 @@ void uvlm_ctx::free_all() {
   }
   cudaFree(d_A32);
   cudaFree(d_F32);
+  cudaFree(d_rhs_prev);
+  cudaFree(d_phase);
+  cudaFree(d_feat);
+  cudaFree(d_mlp_y);
+  if (h_phase) cudaFreeHost(h_phase);
+  d_rhs_prev = d_phase = nullptr;
+  h_phase = nullptr;
+  d_feat = d_mlp_y = nullptr;
   cudaFree(d_kin);
   cudaFree(d_flags);
   cudaFree(nb.records);
@@ -207,6 +233,12 @@ Error uvlm_ctx::alloc_all() {
   UVLM_TRY(dalloc(&d_line_uls, 3 * (size_t)lines));
   for (double** p : {&d_tx, &d_ty, &d_tz, &d_vx, &d_vy, &d_vz}) UVLM_TRY(dalloc(p, (size_t)tcap));
   UVLM_TRY(dalloc(&d_row, (size_t)(1 + 2 * num)));
+  UVLM_TRY(dalloc(&d_rhs_prev, (size_t)N));
+  UVLM_TRY(dalloc(&d_phase, (size_t)num));
+  UVLM_TRY(dalloc(&d_feat, (size_t)N * kMlpIn));
+  UVLM_TRY(dalloc(&d_mlp_y, (size_t)N));
+  UVLM_CUDA_TRY(cudaMallocHost(&h_phase, sizeof(double) * num));
+  UVLM_CUDA_TRY(cudaMemset(d_rhs_prev, 0, sizeof(double) * N));
   UVLM_TRY(dalloc(&d_flags, 4));
   UVLM_CUDA_TRY(cudaMallocHost(&h_row, sizeof(double) * (1 + 2 * num)));
   UVLM_CUDA_TRY(cudaMallocHost(&h_flags, sizeof(int) * 8));
@@ -218,7 +250,7 @@ Error uvlm_ctx::alloc_all() {
   // dense matrices
   if (!mixed() || cfg.assembly_fp64) UVLM_TRY(dalloc(&d_A64, (size_t)N * N));
   if (mixed()) {
-    UVLM_CUDA_TRY(cudaMalloc(&d_A32, sizeof(float) * (size_t)N * N));
+    if (!cfg.assembly_fp64) UVLM_CUDA_TRY(cudaMalloc(&d_A32, sizeof(float) * (size_t)N * N));
     UVLM_CUDA_TRY(cudaMalloc(&d_F32, sizeof(float) * (size_t)N * N));
     UVLM_TRY(lu_work_alloc(&lu, N, 4, num_sms));
     UVLM_TRY(gmres_work_alloc(&gm, N, std::max(2, cfg.gmres_restart)));
@@ -318,7 +350,10 @@ Error uvlm_ctx::solve(long long step) {
   const LuUpdate upd = cfg.lu_precision == UVLM_LU_BF16 ? kLuUpdateBF16 : kLuUpdateTF32;
   const LuUpdate use = gemm_tc_available() ? upd : kLuUpdateSimt;
   auto factor = [&]() -> Error {
-    UVLM_CUDA_TRY(cudaMemcpyAsync(d_F32, d_A32, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToDevice, st));
+    if (cfg.assembly_fp64)
+      UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, true, d_F32, true, st));
+    else
+      UVLM_CUDA_TRY(cudaMemcpyAsync(d_F32, d_A32, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToDevice, st));
     UVLM_TRY(lu_factor_f32(d_F32, N, use, &lu, st));
     UVLM_TRY(lu_check(&lu, st));
     have_factors = true;
@@ -332,6 +367,12 @@ Error uvlm_ctx::solve(long long step) {
   // extrapolation 2 g_n - g_{n-1} uses the history kept in d_gamma_hist
   if (cfg.warm_start == UVLM_WARM_EXTRAPOLATE && step >= 2)
     UVLM_TRY(launch_extrapolate(d_gamma, d_gamma_prev, d_gamma_hist, N, st));
+  if (cfg.warm_start == UVLM_WARM_MLP && step >= 2) {
+    if (!mlp) return fail(kErrState, "warm_start MLP needs uvlm_set_mlp");
+    UVLM_TRY(warm_features(step * cur_dt));
+    UVLM_TRY(mlp_forward(mlp_of(mlp), d_feat, N, d_mlp_y, st));
+    UVLM_TRY(mlp_apply_guess(N, d_gamma_prev, d_gamma_hist, d_mlp_y, d_gamma, st));
+  }
   const float* A32 = cfg.assembly_fp64 ? nullptr : d_A32;
   const double* A64 = cfg.assembly_fp64 ? d_A64 : nullptr;
   GmresResult r;
@@ -350,6 +391,7 @@ Error uvlm_ctx::solve(long long step) {
   }
   last.gmres_iters = r.iters;
   last.residual = r.relres;
+  last.initial_residual = r.initial_relres;
   if (!r.converged) return fail(kErrNonFinite, "GMRES did not converge after a fresh factorisation");
   return ok();
 }
@@ -407,10 +449,32 @@ Error uvlm_ctx::advect(double dt) {
   return ok();
 }
 
+// Features of the learned warm start for the solve at time t: G_n (the
+// previous solution), G_{n-1}, the new and the previous RHS and the phase of
+// each wing's dominant motion (first non-zero angular frequency of plug,
+// flap, twist, bend).
+Error uvlm_ctx::warm_features(double t) {
+  for (int n = 0; n < num; ++n) {
+    const uvlm_kinematics& k = kins[n];
+    const double om[4] = {k.plug_omega, k.flap_omega, k.twist_omega, k.bend_omega};
+    double w = 0;
+    for (double o : om)
+      if (o != 0.0) {
+        w = o;
+        break;
+      }
+    h_phase[n] = w * t;
+  }
+  UVLM_CUDA_TRY(cudaMemcpyAsync(d_phase, h_phase, sizeof(double) * num, cudaMemcpyHostToDevice, st));
+  return mlp_features(num, R, C, d_gamma_prev, d_gamma_hist, d_rhs, d_rhs_prev, d_phase, d_feat, st);
+}
+
 Error uvlm_ctx::step(long long step, double dt, double* row) {
   if (!built) return fail(kErrState, "uvlm_begin has not been called");
   const double t = step * dt;
+  cur_dt = dt;
   work_nbody = work_asm = work_lu = 0;
+  last.initial_residual = 0;
   mark(0);
   UVLM_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, st));
   UVLM_CUDA_TRY(cudaMemcpyAsync(d_gamma_hist, d_gamma_prev, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
@@ -421,9 +485,14 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   UVLM_TRY(launch_panel_geometry(d_kin, ws(), d_pos, d_pos_init, t, d_cx, d_cy, d_cz, d_normal, d_area, d_uls, st));
   mark(1);
   // influence matrix (simple_simulator.cpp:76-101)
+  // Mixed form: the matrix of the FP64 residual is assembled every step, in
+  // FP64 (assembly_fp64) or by the FP32 kernel; the FP32 matrix that is
+  // factored is assembled by the FP32 kernel only when a factorisation runs.
   if (mixed()) {
-    UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, true, d_A32, true, st));
-    if (cfg.assembly_fp64) UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, false, d_A64, false, st));
+    if (cfg.assembly_fp64)
+      UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, false, d_A64, false, st));
+    else
+      UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, true, d_A32, true, st));
   } else {
     UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, false, d_A64, false, st));
   }
@@ -443,6 +512,16 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   mark(3);
   UVLM_TRY(solve(step));
   UVLM_TRY(launch_check_finite(d_gamma, N, d_flags, st));
+  if (collect && step >= 2 && collect_n + N <= collect_cap) {
+    // training pair of the learned warm start: features known before the
+    // solve, target = the solved circulation minus the extrapolation
+    UVLM_TRY(warm_features(t));
+    UVLM_CUDA_TRY(cudaMemcpyAsync(d_collect_x + collect_n * kMlpIn, d_feat, sizeof(float) * N * kMlpIn,
+                                  cudaMemcpyDeviceToDevice, st));
+    UVLM_TRY(mlp_targets(N, d_gamma, d_gamma_prev, d_gamma_hist, d_collect_t + collect_n, st));
+    collect_n += N;
+  }
+  UVLM_CUDA_TRY(cudaMemcpyAsync(d_rhs_prev, d_rhs, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
   mark(4);
   if (cfg.compute_loads) {
     const long long lines = (long long)num * R * (2 * C + 1);
@@ -585,6 +664,8 @@ int uvlm_destroy(uvlm_ctx* c) {
   if (!c) return UVLM_OK;
   if (c->st) cudaStreamSynchronize(c->st);
   c->free_all();
+  cudaFree(c->d_collect_x);
+  cudaFree(c->d_collect_t);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
@@ -781,6 +862,41 @@ void* uvlm_stream(uvlm_ctx* c) { return c ? (void*)c->st : nullptr; }
 int64_t uvlm_kernel_launch_count(void) { return g_launches.load(); }
 
 const char* uvlm_nbody_variant_name(int32_t v) { return nbody_variant_name(v); }
+
+int uvlm_set_mlp(uvlm_ctx* c, uvlm_mlp* m) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  c->mlp = m;
+  return UVLM_OK;
+}
+
+int uvlm_collect_training_data(uvlm_ctx* c, int32_t enable, int64_t max_samples) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  cudaFree(c->d_collect_x);
+  cudaFree(c->d_collect_t);
+  c->d_collect_x = nullptr;
+  c->d_collect_t = nullptr;
+  c->collect = false;
+  c->collect_n = c->collect_cap = 0;
+  if (!enable) return UVLM_OK;
+  if (max_samples < 1) return c->fail_with(fail(kErrInvalid, "max_samples must be positive"));
+  if (cudaMalloc(&c->d_collect_x, sizeof(float) * max_samples * kMlpIn) != cudaSuccess ||
+      cudaMalloc(&c->d_collect_t, sizeof(float) * max_samples) != cudaSuccess)
+    return c->fail_with(fail(kErrCuda, "cannot allocate the training-data buffer"));
+  c->collect = true;
+  c->collect_cap = max_samples;
+  return UVLM_OK;
+}
+
+int uvlm_get_training_data(uvlm_ctx* c, float* X, float* T, int64_t* n) {
+  if (!c || !n) return set_global(fail(kErrInvalid, "NULL argument"));
+  *n = c->collect_n;
+  if (c->collect_n == 0 || (!X && !T)) return UVLM_OK;
+  cudaStreamSynchronize(c->st);
+  if ((X && cudaMemcpy(X, c->d_collect_x, sizeof(float) * c->collect_n * kMlpIn, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (T && cudaMemcpy(T, c->d_collect_t, sizeof(float) * c->collect_n, cudaMemcpyDeviceToHost) != cudaSuccess))
+    return c->fail_with(fail(kErrCuda, "training-data copy failed"));
+  return UVLM_OK;
+}
 
 int uvlm_measure_fp32_peak(int32_t device, double* tflops) {
   if (!tflops) return set_global(fail(kErrInvalid, "NULL argument"));

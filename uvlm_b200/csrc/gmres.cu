@@ -146,6 +146,7 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
     double beta = 0;
     UVLM_TRY(norm2(g->V, &beta));
     res->relres = beta / bnorm;
+    if (total == 0) res->initial_relres = res->relres;
     if (!std::isfinite(beta)) return fail(kErrNonFinite, "non-finite GMRES residual");
     if (beta <= tol * bnorm) {
       res->converged = true;

@@ -26,6 +26,7 @@ struct GmresWork {
 struct GmresResult {
   int iters = 0;
   double relres = 0;
+  double initial_relres = 0;  // ||b - A x0|| / ||b|| of the initial guess
   bool converged = false;
 };
 

@@ -73,32 +73,43 @@ __device__ void block_argmax(double& v, int& r) {
 }
 
 // One panel (columns k0..k0+kb-1, rows k0..n-1) of the factorisation.
+// CTA b keeps panel rows [256 b, 256 b + 256) in shared memory, one row per
+// thread (rows padded to kLuNB + 1 elements against bank conflicts).  Per
+// column: block argmax of |a|, publish the CTA's candidate row (and the
+// current diagonal row, by its owner), one grid barrier, every CTA picks the
+// global pivot from the candidates, the two rows trade places and each thread
+// eliminates its own row.
+constexpr int kPanelRows = 256;
+constexpr int kPanelLd = kLuNB + 1;
+
 template <class T>
-__global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int lda, int n, int k0, int kb, int* ipiv,
-                                                        double* cand_val, int* cand_row, T* cand_data,
-                                                        T* diag_data, unsigned* bar, int* err, int rows_per_cta) {
+__global__ void __launch_bounds__(kPanelRows) lu_panel_kernel(T* A, int lda, int n, int k0, int kb, int* ipiv,
+                                                              double* cand_val, int* cand_row, T* cand_data,
+                                                              T* diag_data, unsigned* bar, int* err, int unused) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* rows = reinterpret_cast<T*>(smraw);     // [rows_per_cta][kLuNB]
-  T* urow = rows + rows_per_cta * kLuNB;     // [kLuNB]
+  T* rows = reinterpret_cast<T*>(smraw);         // [kPanelRows][kPanelLd]
+  T* urow = rows + kPanelRows * kPanelLd;        // [kLuNB]
   __shared__ int s_piv, s_owner;
+  (void)unused;
   const int P = gridDim.x, bid = blockIdx.x, tid = threadIdx.x;
   const int m = n - k0;
-  const int rb = bid * rows_per_cta;
-  const int re = min(rb + rows_per_cta, m);
-  const int nloc = max(0, re - rb);
+  const int rb = bid * kPanelRows;
+  const int nloc = max(0, min(kPanelRows, m - rb));
   for (int q = tid; q < nloc * kb; q += blockDim.x) {
     const int r = q / kb, c = q % kb;
-    rows[r * kLuNB + c] = A[(long long)(k0 + rb + r) * lda + k0 + c];
+    rows[r * kPanelLd + c] = A[(long long)(k0 + rb + r) * lda + k0 + c];
   }
   __syncthreads();
+  const bool mine = tid < nloc;
+  T* my = rows + tid * kPanelLd;
+  const int pr = rb + tid;  // this thread's panel row
   for (int c = 0; c < kb; ++c) {
     const int par = c & 1;
     double bv = -1.0;
     int br = INT_MAX;
-    for (int r = tid; r < nloc; r += blockDim.x) {
-      const int pr = rb + r;
-      if (pr < c) continue;
-      argmax_merge(bv, br, fabs((double)rows[r * kLuNB + c]), pr);
+    if (mine && pr >= c) {
+      bv = fabs((double)my[c]);
+      br = pr;
     }
     block_argmax(bv, br);
     if (tid == 0) {
@@ -107,9 +118,9 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int lda, int n, int
     }
     if (bv >= 0.0)
       for (int q = tid; q < kb; q += blockDim.x)
-        cand_data[((long long)par * kLuMaxCtas + bid) * kLuNB + q] = rows[(br - rb) * kLuNB + q];
-    if (c >= rb && c < re)
-      for (int q = tid; q < kb; q += blockDim.x) diag_data[par * kLuNB + q] = rows[(c - rb) * kLuNB + q];
+        cand_data[((long long)par * kLuMaxCtas + bid) * kLuNB + q] = rows[(br - rb) * kPanelLd + q];
+    if (c >= rb && c < rb + nloc)
+      for (int q = tid; q < kb; q += blockDim.x) diag_data[par * kLuNB + q] = rows[(c - rb) * kPanelLd + q];
     __threadfence();
     if (!grid_sync(bar, (unsigned)P, err)) return;
     if (tid < 32) {
@@ -142,31 +153,22 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(T* A, int lda, int n, int
     const T* src = (ow >= 0) ? cand_data + ((long long)par * kLuMaxCtas + ow) * kLuNB : diag_data + par * kLuNB;
     for (int q = tid; q < kb; q += blockDim.x) urow[q] = ((volatile T*)src)[q];
     __syncthreads();
-    if (p != c && p >= rb && p < re)
-      for (int q = tid; q < kb; q += blockDim.x) rows[(p - rb) * kLuNB + q] = ((volatile T*)diag_data)[par * kLuNB + q];
-    if (c >= rb && c < re)
-      for (int q = tid; q < kb; q += blockDim.x) rows[(c - rb) * kLuNB + q] = urow[q];
-    __syncthreads();
-    const T piv = urow[c];
-    for (int r = tid; r < nloc; r += blockDim.x) {
-      if (rb + r > c) {
-        const T a = rows[r * kLuNB + c];
-        rows[r * kLuNB + c] = (piv != (T)0) ? a / piv : (T)0;
-      }
-    }
-    __syncthreads();
-    const int w = kb - c - 1;
-    if (w > 0) {
-      for (int q = tid; q < nloc * w; q += blockDim.x) {
-        const int r = q / w, cc = c + 1 + q % w;
-        if (rb + r > c) rows[r * kLuNB + cc] -= rows[r * kLuNB + c] * urow[cc];
-      }
+    // the pivot row's slot receives the old diagonal row; row c becomes the pivot row
+    if (mine && pr == p && p != c)
+      for (int q = 0; q < kb; ++q) my[q] = ((volatile T*)diag_data)[par * kLuNB + q];
+    if (mine && pr == c)
+      for (int q = 0; q < kb; ++q) my[q] = urow[q];
+    if (mine && pr > c) {
+      const T piv = urow[c];
+      const T l = (piv != (T)0) ? my[c] / piv : (T)0;
+      my[c] = l;
+      for (int q = c + 1; q < kb; ++q) my[q] -= l * urow[q];
     }
     __syncthreads();
   }
   for (int q = tid; q < nloc * kb; q += blockDim.x) {
     const int r = q / kb, c = q % kb;
-    A[(long long)(k0 + rb + r) * lda + k0 + c] = rows[r * kLuNB + c];
+    A[(long long)(k0 + rb + r) * lda + k0 + c] = rows[r * kPanelLd + c];
   }
 }
 
@@ -437,10 +439,10 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
   for (int k0 = 0; k0 < n; k0 += kLuNB) {
     const int kb = std::min(kLuNB, n - k0);
     const int m = n - k0;
-    int P = std::min(std::min(w->num_sms, kLuMaxCtas), std::max(1, ceil_div(m, 16)));
-    const int rpc = ceil_div(m, P);
-    P = ceil_div(m, rpc);
-    size_t smem = sizeof(T) * ((size_t)rpc * kLuNB + kLuNB);
+    const int P = ceil_div(m, kPanelRows);
+    if (P > std::min(w->num_sms, kLuMaxCtas)) return fail(kErrUnsupported, "matrix too large for the panel kernel");
+    const int rpc = kPanelRows;
+    size_t smem = sizeof(T) * ((size_t)kPanelRows * kPanelLd + kLuNB);
     if (smem > 48 * 1024) UVLM_CUDA_TRY(cudaFuncSetAttribute(panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int lda = n;
     int* ipiv = w->ipiv;
@@ -452,7 +454,7 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
     int* err = w->err;
     int nn = n, kk0 = k0, kkb = kb, rr = rpc;
     void* args[] = {&A, &lda, &nn, &kk0, &kkb, &ipiv, &cv, &cr, &cd, &dd, &bar, &err, &rr};
-    UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(256), args, smem, st));
+    UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(kPanelRows), args, smem, st));
     note_launch();
     if (n - kb > 0) {
       const int other = n - kb;
