@@ -272,6 +272,11 @@ int uvlm_collect_training_data(uvlm_ctx* ctx, int32_t enable, int64_t max_sample
 /* n = samples recorded; X [n][8] and T [n] (either may be NULL). */
 int uvlm_get_training_data(uvlm_ctx* ctx, float* X, float* T, int64_t* n);
 
+/* FP32 LU with partial pivoting of a row-major n x n matrix (host arrays);
+ * update: 0 SIMT FP32, 1 tcgen05 TF32, 2 tcgen05 BF16 trailing updates.  LU
+ * receives L (unit diagonal, below) and U; ipiv the LAPACK-style row swaps
+ * (0-based).  The factorisation stage of the mixed-precision solve. */
+int uvlm_lu_factor_f32(const float* A, int64_t n, int32_t update, float* LU, int32_t* ipiv);
 /* Dense solve A x = b, A row-major n x n (FullPivLU replacement).  method:
  * 0 FP64 LU; 1 TF32 LU + FP64-residual GMRES; 2 BF16 LU + GMRES.
  * iters (may be NULL) receives the GMRES iteration count. */

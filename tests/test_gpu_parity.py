@@ -320,3 +320,29 @@ def test_dense_solve_singular_reports():
     with pytest.raises(M.UVLMError) as ei:
         M.dense_solve(A, np.ones(4), "fp64")
     assert ei.value.code == 3
+
+
+def _reconstruct(A, LU, ipiv):
+    n = A.shape[0]
+    PA = A.astype(np.float64).copy()
+    for k in range(n):
+        p = ipiv[k]
+        if p != k:
+            PA[[k, p]] = PA[[p, k]]
+    L = np.tril(LU.astype(np.float64), -1) + np.eye(n)
+    U = np.triu(LU.astype(np.float64))
+    return np.max(np.abs(PA - L @ U)) / np.max(np.abs(A))
+
+
+@pytest.mark.parametrize("update,tol", [("simt", 1e-5), ("tf32", 2e-3), ("bf16", 2e-2)])
+@pytest.mark.parametrize("n", [512, 704])
+def test_lu_factor_f32_tensor_core_updates(update, tol, n):
+    # n = 704: trailing blocks that are not multiples of the 128 x 128 tile
+    A = _influence_like(n, 21 + n).astype(np.float32)
+    LU, ipiv = U().lu_factor_f32(A, update)
+    err = _reconstruct(A, LU, ipiv)
+    print(f"LU {update} n={n}: max|PA - LU| / max|A| = {err:.2e}")
+    assert err < tol
+    if update != "simt":
+        LU0, ipiv0 = U().lu_factor_f32(A, "simt")
+        np.testing.assert_array_equal(ipiv, ipiv0)  # diagonally heavy: same pivots

@@ -348,5 +348,18 @@ def dense_solve(A, b, method: str = "fp64"):
     return x, it.value
 
 
+def lu_factor_f32(A, update: str = "tf32"):
+    """FP32 LU with partial pivoting on the GPU; update "simt", "tf32" or
+    "bf16" (tcgen05 tensor-core trailing updates).  Returns (LU, ipiv)."""
+    A = np.ascontiguousarray(np.asarray(A, dtype=np.float32))
+    n = A.shape[0]
+    LU = np.zeros_like(A)
+    ipiv = np.zeros(n, np.int32)
+    FP = C.POINTER(C.c_float)
+    check(lib().uvlm_lu_factor_f32(A.ctypes.data_as(FP), n, {"simt": 0, "tf32": 1, "bf16": 2}[update],
+                                   LU.ctypes.data_as(FP), ipiv.ctypes.data_as(C.POINTER(C.c_int32))))
+    return LU, ipiv
+
+
 from . import rings  # noqa: E402  (legacy AoS API)
 from . import warmstart  # noqa: E402  (learned warm start)

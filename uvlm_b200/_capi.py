@@ -118,6 +118,8 @@ SIGNATURES = [
     ("uvlm_set_mlp", C.c_int, [_V, _V]),
     ("uvlm_collect_training_data", C.c_int, [_V, C.c_int32, _I]),
     ("uvlm_get_training_data", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(_I)]),
+    ("uvlm_lu_factor_f32", C.c_int, [C.POINTER(C.c_float), _I, C.c_int32, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_int32)]),
     ("uvlm_dense_solve", C.c_int, [_P, _I, _P, _P, C.c_int32, C.POINTER(C.c_int32)]),
 ]
 

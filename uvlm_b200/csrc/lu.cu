@@ -473,7 +473,8 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
         UVLM_TRY(gemm_update_f64(reinterpret_cast<double*>(C), n, reinterpret_cast<const double*>(L21), n,
                                  reinterpret_cast<const double*>(U12), n, rest, rest, kb, st));
       } else {
-        if (upd == kLuUpdateSimt || kb % 32 != 0) {
+        // tensor-core update needs TMA-aligned rows (n % 4 == 0) and whole K chunks
+        if (upd == kLuUpdateSimt || kb % 64 != 0 || n % 4 != 0) {
           UVLM_TRY(gemm_update_f32_simt(reinterpret_cast<float*>(C), n, reinterpret_cast<const float*>(L21), n,
                                         reinterpret_cast<const float*>(U12), n, rest, rest, kb, st));
         } else {

@@ -439,6 +439,29 @@ int uvlm_rings_solve_linear_problem(const double* bound_rings, const double* bou
   return report(run());
 }
 
+int uvlm_lu_factor_f32(const float* A, int64_t n, int32_t update, float* LU, int32_t* ipiv) {
+  if (!A || !LU || n < 1 || update < 0 || update > 2) return report(fail(kErrInvalid, "invalid argument"));
+  if (update != 0 && !gemm_tc_available()) return report(fail(kErrUnsupported, "no tcgen05 device"));
+  Scratch S;
+  auto run = [&]() -> Error {
+    const int N = (int)n;
+    float* dA;
+    UVLM_TRY(S.up(&dA, A, (size_t)N * N));
+    LuWork lu;
+    UVLM_TRY(lu_work_alloc(&lu, N, 4, sms()));
+    const LuUpdate u = update == 0 ? kLuUpdateSimt : (update == 1 ? kLuUpdateTF32 : kLuUpdateBF16);
+    Error e = lu_factor_f32(dA, N, u, &lu, 0);
+    if (!e.code) e = lu_check(&lu, 0);
+    if (!e.code && cudaMemcpy(LU, dA, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+      e = fail(kErrCuda, "copy failed");
+    if (!e.code && ipiv && cudaMemcpy(ipiv, lu.ipiv, sizeof(int) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+      e = fail(kErrCuda, "copy failed");
+    lu_work_free(&lu);
+    return e;
+  };
+  return report(run());
+}
+
 int uvlm_dense_solve(const double* A, int64_t n, const double* b, double* x, int32_t method, int32_t* iters) {
   if (!A || !b || !x || n < 1 || method < 0 || method > 2) return report(fail(kErrInvalid, "invalid argument"));
   Scratch S;
