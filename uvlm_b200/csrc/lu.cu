@@ -1,6 +1,8 @@
 // lu.cu -- blocked LU with partial pivoting, FP64 and FP32 factor types.
 #include <climits>
 
+#include <cooperative_groups.h>
+
 #include "lu.cuh"
 
 namespace uvlm {
@@ -170,6 +172,152 @@ __global__ void __launch_bounds__(kPanelRows) lu_panel_kernel(T* A, int lda, int
     const int r = q / kb, c = q % kb;
     A[(long long)(k0 + rb + r) * lda + k0 + c] = rows[r * kPanelLd + c];
   }
+}
+
+// The same panel factorisation for panels of at most kMaxClusterCtas x 256
+// rows, as one thread-block cluster: the per-column pivot candidates, the
+// pivot row and the displaced diagonal row are exchanged through distributed
+// shared memory, and one hardware cluster barrier per column replaces the
+// global-memory barrier.  Every CTA runs the same number of barriers.
+constexpr int kMaxClusterCtas = 16;
+
+template <class T>
+__global__ void __launch_bounds__(kPanelRows) lu_panel_cluster_kernel(T* A, int lda, int n, int k0, int kb,
+                                                                      int* ipiv, int* err) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* rows = reinterpret_cast<T*>(smraw);           // [kPanelRows][kPanelLd]
+  T* urow = rows + kPanelRows * kPanelLd;          // [kLuNB]
+  T* cand_data = urow + kLuNB;                     // [2][kLuNB]
+  T* diag_data = cand_data + 2 * kLuNB;            // [2][kLuNB]
+  double* cand_val = reinterpret_cast<double*>(diag_data + 2 * kLuNB);  // [2]
+  int* cand_row = reinterpret_cast<int*>(cand_val + 2);               // [2]
+  __shared__ int s_piv, s_owner;
+  const int P = (int)cl.num_blocks(), bid = (int)cl.block_rank(), tid = threadIdx.x;
+  const int m = n - k0;
+  const int rb = bid * kPanelRows;
+  const int nloc = max(0, min(kPanelRows, m - rb));
+  for (int q = tid; q < nloc * kb; q += blockDim.x) {
+    const int r = q / kb, c = q % kb;
+    rows[r * kPanelLd + c] = A[(long long)(k0 + rb + r) * lda + k0 + c];
+  }
+  __syncthreads();
+  const bool mine = tid < nloc;
+  T* my = rows + tid * kPanelLd;
+  const int pr = rb + tid;
+  for (int c = 0; c < kb; ++c) {
+    const int par = c & 1;
+    double bv = -1.0;
+    int br = INT_MAX;
+    if (mine && pr >= c) {
+      bv = fabs((double)my[c]);
+      br = pr;
+    }
+    block_argmax(bv, br);
+    if (tid == 0) {
+      cand_val[par] = bv;
+      cand_row[par] = (bv >= 0.0) ? br : -1;
+    }
+    if (bv >= 0.0)
+      for (int q = tid; q < kb; q += blockDim.x) cand_data[par * kLuNB + q] = rows[(br - rb) * kPanelLd + q];
+    if (c >= rb && c < rb + nloc)
+      for (int q = tid; q < kb; q += blockDim.x) diag_data[par * kLuNB + q] = rows[(c - rb) * kPanelLd + q];
+    cl.sync();
+    if (tid < 32) {
+      double v = -1.0;
+      int r = INT_MAX, ow = -1;
+      for (int q = tid; q < P; q += 32) {
+        const double cv = *cl.map_shared_rank(cand_val + par, q);
+        const int cr = *cl.map_shared_rank(cand_row + par, q);
+        if (cr >= 0 && (cv > v || (cv == v && cr < r))) { v = cv; r = cr; ow = q; }
+      }
+      for (int off = 16; off; off >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, v, off);
+        const int orow = __shfl_down_sync(0xffffffffu, r, off);
+        const int oow = __shfl_down_sync(0xffffffffu, ow, off);
+        if (oow >= 0 && (ov > v || (ov == v && orow < r))) { v = ov; r = orow; ow = oow; }
+      }
+      if (tid == 0) {
+        if (!(v > 0.0)) {
+          atomicExch(err + 1, 1);
+          r = c;
+          ow = -1;
+        }
+        s_piv = r;
+        s_owner = ow;
+        if (bid == 0) ipiv[k0 + c] = k0 + r;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv, ow = s_owner;
+    const int diag_owner = c / kPanelRows;
+    const T* src = (ow >= 0) ? cl.map_shared_rank(cand_data + par * kLuNB, ow)
+                             : cl.map_shared_rank(diag_data + par * kLuNB, diag_owner);
+    for (int q = tid; q < kb; q += blockDim.x) urow[q] = src[q];
+    __syncthreads();
+    if (mine && pr == p && p != c) {
+      const T* dsrc = cl.map_shared_rank(diag_data + par * kLuNB, diag_owner);
+      for (int q = 0; q < kb; ++q) my[q] = dsrc[q];
+    }
+    if (mine && pr == c)
+      for (int q = 0; q < kb; ++q) my[q] = urow[q];
+    if (mine && pr > c) {
+      const T piv = urow[c];
+      const T l = (piv != (T)0) ? my[c] / piv : (T)0;
+      my[c] = l;
+      for (int q = c + 1; q < kb; ++q) my[q] -= l * urow[q];
+    }
+    __syncthreads();
+  }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+  for (int q = tid; q < nloc * kb; q += blockDim.x) {
+    const int r = q / kb, c = q % kb;
+    A[(long long)(k0 + rb + r) * lda + k0 + c] = rows[r * kPanelLd + c];
+  }
+}
+
+// Launches the cluster panel kernel; false if the cluster cannot be formed
+// (the caller then uses the cooperative kernel).
+template <class T>
+bool launch_panel_cluster(T* A, int n, int k0, int kb, int P, int* ipiv, int* err, cudaStream_t st) {
+  if (P > kMaxClusterCtas) return false;
+  auto kern = lu_panel_cluster_kernel<T>;
+  const size_t smem = sizeof(T) * ((size_t)kPanelRows * kPanelLd + 5 * kLuNB) + 2 * sizeof(double) + 2 * sizeof(int);
+  static int configured = 0;
+  if (!configured) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      configured = -1;
+    } else {
+      configured = 1;
+    }
+  }
+  if (configured < 0) return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P);
+  cfg.blockDim = dim3(kPanelRows);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = P;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaLaunchKernelEx(&cfg, kern, A, n, n, k0, kb, ipiv, err) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  note_launch();
+  return true;
 }
 
 // Row swaps of one panel applied to the columns outside the panel.
@@ -453,9 +601,11 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
     unsigned* bar = w->bar;
     int* err = w->err;
     int nn = n, kk0 = k0, kkb = kb, rr = rpc;
-    void* args[] = {&A, &lda, &nn, &kk0, &kkb, &ipiv, &cv, &cr, &cd, &dd, &bar, &err, &rr};
-    UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(kPanelRows), args, smem, st));
-    note_launch();
+    if (!launch_panel_cluster<T>(A, n, k0, kb, P, ipiv, err, st)) {
+      void* args[] = {&A, &lda, &nn, &kk0, &kkb, &ipiv, &cv, &cr, &cd, &dd, &bar, &err, &rr};
+      UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(kPanelRows), args, smem, st));
+      note_launch();
+    }
     if (n - kb > 0) {
       const int other = n - kb;
       laswp_kernel<T><<<std::min(ceil_div(other, 256), 1024), 256, 0, st>>>(A, n, n, k0, kb, w->ipiv);
