@@ -295,6 +295,10 @@ def run_ours(args, rank, world, local_rank):
     simmx.set_stage_timing(False)
     step0 += 1
     stage_ms = [float(x) for x in stmx.stage_ms]
+    sim64.set_stage_timing(True)
+    sim64.step(step0 - 1, DT)
+    stage64 = [float(x) for x in sim64.stats().stage_ms]
+    sim64.set_stage_timing(False)
     C1 = COLS + 1
     W = WAKE_ROWS + 1  # ring rows during the advect stage (before the erase)
     segs_bound = (ROWS + 1) * COLS + ROWS * C1
@@ -347,6 +351,9 @@ def run_ours(args, rank, world, local_rank):
             "nbody_variant": U.lib().uvlm_nbody_variant_name(int(st.nbody_variant)).decode(),
             "stage_ms": {"kin_shed": stage_ms[0], "assembly": stage_ms[1], "rhs": stage_ms[2], "solve": stage_ms[3],
                          "loads": stage_ms[4], "advect": stage_ms[5], "total": stage_ms[7]},
+            "plain_fp64_stage_ms": {"kin_shed": stage64[0], "assembly": stage64[1], "rhs": stage64[2],
+                                    "solve": stage64[3], "loads": stage64[4], "advect": stage64[5],
+                                    "total": stage64[7]},
             "roofline": {"bound": "fp32_simt", "kernel": "nbody_kernel (RK2 advection stage)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "FP32 FMA probe on this GPU (uvlm_measure_fp32_peak)",

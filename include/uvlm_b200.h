@@ -64,6 +64,10 @@ extern "C" {
 #define UVLM_WARM_EXTRAPOLATE 1 /* 2*Gamma_n - Gamma_{n-1} */
 #define UVLM_WARM_MLP 2         /* learned warm start (uvlm_set_mlp) */
 
+/* How the stale FP32 factors precondition the GMRES solve. */
+#define UVLM_PRECOND_INVERSE 0    /* dense FP32 (LU)^-1 P formed once per factorisation; one matvec per iteration */
+#define UVLM_PRECOND_TRIANGULAR 1 /* forward + backward triangular solves with the factors every iteration */
+
 /* Factor precision of the mixed form (trailing updates on tcgen05). */
 #define UVLM_LU_TF32 0
 #define UVLM_LU_BF16 1
@@ -88,6 +92,7 @@ typedef struct {
                                (the FP32 kernel then assembles only the matrix that is
                                factored); 0: FP32 assembly serves both */
   int32_t nbody_variant;    /* -1: autotune; else a tile variant index */
+  int32_t preconditioner;   /* UVLM_PRECOND_* (mixed form, GMRES solver) */
 } uvlm_config;
 
 /* Closed-form kinematics of one wing (Morphing, src/morphing.h:70-92, with the
@@ -281,6 +286,61 @@ int uvlm_lu_factor_f32(const float* A, int64_t n, int32_t update, float* LU, int
  * 0 FP64 LU; 1 TF32 LU + FP64-residual GMRES; 2 BF16 LU + GMRES.
  * iters (may be NULL) receives the GMRES iteration count. */
 int uvlm_dense_solve(const double* A, int64_t n, const double* b, double* x, int32_t method, int32_t* iters);
+
+/* ---------------------------------------------------------------------------
+ * Batched independent cases (no counterpart in the reference, whose drivers
+ * run one SimpleSimulator per process).  Every case is one wing with its own
+ * lattice, kinematics, forward flight and dt; all cases advance together, one
+ * MainLoop (simple_simulator.cpp:240-286) per step: kinematics, shed,
+ * influence matrix, RHS, solve, Joukowski loads, advection.  Each stage is one
+ * launch over all cases (persistent N-body over (case, target tile, source
+ * split) items, one CTA per case for the dense solve), the stage sizes are
+ * derived on the device from a step counter, and one step is captured as a
+ * CUDA graph that every further step replays.
+ * ------------------------------------------------------------------------- */
+typedef struct uvlm_batch uvlm_batch;
+
+typedef struct {
+  double chord, span;
+  int64_t rows, cols;        /* rings chordwise x spanwise (cols even, <= 64 x 64 per case) */
+  double origin[3];          /* wing origin (also the Morphing origin) */
+  double forward_flight[3];  /* SimpleSimulator::set_forward_flight */
+  double dt;                 /* this case's time step; t = step * dt */
+  uvlm_kinematics kin;       /* origin is overwritten with the wing origin */
+  int32_t chebyshev_chord, chebyshev_span;
+} uvlm_batch_case;
+
+typedef struct {
+  int32_t precision;       /* FP64: FP64 N-body and LU; MIXED: FP32 N-body, FP32 LU with FP64 iterative
+                              refinement (residual b - A g with the FP64 matrix) */
+  int32_t advection;       /* UVLM_ADVECT_EULER or UVLM_ADVECT_RK2 */
+  int32_t rk_ignore_rows;  /* RK2: Euler for wake rows i <= this (5, src/advect.h:77) */
+  int32_t refine_max_iter; /* MIXED: refinement sweeps at most */
+  double refine_tol;       /* MIXED: stop when ||b - A g|| <= tol ||b|| */
+  int64_t max_steps;       /* MainLoops the batch can run (wake capacity) */
+  int32_t device;
+  int32_t use_graph;       /* 1: capture one step as a CUDA graph and replay it */
+} uvlm_batch_config;
+
+int uvlm_batch_config_default(uvlm_batch_config* cfg);
+int uvlm_batch_create(const uvlm_batch_config* cfg, const uvlm_batch_case* cases, int32_t n_cases,
+                      uvlm_batch** out);
+int uvlm_batch_destroy(uvlm_batch* b);
+const char* uvlm_batch_last_error(const uvlm_batch* b);
+/* n_steps more MainLoops of every case (step = steps_done, steps_done+1, ...). */
+int uvlm_batch_run(uvlm_batch* b, int64_t n_steps);
+int uvlm_batch_steps_done(const uvlm_batch* b, int64_t* steps);
+/* rows [steps_done][n_cases][3] = (t, CD, CL) of every MainLoop so far. */
+int uvlm_batch_get_loads(const uvlm_batch* b, double* rows);
+/* State of case c (any pointer may be NULL): wing_pos [(rows+1)(cols+1)][3],
+ * wing_gamma [rows][cols], wake_pos [wake_rows+1][cols+1][3] (row 0 newest),
+ * wake_gamma [wake_rows][cols]. */
+int uvlm_batch_get_case(const uvlm_batch* b, int32_t c, double* wing_pos, double* wing_gamma, double* wake_pos,
+                        double* wake_gamma, int64_t* wake_rows);
+/* Last step's solve per case: refinement sweeps and final relative residual. */
+int uvlm_batch_get_solve_stats(const uvlm_batch* b, int32_t* sweeps, double* residual);
+/* Kernels one step launches (nodes of the captured graph). */
+int uvlm_batch_launches_per_step(const uvlm_batch* b, int64_t* launches);
 
 #ifdef __cplusplus
 }

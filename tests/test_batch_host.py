@@ -1,0 +1,71 @@
+"""Host logic of the batched sweep: seeded case draws, cost model and the
+case sharding over ranks (world size 2, gloo on CPU; no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+
+def test_draw_cases_ranges_and_seed():
+    from uvlm_b200.batch import draw_cases
+
+    a = draw_cases(256, seed=0)
+    b = draw_cases(256, seed=0)
+    assert a == b
+    assert draw_cases(256, seed=1) != a
+    for d in a:
+        assert 4 <= d["rows"] <= 16
+        assert 8 <= d["cols"] <= 64 and d["cols"] % 2 == 0
+        assert 2 <= d["span"] <= 10
+        assert 0.1 <= d["k"] <= 1.0
+        assert 0.05 <= d["heave"] <= 0.3
+        assert 0 <= d["pitch_deg"] <= 20
+        assert abs(d["dt"] - 2 * np.pi / (2 * d["k"]) / 40) < 1e-15
+
+
+def test_shard_cases_balances_work():
+    from uvlm_b200.batch import case_cost, draw_cases, shard_cases
+
+    cases = draw_cases(256, seed=0)
+    costs = [case_cost(d, 150) for d in cases]
+    for world in (1, 2, 4, 8):
+        parts = shard_cases(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(256))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= 1.02 * (sum(costs) / world) + max(costs)
+
+
+def _rank(rank, world, port, out_dir):
+    import torch.distributed as dist
+
+    from uvlm_b200.batch import case_cost, draw_cases, shard_cases
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    cases = draw_cases(256, seed=0)
+    costs = [case_cost(d, 150) for d in cases]
+    mine = shard_cases(costs, world)[rank]
+    # every rank reports the cases it would step and their work; rank 0 checks
+    # the union is the whole sweep exactly once
+    got = [None] * world
+    dist.all_gather_object(got, (mine, sum(costs[i] for i in mine)))
+    if rank == 0:
+        seen = sorted(i for m, _ in got for i in m)
+        np.save(os.path.join(out_dir, "seen.npy"), np.array(seen))
+        np.save(os.path.join(out_dir, "work.npy"), np.array([w for _, w in got]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_case_sharding_world_size_two(tmp_path):
+    import socket
+
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.start_processes(_rank, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn")
+    seen = np.load(tmp_path / "seen.npy")
+    work = np.load(tmp_path / "work.npy")
+    assert list(seen) == list(range(256))
+    assert abs(work[0] - work[1]) / work.sum() < 0.02

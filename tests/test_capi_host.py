@@ -53,6 +53,9 @@ int main(void) {
          sizeof(uvlm_step_stats));
   printf("%zu %zu %zu\n", offsetof(uvlm_config, gmres_tol), offsetof(uvlm_kinematics, origin),
          offsetof(uvlm_step_stats, stage_ms));
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(uvlm_batch_case), sizeof(uvlm_batch_config),
+         offsetof(uvlm_batch_case, kin), offsetof(uvlm_batch_case, chebyshev_span),
+         offsetof(uvlm_batch_config, max_steps), offsetof(uvlm_config, preconditioner));
   return 0;
 }
 ''')
@@ -65,6 +68,9 @@ int main(void) {
     assert sizes[4] == _capi.Config.gmres_tol.offset
     assert sizes[5] == _capi.Kinematics.origin.offset
     assert sizes[6] == _capi.StepStats.stage_ms.offset
+    assert sizes[7:] == [C.sizeof(_capi.BatchCase), C.sizeof(_capi.BatchConfig), _capi.BatchCase.kin.offset,
+                         _capi.BatchCase.chebyshev_span.offset, _capi.BatchConfig.max_steps.offset,
+                         _capi.Config.preconditioner.offset]
 
 
 def test_oracle_kinematics_layout_matches_product():

@@ -1,0 +1,151 @@
+"""Batched independent cases (uvlm_batch_*) against the FP64 oracle and the
+single-case library path, on a B200.
+
+Cases come from the seeded flapping-wing sweep (rows 4-16, even cols 8-64,
+aspect ratio 2-10, k 0.1-1, heave 0.05-0.3, pitch 0-20 deg), cut to sizes the
+oracle finishes in seconds.  Each case of the batch must reproduce its own
+SimpleSimulator run: FP64 batch within 1e-9 of the oracle on the loads and
+circulation; the mixed batch (FP32 N-body, FP32 LU + FP64 refinement) within
+1e-6 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 20
+
+
+def _small_cases(n, seed=3):
+    from uvlm_b200.batch import draw_cases
+
+    cs = draw_cases(n, seed)
+    for d in cs:  # cut to oracle-sized lattices, keep the drawn kinematics
+        d["rows"] = 2 + d["rows"] // 4
+        d["cols"] = 2 * (2 + d["cols"] // 16)
+        d["span"] = min(d["span"], 6.0)
+    return cs
+
+
+def _oracle(d, steps, advection="euler"):
+    import pyoracle as o
+
+    sim = o.Simulator()
+    kin = o.kinematics(plug_amp=d["heave"], plug_omega=d["omega"], twist_amp=math.radians(d["pitch_deg"]),
+                       twist_omega=d["omega"], twist_phase=math.pi / 2)
+    sim.add_wing(d["chord"], d["span"], d["rows"], d["cols"], kin=kin)
+    sim.set_forward_flight((-1.0, 0.0, 0.0))
+    sim.set_advection(advection)
+    loads = sim.run(steps - 1, d["dt"])
+    return np.asarray(loads), sim.state()
+
+
+@pytest.mark.parametrize("advection", ["euler", "RK2"])
+def test_batch_fp64_matches_oracle(advection):
+    from uvlm_b200.batch import make_batch
+
+    cases = _small_cases(5)
+    sim = make_batch(cases, precision="fp64", advection=advection, max_steps=STEPS)
+    sim.run(STEPS)
+    L = sim.loads()
+    assert L.shape == (STEPS, len(cases), 3)
+    for c, d in enumerate(cases):
+        ref, st = _oracle(d, STEPS, advection)
+        np.testing.assert_allclose(L[:, c, 0], ref[:, 0], rtol=0, atol=1e-12)
+        scale = np.max(np.abs(ref[:, 1:])) + 1e-30
+        np.testing.assert_allclose(L[:, c, 1:], ref[:, 1:], rtol=0, atol=1e-9 * scale)
+        got = sim.case_state(c)
+        np.testing.assert_allclose(got["wing_gamma"], st["wing_gamma"][0], rtol=0,
+                                   atol=1e-9 * np.max(np.abs(st["wing_gamma"])))
+        np.testing.assert_allclose(got["wake_pos"], st["wake_pos"][0], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(got["wake_gamma"], st["wake_gamma"][0], rtol=0,
+                                   atol=1e-9 * np.max(np.abs(st["wing_gamma"])))
+    sim.close()
+
+
+def test_batch_mixed_refinement_matches_oracle():
+    from uvlm_b200.batch import make_batch
+
+    cases = _small_cases(6, seed=11)
+    sim = make_batch(cases, precision="mixed", max_steps=STEPS)
+    sim.run(STEPS)
+    L = sim.loads()
+    sweeps, res = sim.solve_stats()
+    assert np.all(res <= 1e-12)
+    for c, d in enumerate(cases):
+        ref, st = _oracle(d, STEPS)
+        scale = np.max(np.abs(ref[:, 1:]))
+        assert np.max(np.abs(L[:, c, 1:] - ref[:, 1:])) <= 1e-6 * scale
+    sim.close()
+
+
+def test_batch_graph_replay_equals_direct_launches():
+    from uvlm_b200.batch import make_batch
+
+    cases = _small_cases(7, seed=5)
+    out = []
+    for g in (True, False):
+        sim = make_batch(cases, precision="mixed", max_steps=12, use_graph=g)
+        sim.run(5)
+        sim.run(7)
+        out.append((sim.loads(), [sim.case_state(c)["wake_pos"] for c in range(len(cases))]))
+        if g:
+            assert sim.launches_per_step() > 10
+        sim.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_batch_case_equals_single_case_library_path():
+    """A case inside a ragged batch gives the single-case FP64 path's answer."""
+    import uvlm_b200 as U
+    from uvlm_b200.batch import case_morphing, make_batch
+
+    cases = _small_cases(4, seed=9)
+    sim = make_batch(cases, precision="fp64", max_steps=10)
+    sim.run(10)
+    L = sim.loads()
+    for c, d in enumerate(cases):
+        one = U.SimpleSimulator(precision="fp64")
+        one.AddWing(U.RectGenerator(), case_morphing(d), d["chord"], d["span"], d["rows"], d["cols"])
+        one.set_forward_flight([-1.0, 0.0, 0.0])
+        one.set_advection("euler")
+        one.begin()
+        rows = np.array([one.step(s, d["dt"]) for s in range(10)])
+        np.testing.assert_allclose(L[:, c, 1:], rows[:, 1:], rtol=0, atol=1e-10 * np.max(np.abs(rows[:, 1:])))
+        one.close()
+    sim.close()
+
+
+def test_batch_full_sweep_shapes_run():
+    """The 256-case sweep at its drawn sizes: a few steps, finite loads,
+    refinement converged in every case."""
+    from uvlm_b200.batch import draw_cases, make_batch
+
+    cases = draw_cases(256, seed=0)
+    sim = make_batch(cases, precision="mixed", max_steps=8)
+    sim.run(8)
+    L = sim.loads()
+    assert np.all(np.isfinite(L))
+    sweeps, res = sim.solve_stats()
+    assert np.all(res <= 1e-12)
+    sim.close()
+
+
+def test_batch_rejects_bad_cases():
+    import uvlm_b200 as U
+    from uvlm_b200.batch import BatchError, BatchSimulator
+
+    sim = BatchSimulator()
+    sim.add_case(U.Morphing(), 1.0, 4.0, 4, 7, 0.1)  # odd cols
+    with pytest.raises(BatchError):
+        sim.begin()
+    sim2 = BatchSimulator(max_steps=3)
+    sim2.add_case(U.Morphing(), 1.0, 4.0, 4, 8, 0.1)
+    sim2.run(3)
+    with pytest.raises(BatchError):
+        sim2.run(1)
+    sim2.close()

@@ -346,3 +346,28 @@ def test_lu_factor_f32_tensor_core_updates(update, tol, n):
     if update != "simt":
         LU0, ipiv0 = U().lu_factor_f32(A, "simt")
         np.testing.assert_array_equal(ipiv, ipiv0)  # diagonally heavy: same pivots
+
+
+def test_inverse_preconditioner_matches_triangular_solves():
+    """The dense (LU)^-1 of the stale factors and the triangular solves with
+    the same factors precondition GMRES to the same FP64 answer."""
+    import uvlm_b200 as U
+
+    dt = 2 * math.pi / 40
+    res = {}
+    for pc in ("inverse", "triangular"):
+        sim = U.SimpleSimulator(precision="mixed", warm_start="extrapolate", preconditioner=pc)
+        m = U.Morphing().set_plug(0.2, 1.0).set_twist(math.radians(10), 1.0, math.pi / 2)
+        sim.AddWing(U.RectGenerator(), m, 1.0, 8.0, 12, 40)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.set_advection("RK2")
+        sim.begin()
+        rows, its = [], []
+        for s in range(30):
+            rows.append(sim.step(s, dt))
+            its.append(sim.stats().gmres_iters)
+        res[pc] = (np.array(rows), sim.state()["wing_gamma"], its)
+        sim.close()
+    np.testing.assert_allclose(res["inverse"][1], res["triangular"][1], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(res["inverse"][0], res["triangular"][0], rtol=0, atol=1e-9)
+    assert abs(sum(res["inverse"][2]) - sum(res["triangular"][2])) <= 3

@@ -115,12 +115,16 @@ class SimpleSimulator:
       solver      "lu" (factor every step) or "gmres_stale" (GMRES
                   preconditioned by stale LU factors, fresh-LU fallback)
       warm_start  "previous", "extrapolate" or "mlp"
+      preconditioner  "inverse" (dense (LU)^-1 of the stale factors, one
+                  matrix-vector product per GMRES iteration) or "triangular"
+                  (forward/backward solves with the factors)
     """
 
     def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
                  lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
                  gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
-                 assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True):
+                 assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True,
+                 preconditioner: str = "inverse"):
         cfg = Config()
         lib().uvlm_config_default(C.byref(cfg))
         cfg.precision = PRECISION[precision]
@@ -139,6 +143,7 @@ class SimpleSimulator:
         cfg.assembly_fp64 = int(precision == "mixed" if assembly_fp64 is None else bool(assembly_fp64))
         cfg.nbody_variant = int(nbody_variant)
         cfg.compute_loads = int(bool(compute_loads))
+        cfg.preconditioner = {"inverse": 0, "triangular": 1}[preconditioner]
         self._cfg = cfg
         h = C.c_void_p()
         check(lib().uvlm_create(C.byref(cfg), C.byref(h)))
@@ -363,3 +368,6 @@ def lu_factor_f32(A, update: str = "tf32"):
 
 from . import rings  # noqa: E402  (legacy AoS API)
 from . import warmstart  # noqa: E402  (learned warm start)
+
+
+from .batch import BatchSimulator, draw_cases, shard_cases  # noqa: E402,F401

@@ -31,7 +31,7 @@ class Config(C.Structure):
         ("max_wake_rows", C.c_int64), ("erase_wake_after", C.c_int64),
         ("gmres_restart", C.c_int32), ("gmres_max_iter", C.c_int32), ("gmres_tol", C.c_double),
         ("device", C.c_int32), ("compute_loads", C.c_int32), ("assembly_fp64", C.c_int32),
-        ("nbody_variant", C.c_int32),
+        ("nbody_variant", C.c_int32), ("preconditioner", C.c_int32),
     ]
 
 
@@ -61,6 +61,22 @@ class StepStats(C.Structure):
         ("residual", C.c_double), ("refactored", C.c_int32), ("wake_rows", C.c_int32),
         ("stage_ms", C.c_double * 8), ("nbody_variant", C.c_int32), ("pad_", C.c_int32),
         ("initial_residual", C.c_double),
+    ]
+
+
+class BatchCase(C.Structure):
+    _fields_ = [
+        ("chord", C.c_double), ("span", C.c_double), ("rows", C.c_int64), ("cols", C.c_int64),
+        ("origin", C.c_double * 3), ("forward_flight", C.c_double * 3), ("dt", C.c_double),
+        ("kin", Kinematics), ("chebyshev_chord", C.c_int32), ("chebyshev_span", C.c_int32),
+    ]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int32), ("advection", C.c_int32), ("rk_ignore_rows", C.c_int32),
+        ("refine_max_iter", C.c_int32), ("refine_tol", C.c_double), ("max_steps", C.c_int64),
+        ("device", C.c_int32), ("use_graph", C.c_int32),
     ]
 
 
@@ -121,6 +137,16 @@ SIGNATURES = [
     ("uvlm_lu_factor_f32", C.c_int, [C.POINTER(C.c_float), _I, C.c_int32, C.POINTER(C.c_float),
                                      C.POINTER(C.c_int32)]),
     ("uvlm_dense_solve", C.c_int, [_P, _I, _P, _P, C.c_int32, C.POINTER(C.c_int32)]),
+    ("uvlm_batch_config_default", C.c_int, [C.POINTER(BatchConfig)]),
+    ("uvlm_batch_create", C.c_int, [C.POINTER(BatchConfig), C.POINTER(BatchCase), C.c_int32, C.POINTER(_V)]),
+    ("uvlm_batch_destroy", C.c_int, [_V]),
+    ("uvlm_batch_last_error", C.c_char_p, [_V]),
+    ("uvlm_batch_run", C.c_int, [_V, _I]),
+    ("uvlm_batch_steps_done", C.c_int, [_V, C.POINTER(_I)]),
+    ("uvlm_batch_get_loads", C.c_int, [_V, _P]),
+    ("uvlm_batch_get_case", C.c_int, [_V, C.c_int32, _P, _P, _P, _P, C.POINTER(_I)]),
+    ("uvlm_batch_get_solve_stats", C.c_int, [_V, C.POINTER(C.c_int32), _P]),
+    ("uvlm_batch_launches_per_step", C.c_int, [_V, C.POINTER(_I)]),
 ]
 
 _lib = None

@@ -10,6 +10,7 @@
 
 #include "../../include/uvlm_b200.h"
 #include "gmres.cuh"
+#include "host_lattice.h"
 #include "mlp.cuh"
 #include "lu.cuh"
 #include "nbody.cuh"
@@ -33,46 +34,6 @@ namespace {
 int set_global(const Error& e) {
   if (e.code) g_last_error = e.msg;
   return e.code;
-}
-
-// RectGenerator (src/wing/rect.cpp:18-45) with linspace (src/util.h:36-43)
-// and TransformChebyshev (src/wing/rect.h:16-25); host set-up, once per case.
-std::vector<double> linspace(double a, double b, size_t N) {
-  const double dx = (b - a) / (N - 1);
-  std::vector<double> r;
-  for (size_t i = 0; i < N; i++) r.push_back(a + i * dx);
-  return r;
-}
-std::vector<double> chebyshev(size_t N, double xmin, double xmax) {
-  auto th = linspace(-M_PI_2, 0, N);
-  std::vector<double> r;
-  for (double t : th) r.push_back(xmin + (xmax - xmin) * std::cos(t));
-  r.front() = xmin;
-  r.back() = xmax;
-  return r;
-}
-// WholeWing (src/wing/wing.cpp:12-52) of the half wing (chord, span/2,
-// rows, cols/2), shifted by the wing origin (simple_simulator.cpp:159-166).
-std::vector<double> whole_wing_nodes(const uvlm_wing_desc& w) {
-  const size_t rows = (size_t)w.rows, hc = (size_t)w.cols / 2;
-  auto xs = w.chebyshev_chord ? chebyshev(rows + 1, 0, w.chord) : linspace(0, w.chord, rows + 1);
-  auto ys = w.chebyshev_span ? chebyshev(hc + 1, 0, w.span / 2) : linspace(0, w.span / 2, hc + 1);
-  std::vector<double> out;
-  out.reserve((rows + 1) * (2 * hc + 1) * 3);
-  for (size_t i = 0; i <= rows; i++) {
-    for (size_t q = 0; q <= hc; q++) {  // mirrored half, reversed
-      const size_t jj = hc - q;
-      out.push_back(xs[i] + 0.0 + w.origin[0]);
-      out.push_back(ys[jj] * -1 + w.origin[1]);
-      out.push_back(0.0 + w.origin[2]);
-    }
-    for (size_t jj = 1; jj <= hc; jj++) {
-      out.push_back(xs[i] + w.origin[0]);
-      out.push_back(ys[jj] + w.origin[1]);
-      out.push_back(0.0 + w.origin[2]);
-    }
-  }
-  return out;
 }
 
 template <class T>
@@ -127,6 +88,7 @@ struct uvlm_ctx {
   double* d_A64 = nullptr;   // FP64 matrix (plain: factored in place; mixed: residual matrix if assembly_fp64)
   float* d_A32 = nullptr;    // FP32 matrix of the mixed form
   float* d_F32 = nullptr;    // FP32 factors of the mixed form
+  float* d_Minv = nullptr;   // dense (LU)^-1 P of those factors (UVLM_PRECOND_INVERSE)
   double* d_tmp = nullptr;   // [N] scratch
   double* d_row = nullptr;   // [1+2num] load row
   int* d_flags = nullptr;    // [4] non-finite etc.
@@ -187,6 +149,8 @@ void uvlm_ctx::free_all() {
   }
   cudaFree(d_A32);
   cudaFree(d_F32);
+  cudaFree(d_Minv);
+  d_Minv = nullptr;
   cudaFree(d_rhs_prev);
   cudaFree(d_phase);
   cudaFree(d_feat);
@@ -252,6 +216,8 @@ Error uvlm_ctx::alloc_all() {
   if (mixed()) {
     if (!cfg.assembly_fp64) UVLM_CUDA_TRY(cudaMalloc(&d_A32, sizeof(float) * (size_t)N * N));
     UVLM_CUDA_TRY(cudaMalloc(&d_F32, sizeof(float) * (size_t)N * N));
+    if (cfg.solver == UVLM_SOLVER_GMRES_STALE && cfg.preconditioner == UVLM_PRECOND_INVERSE)
+      UVLM_CUDA_TRY(cudaMalloc(&d_Minv, sizeof(float) * (size_t)N * N));
     UVLM_TRY(lu_work_alloc(&lu, N, 4, num_sms));
     UVLM_TRY(gmres_work_alloc(&gm, N, std::max(2, cfg.gmres_restart)));
   } else {
@@ -356,6 +322,7 @@ Error uvlm_ctx::solve(long long step) {
       UVLM_CUDA_TRY(cudaMemcpyAsync(d_F32, d_A32, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToDevice, st));
     UVLM_TRY(lu_factor_f32(d_F32, N, use, &lu, st));
     UVLM_TRY(lu_check(&lu, st));
+    if (d_Minv) UVLM_TRY(lu_inverse_f32(d_F32, N, &lu, d_Minv, st));
     have_factors = true;
     last.refactored = 1;
     work_lu += 2.0 / 3.0 * (double)N * N * N;
@@ -376,14 +343,14 @@ Error uvlm_ctx::solve(long long step) {
   const float* A32 = cfg.assembly_fp64 ? nullptr : d_A32;
   const double* A64 = cfg.assembly_fp64 ? d_A64 : nullptr;
   GmresResult r;
-  UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_rhs, d_gamma, cfg.gmres_tol, cfg.gmres_max_iter, &gm, &r, st));
+  UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_Minv, d_rhs, d_gamma, cfg.gmres_tol, cfg.gmres_max_iter, &gm, &r, st));
   last.solve_path = fresh ? 0 : 1;
   if (!r.converged && !fresh) {
     // fresh-LU fallback: factor the current matrix and solve again
     UVLM_TRY(factor());
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_gamma, d_gamma_prev, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     GmresResult r2;
-    UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_rhs, d_gamma, cfg.gmres_tol, 4 * cfg.gmres_max_iter, &gm, &r2,
+    UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_Minv, d_rhs, d_gamma, cfg.gmres_tol, 4 * cfg.gmres_max_iter, &gm, &r2,
                          st));
     r2.iters += r.iters;
     r = r2;
@@ -592,6 +559,7 @@ void uvlm_config_default(uvlm_config* c) {
   c->compute_loads = 1;
   c->assembly_fp64 = 0;
   c->nbody_variant = -1;
+  c->preconditioner = UVLM_PRECOND_INVERSE;
 }
 
 const char* uvlm_status_string(int s) {
@@ -625,7 +593,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
     return set_global(fail(kErrInvalid, "unknown precision"));
   }
   if (k.advection < 0 || k.advection > 3 || k.max_wake_rows < 1 || k.gmres_restart < 1 || k.gmres_max_iter < 1 ||
-      !(k.gmres_tol > 0)) {
+      !(k.gmres_tol > 0) || k.preconditioner < 0 || k.preconditioner > 1) {
     delete c;
     return set_global(fail(kErrInvalid, "invalid configuration"));
   }

@@ -109,8 +109,9 @@ void gmres_work_free(GmresWork* g) {
   *g = GmresWork{};
 }
 
-Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, LuWork* lu, const double* b,
-                  double* x, double tol, int max_iter, GmresWork* g, GmresResult* res, cudaStream_t st) {
+Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, LuWork* lu, const float* Minv,
+                  const double* b, double* x, double tol, int max_iter, GmresWork* g, GmresResult* res,
+                  cudaStream_t st) {
   const int m = g->m;
   res->iters = 0;
   res->converged = false;
@@ -167,7 +168,10 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
     for (; j < m && total < max_iter; ++j) {
       double* Vj = g->V + (size_t)j * n;
       double* Zj = g->Z + (size_t)j * n;
-      UVLM_TRY(lu_solve_f32(LU, n, lu, Vj, Zj, g->ptmp, st));
+      if (Minv)
+        UVLM_TRY(matvec(Minv, nullptr, n, Vj, Zj, st));
+      else
+        UVLM_TRY(lu_solve_f32(LU, n, lu, Vj, Zj, g->ptmp, st));
       UVLM_TRY(matvec(A32, A64, n, Zj, g->w, st));
       // classical Gram-Schmidt, applied twice (CGS2)
       for (int pass = 0; pass < 2; ++pass) {

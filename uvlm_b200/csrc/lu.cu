@@ -677,7 +677,85 @@ Error tri_solve(const T* LU, int n, LuWork* w, const double* vin, V* y, V* z, do
   return ok();
 }
 
+// Y = P (the row permutation of the factorisation as a dense matrix).
+__global__ void perm_matrix_kernel(const int* __restrict__ perm, int n, float* Y) {
+  const long long total = (long long)n * n;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(q / n), c = (int)(q % n);
+    Y[q] = (c == perm[r]) ? 1.f : 0.f;
+  }
+}
+
+// Y[rows r0 .. r0+nb) = D * Y[rows r0 .. r0+nb), D a kTriB x kTriB block
+// (rows/cols >= nb are identity padding), in place: each CTA owns 64 columns
+// and reads its whole tile before writing.
+__global__ void __launch_bounds__(256) apply_block_kernel(const float* __restrict__ D, float* Y, int n, int r0,
+                                                          int nb) {
+  __shared__ float Ds[kTriB][kTriB + 1];
+  __shared__ float Ts[kTriB][kTriB];
+  const int c0 = blockIdx.x * 64;
+  const int tid = threadIdx.x;
+  for (int q = tid; q < kTriB * kTriB; q += 256) {
+    const int i = q / kTriB, j = q % kTriB;
+    Ds[i][j] = D[q];
+    Ts[i][j] = (i < nb && c0 + j < n) ? Y[(long long)(r0 + i) * n + c0 + j] : 0.f;
+  }
+  __syncthreads();
+  const int tx = tid & 15, ty = tid >> 4;
+  float acc[4][4] = {};
+  for (int s = 0; s < kTriB; ++s) {
+    float a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = Ds[ty * 4 + i][s];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = Ts[s][tx * 4 + j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = ty * 4 + i;
+    if (r >= nb) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + tx * 4 + j;
+      if (c < n) Y[(long long)(r0 + r) * n + c] = acc[i][j];
+    }
+  }
+}
+
 }  // namespace
+
+Error lu_inverse_f32(const float* LU, int n, LuWork* w, float* X, cudaStream_t st) {
+  if (n <= 0) return ok();
+  const int nblk = ceil_div(n, kTriB);
+  const int* perm = w->ipiv + n;
+  const float* dl = reinterpret_cast<const float*>(w->dinv_l);
+  const float* du = reinterpret_cast<const float*>(w->dinv_u);
+  perm_matrix_kernel<<<std::min<long long>(ceil_div((long long)n * n, 256), 4096), 256, 0, st>>>(perm, n, X);
+  UVLM_LAUNCH_CHECK();
+  const int cg = ceil_div(n, 64);
+  // X = L^-1 P: block forward substitution, X_I = Linv_II (P_I - L_I,<I X_<I)
+  for (int I = 0; I < nblk; ++I) {
+    const int r0 = I * kTriB, nb = std::min(kTriB, n - r0);
+    if (r0 > 0) UVLM_TRY(gemm_update_f32_simt(X + (long long)r0 * n, n, LU + (long long)r0 * n, n, X, n, nb, n, r0, st));
+    apply_block_kernel<<<cg, 256, 0, st>>>(dl + (long long)I * kTriB * kTriB, X, n, r0, nb);
+    UVLM_LAUNCH_CHECK();
+  }
+  // X = U^-1 X: block backward substitution, X_I = Uinv_II (X_I - U_I,>I X_>I)
+  for (int I = nblk - 1; I >= 0; --I) {
+    const int r0 = I * kTriB, nb = std::min(kTriB, n - r0), r1 = r0 + nb;
+    if (r1 < n)
+      UVLM_TRY(gemm_update_f32_simt(X + (long long)r0 * n, n, LU + (long long)r0 * n + r1, n, X + (long long)r1 * n, n,
+                                    nb, n, n - r1, st));
+    apply_block_kernel<<<cg, 256, 0, st>>>(du + (long long)I * kTriB * kTriB, X, n, r0, nb);
+    UVLM_LAUNCH_CHECK();
+  }
+  return ok();
+}
 
 Error lu_work_alloc(LuWork* w, int n, int elem_size, int num_sms) {
   lu_work_free(w);

@@ -69,6 +69,12 @@ Error lu_solve_f64(const double* LU, int n, LuWork* w, const double* b, double* 
 // z = (LU)^-1 v with FP32 factors: FP64 in/out, FP32 arithmetic (preconditioner).
 Error lu_solve_f32(const float* LU, int n, LuWork* w, const double* v, double* z, float* tmp, cudaStream_t st);
 
+// X = (LU)^-1 P = A^-1 as a dense row-major FP32 matrix from the factors of
+// lu_factor_f32 (block forward then backward substitution on the identity
+// permuted by the pivots, GEMM updates between the diagonal-block inverses).
+// A stale preconditioner applied as one dense matrix-vector product.
+Error lu_inverse_f32(const float* LU, int n, LuWork* w, float* X, cudaStream_t st);
+
 // Trailing update used by the factorisation (exposed for tests/benches):
 // C[m x nc] -= A[m x k] * B[k x nc], row-major with leading dims.
 Error gemm_update_f64(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int m, int nc, int k,

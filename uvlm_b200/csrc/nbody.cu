@@ -4,90 +4,12 @@
 namespace uvlm {
 namespace {
 
-// ------------------------------------------------------------ record build
-__device__ inline double ring_gamma(const SheetView& v, int n, int i, int j) {
-  const int R = v.node_rows - 1;
-  if (i < 0 || i >= R || j < 0 || j >= v.cols) return 0.0;
-  return v.gamma[((long long)n * v.g_rows_alloc + v.g_row0 + i) * v.cols + j];
-}
-
 template <class Rec>
 __global__ void build_records_kernel(SheetView v, Rec* out) {
   const long long total = (long long)v.num * v.node_rows * (v.cols + 1);
-  const double s = 1.0 / (4.0 * kPi);
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
-       k += (long long)gridDim.x * blockDim.x) {
-    const int C1 = v.cols + 1;
-    const int j = (int)(k % C1);
-    const long long nr = k / C1;
-    const int i = (int)(nr % v.node_rows);
-    const int n = (int)(nr / v.node_rows);
-    const double* p = v.pos + (((long long)n * v.rows_alloc + v.row0 + i) * C1 + j) * 3;
-    const int R = v.node_rows - 1;
-    // strengths: spanwise S(i,j) and chordwise H(i,j) (nbody.cuh)
-    const double gS = (j < v.cols) ? ring_gamma(v, n, i, j) - ring_gamma(v, n, i - 1, j) : 0.0;
-    const double gH = (i < R && !v.spanwise_only) ? ring_gamma(v, n, i, j - 1) - ring_gamma(v, n, i, j) : 0.0;
-    // segment vectors s0 = p(i,j+1) - p(i,j), h0 = p(i+1,j) - p(i,j)
-    double s0[3] = {0, 0, 0}, h0[3] = {0, 0, 0};
-    if (j < v.cols)
-      for (int d = 0; d < 3; ++d) s0[d] = p[3 + d] - p[d];
-    if (i < R)
-      for (int d = 0; d < 3; ++d) h0[d] = p[3 * C1 + d] - p[d];
-    Rec r;
-    if constexpr (sizeof(Rec) == sizeof(RecF)) {
-      const float hx = (float)p[0], hy = (float)p[1], hz = (float)p[2];
-      r.hi = make_float4(hx, hy, hz, (float)(gS * s));
-      r.lo = make_float4((float)(p[0] - (double)hx), (float)(p[1] - (double)hy),
-                         (float)(p[2] - (double)hz), (float)(gH * s));
-      r.sv = make_float4((float)s0[0], (float)s0[1], (float)s0[2], (float)h0[0]);
-      r.hv = make_float4((float)h0[1], (float)h0[2], 0.f, 0.f);
-    } else {
-      r.a = make_double4(p[0], p[1], p[2], gS * s);
-      r.b = make_double4(gH * s, s0[0], s0[1], s0[2]);
-      r.c = make_double4(h0[0], h0[1], h0[2], 0.0);
-    }
-    out[k] = r;
-  }
-}
-
-// ---------------------------------------------------------- strip decode
-struct StripInfo {
-  long long first;  // record index of node (i0, j0)
-  int row_stride;   // cols + 1
-  int n_rows;       // owned node rows
-  int nr;           // node rows loaded (n_rows + has_lower)
-  int n_cols;       // node columns in the chunk
-  bool last_h;      // owns the chordwise segments of its last column
-};
-
-struct Blocks {
-  SourceBlock b[4];
-  int n;
-  int strips_per_sheet[4];
-  int chunks[4];
-  long long strip_begin[5];
-};
-
-template <int H>
-__device__ inline StripInfo decode_strip(const Blocks& B, long long s) {
-  int bi = 0;
-  while (bi + 1 < B.n && s >= B.strip_begin[bi + 1]) ++bi;
-  const SourceBlock& sb = B.b[bi];
-  const long long local = s - B.strip_begin[bi];
-  const int sps = B.strips_per_sheet[bi];
-  const int chunks = B.chunks[bi];
-  const int n = (int)(local / sps);
-  const int rem = (int)(local % sps);
-  const int g = rem / chunks, c = rem % chunks;
-  StripInfo si;
-  const int i0 = g * H, j0 = c * kStripCols;
-  si.n_rows = min(H, sb.node_rows - i0);
-  si.nr = si.n_rows + ((i0 + si.n_rows < sb.node_rows) ? 1 : 0);
-  si.n_cols = min(kStripCols, sb.cols - j0) + 1;
-  si.last_h = (j0 + si.n_cols - 1 == sb.cols);
-  si.row_stride = sb.cols + 1;
-  si.first = sb.rec_off + ((long long)n * sb.node_rows + i0) * (sb.cols + 1) + j0;
-  return si;
+       k += (long long)gridDim.x * blockDim.x)
+    out[k] = build_record<Rec>(v, k);
 }
 
 // cp.async 16-byte staging of one strip into shared memory ([r][j] records)
@@ -103,6 +25,31 @@ __device__ inline void stage_strip(Rec* sm, const Rec* rec, const StripInfo& si)
     char* dst = reinterpret_cast<char*>(sm + rj) + 16 * part;
     const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst), "l"(src));
+  }
+  asm volatile("cp.async.commit_group;");
+}
+
+// Full-tile staging: always (H + 1) x (kStripCols + 1) records; entries past
+// the strip's rows or columns are all-zero records (zero strengths, zero
+// segment vectors), whose segments have d = 0 and are cut exactly like a
+// degenerate segment, so they add +0 to every target.
+template <class Rec, int H>
+__device__ inline void stage_strip_padded(Rec* sm, const Rec* rec, const StripInfo& si) {
+  constexpr int kChunks = sizeof(Rec) / 16;
+  constexpr int kCols = kStripCols + 1;
+  constexpr int total = (H + 1) * kCols * kChunks;
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int part = q % kChunks;
+    const int rj = q / kChunks;
+    const int r = rj / kCols, j = rj % kCols;
+    char* dst = reinterpret_cast<char*>(sm + rj) + 16 * part;
+    if (r < si.nr && j < si.n_cols) {
+      const char* src = reinterpret_cast<const char*>(rec + si.first + (long long)r * si.row_stride + j) + 16 * part;
+      const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst), "l"(src));
+    } else {
+      *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
   }
   asm volatile("cp.async.commit_group;");
 }
@@ -250,7 +197,133 @@ __device__ __forceinline__ void walk_strip(const Rec* sm, const StripInfo& si, c
   }
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
+// One node column of a full strip (H owned node rows plus the row below,
+// kStripCols + 1 columns, record stride kStripCols + 1 in shared memory): the
+// node quantities of the column, its H chordwise segments (DO_H) and the H
+// spanwise segments that end in it (!FIRST).  The column's quantities become
+// `prev` for the next column; with the column loop unrolled by two the
+// compiler renames instead of copying.
+template <class T, class Rec, int H, int TPT, bool FIRST, bool DO_H>
+__device__ __forceinline__ void full_column(const Rec* col, const Tgt<T> (&tg)[TPT], NodeV<T> (&prev)[TPT][H],
+                                            SegV<T> (&ps0)[H], T (&pgS)[H], T (&acc)[TPT][3]) {
+  NodeV<T> cur[TPT][H + 1];
+  T gS[H], gH[H];
+  SegV<T> s0[H], h0[H];
+#pragma unroll
+  for (int r = 0; r <= H; ++r) {
+    const Rec rec = col[r * (kStripCols + 1)];
+    if (r < H) rec_fields<T, Rec>(rec, gS[r], gH[r], s0[r], h0[r]);
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) cur[q][r] = node_from<T, Rec>(rec, tg[q]);
+  }
+  if (DO_H) {
+#pragma unroll
+    for (int r = 0; r < H; ++r)
+#pragma unroll
+      for (int q = 0; q < TPT; ++q) seg<T>(h0[r], cur[q][r], cur[q][r + 1], gH[r], acc[q][0], acc[q][1], acc[q][2]);
+  }
+  if (!FIRST) {
+#pragma unroll
+    for (int r = 0; r < H; ++r)
+#pragma unroll
+      for (int q = 0; q < TPT; ++q) seg<T>(ps0[r], prev[q][r], cur[q][r], pgS[r], acc[q][0], acc[q][1], acc[q][2]);
+  }
+#pragma unroll
+  for (int r = 0; r < H; ++r) {
+    pgS[r] = gS[r];
+    ps0[r] = s0[r];
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) prev[q][r] = cur[q][r];
+  }
+}
+
+// A full strip: compile-time bounds, no per-column predicates.  The last
+// column owns its chordwise segments only at the sheet's last column.
+template <class T, class Rec, int H, int TPT>
+__device__ __forceinline__ void walk_full_strip(const Rec* sm, bool last_h, const Tgt<T> (&tg)[TPT],
+                                                T (&acc)[TPT][3]) {
+  NodeV<T> prev[TPT][H];
+  SegV<T> ps0[H];
+  T pgS[H];
+  full_column<T, Rec, H, TPT, true, true>(sm, tg, prev, ps0, pgS, acc);
+#pragma unroll 2
+  for (int j = 1; j < kStripCols; ++j) full_column<T, Rec, H, TPT, false, true>(sm + j, tg, prev, ps0, pgS, acc);
+  if (last_h)
+    full_column<T, Rec, H, TPT, false, true>(sm + kStripCols, tg, prev, ps0, pgS, acc);
+  else
+    full_column<T, Rec, H, TPT, false, false>(sm + kStripCols, tg, prev, ps0, pgS, acc);
+}
+
+// Targets tile0 + threadIdx.x + q BLOCK (clamped to the last one) of the
+// SoA arrays, as hi/lo FP32 pairs or FP64.
+template <class T, int TPT, int BLOCK>
+__device__ __forceinline__ void load_targets(const double* __restrict__ tx, const double* __restrict__ ty,
+                                             const double* __restrict__ tz, long long base, long long tile0,
+                                             long long n_targets, Tgt<T> (&tg)[TPT]) {
+#pragma unroll
+  for (int q = 0; q < TPT; ++q) {
+    long long t = tile0 + threadIdx.x + (long long)q * BLOCK;
+    if (t >= n_targets) t = n_targets - 1;  // padded lanes recompute the last target
+    const double x = tx[base + t], y = ty[base + t], z = tz[base + t];
+    if constexpr (sizeof(T) == 4) {
+      tg[q].hx = (float)x; tg[q].hy = (float)y; tg[q].hz = (float)z;
+      tg[q].lx = (float)(x - (double)tg[q].hx);
+      tg[q].ly = (float)(y - (double)tg[q].hy);
+      tg[q].lz = (float)(z - (double)tg[q].hz);
+    } else {
+      tg[q].hx = x; tg[q].hy = y; tg[q].hz = z;
+      tg[q].lx = tg[q].ly = tg[q].lz = 0;
+    }
+  }
+}
+
+// Strips [s_begin, s_end) of B for the thread's targets, double-buffered
+// through shared memory; FP32 partial sums per strip, FP64 across strips.
+template <class T, class Rec, int H, int TPT, bool PAD>
+__device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, long long s_end,
+                                            const Rec* __restrict__ rec, Rec* buf0, Rec* buf1,
+                                            const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3]) {
+  if (s_begin >= s_end) return;
+  StripInfo si = decode_strip<H>(B, s_begin);
+  if constexpr (PAD)
+    stage_strip_padded<Rec, H>(buf0, rec, si);
+  else
+    stage_strip<Rec>(buf0, rec, si);
+  for (long long s = s_begin; s < s_end; ++s) {
+    Rec* cur = ((s - s_begin) & 1) ? buf1 : buf0;
+    Rec* nxt = ((s - s_begin) & 1) ? buf0 : buf1;
+    StripInfo sn;
+    const bool has_next = s + 1 < s_end;
+    if (has_next) {
+      sn = decode_strip<H>(B, s + 1);
+      if constexpr (PAD)
+        stage_strip_padded<Rec, H>(nxt, rec, sn);
+      else
+        stage_strip<Rec>(nxt, rec, sn);
+      asm volatile("cp.async.wait_group 1;");
+    } else {
+      asm volatile("cp.async.wait_group 0;");
+    }
+    __syncthreads();
+    T acc[TPT][3];
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = (T)0;
+    if constexpr (PAD)
+      walk_full_strip<T, Rec, H, TPT>(cur, si.last_h, tg, acc);
+    else
+      walk_strip<T, Rec, H, TPT>(cur, si, tg, acc);
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) {
+      accd[q][0] += (double)acc[q][0];
+      accd[q][1] += (double)acc[q][1];
+      accd[q][2] += (double)acc[q][2];
+    }
+    __syncthreads();  // everyone done with `cur` before it is refilled
+    if (has_next) si = sn;
+  }
+}
+
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD>
 __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
                                                        const double* __restrict__ tx, const double* __restrict__ ty,
                                                        const double* __restrict__ tz, long long n_targets,
@@ -262,55 +335,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   const long long tile0 = (long long)blockIdx.x * BLOCK * TPT;
   Tgt<T> tg[TPT];
   double accd[TPT][3];
+  load_targets<T, TPT, BLOCK>(tx, ty, tz, 0, tile0, n_targets, tg);
 #pragma unroll
-  for (int q = 0; q < TPT; ++q) {
-    long long t = tile0 + threadIdx.x + (long long)q * BLOCK;
-    if (t >= n_targets) t = n_targets - 1;  // padded lanes recompute the last target
-    const double x = tx[t], y = ty[t], z = tz[t];
-    if constexpr (sizeof(T) == 4) {
-      tg[q].hx = (float)x; tg[q].hy = (float)y; tg[q].hz = (float)z;
-      tg[q].lx = (float)(x - (double)tg[q].hx);
-      tg[q].ly = (float)(y - (double)tg[q].hy);
-      tg[q].lz = (float)(z - (double)tg[q].hz);
-    } else {
-      tg[q].hx = x; tg[q].hy = y; tg[q].hz = z;
-      tg[q].lx = tg[q].ly = tg[q].lz = 0;
-    }
-    accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
-  }
-
+  for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
   const long long s_begin = (long long)blockIdx.y * strips_per_split;
   const long long s_end = min(n_strips, s_begin + strips_per_split);
-  if (s_begin < s_end) {
-    StripInfo si = decode_strip<H>(B, s_begin);
-    stage_strip<Rec>(buf0, rec, si);
-    for (long long s = s_begin; s < s_end; ++s) {
-      Rec* cur = ((s - s_begin) & 1) ? buf1 : buf0;
-      Rec* nxt = ((s - s_begin) & 1) ? buf0 : buf1;
-      StripInfo sn;
-      const bool has_next = s + 1 < s_end;
-      if (has_next) {
-        sn = decode_strip<H>(B, s + 1);
-        stage_strip<Rec>(nxt, rec, sn);
-        asm volatile("cp.async.wait_group 1;");
-      } else {
-        asm volatile("cp.async.wait_group 0;");
-      }
-      __syncthreads();
-      T acc[TPT][3];
-#pragma unroll
-      for (int q = 0; q < TPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = (T)0;
-      walk_strip<T, Rec, H, TPT>(cur, si, tg, acc);
-#pragma unroll
-      for (int q = 0; q < TPT; ++q) {
-        accd[q][0] += (double)acc[q][0];
-        accd[q][1] += (double)acc[q][1];
-        accd[q][2] += (double)acc[q][2];
-      }
-      __syncthreads();  // everyone done with `cur` before it is refilled
-      if (has_next) si = sn;
-    }
-  }
+  eval_strips<T, Rec, H, TPT, PAD>(B, s_begin, s_end, rec, buf0, buf1, tg, accd);
   double* px = partial + (long long)blockIdx.y * 3 * n_targets;
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
@@ -322,6 +352,140 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
     }
   }
 }
+
+// ------------------------------------------------------ batched evaluation
+// Plans of all problems: strips, tiles, splits and the exclusive prefixes of
+// items, partial sums and targets.  One CTA; a blockwide scan in chunks.
+template <int H, int TPC>
+__global__ void __launch_bounds__(256) batch_plan_kernel(const NBodyBatchInput* __restrict__ in, int n,
+                                                         NBodyBatchPlan* __restrict__ plan, long long partial_cap,
+                                                         long long* totals, int* status) {
+  __shared__ long long sh[3][256];
+  __shared__ long long carry[3];
+  if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 256) {
+    const int c = base + threadIdx.x;
+    long long v[3] = {0, 0, 0};
+    NBodyBatchPlan p{};
+    if (c < n) {
+      const NBodyBatchInput& x = in[c];
+      p.n_strips = fill_blocks(p.B, x.blocks, x.n_blocks, H);
+      p.tgt_off = x.tgt_off;
+      p.n_tgt = x.n_tgt;
+      p.tiles = (x.n_tgt + TPC - 1) / TPC;
+      p.splits = (p.n_strips + kBatchStripsPerItem - 1) / kBatchStripsPerItem;
+      v[0] = p.tiles * p.splits;
+      v[1] = p.splits * 3 * x.n_tgt;
+      v[2] = x.n_tgt;
+    }
+    for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = v[k];
+    __syncthreads();
+    // Hillis-Steele inclusive scan of the three counters
+    for (int off = 1; off < 256; off <<= 1) {
+      long long t[3];
+      for (int k = 0; k < 3; ++k) t[k] = threadIdx.x >= off ? sh[k][threadIdx.x - off] : 0;
+      __syncthreads();
+      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += t[k];
+      __syncthreads();
+    }
+    if (c < n) {
+      p.item_off = carry[0] + sh[0][threadIdx.x] - v[0];
+      p.part_off = carry[1] + sh[1][threadIdx.x] - v[1];
+      p.tgt_prefix = carry[2] + sh[2][threadIdx.x] - v[2];
+      plan[c] = p;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) carry[threadIdx.x] += sh[threadIdx.x][255];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const bool fits = carry[1] <= partial_cap;
+    totals[0] = fits ? carry[0] : 0;
+    totals[1] = carry[1];
+    totals[2] = carry[2];
+    if (!fits) status[0] = 1;
+  }
+}
+
+// Last problem whose prefix (member at `Off`) is <= w.
+template <class F>
+__device__ inline int plan_search(const NBodyBatchPlan* plan, int n, long long w, F key) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (key(plan[mid]) <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBatchPlan* __restrict__ plan, int n,
+                                                             const long long* __restrict__ totals,
+                                                             const double* __restrict__ tx,
+                                                             const double* __restrict__ ty,
+                                                             const double* __restrict__ tz,
+                                                             const Rec* __restrict__ rec,
+                                                             double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
+  Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
+  const long long items = totals[0];
+  for (long long w = blockIdx.x; w < items; w += gridDim.x) {
+    const int c = plan_search(plan, n, w, [](const NBodyBatchPlan& p) { return p.item_off; });
+    const NBodyBatchPlan& P = plan[c];
+    const long long local = w - P.item_off;
+    const long long tile = local / P.splits, split = local % P.splits;
+    const long long tile0 = tile * BLOCK * TPT;
+    Tgt<T> tg[TPT];
+    double accd[TPT][3];
+    load_targets<T, TPT, BLOCK>(tx, ty, tz, P.tgt_off, tile0, P.n_tgt, tg);
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
+    const long long s_begin = split * kBatchStripsPerItem;
+    const long long s_end = min(P.n_strips, s_begin + kBatchStripsPerItem);
+    eval_strips<T, Rec, H, TPT, false>(P.B, s_begin, s_end, rec, buf0, buf1, tg, accd);
+    double* px = partial + P.part_off + split * 3 * P.n_tgt;
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) {
+      const long long t = tile0 + threadIdx.x + (long long)q * BLOCK;
+      if (t < P.n_tgt) {
+        px[t] = accd[q][0];
+        px[P.n_tgt + t] = accd[q][1];
+        px[2 * P.n_tgt + t] = accd[q][2];
+      }
+    }
+  }
+}
+
+__global__ void batch_reduce_kernel(const NBodyBatchPlan* __restrict__ plan, int n,
+                                    const long long* __restrict__ totals, const double* __restrict__ partial,
+                                    double* vx, double* vy, double* vz) {
+  const long long total = totals[2];
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int c = plan_search(plan, n, g, [](const NBodyBatchPlan& p) { return p.tgt_prefix; });
+    const NBodyBatchPlan& P = plan[c];
+    const long long t = g - P.tgt_prefix;
+    double x = 0, y = 0, z = 0;
+    for (long long s = 0; s < P.splits; ++s) {
+      const double* p = partial + P.part_off + s * 3 * P.n_tgt;
+      x += p[t];
+      y += p[P.n_tgt + t];
+      z += p[2 * P.n_tgt + t];
+    }
+    vx[P.tgt_off + t] = x;
+    vy[P.tgt_off + t] = y;
+    vz[P.tgt_off + t] = z;
+  }
+}
+
+// Batched tiles: FP32 h4 t2 b128 (3 CTAs/SM), FP64 h2 t1 b128 (3 CTAs/SM).
+constexpr int kBatchBlock = 128;
+constexpr int kBatchTptF = 2, kBatchHF = 4, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
 
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, int splits, long long n, double* vx,
                                        double* vy, double* vz) {
@@ -360,19 +524,33 @@ constexpr Variant kVariants[] = {
     {"fp64_h2_t2_b128", kNBodyFP64, 2, 2, 128, 1},
     {"fp64_h2_t1_b128_m3", kNBodyFP64, 2, 1, 128, 3},
     {"fp64_h2_t1_b256_m2", kNBodyFP64, 2, 1, 256, 2},
+    {"fp32_h3_t2_b128", kNBodyFP32, 3, 2, 128, 3},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+// Full-tile (padded) walking pays when the sheets fill most of the padded
+// columns: a sheet of C rings per row uses C + chunks of the chunks x
+// (kStripCols + 1) staged node columns.
+bool use_padded(const Blocks& B) {
+  for (int i = 0; i < B.n; ++i) {
+    const long long real = B.b[i].cols + B.chunks[i];
+    const long long staged = (long long)B.chunks[i] * (kStripCols + 1);
+    if (4 * real < 3 * staged) return false;
+  }
+  return true;
+}
 
 template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
 Error launch_variant(const Blocks& B, long long n_strips, const double* tx, const double* ty, const double* tz,
                      long long n_targets, const Rec* rec, NBodyWork* work, double* vx, double* vy, double* vz,
                      int num_sms, cudaStream_t st) {
-  auto kern = nbody_kernel<T, Rec, H, TPT, BLOCK, MINB>;
+  const bool pad = use_padded(B);
+  auto kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false>;
   const size_t smem = 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static bool attr_done[2] = {false, false};
+  if (!attr_done[pad]) {
     UVLM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_done = true;
+    attr_done[pad] = true;
   }
   int occ = 0;
   UVLM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, BLOCK, smem));
@@ -446,21 +624,7 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
     return fail(kErrInvalid, "nbody variant does not match precision");
   const Variant& V = kVariants[variant];
   Blocks B{};
-  B.n = 0;
-  long long strips = 0;
-  for (int i = 0; i < n_blocks && B.n < 4; ++i) {
-    const SourceBlock& sb = blocks[i];
-    if (sb.num <= 0 || sb.node_rows < 2 || sb.cols <= 0) continue;  // no rings -> no segments
-    B.b[B.n] = sb;
-    const int groups = (sb.node_rows + V.H - 1) / V.H;
-    const int chunks = (sb.cols + kStripCols - 1) / kStripCols;
-    B.chunks[B.n] = chunks;
-    B.strips_per_sheet[B.n] = groups * chunks;
-    B.strip_begin[B.n] = strips;
-    strips += (long long)sb.num * groups * chunks;
-    B.n++;
-  }
-  B.strip_begin[B.n] = strips;
+  const long long strips = fill_blocks(B, blocks, n_blocks, V.H);
   if (strips == 0) {
     UVLM_CUDA_TRY(cudaMemsetAsync(vx, 0, sizeof(double) * n_targets, st));
     UVLM_CUDA_TRY(cudaMemsetAsync(vy, 0, sizeof(double) * n_targets, st));
@@ -482,9 +646,85 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
     case 8: return launch_variant<double, RecD, 2, 2, 128, 1>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     case 9: return launch_variant<double, RecD, 2, 1, 128, 3>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     case 10: return launch_variant<double, RecD, 2, 1, 256, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 11: return launch_variant<float, RecF, 3, 2, 128, 3>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
     default: return fail(kErrInvalid, "bad nbody variant");
   }
 
+}
+
+}  // namespace uvlm
+
+namespace uvlm {
+
+void nbody_batch_shape(NBodyPrec prec, int* targets_per_cta, int* H) {
+  if (prec == kNBodyFP32) {
+    *targets_per_cta = kBatchBlock * kBatchTptF;
+    *H = kBatchHF;
+  } else {
+    *targets_per_cta = kBatchBlock * kBatchTptD;
+    *H = kBatchHD;
+  }
+}
+
+long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n) {
+  int tpc = 0, H = 0;
+  nbody_batch_shape(prec, &tpc, &H);
+  long long total = 0;
+  for (int c = 0; c < n; ++c) {
+    Blocks B{};
+    const long long strips = fill_blocks(B, in[c].blocks, in[c].n_blocks, H);
+    const long long splits = (strips + kBatchStripsPerItem - 1) / kBatchStripsPerItem;
+    total += splits * 3 * in[c].n_tgt;
+  }
+  return total;
+}
+
+namespace {
+template <class T, class Rec, int H, int TPT>
+void* batch_kernel_ptr() {
+  return (void*)batch_nbody_kernel<T, Rec, H, TPT, kBatchBlock, kBatchMinB>;
+}
+template <class Rec, int H>
+constexpr size_t batch_smem() {
+  return 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
+}
+}  // namespace
+
+int nbody_batch_grid(NBodyPrec prec, int num_sms) {
+  const void* k = prec == kNBodyFP32 ? batch_kernel_ptr<float, RecF, kBatchHF, kBatchTptF>()
+                                     : batch_kernel_ptr<double, RecD, kBatchHD, kBatchTptD>();
+  const size_t smem = prec == kNBodyFP32 ? batch_smem<RecF, kBatchHF>() : batch_smem<RecD, kBatchHD>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBatchBlock, smem) != cudaSuccess || occ < 1) occ = 1;
+  return num_sms * occ;
+}
+
+Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const double* tx, const double* ty,
+                       const double* tz, double* vx, double* vy, double* vz, const void* records, double* partial,
+                       long long partial_cap, NBodyBatchPlan* d_plan, long long* d_totals, int* status, int grid,
+                       cudaStream_t st) {
+  if (n <= 0) return ok();
+  if (prec == kNBodyFP32) {
+    batch_plan_kernel<kBatchHF, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, d_plan, partial_cap, d_totals,
+                                                                             status);
+    UVLM_LAUNCH_CHECK();
+    batch_nbody_kernel<float, RecF, kBatchHF, kBatchTptF, kBatchBlock, kBatchMinB>
+        <<<grid, kBatchBlock, batch_smem<RecF, kBatchHF>(), st>>>(d_plan, n, d_totals, tx, ty, tz,
+                                                                   reinterpret_cast<const RecF*>(records), partial);
+    UVLM_LAUNCH_CHECK();
+  } else {
+    batch_plan_kernel<kBatchHD, kBatchBlock * kBatchTptD><<<1, 256, 0, st>>>(d_in, n, d_plan, partial_cap, d_totals,
+                                                                             status);
+    UVLM_LAUNCH_CHECK();
+    batch_nbody_kernel<double, RecD, kBatchHD, kBatchTptD, kBatchBlock, kBatchMinB>
+        <<<grid, kBatchBlock, batch_smem<RecD, kBatchHD>(), st>>>(d_plan, n, d_totals, tx, ty, tz,
+                                                                   reinterpret_cast<const RecD*>(records), partial);
+    UVLM_LAUNCH_CHECK();
+  }
+  batch_reduce_kernel<<<grid, 256, 0, st>>>(d_plan, n, d_totals, partial, vx, vy, vz);
+  UVLM_LAUNCH_CHECK();
+  return ok();
 }
 
 }  // namespace uvlm

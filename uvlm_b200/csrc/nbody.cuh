@@ -85,6 +85,148 @@ struct NBodyWork {
   long long max_splits = 0;   // > 0: at most this many source splits (bounded scratch)
 };
 
+// ------------------------------------------------------------ record build
+__device__ inline double sheet_ring_gamma(const SheetView& v, int n, int i, int j) {
+  const int R = v.node_rows - 1;
+  if (i < 0 || i >= R || j < 0 || j >= v.cols) return 0.0;
+  return v.gamma[((long long)n * v.g_rows_alloc + v.g_row0 + i) * v.cols + j];
+}
+
+// Record k (sheet-major, row-major) of a sheet view: node position, the
+// spanwise S(i,j) and chordwise H(i,j) strengths and segment vectors.
+template <class Rec>
+__device__ inline Rec build_record(const SheetView& v, long long k) {
+  const double s = 1.0 / (4.0 * kPi);
+  const int C1 = v.cols + 1;
+  const int j = (int)(k % C1);
+  const long long nr = k / C1;
+  const int i = (int)(nr % v.node_rows);
+  const int n = (int)(nr / v.node_rows);
+  const double* p = v.pos + (((long long)n * v.rows_alloc + v.row0 + i) * C1 + j) * 3;
+  const int R = v.node_rows - 1;
+  const double gS = (j < v.cols) ? sheet_ring_gamma(v, n, i, j) - sheet_ring_gamma(v, n, i - 1, j) : 0.0;
+  const double gH =
+      (i < R && !v.spanwise_only) ? sheet_ring_gamma(v, n, i, j - 1) - sheet_ring_gamma(v, n, i, j) : 0.0;
+  double s0[3] = {0, 0, 0}, h0[3] = {0, 0, 0};
+  if (j < v.cols)
+    for (int d = 0; d < 3; ++d) s0[d] = p[3 + d] - p[d];
+  if (i < R)
+    for (int d = 0; d < 3; ++d) h0[d] = p[3 * C1 + d] - p[d];
+  Rec r;
+  if constexpr (sizeof(Rec) == sizeof(RecF)) {
+    const float hx = (float)p[0], hy = (float)p[1], hz = (float)p[2];
+    r.hi = make_float4(hx, hy, hz, (float)(gS * s));
+    r.lo = make_float4((float)(p[0] - (double)hx), (float)(p[1] - (double)hy), (float)(p[2] - (double)hz),
+                       (float)(gH * s));
+    r.sv = make_float4((float)s0[0], (float)s0[1], (float)s0[2], (float)h0[0]);
+    r.hv = make_float4((float)h0[1], (float)h0[2], 0.f, 0.f);
+  } else {
+    r.a = make_double4(p[0], p[1], p[2], gS * s);
+    r.b = make_double4(gH * s, s0[0], s0[1], s0[2]);
+    r.c = make_double4(h0[0], h0[1], h0[2], 0.0);
+  }
+  return r;
+}
+
+// ---------------------------------------------------------- strip decode
+struct StripInfo {
+  long long first;  // record index of node (i0, j0)
+  int row_stride;   // cols + 1
+  int n_rows;       // owned node rows
+  int nr;           // node rows loaded (n_rows + has_lower)
+  int n_cols;       // node columns in the chunk
+  bool last_h;      // owns the chordwise segments of its last column
+};
+
+// Source blocks of one evaluation cut into strips of H owned node rows x
+// kStripCols segment columns (sheet-major, row groups, column chunks).
+struct Blocks {
+  SourceBlock b[4];
+  int n;
+  int strips_per_sheet[4];
+  int chunks[4];
+  long long strip_begin[5];
+};
+
+// Fills B from the blocks that carry segments; returns the strip count.
+__host__ __device__ inline long long fill_blocks(Blocks& B, const SourceBlock* blocks, int n_blocks, int H) {
+  B.n = 0;
+  long long strips = 0;
+  for (int i = 0; i < n_blocks && B.n < 4; ++i) {
+    const SourceBlock& sb = blocks[i];
+    if (sb.num <= 0 || sb.node_rows < 2 || sb.cols <= 0) continue;  // no rings -> no segments
+    B.b[B.n] = sb;
+    const int groups = (sb.node_rows + H - 1) / H;
+    const int chunks = (sb.cols + kStripCols - 1) / kStripCols;
+    B.chunks[B.n] = chunks;
+    B.strips_per_sheet[B.n] = groups * chunks;
+    B.strip_begin[B.n] = strips;
+    strips += (long long)sb.num * groups * chunks;
+    B.n++;
+  }
+  B.strip_begin[B.n] = strips;
+  return strips;
+}
+
+template <int H>
+__device__ inline StripInfo decode_strip(const Blocks& B, long long s) {
+  int bi = 0;
+  while (bi + 1 < B.n && s >= B.strip_begin[bi + 1]) ++bi;
+  const SourceBlock& sb = B.b[bi];
+  const long long local = s - B.strip_begin[bi];
+  const int sps = B.strips_per_sheet[bi];
+  const int chunks = B.chunks[bi];
+  const int n = (int)(local / sps);
+  const int rem = (int)(local % sps);
+  const int g = rem / chunks, c = rem % chunks;
+  StripInfo si;
+  const int i0 = g * H, j0 = c * kStripCols;
+  si.n_rows = min(H, sb.node_rows - i0);
+  si.nr = si.n_rows + ((i0 + si.n_rows < sb.node_rows) ? 1 : 0);
+  si.n_cols = min(kStripCols, sb.cols - j0) + 1;
+  si.last_h = (j0 + si.n_cols - 1 == sb.cols);
+  si.row_stride = sb.cols + 1;
+  si.first = sb.rec_off + ((long long)n * sb.node_rows + i0) * (sb.cols + 1) + j0;
+  return si;
+}
+
+// ------------------------------------------------------ batched evaluation
+// Many independent problems in one persistent launch: problem c has its own
+// source blocks (records already built) and targets [tgt_off, tgt_off+n_tgt)
+// of the shared SoA target arrays; its velocities land at the same indices.
+// Work items = (problem, target tile, source split) with at most
+// kBatchStripsPerItem strips each; every CTA strides over the items, so the
+// launch shape is fixed while the problem sizes change from step to step.
+constexpr int kBatchStripsPerItem = 8;
+
+struct NBodyBatchInput {
+  SourceBlock blocks[2];
+  int n_blocks;
+  long long tgt_off, n_tgt;
+};
+
+struct NBodyBatchPlan {
+  Blocks B;
+  long long n_strips, tgt_off, n_tgt;
+  long long tiles, splits, item_off, part_off, tgt_prefix;
+};
+
+// Tile of the batched kernel for a precision (targets per CTA and H).
+void nbody_batch_shape(NBodyPrec prec, int* targets_per_cta, int* H);
+// Upper bound of the partial-sum doubles for the given inputs (host copy).
+long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n);
+// Persistent grid size used by nbody_batch_eval on this device.
+int nbody_batch_grid(NBodyPrec prec, int num_sms);
+
+// d_in: n problems on the device.  Plans on the device (one CTA), evaluates
+// with `grid` persistent CTAs and reduces the splits; d_plan holds n plans
+// and d_totals 4 counters.  status[0] is set non-zero when the partial
+// buffer is too small (nothing is evaluated then).
+Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const double* tx, const double* ty,
+                       const double* tz, double* vx, double* vy, double* vz, const void* records, double* partial,
+                       long long partial_cap, NBodyBatchPlan* d_plan, long long* d_totals, int* status, int grid,
+                       cudaStream_t st);
+
 int nbody_num_variants();
 int nbody_variant_prec(int v);
 const char* nbody_variant_name(int v);

@@ -495,7 +495,7 @@ int uvlm_dense_solve(const double* A, int64_t n, const double* b, double* x, int
       if (!e.code) e = gmres_work_alloc(&gw, N, 20);
       if (!e.code) {
         UVLM_CUDA_TRY(cudaMemset(dx, 0, sizeof(double) * N));
-        e = gmres_solve(nullptr, dA, N, F, &lu, db, dx, 1e-13, 200, &gw, &r, 0);
+        e = gmres_solve(nullptr, dA, N, F, &lu, nullptr, db, dx, 1e-13, 200, &gw, &r, 0);
       }
       if (!e.code) e = lu_check(&lu, 0);
       gmres_work_free(&gw);
