@@ -401,9 +401,10 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(const NBodyBatchInput* 
   }
   if (threadIdx.x == 0) {
     const bool fits = carry[1] <= partial_cap;
+    // an over-full plan evaluates and reduces nothing (the status reports it)
     totals[0] = fits ? carry[0] : 0;
     totals[1] = carry[1];
-    totals[2] = carry[2];
+    totals[2] = fits ? carry[2] : 0;
     if (!fits) status[0] = 1;
   }
 }
