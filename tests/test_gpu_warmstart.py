@@ -111,3 +111,39 @@ def test_learned_warm_start_gain_over_extrapolation():
     np.testing.assert_allclose(res["mlp"][2], res["extrapolate"][2], rtol=0, atol=1e-9)
     # the network's guess starts closer than the extrapolation
     assert res["mlp"][0] < res["extrapolate"][0]
+
+
+def test_shipped_weights_beat_extrapolation_on_the_workload():
+    """The committed network (trained on 20k plain-solver steps of seeded
+    heave/pitch variations, 32 x 128 rings) starts the GMRES solve of the
+    workload itself closer than the extrapolation, and the converged answer is
+    the same."""
+    import os
+
+    import uvlm_b200 as U
+    from uvlm_b200.warmstart import MLP
+
+    path = os.path.join(os.path.dirname(U.__file__), "weights", "warmstart_heave_pitch_32x128.npz")
+    net = MLP.load(path)
+    dt, steps = 2 * math.pi / 40, 40
+    res = {}
+    for warm in ("extrapolate", "mlp"):
+        sim = U.SimpleSimulator(precision="mixed", warm_start=warm)
+        if warm == "mlp":
+            sim.set_mlp(net)
+        m = U.Morphing().set_plug(0.2, 1.0).set_twist(math.radians(10), 1.0, math.pi / 2)
+        sim.AddWing(U.RectGenerator(), m, 1.0, 8.0, 32, 128)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.set_advection("RK2")
+        sim.begin()
+        r0, rows = [], []
+        for s in range(steps + 1):
+            rows.append(sim.step(s, dt))
+            if s >= 3:
+                r0.append(sim.stats().initial_residual)
+        res[warm] = (float(np.mean(r0)), np.array(rows))
+        sim.close()
+    print(f"initial relative residual on the workload: extrapolation {res['extrapolate'][0]:.3e}, "
+          f"MLP {res['mlp'][0]:.3e}")
+    assert res["mlp"][0] < 0.5 * res["extrapolate"][0]
+    np.testing.assert_allclose(res["mlp"][1], res["extrapolate"][1], rtol=0, atol=1e-9)
