@@ -45,38 +45,130 @@ OMEGA = 1.0  # k = 0.5, c = 1, U = 1
 DT = 2 * math.pi / OMEGA / 40
 WAKE_ROWS = 400
 FLOP_PER_PAIR = 59
-WEIGHTS = os.path.join(ROOT, "uvlm_b200", "weights", "warmstart_heave_pitch_32x128.npz")
 
 
-def make_mixed(device=0, warm_start="mlp"):
+def make_mixed(device=0, warm_start=None, wl=None):
     """The mixed-precision form: FP32 N-body, TF32 tensor-core LU factored
     once and used stale as the GMRES preconditioner (its dense inverse), FP64
-    residuals, learned warm start (weights trained on 20k plain-solver steps
-    of seeded variations of this workload, uvlm_b200/train_warmstart.py)."""
-    sim = make_sim("mixed", device=device, solver="gmres_stale", warm_start=warm_start)
+    residuals, learned warm start where the workload has trained weights
+    (trained on 20k plain-solver steps of seeded variations of the workload,
+    uvlm_b200/train_warmstart.py), else the extrapolation 2 g_n - g_{n-1}."""
+    wl = wl or _heave_pitch()
+    if warm_start is None:
+        warm_start = "mlp" if wl.weights and os.path.exists(wl.weights) else "extrapolate"
+    sim = wl.build("mixed", device=device, solver="gmres_stale", warm_start=warm_start)
     if warm_start == "mlp":
         from uvlm_b200.warmstart import MLP
 
-        sim.set_mlp(MLP.load(WEIGHTS))
+        sim.set_mlp(MLP.load(wl.weights))
     return sim
+
+
+class Workload:
+    """A SimpleSimulator set-up in the reference's terms: wings (RectGenerator
+    lattice, Morphing kinematics as closed-form sinusoids), forward flight,
+    advection scheme, dt, and the wake length held by erase_wake_after."""
+
+    def __init__(self, name, metric, description, wings, advection, dt, wake_rows, weights=None):
+        self.name, self.metric, self.description = name, metric, description
+        self.wings, self.advection, self.dt, self.wake_rows, self.weights = wings, advection, dt, wake_rows, weights
+        self.num = len(wings)
+        self.rows, self.cols = wings[0]["rows"], wings[0]["cols"]
+
+    def config(self):
+        return {"workload": self.description, "wings": self.num, "rows": self.rows, "cols": self.cols,
+                "wake_rings": self.wake_rows * self.cols * self.num, "dt": self.dt, "advection": self.advection,
+                "l2": "flushed between timed steps (256 MiB write)"}
+
+    def build(self, precision, **kw):
+        import uvlm_b200 as U
+
+        sim = U.SimpleSimulator(precision=precision, erase_wake_after=self.wake_rows,
+                                max_wake_rows=self.wake_rows + 8, **kw)
+        for w in self.wings:
+            m = U.Morphing()
+            k = w["kin"]
+            m.set_alpha(k.get("alpha", 0.0))
+            m.set_plug(k.get("plug_amp", 0.0), k.get("plug_omega", 0.0), k.get("plug_phase", 0.0))
+            m.set_twist(k.get("twist_amp", 0.0), k.get("twist_omega", 0.0), k.get("twist_phase", 0.0))
+            m.set_bend(k.get("bend_cx", 0.0), k.get("bend_cy", 0.0), k.get("bend_omega", 0.0),
+                       k.get("bend_phase", 0.0))
+            sim.AddWing(U.RectGenerator(), m, w["chord"], w["span"], w["rows"], w["cols"], w["origin"])
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.set_advection(self.advection)
+        return sim
+
+    def oracle(self):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as o
+
+        sim = o.Simulator()
+        for w in self.wings:
+            sim.add_wing(w["chord"], w["span"], w["rows"], w["cols"], origin=w["origin"], kin=o.kinematics(**w["kin"]))
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.set_advection(self.advection)
+        return sim
+
+    def advect_pairs(self):
+        """(target, unique segment) pairs of the advection stage at the held
+        wake: W + 1 ring rows before the erase, node rows 1..W+1 as targets."""
+        R, Cc, W = self.rows, self.cols, self.wake_rows + 1
+        segs = self.num * ((R + 1) * Cc + R * (Cc + 1) + (W + 1) * Cc + W * (Cc + 1))
+        evals = {"euler": 1, "RK2": 2, "RK4": 3, "AB2": 1}[self.advection]
+        return evals * self.num * W * (Cc + 1) * segs
+
+
+def _heave_pitch():
+    return Workload(
+        "heave_pitch", METRIC,
+        "single flapping wing 32x128 (4096 rings), heave 0.2 sin(wt) + pitch 10deg sin(wt+90deg), k=0.5, RK2, "
+        "wake held at 400 rows (51,200 rings) by erase_wake_after=400",
+        [dict(chord=CHORD, span=SPAN, rows=ROWS, cols=COLS, origin=(0.0, 0.0, 0.0),
+              kin=dict(plug_amp=0.2, plug_omega=OMEGA, twist_amp=math.radians(10), twist_omega=OMEGA,
+                       twist_phase=math.pi / 2))],
+        "RK2", DT, WAKE_ROWS,
+        weights=os.path.join(ROOT, "uvlm_b200", "weights", "warmstart_heave_pitch_32x128.npz"))
+
+
+def _tandem4():
+    # 2 x 2 tandem/biplane arrangement {x=0,1.5} x {z=0,0.5}: phases 0/90 deg
+    # for the front lower/upper wing and 180/270 deg for the rear pair, so
+    # biplane partners move a quarter period apart (in anti-phase their
+    # trailing edges cross and the core-free Biot-Savart diverges); k = 0.4
+    # (w = 0.8), heave 0.15 c, pitch 15 deg (90 deg ahead of the heave)
+    w, wings = 0.8, []
+    for q, (x, z) in enumerate([(0.0, 0.0), (0.0, 0.5), (1.5, 0.0), (1.5, 0.5)]):
+        ph = q * math.pi / 2
+        wings.append(dict(chord=1.0, span=4.0, rows=16, cols=64, origin=(x, 0.0, z),
+                          kin=dict(plug_amp=0.15, plug_omega=w, plug_phase=ph, twist_amp=math.radians(15),
+                                   twist_omega=w, twist_phase=ph + math.pi / 2)))
+    return Workload("tandem4", "UVLM steps/s (4 wings x 16x64 = 4096 panels, 77k wake), mixed vs plain FP64",
+                    "4 flapping wings 16x64 (chord 1, span 4) in a 2x2 tandem/biplane arrangement "
+                    "{x=0,1.5}x{z=0,0.5}, phases 0/90 (front) 180/270 deg (rear), k=0.4, heave 0.15 c, "
+                    "pitch 15 deg, RK2, wake held at 300 rows per wing (76,800 rings)", wings, "RK2",
+                    2 * math.pi / w / 40, 300)
+
+
+def _morphing():
+    # camber z = 0.05 sin(wt) x(1-x) and span bend 0.1 sin(wt) y^2, k = 0.3
+    w = 0.6
+    return Workload("morphing", "UVLM steps/s (24x96 morphing wing, 57.6k wake), mixed vs plain FP64",
+                    "morphing wing 24x96 (chord 1, span 8), camber 0.05 sin(wt) x(1-x) + span bend "
+                    "0.1 sin(wt) y^2, k=0.3, Euler, wake held at 600 rows (57,600 rings)",
+                    [dict(chord=1.0, span=8.0, rows=24, cols=96, origin=(0.0, 0.0, 0.0),
+                          kin=dict(bend_cx=0.05, bend_cy=0.1, bend_omega=w))],
+                    "euler", 2 * math.pi / w / 40, 600)
+
+
+WORKLOADS = {"heave_pitch": _heave_pitch, "tandem4": _tandem4, "morphing": _morphing}
 
 
 def workload_config():
-    return {"workload": "single flapping wing 32x128 (4096 rings), heave 0.2 sin(wt) + pitch 10deg sin(wt+90deg), "
-                        "k=0.5, RK2, wake held at 400 rows (51,200 rings) by erase_wake_after=400",
-            "rows": ROWS, "cols": COLS, "wake_rings": WAKE_ROWS * COLS, "dt": DT, "advection": "RK2",
-            "l2": "flushed between timed steps (256 MiB write)"}
+    return _heave_pitch().config()
 
 
-def make_sim(precision, **kw):
-    import uvlm_b200 as U
-
-    sim = U.SimpleSimulator(precision=precision, erase_wake_after=WAKE_ROWS, max_wake_rows=WAKE_ROWS + 8, **kw)
-    m = U.Morphing().set_plug(0.2, OMEGA).set_twist(math.radians(10), OMEGA, math.pi / 2)
-    sim.AddWing(U.RectGenerator(), m, CHORD, SPAN, ROWS, COLS, (0.0, 0.0, 0.0))
-    sim.set_forward_flight([-1.0, 0.0, 0.0])
-    sim.set_advection("RK2")
-    return sim
+def make_sim(precision, wl=None, **kw):
+    return (wl or _heave_pitch()).build(precision, **kw)
 
 
 class Clocks:
@@ -120,23 +212,15 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def oracle_sample(state, stride, lu_n, threads):
+def oracle_sample(wl, state, stride, lu_n, threads):
     """Time one MainLoop of the FP64 CPU oracle on a bounded sample."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as o
-
-    sim = o.Simulator()
-    kin = o.kinematics(plug_amp=0.2, plug_omega=OMEGA, twist_amp=math.radians(10), twist_omega=OMEGA,
-                       twist_phase=math.pi / 2)
-    sim.add_wing(CHORD, SPAN, ROWS, COLS, kin=kin)
-    sim.set_forward_flight([-1.0, 0.0, 0.0])
-    sim.set_advection("RK2")
+    sim = wl.oracle()
     sim.set_threads(threads)
     sim.begin()
     wr = state["wake_gamma"].shape[1]
     sim.set_state(wr, state["wing_pos"], state["wake_pos"], state["wing_gamma"], state["wing_gamma_prev"],
                   state["wake_gamma"])
-    sec = sim.time_step_sampled(WAKE_ROWS + 1, DT, stride, lu_n)
+    sec = sim.time_step_sampled(wl.wake_rows + 1, wl.dt, stride, lu_n)
     return float(np.sum(sec)), sec
 
 
@@ -197,10 +281,10 @@ def run_reference(args, rank, world):
     state = synthetic_state_np()
     stride, lu_n = 1024, 512
     for _ in range(args.warmup):
-        oracle_sample(state, stride, lu_n, threads)
+        oracle_sample(_heave_pitch(), state, stride, lu_n, threads)
     times = []
     for _ in range(args.steps):
-        t, _ = oracle_sample(state, stride, lu_n, threads)
+        t, _ = oracle_sample(_heave_pitch(), state, stride, lu_n, threads)
         times.append(t)
     value = args.steps / float(np.sum(times))
     sample = (f"one MainLoop per step at the 51,200-ring state: N-body stages (assembly, RHS, loads, RK2 advection) on "
@@ -240,49 +324,62 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
 
-    # --- accuracy run: both forms from step 0 to the 400-row wake ------------
-    sim64 = make_sim("fp64", device=dev)
-    simmx = make_mixed(dev)
-    simex = make_mixed(dev, warm_start="extrapolate")  # ablation: the method without the network
+    wl = WORKLOADS[args.workload]()
+    DT, WAKE_ROWS, ROWS, COLS = wl.dt, wl.wake_rows, wl.rows, wl.cols
+    # --- accuracy run: both forms from step 0 to the held wake ----------------
+    sim64 = wl.build("fp64", device=dev)
+    simmx = make_mixed(dev, wl=wl)
+    learned = simmx._cfg.warm_start == 2
+    # ablation: the method without the network
+    simex = make_mixed(dev, warm_start="extrapolate", wl=wl) if learned else None
     sim64.begin()
     simmx.begin()
-    simex.begin()
+    if simex:
+        simex.begin()
     cl64, clmx = [], []
     abl = {"mlp": ([], []), "extrapolate": ([], [])}
     t0 = time.time()
     for s in range(WAKE_ROWS + 1):
         cl64.append(sim64.step(s, DT))
         clmx.append(simmx.step(s, DT))
-        simex.step(s, DT)
+        if simex:
+            simex.step(s, DT)
         if s >= 3:
             for name, sm in (("mlp", simmx), ("extrapolate", simex)):
+                if sm is None:
+                    continue
                 st_ = sm.stats()
                 abl[name][0].append(st_.initial_residual)
                 abl[name][1].append(st_.gmres_iters)
-    simex.close()
+    if simex:
+        simex.close()
     preroll_s = time.time() - t0
     warm_ablation = {k: {"initial_residual_mean": float(np.mean(v[0])), "gmres_iters_total": int(np.sum(v[1])),
-                         "steps": len(v[1])} for k, v in abl.items()}
+                         "steps": len(v[1])} for k, v in abl.items() if v[1]}
     cl64, clmx = np.array(cl64), np.array(clmx)
-    cl_err = float(np.max(np.abs(clmx[:, 2] - cl64[:, 2])) / np.max(np.abs(cl64[:, 2])))
-    cd_err = float(np.max(np.abs(clmx[:, 1] - cl64[:, 1])) / np.max(np.abs(cl64[:, 1])))
+    CLc, CDc = list(range(2, 1 + 2 * wl.num, 2)), list(range(1, 1 + 2 * wl.num, 2))
+
+    def rel_err(a, b, cols, end=None):
+        # max over wings of max_t |a - b| / max_t |b|
+        return float(max(np.max(np.abs(a[:end, c] - b[:end, c])) / np.max(np.abs(b[:, c])) for c in cols))
+
+    cl_err = rel_err(clmx, cl64, CLc)
+    cd_err = rel_err(clmx, cl64, CDc)
     # rounding floor of the FP64 form itself: the same run with the forward
     # flight perturbed by one ulp (the wake roll-up amplifies any rounding)
     accuracy = {}
     if not args.no_floor:
-        simf = make_sim("fp64", device=dev)
+        simf = wl.build("fp64", device=dev)
         simf.set_forward_flight([-(1.0 + 2.0 ** -52), 0.0, 0.0])
         simf.begin()
         clf = np.array([simf.step(s, DT) for s in range(WAKE_ROWS + 1)])
         simf.close()
         accuracy["fp64_one_ulp_cl_rel_err"] = {}
     accuracy["mixed_cl_rel_err"] = {}
-    scale = np.max(np.abs(cl64[:, 2]))
-    for end in (50, 100, 200, 300, WAKE_ROWS + 1):
-        accuracy["mixed_cl_rel_err"][f"steps_0_{end - 1}"] = float(np.max(np.abs(clmx[:end, 2] - cl64[:end, 2])) / scale)
+    for end in sorted({e for e in (50, 100, 200, 300, 400, 600) if e < WAKE_ROWS + 1} | {WAKE_ROWS + 1}):
+        accuracy["mixed_cl_rel_err"][f"steps_0_{end - 1}"] = rel_err(clmx, cl64, CLc, end)
         if not args.no_floor:
-            accuracy["fp64_one_ulp_cl_rel_err"][f"steps_0_{end - 1}"] = float(
-                np.max(np.abs(clf[:end, 2] - cl64[:end, 2])) / scale)
+            accuracy["fp64_one_ulp_cl_rel_err"][f"steps_0_{end - 1}"] = rel_err(clf, cl64, CLc, end)
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
     step0 = WAKE_ROWS + 1
@@ -325,11 +422,7 @@ def run_ours(args, rank, world, local_rank):
     sim64.step(step0 - 1, DT)
     stage64 = [float(x) for x in sim64.stats().stage_ms]
     sim64.set_stage_timing(False)
-    C1 = COLS + 1
-    W = WAKE_ROWS + 1  # ring rows during the advect stage (before the erase)
-    segs_bound = (ROWS + 1) * COLS + ROWS * C1
-    segs_wake = (W + 1) * COLS + W * C1
-    pairs_advect = 2 * W * C1 * (segs_bound + segs_wake)
+    pairs_advect = wl.advect_pairs()
     adv_ms = stage_ms[5]
     achieved = FLOP_PER_PAIR * pairs_advect / (adv_ms * 1e-3) / 1e12
     peak = U._capi.c_double() if False else None
@@ -341,7 +434,7 @@ def run_ours(args, rank, world, local_rank):
 
     # --- end-to-end through the C-ABI with host buffers ------------------------
     e2e_t = []
-    gam = np.zeros((1, ROWS, COLS))
+    gam = np.zeros((wl.num, ROWS, COLS))
     for i in range(args.steps):
         t1 = time.perf_counter()
         simmx.step(step0 + i, DT)
@@ -356,22 +449,26 @@ def run_ours(args, rank, world, local_rank):
         state = simmx.state()
         threads = cpu_threads()
         stride, lu_n = 128, 1024
-        tcpu, secs = oracle_sample(state, stride, lu_n, threads)
+        tcpu, secs = oracle_sample(wl, state, stride, lu_n, threads)
+        n_panels = wl.num * ROWS * COLS
         cpu = {"value": 1.0 / tcpu, "unit": "steps/s", "cores": threads, "kind": "port",
-               "sample": (f"FP64 CPU oracle, one MainLoop at the 51,200-ring state: N-body stages on every "
-                          f"{stride}th target scaled x{stride}, FullPivLU on the leading {lu_n}^2 block scaled by "
-                          f"(4096/{lu_n})^3; stage seconds {[round(float(x), 3) for x in secs]}")}
+               "sample": (f"FP64 CPU oracle, one MainLoop at the {wl.num * WAKE_ROWS * COLS:,}-ring state: N-body "
+                          f"stages on every {stride}th target scaled x{stride}, FullPivLU on the leading {lu_n}^2 "
+                          f"block scaled by ({n_panels}/{lu_n})^3; stage seconds "
+                          f"{[round(float(x), 3) for x in secs]}")}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "metric": wl.metric, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_mx / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": dict(workload_config(), parallelism=f"replicas x{world}",
-                           form="mixed+learned: FP32 N-body, TF32 tcgen05 LU factored once (dense inverse "
-                                "as the GMRES preconditioner), FP64 matrix and residuals, MLP warm start"),
+            "config": dict(wl.config(), parallelism=f"replicas x{world}",
+                           form=("mixed+learned" if learned else "mixed") + ": FP32 N-body, TF32 tcgen05 LU "
+                                "factored once (dense inverse as the GMRES preconditioner), FP64 matrix and "
+                                "residuals, " + ("MLP warm start" if learned else "warm start 2 g_n - g_{n-1}")),
             "plain_fp64_steps_per_s": plain, "speedup_vs_plain_fp64": value / world / plain,
-            "cl_rel_err": cl_err, "cd_rel_err": cd_err, "cl_err_reference": "plain FP64 GPU form, same 400 steps",
+            "cl_rel_err": cl_err, "cd_rel_err": cd_err,
+            "cl_err_reference": f"plain FP64 GPU form, same {WAKE_ROWS} steps",
             "accuracy": accuracy, "warm_start_ablation": warm_ablation,
             "gmres_iters_last": int(st.gmres_iters), "solve_path_last": int(st.solve_path),
             "nbody_variant": U.lib().uvlm_nbody_variant_name(int(st.nbody_variant)).decode(),
@@ -380,13 +477,13 @@ def run_ours(args, rank, world, local_rank):
             "plain_fp64_stage_ms": {"kin_shed": stage64[0], "assembly": stage64[1], "rhs": stage64[2],
                                     "solve": stage64[3], "loads": stage64[4], "advect": stage64[5],
                                     "total": stage64[7]},
-            "roofline": {"bound": "fp32_simt", "kernel": "nbody_kernel (RK2 advection stage)",
+            "roofline": {"bound": "fp32_simt", "kernel": f"nbody_kernel ({wl.advection} advection stage)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "FP32 FMA probe on this GPU (uvlm_measure_fp32_peak)",
                          "per_unit": f"{FLOP_PER_PAIR} FLOP per (target, unique segment) pair",
                          "units_per_step": pairs_advect, "traffic": None},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 8 * (3 + ROWS * COLS),
+                    "d2h_bytes_per_step": 8 * (1 + 2 * wl.num + wl.num * ROWS * COLS),
                     "note": "wall clock per uvlm_step + circulation download; per-step inputs are scalars"},
             "gpu_launches": int(launches), "clocks": clk, "preroll_s": preroll_s,
             "cpu_baseline": cpu,
@@ -394,6 +491,63 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
     sim64.close()
     simmx.close()
+
+
+def run_batch(args):
+    """The 256-case seeded flapping-wing sweep (chordwise 4-16, spanwise 8-64,
+    AR 2-10, k 0.1-1, heave 0.05-0.3 c, pitch 0-20 deg, 150 Euler steps per
+    case) in one batch: aggregate case-steps/s over steps 1..149, device-timed
+    on the batch's stream; the FP64 batch beside it and the CL error of the
+    mixed batch against it."""
+    import torch
+
+    import uvlm_b200 as U
+    from uvlm_b200.batch import draw_cases, make_batch
+
+    cases = draw_cases(256, seed=0)
+    steps = 150
+    warm = make_batch(cases, precision="mixed", max_steps=args.warmup + 1)
+    warm.run(args.warmup + 1)  # module load, graph capture, first launches
+    warm.close()
+    out = {}
+    for prec in ("mixed", "fp64"):
+        sim = make_batch(cases, precision=prec, max_steps=steps)
+        sim.run(1)
+        stream = torch.cuda.ExternalStream(sim.stream(), device=0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        clocks = Clocks(0) if prec == "mixed" else None
+        if clocks:
+            clocks.start()
+        l0 = U.lib().uvlm_kernel_launch_count()
+        e0.record(stream)
+        sim.run(steps - 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = U.lib().uvlm_kernel_launch_count() - l0
+        clk = clocks.stop() if clocks else None
+        ms = e0.elapsed_time(e1)
+        out[prec] = dict(ms=ms, loads=sim.loads(), launches=launches, per_step=sim.launches_per_step(), clocks=clk,
+                         res=sim.solve_stats()[1])
+        sim.close()
+    L, L64 = out["mixed"]["loads"], out["fp64"]["loads"]
+    cl_err = float(np.max(np.abs(L[:, :, 2] - L64[:, :, 2]).max(axis=0) / np.abs(L64[:, :, 2]).max(axis=0)))
+    value = 256 * (steps - 1) / (out["mixed"]["ms"] * 1e-3)
+    line = {"metric": "case-steps/s (256 seeded flapping-wing cases x 150 steps, batched, mixed)", "value": value,
+            "unit": "case-steps/s", "n_gpus": 1, "steps": steps - 1, "warmup": args.warmup,
+            "ms_per_step": out["mixed"]["ms"] / (steps - 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "batch256: seed 0 draws, rows U{4..16}, even cols U{8..64}, AR U[2,10], "
+                                   "k U[0.1,1], heave U[0.05,0.3] c, pitch U[0,20] deg, phase 90 deg, Euler, "
+                                   "150 MainLoops each, all cases in one graph-replayed step",
+                       "panels_total": int(sum(d["rows"] * d["cols"] for d in cases)),
+                       "form": "FP32 N-body, per-case FP32 LU + FP64 refinement (residual <= 1e-12)"},
+            "plain_fp64_case_steps_per_s": 256 * (steps - 1) / (out["fp64"]["ms"] * 1e-3),
+            "cl_rel_err_max_over_cases": cl_err,
+            "refinement_residual_max": float(np.max(out["mixed"]["res"])),
+            "gpu_launches": int(out["mixed"]["launches"]), "launches_per_step": int(out["mixed"]["per_step"]),
+            "clocks": out["mixed"]["clocks"], "cpu_baseline": None}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -406,6 +560,8 @@ def main():
     ap.add_argument("--no-floor", action="store_true", help="skip the one-ulp FP64 rounding-floor run")
     ap.add_argument("--profile", action="store_true", help="one form on a synthesized state, for ncu")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"], help="form run by --profile")
+    ap.add_argument("--workload", default="heave_pitch", choices=list(WORKLOADS) + ["batch256"],
+                    help="heave_pitch (the metric's configuration, default), tandem4, morphing, batch256")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -416,6 +572,9 @@ def main():
         return
     if args.profile:
         run_profile(args)
+        return
+    if args.workload == "batch256":
+        run_batch(args)
         return
     if world > 1:
         import datetime

@@ -341,6 +341,8 @@ int uvlm_batch_get_case(const uvlm_batch* b, int32_t c, double* wing_pos, double
 int uvlm_batch_get_solve_stats(const uvlm_batch* b, int32_t* sweeps, double* residual);
 /* Kernels one step launches (nodes of the captured graph). */
 int uvlm_batch_launches_per_step(const uvlm_batch* b, int64_t* launches);
+/* The batch's CUDA stream (a cudaStream_t), for events around uvlm_batch_run. */
+void* uvlm_batch_stream(const uvlm_batch* b);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,23 @@ CASES = {
         wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
                     kin=dict(alpha=5 * DEG, plug_amp=0.1, plug_omega=1.0))],
         ff=(-1.0, 0.0, 0.0), advection="euler", dt=0.2, steps=14, erase_wake_after=8),
+    # the 4-wing tandem/biplane formation at small size: 2 x 2 arrangement
+    # {x=0,1.5} x {z=0,0.5}; phases 0/90 deg (front lower/upper) and 180/270
+    # deg (rear lower/upper), so biplane partners move a quarter period apart
+    # (in anti-phase their trailing edges cross and the core-free kernel
+    # diverges); heave 0.15 c + pitch 15 deg
+    "tandem4_rk2_3x6": dict(
+        wings=[dict(chord=1.0, span=4.0, rows=3, cols=6, origin=(x, 0.0, z),
+                    kin=dict(plug_amp=0.15, plug_omega=0.8, plug_phase=q * math.pi / 2, twist_amp=15 * DEG,
+                             twist_omega=0.8, twist_phase=q * math.pi / 2 + math.pi / 2))
+               for q, (x, z) in enumerate([(0.0, 0.0), (0.0, 0.5), (1.5, 0.0), (1.5, 0.5)])],
+        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / 0.8 / 40, steps=12),
+    # the morphing shape at small size: camber 0.05 sin(wt) x(1-x) + span bend
+    # 0.1 sin(wt) y^2, k = 0.3, Euler
+    "morph_camber_euler_4x8": dict(
+        wings=[dict(chord=1.0, span=8.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
+                    kin=dict(bend_cx=0.05, bend_cy=0.1, bend_omega=0.6))],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=2 * math.pi / 0.6 / 40, steps=16),
     "chebyshev_euler_4x8": dict(
         wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0), cheb_chord=True, cheb_span=True,
                     kin=dict(alpha=6 * DEG, plug_amp=0.05, plug_omega=1.5))],

@@ -147,6 +147,7 @@ SIGNATURES = [
     ("uvlm_batch_get_case", C.c_int, [_V, C.c_int32, _P, _P, _P, _P, C.POINTER(_I)]),
     ("uvlm_batch_get_solve_stats", C.c_int, [_V, C.POINTER(C.c_int32), _P]),
     ("uvlm_batch_launches_per_step", C.c_int, [_V, C.POINTER(_I)]),
+    ("uvlm_batch_stream", _V, [_V]),
 ]
 
 _lib = None

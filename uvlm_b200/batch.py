@@ -128,6 +128,10 @@ class BatchSimulator:
         _check(lib().uvlm_batch_launches_per_step(self._h, C.byref(v)), self._h)
         return v.value
 
+    def stream(self) -> int:
+        """The batch's cudaStream_t as an integer handle."""
+        return lib().uvlm_batch_stream(self._h)
+
     def close(self) -> None:
         if self._h is not None:
             lib().uvlm_batch_destroy(self._h)

@@ -1170,4 +1170,6 @@ int uvlm_batch_launches_per_step(const uvlm_batch* b, int64_t* launches) {
   return UVLM_OK;
 }
 
+void* uvlm_batch_stream(const uvlm_batch* b) { return b ? (void*)b->st : nullptr; }
+
 }  // extern "C"
