@@ -133,6 +133,7 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
   };
   double bnorm = 0;
   UVLM_TRY(norm2(b, &bnorm));
+  if (!std::isfinite(bnorm)) return fail(kErrNonFinite, "non-finite right-hand side");
   if (!(bnorm > 0)) {
     UVLM_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
     res->converged = true;

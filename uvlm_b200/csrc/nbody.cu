@@ -63,7 +63,7 @@ struct Tgt {
 template <class T>
 struct NodeV {
   T rx, ry, rz;  // x - p
-  T ux, uy, uz;  // (x - p)/|x - p|  (NaN/inf lanes when x == p are cut by |d|^2)
+  T n;           // |x - p| (0 when x == p; such pairs are cut by |d|^2)
 };
 
 __device__ __forceinline__ float nb_rsqrt(float x) {
@@ -84,18 +84,14 @@ __device__ __forceinline__ NodeV<T> node_from(const Rec& r, const Tgt<T>& t) {
     n.rx = (t.hx - r.hi.x) + (t.lx - r.lo.x);
     n.ry = (t.hy - r.hi.y) + (t.ly - r.lo.y);
     n.rz = (t.hz - r.hi.z) + (t.lz - r.lo.z);
-    const float inv = nb_rsqrt(n.rx * n.rx + n.ry * n.ry + n.rz * n.rz);
-    n.ux = n.rx * inv;
-    n.uy = n.ry * inv;
-    n.uz = n.rz * inv;
+    const float q = n.rx * n.rx + n.ry * n.ry + n.rz * n.rz;
+    n.n = q >= (float)kCutR2 ? q * nb_rsqrt(q) : 0.f;  // |x - p| < 1e-10: marked 0 for the node cut
   } else {
     n.rx = t.hx - r.a.x;
     n.ry = t.hy - r.a.y;
     n.rz = t.hz - r.a.z;
-    const double inv = rsqrt(n.rx * n.rx + n.ry * n.ry + n.rz * n.rz);
-    n.ux = n.rx * inv;
-    n.uy = n.ry * inv;
-    n.uz = n.rz * inv;
+    const double q = n.rx * n.rx + n.ry * n.ry + n.rz * n.rz;
+    n.n = q >= kCutR2 ? q * rsqrt(q) : 0.0;
   }
   return n;
 }
@@ -120,11 +116,21 @@ __device__ __forceinline__ void rec_fields(const Rec& r, T& gS, T& gH, SegV<T>& 
   }
 }
 
-// Segment start=A -> end=B at x (src/vortex.cpp:24-38): r0 = B - A, r1 = x - A,
-// d = r0 x r1 (= r1 x r2), K = g r0.(u1 - u2) / |d|^2, cut when |d|^2 < 1e-10.
-// |x - A| < 1e-10 or |x - B| < 1e-10 implies |d|^2 < 1e-10 for |x - p| < 1e5,
-// so the reference's node cut-off is contained in the |d|^2 test (and the
-// select also discards the NaN that rsqrt(0) produces in u).
+// Segment start=A -> end=B at x (src/vortex.cpp:24-38): r1 = x - A,
+// r2 = x - B, r0 = B - A, d = r1 x r2 = r0 x r1 and the reference's factor
+// F = r0.(r1/|r1| - r2/|r2|) / |d|^2.  F is evaluated in forms that are
+// algebraically equal to it but free of cancellation:
+//   r1.r2 >= 0 (x beyond an end):  F = (|r1| + |r2|) / (|r1||r2| (|r1||r2| + r1.r2))
+//   r1.r2 <  0 (x alongside):      F = (|r1| + |r2|) (|r1||r2| - r1.r2) / (|r1||r2| |d|^2)
+// (the second from |r1|^2|r2|^2 - (r1.r2)^2 = |d|^2).  The reference form
+// subtracts two nearly equal unit vectors when x is near the extension of the
+// segment, which is where every wake node sees its lattice neighbours; in FP32
+// that costs up to O(1) relative error there (1e-7 .. 1e-4 with these forms).
+// Cut, as the reference does, when |d|^2 < 1e-10 or |x - A| < 1e-10 or
+// |x - B| < 1e-10 (node_from marks such nodes with n = 0).  The node test is
+// not implied by the |d|^2 test in FP32: for a stretched wake segment
+// (|r0| ~ 10) whose end node is the target itself, the once-rounded r0 and
+// x - A differ by an ulp and leave |d|^2 just above 1e-10.
 template <class T>
 __device__ __forceinline__ void seg(const SegV<T>& r0, const NodeV<T>& a, const NodeV<T>& b, T g, T& vx, T& vy,
                                     T& vz) {
@@ -132,14 +138,18 @@ __device__ __forceinline__ void seg(const SegV<T>& r0, const NodeV<T>& a, const 
   const T dy = r0.z * a.rx - r0.x * a.rz;
   const T dz = r0.x * a.ry - r0.y * a.rx;
   const T d2 = dx * dx + dy * dy + dz * dz;
-  const T dot = r0.x * (a.ux - b.ux) + r0.y * (a.uy - b.uy) + r0.z * (a.uz - b.uz);
+  const T dot12 = a.rx * b.rx + a.ry * b.ry + a.rz * b.rz;
+  const T nn = a.n * b.n;
+  const bool beyond = dot12 >= (T)0;
+  const T num = (a.n + b.n) * (beyond ? (T)1 : nn - dot12);
+  const T den = nn * (beyond ? nn + dot12 : d2);
   T k;
   if constexpr (sizeof(T) == 4) {
-    k = g * dot * nb_rcp(d2);
+    k = g * num * nb_rcp(den);
   } else {
-    k = g * dot * __drcp_rn(d2);
+    k = g * num * __drcp_rn(den);
   }
-  k = (d2 < (T)kCutD2) ? (T)0 : k;
+  k = (d2 >= (T)kCutD2 && nn > (T)0) ? k : (T)0;
   vx += k * dx;
   vy += k * dy;
   vz += k * dz;
