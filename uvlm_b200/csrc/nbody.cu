@@ -264,6 +264,108 @@ __device__ __forceinline__ void walk_full_strip(const Rec* sm, bool last_h, cons
     full_column<T, Rec, H, TPT, false, false>(sm + kStripCols, tg, prev, ps0, pgS, acc);
 }
 
+// ------------------------------------------------ packed FP32x2 walker
+// The same arithmetic for the thread's two targets at once: lane .x is
+// target 0, lane .y target 1, and every add/mul/fma is one sm_100 FP32x2
+// instruction (__fadd2_rn / __fmul2_rn / __ffma2_rn) instead of two.  The
+// reciprocal square roots, reciprocals and the per-lane selects stay scalar.
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+struct Node2 {
+  float2 rx, ry, rz, n;
+};
+
+__device__ __forceinline__ float node_len(float q) { return q >= (float)kCutR2 ? q * nb_rsqrt(q) : 0.f; }
+
+__device__ __forceinline__ Node2 node_from2(const RecF& r, const Tgt<float> (&tg)[2]) {
+  const float2 thx = make_float2(tg[0].hx, tg[1].hx), thy = make_float2(tg[0].hy, tg[1].hy),
+               thz = make_float2(tg[0].hz, tg[1].hz);
+  const float2 tlx = make_float2(tg[0].lx, tg[1].lx), tly = make_float2(tg[0].ly, tg[1].ly),
+               tlz = make_float2(tg[0].lz, tg[1].lz);
+  Node2 n;
+  n.rx = add2(add2(thx, bc2(-r.hi.x)), add2(tlx, bc2(-r.lo.x)));
+  n.ry = add2(add2(thy, bc2(-r.hi.y)), add2(tly, bc2(-r.lo.y)));
+  n.rz = add2(add2(thz, bc2(-r.hi.z)), add2(tlz, bc2(-r.lo.z)));
+  const float2 q = fma2(n.rz, n.rz, fma2(n.ry, n.ry, mul2(n.rx, n.rx)));
+  n.n = make_float2(node_len(q.x), node_len(q.y));
+  return n;
+}
+
+// seg() for both lanes (same forms, same cut-offs).
+__device__ __forceinline__ void seg2(const SegV<float>& r0, const Node2& a, const Node2& b, float g, float2& vx,
+                                     float2& vy, float2& vz) {
+  const float2 dx = fma2(bc2(r0.y), a.rz, mul2(bc2(-r0.z), a.ry));
+  const float2 dy = fma2(bc2(r0.z), a.rx, mul2(bc2(-r0.x), a.rz));
+  const float2 dz = fma2(bc2(r0.x), a.ry, mul2(bc2(-r0.y), a.rx));
+  const float2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+  const float2 dot12 = fma2(a.rz, b.rz, fma2(a.ry, b.ry, mul2(a.rx, b.rx)));
+  const float2 nn = mul2(a.n, b.n);
+  const float2 sn = add2(a.n, b.n);
+  const float2 tp = add2(nn, dot12);
+  const float2 tm = fma2(dot12, bc2(-1.f), nn);
+  const bool bx = dot12.x >= 0.f, by = dot12.y >= 0.f;
+  const float2 num = mul2(sn, make_float2(bx ? 1.f : tm.x, by ? 1.f : tm.y));
+  const float2 den = mul2(nn, make_float2(bx ? tp.x : d2.x, by ? tp.y : d2.y));
+  float2 k = mul2(mul2(bc2(g), num), make_float2(nb_rcp(den.x), nb_rcp(den.y)));
+  k.x = (d2.x >= (float)kCutD2 && nn.x > 0.f) ? k.x : 0.f;
+  k.y = (d2.y >= (float)kCutD2 && nn.y > 0.f) ? k.y : 0.f;
+  vx = fma2(k, dx, vx);
+  vy = fma2(k, dy, vy);
+  vz = fma2(k, dz, vz);
+}
+
+template <int H, bool FIRST, bool DO_H>
+__device__ __forceinline__ void full_column2(const RecF* col, const Tgt<float> (&tg)[2], Node2 (&prev)[H],
+                                             SegV<float> (&ps0)[H], float (&pgS)[H], float2 (&acc)[3]) {
+  Node2 cur[H + 1];
+  float gS[H], gH[H];
+  SegV<float> s0[H], h0[H];
+#pragma unroll
+  for (int r = 0; r <= H; ++r) {
+    const RecF rec = col[r * (kStripCols + 1)];
+    if (r < H) rec_fields<float, RecF>(rec, gS[r], gH[r], s0[r], h0[r]);
+    cur[r] = node_from2(rec, tg);
+  }
+  if (DO_H) {
+#pragma unroll
+    for (int r = 0; r < H; ++r) seg2(h0[r], cur[r], cur[r + 1], gH[r], acc[0], acc[1], acc[2]);
+  }
+  if (!FIRST) {
+#pragma unroll
+    for (int r = 0; r < H; ++r) seg2(ps0[r], prev[r], cur[r], pgS[r], acc[0], acc[1], acc[2]);
+  }
+#pragma unroll
+  for (int r = 0; r < H; ++r) {
+    pgS[r] = gS[r];
+    ps0[r] = s0[r];
+    prev[r] = cur[r];
+  }
+}
+
+template <int H>
+__device__ __forceinline__ void walk_full_strip2(const RecF* sm, bool last_h, const Tgt<float> (&tg)[2],
+                                                 float (&acc)[2][3]) {
+  Node2 prev[H];
+  SegV<float> ps0[H];
+  float pgS[H];
+  float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  full_column2<H, true, true>(sm, tg, prev, ps0, pgS, a2);
+#pragma unroll 2
+  for (int j = 1; j < kStripCols; ++j) full_column2<H, false, true>(sm + j, tg, prev, ps0, pgS, a2);
+  if (last_h)
+    full_column2<H, false, true>(sm + kStripCols, tg, prev, ps0, pgS, a2);
+  else
+    full_column2<H, false, false>(sm + kStripCols, tg, prev, ps0, pgS, a2);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    acc[0][c] += a2[c].x;
+    acc[1][c] += a2[c].y;
+  }
+}
+
 // Targets tile0 + threadIdx.x + q BLOCK (clamped to the last one) of the
 // SoA arrays, as hi/lo FP32 pairs or FP64.
 template <class T, int TPT, int BLOCK>
@@ -289,7 +391,7 @@ __device__ __forceinline__ void load_targets(const double* __restrict__ tx, cons
 
 // Strips [s_begin, s_end) of B for the thread's targets, double-buffered
 // through shared memory; FP32 partial sums per strip, FP64 across strips.
-template <class T, class Rec, int H, int TPT, bool PAD>
+template <class T, class Rec, int H, int TPT, bool PAD, bool PK = false>
 __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, long long s_end,
                                             const Rec* __restrict__ rec, Rec* buf0, Rec* buf1,
                                             const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3]) {
@@ -318,7 +420,9 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
     T acc[TPT][3];
 #pragma unroll
     for (int q = 0; q < TPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = (T)0;
-    if constexpr (PAD)
+    if constexpr (PAD && PK && sizeof(T) == 4 && TPT == 2)
+      walk_full_strip2<H>(cur, si.last_h, tg, acc);
+    else if constexpr (PAD)
       walk_full_strip<T, Rec, H, TPT>(cur, si.last_h, tg, acc);
     else
       walk_strip<T, Rec, H, TPT>(cur, si, tg, acc);
@@ -333,7 +437,7 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
   }
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, bool PK>
 __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
                                                        const double* __restrict__ tx, const double* __restrict__ ty,
                                                        const double* __restrict__ tz, long long n_targets,
@@ -350,7 +454,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
   const long long s_begin = (long long)blockIdx.y * strips_per_split;
   const long long s_end = min(n_strips, s_begin + strips_per_split);
-  eval_strips<T, Rec, H, TPT, PAD>(B, s_begin, s_end, rec, buf0, buf1, tg, accd);
+  eval_strips<T, Rec, H, TPT, PAD, PK>(B, s_begin, s_end, rec, buf0, buf1, tg, accd);
   double* px = partial + (long long)blockIdx.y * 3 * n_targets;
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
@@ -519,23 +623,27 @@ struct Variant {
   const char* name;
   int prec;  // NBodyPrec
   int H, TPT, BLOCK, MINB;
+  int packed;  // FP32x2 walker for full strips (FP32, TPT = 2)
 };
 
 // Tile shapes: H owned node rows per strip, TPT targets per thread, BLOCK
 // threads, MINB resident CTAs per SM requested from the register allocator.
 constexpr Variant kVariants[] = {
-    {"fp64_h4_t1_b128", kNBodyFP64, 4, 1, 128, 1},
-    {"fp64_h2_t1_b256", kNBodyFP64, 2, 1, 256, 1},
-    {"fp32_h4_t1_b256", kNBodyFP32, 4, 1, 256, 2},
-    {"fp32_h4_t2_b128", kNBodyFP32, 4, 2, 128, 3},
-    {"fp32_h2_t2_b128", kNBodyFP32, 2, 2, 128, 3},
-    {"fp32_h4_t1_b128_m4", kNBodyFP32, 4, 1, 128, 4},
-    {"fp32_h3_t2_b128_m4", kNBodyFP32, 3, 2, 128, 4},
-    {"fp32_h2_t1_b256_m3", kNBodyFP32, 2, 1, 256, 3},
-    {"fp64_h2_t2_b128", kNBodyFP64, 2, 2, 128, 1},
-    {"fp64_h2_t1_b128_m3", kNBodyFP64, 2, 1, 128, 3},
-    {"fp64_h2_t1_b256_m2", kNBodyFP64, 2, 1, 256, 2},
-    {"fp32_h3_t2_b128", kNBodyFP32, 3, 2, 128, 3},
+    {"fp64_h4_t1_b128", kNBodyFP64, 4, 1, 128, 1, 0},
+    {"fp64_h2_t1_b256", kNBodyFP64, 2, 1, 256, 1, 0},
+    {"fp32_h4_t1_b256", kNBodyFP32, 4, 1, 256, 2, 0},
+    {"fp32_h4_t2_b128", kNBodyFP32, 4, 2, 128, 3, 0},
+    {"fp32_h2_t2_b128", kNBodyFP32, 2, 2, 128, 3, 0},
+    {"fp32_h4_t1_b128_m4", kNBodyFP32, 4, 1, 128, 4, 0},
+    {"fp32_h3_t2_b128_m4", kNBodyFP32, 3, 2, 128, 4, 0},
+    {"fp32_h2_t1_b256_m3", kNBodyFP32, 2, 1, 256, 3, 0},
+    {"fp64_h2_t2_b128", kNBodyFP64, 2, 2, 128, 1, 0},
+    {"fp64_h2_t1_b128_m3", kNBodyFP64, 2, 1, 128, 3, 0},
+    {"fp64_h2_t1_b256_m2", kNBodyFP64, 2, 1, 256, 2, 0},
+    {"fp32_h3_t2_b128", kNBodyFP32, 3, 2, 128, 3, 0},
+    {"fp32_h4_t2_b128_x2", kNBodyFP32, 4, 2, 128, 3, 1},
+    {"fp32_h3_t2_b128_x2", kNBodyFP32, 3, 2, 128, 3, 1},
+    {"fp32_h2_t2_b128_x2", kNBodyFP32, 2, 2, 128, 3, 1},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -551,12 +659,12 @@ bool use_padded(const Blocks& B) {
   return true;
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PK = false>
 Error launch_variant(const Blocks& B, long long n_strips, const double* tx, const double* ty, const double* tz,
                      long long n_targets, const Rec* rec, NBodyWork* work, double* vx, double* vy, double* vz,
                      int num_sms, cudaStream_t st) {
   const bool pad = use_padded(B);
-  auto kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false>;
+  auto kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false, PK>;
   const size_t smem = 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
   static bool attr_done[2] = {false, false};
   if (!attr_done[pad]) {
@@ -658,6 +766,9 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
     case 9: return launch_variant<double, RecD, 2, 1, 128, 3>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     case 10: return launch_variant<double, RecD, 2, 1, 256, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     case 11: return launch_variant<float, RecF, 3, 2, 128, 3>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 12: return launch_variant<float, RecF, 4, 2, 128, 3, true>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 13: return launch_variant<float, RecF, 3, 2, 128, 3, true>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 14: return launch_variant<float, RecF, 2, 2, 128, 3, true>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
     default: return fail(kErrInvalid, "bad nbody variant");
   }
 
