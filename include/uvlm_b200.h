@@ -302,7 +302,7 @@ typedef struct uvlm_batch uvlm_batch;
 
 typedef struct {
   double chord, span;
-  int64_t rows, cols;        /* rings chordwise x spanwise (cols even, <= 64 x 64 per case) */
+  int64_t rows, cols;        /* rings chordwise x spanwise (cols even; rows, cols <= 64, rows*cols <= 1024) */
   double origin[3];          /* wing origin (also the Morphing origin) */
   double forward_flight[3];  /* SimpleSimulator::set_forward_flight */
   double dt;                 /* this case's time step; t = step * dt */

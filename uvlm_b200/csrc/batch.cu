@@ -271,71 +271,50 @@ __global__ void b_rhs_kernel(const BCase* __restrict__ cs, BPrefix P, int n, con
 
 // ------------------------------------------------------------- dense solve
 constexpr int kSolveThreads = 256;
-constexpr int kSolveNB = 32;
 
+// Panel width of the shared-memory LU: 32 FP32 / 16 FP64 columns, so that
+// the whole panel of the largest case (1024 rows) stays in shared memory.
 template <class T>
-__device__ void cta_gemm_update(T* A, int N, int k0, int kb, int c0) {
-  __shared__ T As[kSolveNB][64];
-  __shared__ T Bs[kSolveNB][64];
-  const int m = N - c0;
-  const int tiles = (m + 63) / 64;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  for (int t = 0; t < tiles * tiles; ++t) {
-    const int r0 = c0 + (t / tiles) * 64, q0 = c0 + (t % tiles) * 64;
-    for (int q = tid; q < 64 * kSolveNB; q += kSolveThreads) {
-      const int r = q / kSolveNB, l = q % kSolveNB;
-      As[l][r] = (r0 + r < N && l < kb) ? A[(long long)(r0 + r) * N + k0 + l] : (T)0;
-      const int l2 = q / 64, cc = q % 64;
-      Bs[l2][cc] = (q0 + cc < N && l2 < kb) ? A[(long long)(k0 + l2) * N + q0 + cc] : (T)0;
-    }
-    __syncthreads();
-    T acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
-    for (int l = 0; l < kb; ++l) {
-      T a[4], bb[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[l][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bb[j] = Bs[l][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * bb[j];
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = r0 + ty * 4 + i;
-      if (r >= N) continue;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int cc = q0 + tx * 4 + j;
-        if (cc < N) A[(long long)r * N + cc] -= acc[i][j];
-      }
-    }
-    __syncthreads();
-  }
+struct PanelCfg {
+  static constexpr int NB = sizeof(T) == 4 ? 32 : 16;
+  static constexpr int LD = NB + 1;  // padded row (conflict-free column walks)
+};
+
+inline size_t panel_smem_bytes(int max_N, int elem) {
+  const int nb = elem == 4 ? 32 : 16;
+  return (size_t)max_N * (nb + 1) * elem;
 }
 
 // Right-looking blocked LU with partial pivoting of the row-major N x N
-// matrix A by one CTA (panel width 32; the pivot of column j is the largest
-// |a| at or below the diagonal, ties to the lower index; rows are swapped
-// across the whole matrix as LAPACK does).  piv[j] = row swapped with j.
+// matrix A by one CTA.  Each panel of NB columns is held in shared memory
+// while it is factored (the pivot of column j is the largest |a| at or below
+// the diagonal, ties to the lower index; pivot search, swaps, scaling and the
+// rank-1 updates walk shared memory instead of strided rows in L2).  The
+// panel's row swaps are then applied to the other columns (LAPACK order),
+// U12 = L11^-1 A12 is solved column per thread with L11 from shared memory,
+// and A22 -= L21 U12 reads L21 from shared memory.  piv[j] = row swapped
+// with j.  P: (N - k0) x LD panel buffer in dynamic shared memory.
 template <class T>
-__device__ void cta_lu(T* A, int N, int* piv, int* status) {
+__device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
+  constexpr int NB = PanelCfg<T>::NB, LD = PanelCfg<T>::LD;
   __shared__ double s_val[kSolveThreads / 32];
   __shared__ int s_idx[kSolveThreads / 32];
-  __shared__ int s_piv;
+  __shared__ int s_piv[NB];
+  __shared__ T Bs[NB][64];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int k0 = 0; k0 < N; k0 += kSolveNB) {
-    const int kb = min(kSolveNB, N - k0);
-    for (int j = k0; j < k0 + kb; ++j) {
+  for (int k0 = 0; k0 < N; k0 += NB) {
+    const int kb = min(NB, N - k0);
+    const int m = N - k0;
+    for (int q = tid; q < m * NB; q += kSolveThreads) {
+      const int r = q / NB, c = q % NB;
+      P[r * LD + c] = c < kb ? A[(long long)(k0 + r) * N + k0 + c] : (T)0;
+    }
+    __syncthreads();
+    for (int jj = 0; jj < kb; ++jj) {
       double best = -1.0;
-      int bi = j;
-      for (int i = j + tid; i < N; i += kSolveThreads) {
-        const double v = fabs((double)A[(long long)i * N + j]);
+      int bi = jj;
+      for (int i = jj + tid; i < m; i += kSolveThreads) {
+        const double v = fabs((double)P[i * LD + jj]);
         if (v > best) {
           best = v;
           bi = i;
@@ -362,40 +341,109 @@ __device__ void cta_lu(T* A, int N, int* piv, int* status) {
             bv = s_val[w];
             ii = s_idx[w];
           }
-        s_piv = ii;
-        piv[j] = ii;
+        s_piv[jj] = ii;
+        piv[k0 + jj] = k0 + ii;
         if (!(bv > 0)) status[1] = 1;
       }
       __syncthreads();
-      const int p = s_piv;
-      if (p != j)
-        for (int c = tid; c < N; c += kSolveThreads) {
-          const T t = A[(long long)j * N + c];
-          A[(long long)j * N + c] = A[(long long)p * N + c];
-          A[(long long)p * N + c] = t;
-        }
+      const int p = s_piv[jj];
+      if (p != jj && tid < NB) {
+        const T t = P[jj * LD + tid];
+        P[jj * LD + tid] = P[p * LD + tid];
+        P[p * LD + tid] = t;
+      }
       __syncthreads();
-      const T d = A[(long long)j * N + j];
-      for (int i = j + 1 + tid; i < N; i += kSolveThreads) {
-        T* row = A + (long long)i * N;
-        const T l = row[j] / d;
-        row[j] = l;
-        for (int c = j + 1; c < k0 + kb; ++c) row[c] -= l * A[(long long)j * N + c];
+      const T d = P[jj * LD + jj];
+      for (int i = jj + 1 + tid; i < m; i += kSolveThreads) {
+        T* row = P + i * LD;
+        const T l = row[jj] / d;
+        row[jj] = l;
+        for (int c = jj + 1; c < kb; ++c) row[c] -= l * P[jj * LD + c];
+      }
+      __syncthreads();
+    }
+    // panel back to global memory
+    for (int q = tid; q < m * NB; q += kSolveThreads) {
+      const int r = q / NB, c = q % NB;
+      if (c < kb) A[(long long)(k0 + r) * N + k0 + c] = P[r * LD + c];
+    }
+    // the panel's swaps on the columns left and right of it, in order
+    for (int jj = 0; jj < kb; ++jj) {
+      const int p = s_piv[jj];
+      if (p != jj) {
+        T* ra = A + (long long)(k0 + jj) * N;
+        T* rb = A + (long long)(k0 + p) * N;
+        for (int c = tid; c < N - kb; c += kSolveThreads) {
+          const int col = c < k0 ? c : c + kb;
+          const T t = ra[col];
+          ra[col] = rb[col];
+          rb[col] = t;
+        }
       }
       __syncthreads();
     }
     const int c0 = k0 + kb;
     if (c0 >= N) break;
-    // U12 = L11^-1 A12 (unit lower, column per thread)
-    for (int c = c0 + tid; c < N; c += kSolveThreads)
-      for (int i = 1; i < kb; ++i) {
-        T s = A[(long long)(k0 + i) * N + c];
-        for (int l = 0; l < i; ++l) s -= A[(long long)(k0 + i) * N + k0 + l] * A[(long long)(k0 + l) * N + c];
-        A[(long long)(k0 + i) * N + c] = s;
+    // U12 = L11^-1 A12: column per thread, the column in registers
+    for (int c = c0 + tid; c < N; c += kSolveThreads) {
+      T u[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) u[i] = i < kb ? A[(long long)(k0 + i) * N + c] : (T)0;
+#pragma unroll
+      for (int i = 1; i < NB; ++i) {
+        T s = u[i];
+#pragma unroll
+        for (int l = 0; l < i; ++l) s -= P[i * LD + l] * u[l];
+        u[i] = s;
       }
+#pragma unroll
+      for (int i = 1; i < NB; ++i)
+        if (i < kb) A[(long long)(k0 + i) * N + c] = u[i];
+    }
     __syncthreads();
-    cta_gemm_update<T>(A, N, k0, kb, c0);  // A22 -= L21 U12
-    __syncthreads();
+    // A22 -= L21 U12 in 64 x 64 tiles, L21 = panel rows kb.. (shared memory)
+    const int mt = N - c0;
+    const int tiles = (mt + 63) / 64;
+    const int tx = tid & 15, ty = tid >> 4;
+    for (int t = 0; t < tiles * tiles; ++t) {
+      const int r0 = (t / tiles) * 64, q0 = c0 + (t % tiles) * 64;  // r0 counts from row c0
+      for (int q = tid; q < NB * 64; q += kSolveThreads) {
+        const int l = q / 64, cc = q % 64;
+        Bs[l][cc] = (q0 + cc < N && l < kb) ? A[(long long)(k0 + l) * N + q0 + cc] : (T)0;
+      }
+      __syncthreads();
+      T acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
+      if (r0 + ty * 4 < mt) {
+        const T* Lp = P + (kb + r0 + ty * 4) * LD;
+#pragma unroll 4
+        for (int l = 0; l < kb; ++l) {
+          T a[4], bb[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = (r0 + ty * 4 + i < mt) ? Lp[i * LD + l] : (T)0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) bb[j] = Bs[l][tx * 4 + j];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * bb[j];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = c0 + r0 + ty * 4 + i;
+        if (r >= N) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int cc = q0 + tx * 4 + j;
+          if (cc < N) A[(long long)r * N + cc] -= acc[i][j];
+        }
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -479,6 +527,7 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
   const int N = b.N;
   double* x = sm;
   double* r = sm + N;
+  T* panel = reinterpret_cast<T*>(sm + 2 * N);
   double* A = A64 + b.mat_off;
   int* piv = piv_all + b.ring_off;
   const double* bb = rhs + b.ring_off;
@@ -490,7 +539,7 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
   } else {
     LU = A;
   }
-  cta_lu<T>(LU, N, piv, status);
+  cta_lu_panel_smem<T>(LU, N, piv, status, panel);
   for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
   __syncthreads();
   cta_lu_solve<T>(LU, N, piv, x);
@@ -900,7 +949,7 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   UVLM_CUDA_TRY(cudaMemset(d_wgamma, 0, sizeof(double) * tot_wring));
   UVLM_CUDA_TRY(cudaMemset(d_status, 0, sizeof(int) * 4));
   UVLM_CUDA_TRY(cudaMemset(d_loads, 0, sizeof(double) * (size_t)cfg.max_steps * n * 3));
-  const size_t solve_smem = sizeof(double) * 2 * (size_t)max_N;
+  const size_t solve_smem = sizeof(double) * 2 * (size_t)max_N + panel_smem_bytes(max_N, mixed() ? 4 : 8);
   if (mixed())
     UVLM_CUDA_TRY(cudaFuncSetAttribute(b_solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)solve_smem));
@@ -948,7 +997,7 @@ Error uvlm_batch::enqueue_step() {
   b_rhs_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, d_vx, d_vy, d_vz, d_uls, d_normal, d_rhs);
   UVLM_LAUNCH_CHECK();
   // solve
-  const size_t smem = sizeof(double) * 2 * (size_t)max_N;
+  const size_t smem = sizeof(double) * 2 * (size_t)max_N + panel_smem_bytes(max_N, mixed() ? 4 : 8);
   if (mixed())
     b_solve_kernel<float><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
                                                           cfg.refine_max_iter, cfg.refine_tol, d_sweeps, d_res,
@@ -1035,10 +1084,11 @@ int uvlm_batch_create(const uvlm_batch_config* cfg, const uvlm_batch_case* cases
   }
   for (int c = 0; c < n_cases; ++c) {
     const uvlm_batch_case& u = cases[c];
-    if (u.rows < 1 || u.cols < 2 || (u.cols & 1) || u.rows > 64 || u.cols > 64 || !(u.chord > 0) ||
+    if (u.rows < 1 || u.cols < 2 || (u.cols & 1) || u.rows > 64 || u.cols > 64 || u.rows * u.cols > 1024 ||
+        !(u.chord > 0) ||
         !(u.span > 0) || !(u.dt > 0)) {
       set_global_error("uvlm_batch_create: every case needs 1 <= rows <= 64, even 2 <= cols <= 64, "
-                            "positive chord, span and dt");
+                            "rows * cols <= 1024, positive chord, span and dt");
       return UVLM_ERR_INVALID;
     }
   }
