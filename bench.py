@@ -45,6 +45,10 @@ OMEGA = 1.0  # k = 0.5, c = 1, U = 1
 DT = 2 * math.pi / OMEGA / 40
 WAKE_ROWS = 400
 FLOP_PER_PAIR = 59
+# DRAM bytes of one advection launch of the N-body kernel at the held wake,
+# from an ncu capture of the packed FP32x2 tile (bench.py --profile): about the
+# algorithmic bytes (56,115 source records x 64 B + targets + outputs).
+NBODY_TRAFFIC = {"heave_pitch": 4955648}
 
 
 def make_mixed(device=0, warm_start=None, wl=None):
@@ -481,7 +485,10 @@ def run_ours(args, rank, world, local_rank):
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "FP32 FMA probe on this GPU (uvlm_measure_fp32_peak)",
                          "per_unit": f"{FLOP_PER_PAIR} FLOP per (target, unique segment) pair",
-                         "units_per_step": pairs_advect, "traffic": None},
+                         "units_per_step": pairs_advect,
+                         "traffic": NBODY_TRAFFIC.get(wl.name),
+                         "traffic_unit": "DRAM bytes per advection launch (ncu dram__bytes_read.sum + "
+                                         "dram__bytes_write.sum, one launch at the held wake)"},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 8 * (1 + 2 * wl.num + wl.num * ROWS * COLS),
                     "note": "wall clock per uvlm_step + circulation download; per-step inputs are scalars"},
