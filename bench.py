@@ -21,7 +21,8 @@ roofline    the N-body advection kernel: 59 FLOP per (target, unique segment)
 cpu_baseline the FP64 CPU oracle (restated reference) on a bounded sample
 
 --impl reference times that CPU oracle alone (the reference cannot be built
-here) on a synthetic state of the same shapes.
+here: its third-party libraries and submodules are absent) on a synthetic
+state of the same shapes.
 """
 from __future__ import annotations
 

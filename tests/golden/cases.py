@@ -2,7 +2,7 @@
 
 Each case is a SimpleSimulator set-up in the reference's own terms (wings from
 RectGenerator + WholeWing, Morphing kinematics, forward flight, advection
-scheme, dt, steps).  ``cfg1`` is the reference's CPU-runnable configuration:
+scheme, dt, steps).  ``plunge_euler_8x16_200`` is the reference's CPU-runnable configuration:
 one 8 x 16 flat-plate wing (chord 1, span 4), plunge 0.1 sin(2 pi 0.25 t) at
 5 degrees, U = 1, dt = 1/8, 200 explicit-Euler steps; its lattice is shifted
 1/4 panel downstream so that the ring centroids (the reference's collocation
@@ -13,7 +13,7 @@ import math
 DEG = math.pi / 180.0
 
 CASES = {
-    "cfg1_euler_200": dict(
+    "plunge_euler_8x16_200": dict(
         wings=[dict(chord=1.0, span=4.0, rows=8, cols=16, origin=(1.0 / 8 / 4, 0.0, 0.0),
                     kin=dict(alpha=5 * DEG, plug_amp=0.1, plug_omega=2 * math.pi * 0.25))],
         ff=(-1.0, 0.0, 0.0), advection="euler", dt=0.125, steps=200),

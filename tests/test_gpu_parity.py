@@ -4,7 +4,7 @@ Every call goes through the C-ABI (include/uvlm_b200.h) via uvlm_b200.
 Tolerances: the plain FP64 form must match the FP64 oracle to rounding
 (circulation 1e-9 relative, load coefficients 1e-8 relative to max|C| on
 short runs, since dGamma/dt amplifies rounding; 1e-7 over the 200-step
-config 1 run, where wake roll-up amplifies rounding); the mixed form is held
+8 x 16 plunge run, where wake roll-up amplifies rounding); the mixed form is held
 to the north-star bound on the load coefficients, 1e-6 relative to max|C|.
 """
 import math
@@ -202,7 +202,7 @@ def test_advection_ab2_history():
 
 
 # --------------------------------------------------------- whole time-stepper
-@pytest.mark.parametrize("name", [n for n in CASES if n != "cfg1_euler_200"])
+@pytest.mark.parametrize("name", [n for n in CASES if n != "plunge_euler_8x16_200"])
 def test_simulator_fp64_matches_golden(name):
     fx = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
     case = CASES[name]
@@ -225,30 +225,30 @@ def _window_errors(loads, ref):
     return out
 
 
-# The wake roll-up of config 1 amplifies rounding: perturbing the oracle's own
+# The wake roll-up of the 8 x 16 plunge amplifies rounding: perturbing the oracle's own
 # input by one ulp changes CL by ~1e-12 up to step 150 and by 2.4e-7 at step
 # 200, and the GPU's FP64 rounding order differs from the oracle's in every
 # operation.  Load coefficients are therefore held tightly over the first 100
 # steps (about three heave periods) and loosely over the full run.
-def test_simulator_fp64_cfg1_full_run():
-    fx = np.load(os.path.join(HERE, "golden", "cfg1_euler_200.npz"))
-    case = CASES["cfg1_euler_200"]
+def test_simulator_fp64_plunge_8x16_full_run():
+    fx = np.load(os.path.join(HERE, "golden", "plunge_euler_8x16_200.npz"))
+    case = CASES["plunge_euler_8x16_200"]
     sim = make_gpu_sim(case)
     loads = sim.Run(case["steps"], case["dt"])
     w = _window_errors(loads, fx["loads"])
-    print("FP64 vs oracle, config 1 (CL, CD) up to step:", w)
+    print("FP64 vs oracle, 8 x 16 plunge (CL, CD) up to step:", w)
     assert max(w[100]) < 1e-9
     assert max(w[150]) < 1e-7
     assert max(w[201]) < 1e-4
 
 
-def test_simulator_mixed_cfg1_within_north_star_bound():
-    fx = np.load(os.path.join(HERE, "golden", "cfg1_euler_200.npz"))
-    case = CASES["cfg1_euler_200"]
+def test_simulator_mixed_plunge_8x16_within_1e6_bound():
+    fx = np.load(os.path.join(HERE, "golden", "plunge_euler_8x16_200.npz"))
+    case = CASES["plunge_euler_8x16_200"]
     sim = make_gpu_sim(case, precision="mixed")
     loads = sim.Run(case["steps"], case["dt"])
     w = _window_errors(loads, fx["loads"])
-    print("mixed vs oracle, config 1 (CL, CD) up to step:", w)
+    print("mixed vs oracle, 8 x 16 plunge (CL, CD) up to step:", w)
     assert max(w[100]) <= 1e-6
     assert max(w[201]) <= 1e-4
 

@@ -15,7 +15,7 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 
 from cases import CASES, run_oracle  # noqa: E402
 
-SMALL = [n for n in CASES if n != "cfg1_euler_200"]
+SMALL = [n for n in CASES if n != "plunge_euler_8x16_200"]
 
 
 @pytest.mark.parametrize("name", SMALL)
@@ -27,8 +27,8 @@ def test_oracle_matches_fixture(name):
     np.testing.assert_allclose(st["wake_pos"], fx["wake_pos"], rtol=1e-11, atol=1e-13)
 
 
-def test_cfg1_fixture_shape_and_physics():
-    fx = np.load(os.path.join(HERE, "golden", "cfg1_euler_200.npz"))
+def test_plunge_8x16_fixture_shape_and_physics():
+    fx = np.load(os.path.join(HERE, "golden", "plunge_euler_8x16_200.npz"))
     loads = fx["loads"]
     assert loads.shape == (201, 3)
     np.testing.assert_allclose(loads[:, 0], np.arange(201) * 0.125)

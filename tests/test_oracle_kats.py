@@ -2,7 +2,7 @@
 
 Each test restates one case of xeno14/UVLM's gtest suite (file:line given),
 with the same inputs, expected values and tolerances.  The oracle
-(oracle/uvlm_oracle.cpp) is the checker for every CUDA parity test, so these
+(oracle/uvlm_oracle.cpp) is what every CUDA parity test compares against, so these
 are the pins that make it trustworthy.
 """
 import math
