@@ -162,7 +162,8 @@ def _morphing():
                     "0.1 sin(wt) y^2, k=0.3, Euler, wake held at 600 rows (57,600 rings)",
                     [dict(chord=1.0, span=8.0, rows=24, cols=96, origin=(0.0, 0.0, 0.0),
                           kin=dict(bend_cx=0.05, bend_cy=0.1, bend_omega=w))],
-                    "euler", 2 * math.pi / w / 40, 600)
+                    "euler", 2 * math.pi / w / 40, 600,
+                    weights=os.path.join(ROOT, "uvlm_b200", "weights", "warmstart_morphing_24x96.npz"))
 
 
 WORKLOADS = {"heave_pitch": _heave_pitch, "tandem4": _tandem4, "morphing": _morphing}
@@ -350,7 +351,7 @@ def run_ours(args, rank, world, local_rank):
         if simex:
             simex.step(s, DT)
         if s >= 3:
-            for name, sm in (("mlp", simmx), ("extrapolate", simex)):
+            for name, sm in (("mlp" if learned else "extrapolate", simmx), ("extrapolate", simex)):
                 if sm is None:
                     continue
                 st_ = sm.stats()

@@ -256,12 +256,14 @@ __global__ void __launch_bounds__(kPanelRows) lu_panel_cluster_kernel(T* A, int 
                              : cl.map_shared_rank(diag_data + par * kLuNB, diag_owner);
     for (int q = tid; q < kb; q += blockDim.x) urow[q] = src[q];
     __syncthreads();
-    if (mine && pr == p && p != c) {
+    // the swap, each row copied by all threads of the CTA that holds it
+    if (p != c && p >= rb && p < rb + nloc) {
       const T* dsrc = cl.map_shared_rank(diag_data + par * kLuNB, diag_owner);
-      for (int q = 0; q < kb; ++q) my[q] = dsrc[q];
+      for (int q = tid; q < kb; q += blockDim.x) rows[(p - rb) * kPanelLd + q] = dsrc[q];
     }
-    if (mine && pr == c)
-      for (int q = 0; q < kb; ++q) my[q] = urow[q];
+    if (c >= rb && c < rb + nloc)
+      for (int q = tid; q < kb; q += blockDim.x) rows[(c - rb) * kPanelLd + q] = urow[q];
+    __syncthreads();
     if (mine && pr > c) {
       const T piv = urow[c];
       const T l = (piv != (T)0) ? my[c] / piv : (T)0;
