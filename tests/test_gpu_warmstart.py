@@ -150,3 +150,37 @@ def test_shipped_weights_beat_extrapolation_on_the_workload():
     # the remaining difference forward, so compare at the mixed form's 1e-6
     scale = np.max(np.abs(res["extrapolate"][1][:, 1:]))
     np.testing.assert_allclose(res["mlp"][1][:, 1:], res["extrapolate"][1][:, 1:], rtol=0, atol=1e-6 * scale)
+
+
+def test_shipped_morphing_weights_beat_extrapolation():
+    """The committed network for the morphing wing (24 x 96, camber and span
+    bend, Euler; trained on 20k plain-solver steps of seeded variations)
+    starts the GMRES solve closer than the extrapolation."""
+    import os
+
+    import uvlm_b200 as U
+    from uvlm_b200.warmstart import MLP
+
+    path = os.path.join(os.path.dirname(U.__file__), "weights", "warmstart_morphing_24x96.npz")
+    net = MLP.load(path)
+    dt, steps = 2 * math.pi / 0.6 / 40, 40
+    res = {}
+    for warm in ("extrapolate", "mlp"):
+        sim = U.SimpleSimulator(precision="mixed", warm_start=warm)
+        if warm == "mlp":
+            sim.set_mlp(net)
+        sim.AddWing(U.RectGenerator(), U.Morphing().set_bend(0.05, 0.1, 0.6), 1.0, 8.0, 24, 96)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.set_advection("euler")
+        sim.begin()
+        r0, rows = [], []
+        for s in range(steps + 1):
+            rows.append(sim.step(s, dt))
+            if s >= 3:
+                r0.append(sim.stats().initial_residual)
+        res[warm] = (float(np.mean(r0)), np.array(rows))
+        sim.close()
+    print(f"morphing: initial residual extrapolation {res['extrapolate'][0]:.3e}, MLP {res['mlp'][0]:.3e}")
+    assert res["mlp"][0] < 0.5 * res["extrapolate"][0]
+    scale = np.max(np.abs(res["extrapolate"][1][:, 1:]))
+    np.testing.assert_allclose(res["mlp"][1][:, 1:], res["extrapolate"][1][:, 1:], rtol=0, atol=1e-6 * scale)
