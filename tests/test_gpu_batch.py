@@ -149,3 +149,26 @@ def test_batch_rejects_bad_cases():
     with pytest.raises(BatchError):
         sim2.run(1)
     sim2.close()
+
+
+def test_batch_wide_and_narrow_cases_mixed_vs_oracle():
+    """Cases wide enough for the padded packed walker (cols >= 48) and narrow
+    ones in one mixed batch, each against its own oracle run."""
+    from uvlm_b200.batch import make_batch
+
+    rng = np.random.default_rng(21)
+    cases = []
+    for cols in (64, 8, 50, 12, 48):
+        k = float(rng.uniform(0.3, 0.8))
+        cases.append(dict(rows=3, cols=cols, chord=1.0, span=float(rng.uniform(3, 8)), k=k, omega=2 * k,
+                          heave=float(rng.uniform(0.05, 0.2)), pitch_deg=float(rng.uniform(2, 15)),
+                          dt=2 * math.pi / (2 * k) / 40))
+    steps = 12
+    sim = make_batch(cases, precision="mixed", max_steps=steps)
+    sim.run(steps)
+    L = sim.loads()
+    sim.close()
+    for c, d in enumerate(cases):
+        ref, _ = _oracle(d, steps)
+        scale = np.max(np.abs(ref[:, 1:]))
+        assert np.max(np.abs(L[:, c, 1:] - ref[:, 1:])) <= 1e-6 * scale, d["cols"]

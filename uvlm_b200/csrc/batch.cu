@@ -738,7 +738,8 @@ using namespace uvlm;
 struct uvlm_batch {
   uvlm_batch_config cfg{};
   std::string err;
-  int n = 0, cap = 0, num_sms = 148, grid = 0, nb_grid = 0;
+  int n = 0, cap = 0, num_sms = 148, grid = 0;
+  NBodyBatchGrids nb_grids;
   int64_t steps_done = 0;
   std::vector<BCase> hc;
   std::vector<long long> pre[7];
@@ -956,7 +957,7 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   else
     UVLM_CUDA_TRY(cudaFuncSetAttribute(b_solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)solve_smem));
-  nb_grid = nbody_batch_grid(prec(), num_sms);
+  nb_grids = nbody_batch_grids(prec(), num_sms);
   grid = num_sms * 8;
   return ok();
 }
@@ -965,7 +966,7 @@ Error uvlm_batch::nbody(int stage, const double* tx, const double* ty, const dou
   b_nbody_inputs_kernel<<<(n + 127) / 128, 128, 0, st>>>(d_cases, n, d_step, stage, d_in);
   UVLM_LAUNCH_CHECK();
   return nbody_batch_eval(prec(), d_in, n, tx, ty, tz, d_vx, d_vy, d_vz, d_rec, d_partial, partial_cap, d_plan,
-                          d_totals, d_status, nb_grid, st);
+                          d_totals, d_status, nb_grids, st);
 }
 
 Error uvlm_batch::enqueue_step() {

@@ -470,8 +470,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
 // ------------------------------------------------------ batched evaluation
 // Plans of all problems: strips, tiles, splits and the exclusive prefixes of
 // items, partial sums and targets.  One CTA; a blockwide scan in chunks.
+// select: -1 all problems, 0 only the general class, 1 only the padded class
+// (the others get no targets, hence no items and no reduction).
 template <int H, int TPC>
-__global__ void __launch_bounds__(256) batch_plan_kernel(const NBodyBatchInput* __restrict__ in, int n,
+__global__ void __launch_bounds__(256) batch_plan_kernel(const NBodyBatchInput* __restrict__ in, int n, int select,
                                                          NBodyBatchPlan* __restrict__ plan, long long partial_cap,
                                                          long long* totals, int* status) {
   __shared__ long long sh[3][256];
@@ -484,14 +486,15 @@ __global__ void __launch_bounds__(256) batch_plan_kernel(const NBodyBatchInput* 
     NBodyBatchPlan p{};
     if (c < n) {
       const NBodyBatchInput& x = in[c];
+      const bool take = select < 0 || (int)batch_input_padded(x) == select;
       p.n_strips = fill_blocks(p.B, x.blocks, x.n_blocks, H);
       p.tgt_off = x.tgt_off;
-      p.n_tgt = x.n_tgt;
-      p.tiles = (x.n_tgt + TPC - 1) / TPC;
+      p.n_tgt = take ? x.n_tgt : 0;
+      p.tiles = (p.n_tgt + TPC - 1) / TPC;
       p.splits = (p.n_strips + kBatchStripsPerItem - 1) / kBatchStripsPerItem;
       v[0] = p.tiles * p.splits;
-      v[1] = p.splits * 3 * x.n_tgt;
-      v[2] = x.n_tgt;
+      v[1] = p.splits * 3 * p.n_tgt;
+      v[2] = p.n_tgt;
     }
     for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = v[k];
     __syncthreads();
@@ -537,7 +540,7 @@ __device__ inline int plan_search(const NBodyBatchPlan* plan, int n, long long w
   return lo;
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, bool PK>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBatchPlan* __restrict__ plan, int n,
                                                              const long long* __restrict__ totals,
                                                              const double* __restrict__ tx,
@@ -562,7 +565,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBat
     for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
     const long long s_begin = split * kBatchStripsPerItem;
     const long long s_end = min(P.n_strips, s_begin + kBatchStripsPerItem);
-    eval_strips<T, Rec, H, TPT, false>(P.B, s_begin, s_end, rec, buf0, buf1, tg, accd);
+    eval_strips<T, Rec, H, TPT, PAD, PK>(P.B, s_begin, s_end, rec, buf0, buf1, tg, accd);
     double* px = partial + P.part_off + split * 3 * P.n_tgt;
 #pragma unroll
     for (int q = 0; q < TPT; ++q) {
@@ -598,9 +601,10 @@ __global__ void batch_reduce_kernel(const NBodyBatchPlan* __restrict__ plan, int
   }
 }
 
-// Batched tiles: FP32 h4 t2 b128 (3 CTAs/SM), FP64 h2 t1 b128 (3 CTAs/SM).
+// Batched tiles: FP32 general h4 t2 b128, FP32 padded (packed FP32x2) h3 t2
+// b128, FP64 h2 t1 b128; 3 CTAs/SM each.
 constexpr int kBatchBlock = 128;
-constexpr int kBatchTptF = 2, kBatchHF = 4, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
+constexpr int kBatchTptF = 2, kBatchHF = 4, kBatchHFP = 3, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
 
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, int splits, long long n, double* vx,
                                        double* vy, double* vz) {
@@ -778,21 +782,14 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
 
 namespace uvlm {
 
-void nbody_batch_shape(NBodyPrec prec, int* targets_per_cta, int* H) {
-  if (prec == kNBodyFP32) {
-    *targets_per_cta = kBatchBlock * kBatchTptF;
-    *H = kBatchHF;
-  } else {
-    *targets_per_cta = kBatchBlock * kBatchTptD;
-    *H = kBatchHD;
-  }
+int nbody_batch_rows(NBodyPrec prec, bool padded) {
+  return prec == kNBodyFP32 ? (padded ? kBatchHFP : kBatchHF) : kBatchHD;
 }
 
 long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n) {
-  int tpc = 0, H = 0;
-  nbody_batch_shape(prec, &tpc, &H);
   long long total = 0;
   for (int c = 0; c < n; ++c) {
+    const int H = nbody_batch_rows(prec, prec == kNBodyFP32 && batch_input_padded(in[c]));
     Blocks B{};
     const long long strips = fill_blocks(B, in[c].blocks, in[c].n_blocks, H);
     const long long splits = (strips + kBatchStripsPerItem - 1) / kBatchStripsPerItem;
@@ -802,51 +799,71 @@ long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in,
 }
 
 namespace {
-template <class T, class Rec, int H, int TPT>
-void* batch_kernel_ptr() {
-  return (void*)batch_nbody_kernel<T, Rec, H, TPT, kBatchBlock, kBatchMinB>;
-}
 template <class Rec, int H>
 constexpr size_t batch_smem() {
   return 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
 }
-}  // namespace
-
-int nbody_batch_grid(NBodyPrec prec, int num_sms) {
-  const void* k = prec == kNBodyFP32 ? batch_kernel_ptr<float, RecF, kBatchHF, kBatchTptF>()
-                                     : batch_kernel_ptr<double, RecD, kBatchHD, kBatchTptD>();
-  const size_t smem = prec == kNBodyFP32 ? batch_smem<RecF, kBatchHF>() : batch_smem<RecD, kBatchHD>();
+template <class T, class Rec, int H, int TPT, bool PAD, bool PK>
+int batch_grid_of(int num_sms) {
+  const void* k = (const void*)batch_nbody_kernel<T, Rec, H, TPT, kBatchBlock, kBatchMinB, PAD, PK>;
+  const size_t smem = batch_smem<Rec, H>();
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBatchBlock, smem) != cudaSuccess || occ < 1) occ = 1;
   return num_sms * occ;
 }
+}  // namespace
+
+NBodyBatchGrids nbody_batch_grids(NBodyPrec prec, int num_sms) {
+  NBodyBatchGrids g;
+  if (prec == kNBodyFP32) {
+    g.general = batch_grid_of<float, RecF, kBatchHF, kBatchTptF, false, false>(num_sms);
+    g.padded = batch_grid_of<float, RecF, kBatchHFP, kBatchTptF, true, true>(num_sms);
+  } else {
+    g.general = batch_grid_of<double, RecD, kBatchHD, kBatchTptD, false, false>(num_sms);
+  }
+  return g;
+}
 
 Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const double* tx, const double* ty,
                        const double* tz, double* vx, double* vy, double* vz, const void* records, double* partial,
-                       long long partial_cap, NBodyBatchPlan* d_plan, long long* d_totals, int* status, int grid,
-                       cudaStream_t st) {
+                       long long partial_cap, NBodyBatchPlan* d_plan, long long* d_totals, int* status,
+                       const NBodyBatchGrids& grids, cudaStream_t st) {
   if (n <= 0) return ok();
+  auto reduce = [&](int grid) -> Error {
+    batch_reduce_kernel<<<grid, 256, 0, st>>>(d_plan, n, d_totals, partial, vx, vy, vz);
+    UVLM_LAUNCH_CHECK();
+    return ok();
+  };
   if (prec == kNBodyFP32) {
-    batch_plan_kernel<kBatchHF, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, d_plan, partial_cap, d_totals,
-                                                                             status);
+    const RecF* rf = reinterpret_cast<const RecF*>(records);
+    // general class
+    batch_plan_kernel<kBatchHF, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, 0, d_plan, partial_cap,
+                                                                             d_totals, status);
     UVLM_LAUNCH_CHECK();
-    batch_nbody_kernel<float, RecF, kBatchHF, kBatchTptF, kBatchBlock, kBatchMinB>
-        <<<grid, kBatchBlock, batch_smem<RecF, kBatchHF>(), st>>>(d_plan, n, d_totals, tx, ty, tz,
-                                                                   reinterpret_cast<const RecF*>(records), partial);
+    batch_nbody_kernel<float, RecF, kBatchHF, kBatchTptF, kBatchBlock, kBatchMinB, false, false>
+        <<<grids.general, kBatchBlock, batch_smem<RecF, kBatchHF>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
+                                                                            partial);
     UVLM_LAUNCH_CHECK();
-  } else {
-    batch_plan_kernel<kBatchHD, kBatchBlock * kBatchTptD><<<1, 256, 0, st>>>(d_in, n, d_plan, partial_cap, d_totals,
-                                                                             status);
+    UVLM_TRY(reduce(grids.general));
+    // padded class: whole strips, packed FP32x2 walker
+    batch_plan_kernel<kBatchHFP, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, 1, d_plan, partial_cap,
+                                                                              d_totals, status);
     UVLM_LAUNCH_CHECK();
-    batch_nbody_kernel<double, RecD, kBatchHD, kBatchTptD, kBatchBlock, kBatchMinB>
-        <<<grid, kBatchBlock, batch_smem<RecD, kBatchHD>(), st>>>(d_plan, n, d_totals, tx, ty, tz,
-                                                                   reinterpret_cast<const RecD*>(records), partial);
+    batch_nbody_kernel<float, RecF, kBatchHFP, kBatchTptF, kBatchBlock, kBatchMinB, true, true>
+        <<<grids.padded, kBatchBlock, batch_smem<RecF, kBatchHFP>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
+                                                                            partial);
     UVLM_LAUNCH_CHECK();
+    return reduce(grids.padded);
   }
-  batch_reduce_kernel<<<grid, 256, 0, st>>>(d_plan, n, d_totals, partial, vx, vy, vz);
+  batch_plan_kernel<kBatchHD, kBatchBlock * kBatchTptD><<<1, 256, 0, st>>>(d_in, n, -1, d_plan, partial_cap,
+                                                                           d_totals, status);
   UVLM_LAUNCH_CHECK();
-  return ok();
+  batch_nbody_kernel<double, RecD, kBatchHD, kBatchTptD, kBatchBlock, kBatchMinB, false, false>
+      <<<grids.general, kBatchBlock, batch_smem<RecD, kBatchHD>(), st>>>(
+          d_plan, n, d_totals, tx, ty, tz, reinterpret_cast<const RecD*>(records), partial);
+  UVLM_LAUNCH_CHECK();
+  return reduce(grids.general);
 }
 
 }  // namespace uvlm

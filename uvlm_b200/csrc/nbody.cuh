@@ -211,12 +211,31 @@ struct NBodyBatchPlan {
   long long tiles, splits, item_off, part_off, tgt_prefix;
 };
 
-// Tile of the batched kernel for a precision (targets per CTA and H).
-void nbody_batch_shape(NBodyPrec prec, int* targets_per_cta, int* H);
+// A problem whose sheets fill at least 3/4 of the staged strip columns is
+// walked as whole padded strips by the packed FP32x2 walker (FP32 only); the
+// others by the general walker.  FP32 evaluations therefore run as two
+// persistent launches, one per class.
+__host__ __device__ inline bool batch_input_padded(const NBodyBatchInput& x) {
+  bool any = false;
+  for (int i = 0; i < x.n_blocks; ++i) {
+    const SourceBlock& b = x.blocks[i];
+    if (b.num <= 0 || b.node_rows < 2 || b.cols <= 0) continue;
+    const long long chunks = (b.cols + kStripCols - 1) / kStripCols;
+    if (4 * (b.cols + chunks) < 3 * chunks * (kStripCols + 1)) return false;
+    any = true;
+  }
+  return any;
+}
+
+// Strip height of the batched tile of a precision and class.
+int nbody_batch_rows(NBodyPrec prec, bool padded);
 // Upper bound of the partial-sum doubles for the given inputs (host copy).
 long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n);
-// Persistent grid size used by nbody_batch_eval on this device.
-int nbody_batch_grid(NBodyPrec prec, int num_sms);
+// Persistent grid sizes used by nbody_batch_eval on this device.
+struct NBodyBatchGrids {
+  int general = 0, padded = 0;
+};
+NBodyBatchGrids nbody_batch_grids(NBodyPrec prec, int num_sms);
 
 // d_in: n problems on the device.  Plans on the device (one CTA), evaluates
 // with `grid` persistent CTAs and reduces the splits; d_plan holds n plans
@@ -224,8 +243,8 @@ int nbody_batch_grid(NBodyPrec prec, int num_sms);
 // buffer is too small (nothing is evaluated then).
 Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const double* tx, const double* ty,
                        const double* tz, double* vx, double* vy, double* vz, const void* records, double* partial,
-                       long long partial_cap, NBodyBatchPlan* d_plan, long long* d_totals, int* status, int grid,
-                       cudaStream_t st);
+                       long long partial_cap, NBodyBatchPlan* d_plan, long long* d_totals, int* status,
+                       const NBodyBatchGrids& grids, cudaStream_t st);
 
 int nbody_num_variants();
 int nbody_variant_prec(int v);
