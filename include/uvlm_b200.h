@@ -320,6 +320,8 @@ typedef struct {
   int64_t max_steps;       /* MainLoops the batch can run (wake capacity) */
   int32_t device;
   int32_t use_graph;       /* 1: capture one step as a CUDA graph and replay it */
+  int32_t stale_factors;   /* MIXED, 1: a case refines from its previous circulation with the FP32 factors
+                              of an earlier step and is factored again only when that does not converge */
 } uvlm_batch_config;
 
 int uvlm_batch_config_default(uvlm_batch_config* cfg);
@@ -339,6 +341,8 @@ int uvlm_batch_get_case(const uvlm_batch* b, int32_t c, double* wing_pos, double
                         double* wake_gamma, int64_t* wake_rows);
 /* Last step's solve per case: refinement sweeps and final relative residual. */
 int uvlm_batch_get_solve_stats(const uvlm_batch* b, int32_t* sweeps, double* residual);
+/* Per-case factorisations so far (every case every step when stale_factors = 0). */
+int uvlm_batch_factorizations(const uvlm_batch* b, int64_t* count);
 /* Kernels one step launches (nodes of the captured graph). */
 int uvlm_batch_launches_per_step(const uvlm_batch* b, int64_t* launches);
 /* The batch's CUDA stream (a cudaStream_t), for events around uvlm_batch_run. */

@@ -172,3 +172,24 @@ def test_batch_wide_and_narrow_cases_mixed_vs_oracle():
         ref, _ = _oracle(d, steps)
         scale = np.max(np.abs(ref[:, 1:]))
         assert np.max(np.abs(L[:, c, 1:] - ref[:, 1:])) <= 1e-6 * scale, d["cols"]
+
+
+def test_batch_stale_factors_same_answer_fewer_factorizations():
+    """Refining from the previous circulation with an earlier step's FP32
+    factors converges to the same 1e-12 residual as a fresh factorisation
+    every step, with fewer factorisations."""
+    from uvlm_b200.batch import make_batch
+
+    cases = _small_cases(6, seed=17)
+    steps = 20
+    out = {}
+    for stale in (False, True):
+        sim = make_batch(cases, precision="mixed", max_steps=steps, stale_factors=stale)
+        sim.run(steps)
+        out[stale] = (sim.loads(), sim.factorizations(), sim.solve_stats()[1])
+        sim.close()
+    assert out[False][1] == len(cases) * steps
+    assert out[True][1] < out[False][1]
+    assert np.all(out[True][2] <= 1e-12)
+    scale = np.max(np.abs(out[False][0][:, :, 1:]))
+    assert np.max(np.abs(out[True][0][:, :, 1:] - out[False][0][:, :, 1:])) <= 1e-9 * scale

@@ -76,7 +76,7 @@ class BatchConfig(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("advection", C.c_int32), ("rk_ignore_rows", C.c_int32),
         ("refine_max_iter", C.c_int32), ("refine_tol", C.c_double), ("max_steps", C.c_int64),
-        ("device", C.c_int32), ("use_graph", C.c_int32),
+        ("device", C.c_int32), ("use_graph", C.c_int32), ("stale_factors", C.c_int32),
     ]
 
 
@@ -147,6 +147,7 @@ SIGNATURES = [
     ("uvlm_batch_get_case", C.c_int, [_V, C.c_int32, _P, _P, _P, _P, C.POINTER(_I)]),
     ("uvlm_batch_get_solve_stats", C.c_int, [_V, C.POINTER(C.c_int32), _P]),
     ("uvlm_batch_launches_per_step", C.c_int, [_V, C.POINTER(_I)]),
+    ("uvlm_batch_factorizations", C.c_int, [_V, C.POINTER(_I)]),
     ("uvlm_batch_stream", _V, [_V]),
 ]
 

@@ -41,7 +41,7 @@ class BatchSimulator:
 
     def __init__(self, precision: str = "mixed", advection: str = "euler", max_steps: int = 151, device: int = 0,
                  use_graph: bool = True, refine_tol: float = 1e-12, refine_max_iter: int = 10,
-                 rk_ignore_rows: int = 5):
+                 rk_ignore_rows: int = 5, stale_factors: bool = True):
         cfg = BatchConfig()
         check(lib().uvlm_batch_config_default(C.byref(cfg)))
         cfg.precision = PRECISION[precision]
@@ -52,6 +52,7 @@ class BatchSimulator:
         cfg.refine_tol = float(refine_tol)
         cfg.refine_max_iter = int(refine_max_iter)
         cfg.rk_ignore_rows = int(rk_ignore_rows)
+        cfg.stale_factors = int(bool(stale_factors))
         self._cfg = cfg
         self._cases = []
         self._h = None
@@ -123,6 +124,12 @@ class BatchSimulator:
                                                 res.ctypes.data_as(C.POINTER(C.c_double))), self._h)
         return sw, res
 
+    def factorizations(self) -> int:
+        """Per-case LU factorisations so far."""
+        v = C.c_int64()
+        _check(lib().uvlm_batch_factorizations(self._h, C.byref(v)), self._h)
+        return v.value
+
     def launches_per_step(self) -> int:
         v = C.c_int64()
         _check(lib().uvlm_batch_launches_per_step(self._h, C.byref(v)), self._h)
@@ -191,9 +198,9 @@ def shard_cases(costs, world: int) -> list[list[int]]:
 
 
 def make_batch(cases: list[dict], precision: str = "mixed", advection: str = "euler", max_steps: int = 151,
-               device: int = 0, use_graph: bool = True) -> BatchSimulator:
+               device: int = 0, use_graph: bool = True, stale_factors: bool = True) -> BatchSimulator:
     sim = BatchSimulator(precision=precision, advection=advection, max_steps=max_steps, device=device,
-                         use_graph=use_graph)
+                         use_graph=use_graph, stale_factors=stale_factors)
     for d in cases:
         sim.add_case(case_morphing(d), d["chord"], d["span"], d["rows"], d["cols"], d["dt"])
     return sim

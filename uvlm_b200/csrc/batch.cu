@@ -514,14 +514,25 @@ __device__ double cta_sum(double v) {
   return t;
 }
 
+// Refinement sweeps a stale factorisation may spend before the case is
+// factored again, and the contraction each sweep must reach.
+constexpr int kStaleSweeps = 12;
+constexpr double kStaleContraction = 0.5;
+
 // One CTA per case: G = A^-1 b.  FP64 form: LU of A in place.  Mixed form:
-// FP32 copy of A factored, then sweeps g += (LU)^-1 (b - A g) with the FP64
-// residual until ||b - A g|| <= tol ||b||.
+// sweeps g += (LU)^-1 (b - A g) with the FP64 residual until
+// ||b - A g|| <= tol ||b||, where LU are FP32 factors of A.  With stale
+// factors allowed, a case that already holds factors (of an earlier step's
+// matrix) first refines from its previous circulation with them; only when
+// that does not reach the tolerance, or a sweep contracts the residual by less
+// than kStaleContraction, is the FP32 copy of the current A factored again
+// (each case decides for itself; refac counts the factorisations).
 template <class T>
 __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __restrict__ cs, double* A64, float* F32,
                                                                 int* piv_all, const double* rhs, double* gamma,
-                                                                int max_sweeps, double tol, int* sweeps_out,
-                                                                double* res_out, int* status) {
+                                                                int max_sweeps, double tol, int stale,
+                                                                int* has_factor, unsigned long long* refac,
+                                                                int* sweeps_out, double* res_out, int* status) {
   extern __shared__ double sm[];
   const BCase& b = cs[blockIdx.x];
   const int N = b.N;
@@ -531,45 +542,75 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
   double* A = A64 + b.mat_off;
   int* piv = piv_all + b.ring_off;
   const double* bb = rhs + b.ring_off;
-  T* LU;
-  if constexpr (sizeof(T) == 4) {
-    LU = F32 + b.mat_off;
-    for (long long q = threadIdx.x; q < (long long)N * N; q += kSolveThreads) LU[q] = (float)A[q];
-    __syncthreads();
-  } else {
-    LU = A;
-  }
-  cta_lu_panel_smem<T>(LU, N, piv, status, panel);
-  for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
-  __syncthreads();
-  cta_lu_solve<T>(LU, N, piv, x);
   int sweeps = 0;
   double rel = 0;
   if constexpr (sizeof(T) == 4) {
+    T* LU = F32 + b.mat_off;
     double bn = 0;
     for (int i = threadIdx.x; i < N; i += kSolveThreads) bn += bb[i] * bb[i];
     bn = sqrt(cta_sum(bn));
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    while (true) {
+    // r = b - A x (FP64), returns ||r|| / ||b|| (same value in every thread)
+    auto residual = [&]() -> double {
       for (int i = wid; i < N; i += kSolveThreads / 32) {
         const double* a = A + (long long)i * N;
-        double s = 0;
-        for (int j = lane; j < N; j += 32) s += a[j] * x[j];
-        for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-        if (lane == 0) r[i] = bb[i] - s;
+        double acc = 0;
+        for (int j = lane; j < N; j += 32) acc += a[j] * x[j];
+        for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (lane == 0) r[i] = bb[i] - acc;
       }
       __syncthreads();
       double rn = 0;
       for (int i = threadIdx.x; i < N; i += kSolveThreads) rn += r[i] * r[i];
       rn = sqrt(cta_sum(rn));
-      rel = bn > 0 ? rn / bn : 0.0;
-      if (rel <= tol || sweeps >= max_sweeps || !(rel == rel)) break;
+      return bn > 0 ? rn / bn : 0.0;
+    };
+    auto sweep = [&]() {
       cta_lu_solve<T>(LU, N, piv, r);
       for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] += r[i];
       __syncthreads();
-      ++sweeps;
+    };
+    bool done = false;
+    if (stale && has_factor[blockIdx.x]) {
+      for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = gamma[b.ring_off + i];
+      __syncthreads();
+      rel = residual();
+      double prev = rel;
+      for (int k = 0; k < kStaleSweeps && rel > tol && rel == rel; ++k) {
+        sweep();
+        ++sweeps;
+        rel = residual();
+        if (!(rel < kStaleContraction * prev)) break;
+        prev = rel;
+      }
+      done = rel <= tol;
+    }
+    if (!done) {
+      for (long long q = threadIdx.x; q < (long long)N * N; q += kSolveThreads) LU[q] = (float)A[q];
+      __syncthreads();
+      cta_lu_panel_smem<T>(LU, N, piv, status, panel);
+      if (threadIdx.x == 0) {
+        has_factor[blockIdx.x] = 1;
+        atomicAdd(refac, 1ull);
+      }
+      for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
+      __syncthreads();
+      cta_lu_solve<T>(LU, N, piv, x);
+      sweeps = 0;
+      while (true) {
+        rel = residual();
+        if (rel <= tol || sweeps >= max_sweeps || !(rel == rel)) break;
+        sweep();
+        ++sweeps;
+      }
     }
     if (threadIdx.x == 0 && !(rel <= tol)) status[3] = 1;
+  } else {
+    cta_lu_panel_smem<T>(A, N, piv, status, panel);
+    if (threadIdx.x == 0) atomicAdd(refac, 1ull);
+    for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
+    __syncthreads();
+    cta_lu_solve<T>(A, N, piv, x);
   }
   bool finite = true;
   for (int i = threadIdx.x; i < N; i += kSolveThreads) {
@@ -774,6 +815,8 @@ struct uvlm_batch {
   long long* d_totals = nullptr;
   int* d_status = nullptr;
   int* d_sweeps = nullptr;
+  int* d_has_factor = nullptr;           // per case: FP32 factors held (stale reuse)
+  unsigned long long* d_refac = nullptr;  // factorisations so far
   double* d_res = nullptr;
   double* d_loads = nullptr;
 
@@ -933,6 +976,8 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   UVLM_TRY(balloc(&d_totals, 4));
   UVLM_TRY(balloc(&d_status, 4));
   UVLM_TRY(balloc(&d_sweeps, n));
+  UVLM_TRY(balloc(&d_has_factor, n));
+  UVLM_TRY(balloc(&d_refac, 1));
   UVLM_TRY(balloc(&d_res, n));
   UVLM_TRY(balloc(&d_loads, (size_t)cfg.max_steps * n * 3));
 
@@ -949,6 +994,8 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   UVLM_CUDA_TRY(cudaMemset(d_wpos, 0, sizeof(double) * 3 * tot_wnode));
   UVLM_CUDA_TRY(cudaMemset(d_wgamma, 0, sizeof(double) * tot_wring));
   UVLM_CUDA_TRY(cudaMemset(d_status, 0, sizeof(int) * 4));
+  UVLM_CUDA_TRY(cudaMemset(d_has_factor, 0, sizeof(int) * n));
+  UVLM_CUDA_TRY(cudaMemset(d_refac, 0, sizeof(unsigned long long)));
   UVLM_CUDA_TRY(cudaMemset(d_loads, 0, sizeof(double) * (size_t)cfg.max_steps * n * 3));
   const size_t solve_smem = sizeof(double) * 2 * (size_t)max_N + panel_smem_bytes(max_N, mixed() ? 4 : 8);
   if (mixed())
@@ -1001,11 +1048,11 @@ Error uvlm_batch::enqueue_step() {
   const size_t smem = sizeof(double) * 2 * (size_t)max_N + panel_smem_bytes(max_N, mixed() ? 4 : 8);
   if (mixed())
     b_solve_kernel<float><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
-                                                          cfg.refine_max_iter, cfg.refine_tol, d_sweeps, d_res,
-                                                          d_status);
+                                                          cfg.refine_max_iter, cfg.refine_tol, cfg.stale_factors,
+                                                          d_has_factor, d_refac, d_sweeps, d_res, d_status);
   else
     b_solve_kernel<double><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma, 0, 0.0,
-                                                           d_sweeps, d_res, d_status);
+                                                           0, d_has_factor, d_refac, d_sweeps, d_res, d_status);
   UVLM_LAUNCH_CHECK();
   // loads: line velocities from the bound sheet (new circulation) and the wake
   b_line_prep_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, d_step, d_pos, d_pos_init, d_lx, d_ly, d_lz, d_line_uls);
@@ -1047,7 +1094,7 @@ void uvlm_batch::release() {
   void* ptrs[] = {d_cases, d_pre, d_step, d_pos_init, d_pos, d_gamma, d_gamma_prev, d_cx, d_cy, d_cz, d_normal,
                   d_area, d_uls, d_rhs, d_lx, d_ly, d_lz, d_line_uls, d_wpos, d_wpos2, d_k1, d_wgamma, d_wtx,
                   d_wty, d_wtz, d_vx, d_vy, d_vz, d_A64, d_F32, d_piv, d_tiles, d_rec, d_partial, d_in, d_plan,
-                  d_totals, d_status, d_sweeps, d_res, d_loads};
+                  d_totals, d_status, d_sweeps, d_res, d_loads, d_has_factor, d_refac};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (st) cudaStreamDestroy(st);
@@ -1067,6 +1114,7 @@ int uvlm_batch_config_default(uvlm_batch_config* c) {
   c->max_steps = 151;
   c->device = 0;
   c->use_graph = 1;
+  c->stale_factors = 1;
   return UVLM_OK;
 }
 
@@ -1212,6 +1260,14 @@ int uvlm_batch_get_solve_stats(const uvlm_batch* b, int32_t* sweeps, double* res
     return UVLM_ERR_CUDA;
   if (residual && cudaMemcpy(residual, b->d_res, sizeof(double) * b->n, cudaMemcpyDeviceToHost) != cudaSuccess)
     return UVLM_ERR_CUDA;
+  return UVLM_OK;
+}
+
+int uvlm_batch_factorizations(const uvlm_batch* b, int64_t* count) {
+  if (!b || !count) return UVLM_ERR_INVALID;
+  unsigned long long v = 0;
+  if (cudaMemcpy(&v, b->d_refac, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return UVLM_ERR_CUDA;
+  *count = (int64_t)v;
   return UVLM_OK;
 }
 
