@@ -285,7 +285,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     state = synthetic_state_np()
-    stride, lu_n = 1024, 512
+    stride, lu_n = 128, 1024  # the same sample as the cpu_baseline of the GPU arm
     for _ in range(args.warmup):
         oracle_sample(_heave_pitch(), state, stride, lu_n, threads)
     times = []

@@ -192,6 +192,13 @@ const char* uvlm_nbody_variant_name(int32_t variant);
  * N-body stage and the assembly (target x segment pairs). */
 int uvlm_get_last_work(const uvlm_ctx* ctx, double* nbody_pairs, double* assembly_pairs, double* lu_flops);
 
+/* SimpleSimulator::Velocity (simple_simulator.h:98-100) at n arbitrary points
+ * (targets, out: n x 3 host arrays): the bound and wake sheets' induced
+ * velocity of the current state, minus the forward flight when
+ * include_freestream != 0 (the reference's velocity-field tools, e.g.
+ * src/tools/3d_velocity_main.cpp:73-78, evaluate this on grids). */
+int uvlm_velocity_at(uvlm_ctx* ctx, const double* targets, int64_t n, int32_t include_freestream, double* out);
+
 /* ------------------------------------------- context-free reference API */
 /* UVLM::InducedVelocity(x, pos, gamma) for n_targets points
  * (src/velocity.h:14-24).  pos: (num, grows+1, gcols+1) nodes; gamma:

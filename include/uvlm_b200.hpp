@@ -306,6 +306,15 @@ class SimpleSimulator {
     detail::check(uvlm_step(h_.get(), (int64_t)step, dt, row.data()), "MainLoop", uvlm_last_error(h_.get()));
     return row;
   }
+  // SimpleSimulator::Velocity (simple_simulator.h:98-100): -ff + U_bound + U_wake
+  // at x for the current state.
+  Vector3 Velocity(const Vector3& x) const {
+    Vector3 out{};
+    detail::check(uvlm_velocity_at(h_.get(), reinterpret_cast<const double*>(&x), 1, 1,
+                                   reinterpret_cast<double*>(&out)),
+                  "Velocity", uvlm_last_error(h_.get()));
+    return out;
+  }
   // State of the last step in the reference's member layout.
   void GetState(MultipleSheet<Vector3>* wing_pos, MultipleSheet<double>* wing_gamma, MultipleSheet<Vector3>* wake_pos,
                 MultipleSheet<double>* wake_gamma) const {

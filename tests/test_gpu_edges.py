@@ -97,3 +97,27 @@ def test_batch_of_one_smallest_case():
     ref.set_advection("euler")
     want = ref.run(steps - 1, dt)
     assert np.max(np.abs(L[:, 0, 1:] - want[:, 1:])) <= 1e-9 * np.max(np.abs(want[:, 1:]))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_velocity_at_points_of_the_current_state(precision):
+    """SimpleSimulator::Velocity on a grid of points (the velocity-field
+    tools' use) equals -ff + the oracle's induced velocity of the state."""
+    import pyoracle as o
+
+    import uvlm_b200 as U
+
+    sim = U.SimpleSimulator(precision=precision)
+    sim.AddWing(U.RectGenerator(), U.Morphing().set_alpha(0.08).set_plug(0.1, 1.0), 1.0, 4.0, 4, 8)
+    sim.set_forward_flight([-1.0, 0.0, 0.0])
+    sim.set_advection("RK2")
+    sim.Run(15, 0.15)
+    st = sim.state()
+    g = np.stack(np.meshgrid(np.linspace(-0.5, 3.5, 9), np.linspace(-2.5, 2.5, 7), [-0.3, 0.21], indexing="ij"),
+                 -1).reshape(-1, 3)
+    got = sim.Velocity(g)
+    sim.close()
+    ref = (o.sheet_induced_velocity(st["wing_pos"], st["wing_gamma"], g)
+           + o.sheet_induced_velocity(st["wake_pos"], st["wake_gamma"], g) + np.array([1.0, 0.0, 0.0]))
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    assert np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref))

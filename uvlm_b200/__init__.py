@@ -231,6 +231,16 @@ class SimpleSimulator:
         check(lib().uvlm_get_last_work(self._h, C.byref(a), C.byref(b), C.byref(c)), self._h)
         return a.value, b.value, c.value
 
+    def Velocity(self, x, include_freestream: bool = True) -> np.ndarray:  # noqa: N802
+        """SimpleSimulator::Velocity (simple_simulator.h:98-100) at points x
+        ((3,) or (T, 3)) for the current state: -ff + U_bound + U_wake."""
+        xs = _f64(x)
+        single = xs.ndim == 1
+        xs = np.ascontiguousarray(xs.reshape(-1, 3))
+        out = np.zeros_like(xs)
+        check(lib().uvlm_velocity_at(self._h, _p(xs), xs.shape[0], int(bool(include_freestream)), _p(out)), self._h)
+        return out[0] if single else out
+
     def set_mlp(self, mlp) -> None:
         """Network of the learned warm start (keep it alive while in use)."""
         self._mlp = mlp

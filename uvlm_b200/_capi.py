@@ -107,6 +107,7 @@ SIGNATURES = [
     ("uvlm_synchronize", C.c_int, [_V]),
     ("uvlm_stream", _V, [_V]),
     ("uvlm_get_last_work", C.c_int, [_V, _P, _P, _P]),
+    ("uvlm_velocity_at", C.c_int, [_V, _P, _I, C.c_int32, _P]),
     ("uvlm_kernel_launch_count", C.c_int64, []),
     ("uvlm_measure_fp32_peak", C.c_int, [C.c_int32, _P]),
     ("uvlm_nbody_variant_name", C.c_char_p, [C.c_int32]),

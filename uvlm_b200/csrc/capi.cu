@@ -872,6 +872,46 @@ int uvlm_measure_fp32_peak(int32_t device, double* tflops) {
   return set_global(measure_fp32_fma_peak(device_sms(device), tflops));
 }
 
+int uvlm_velocity_at(uvlm_ctx* c, const double* targets, int64_t n, int32_t include_freestream, double* out) {
+  if (!c || (n > 0 && (!targets || !out)) || n < 0) return set_global(fail(kErrInvalid, "NULL argument"));
+  if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));
+  if (n == 0) return UVLM_OK;
+  cudaSetDevice(c->cfg.device);
+  auto run = [&]() -> Error {
+    SourceBlock blocks[2];
+    int nbk = 0;
+    UVLM_TRY(c->build_sources(true, c->d_wpos, blocks, &nbk));
+    std::vector<double> sx, sy, sz;
+    for (int64_t k0 = 0; k0 < n; k0 += c->tcap) {
+      const long long cnt = std::min<long long>(c->tcap, n - k0);
+      sx.resize(cnt);
+      sy.resize(cnt);
+      sz.resize(cnt);
+      for (long long q = 0; q < cnt; ++q) {
+        sx[q] = targets[3 * (k0 + q)];
+        sy[q] = targets[3 * (k0 + q) + 1];
+        sz[q] = targets[3 * (k0 + q) + 2];
+      }
+      UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_tx, sx.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
+      UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_ty, sy.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
+      UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_tz, sz.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
+      UVLM_TRY(c->eval(blocks, nbk, cnt));
+      UVLM_CUDA_TRY(cudaMemcpyAsync(sx.data(), c->d_vx, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
+      UVLM_CUDA_TRY(cudaMemcpyAsync(sy.data(), c->d_vy, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
+      UVLM_CUDA_TRY(cudaMemcpyAsync(sz.data(), c->d_vz, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
+      UVLM_CUDA_TRY(cudaStreamSynchronize(c->st));
+      const double f = include_freestream ? 1.0 : 0.0;
+      for (long long q = 0; q < cnt; ++q) {
+        out[3 * (k0 + q)] = sx[q] - f * c->ff[0];
+        out[3 * (k0 + q) + 1] = sy[q] - f * c->ff[1];
+        out[3 * (k0 + q) + 2] = sz[q] - f * c->ff[2];
+      }
+    }
+    return ok();
+  };
+  return c->fail_with(run());
+}
+
 int uvlm_get_last_work(const uvlm_ctx* c, double* nbody_pairs, double* assembly_pairs, double* lu_flops) {
   if (!c) return set_global(fail(kErrInvalid, "NULL context"));
   if (nbody_pairs) *nbody_pairs = c->work_nbody;
