@@ -187,12 +187,11 @@ __global__ void __launch_bounds__(kPanelRows) lu_panel_cluster_kernel(T* A, int 
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* rows = reinterpret_cast<T*>(smraw);           // [kPanelRows][kPanelLd]
-  T* urow = rows + kPanelRows * kPanelLd;          // [kLuNB]
-  T* cand_data = urow + kLuNB;                     // [2][kLuNB]
-  T* diag_data = cand_data + 2 * kLuNB;            // [2][kLuNB]
-  double* cand_val = reinterpret_cast<double*>(diag_data + 2 * kLuNB);  // [2]
-  int* cand_row = reinterpret_cast<int*>(cand_val + 2);               // [2]
+  T* rows = reinterpret_cast<T*>(smraw);                     // [kPanelRows][kPanelLd]
+  T* cand_data = rows + kPanelRows * kPanelLd;               // [2][kMaxClusterCtas][kLuNB]
+  T* diag_data = cand_data + 2 * kMaxClusterCtas * kLuNB;    // [2][kLuNB]
+  double* cand_val = reinterpret_cast<double*>(diag_data + 2 * kLuNB);  // [2][kMaxClusterCtas]
+  int* cand_row = reinterpret_cast<int*>(cand_val + 2 * kMaxClusterCtas);  // [2][kMaxClusterCtas]
   __shared__ int s_piv, s_owner;
   const int P = (int)cl.num_blocks(), bid = (int)cl.block_rank(), tid = threadIdx.x;
   const int m = n - k0;
@@ -215,21 +214,33 @@ __global__ void __launch_bounds__(kPanelRows) lu_panel_cluster_kernel(T* A, int 
       br = pr;
     }
     block_argmax(bv, br);
-    if (tid == 0) {
-      cand_val[par] = bv;
-      cand_row[par] = (bv >= 0.0) ? br : -1;
+    // Every CTA pushes its candidate (value, row, data) into slot `bid` of
+    // every CTA's shared memory, and the CTA holding row c pushes that row;
+    // after the cluster barrier each CTA reduces and swaps locally, so no
+    // remote read follows the barrier.  A slot is rewritten two columns later
+    // (double buffering), after the next barrier, when its readers are done.
+    const bool has = bv >= 0.0;
+    for (int idx = tid; idx < P * kb; idx += blockDim.x) {
+      const int q = idx / kb, j = idx % kb;
+      const T v = has ? rows[(br - rb) * kPanelLd + j] : (T)0;
+      *cl.map_shared_rank(cand_data + (par * kMaxClusterCtas + bid) * kLuNB + j, q) = v;
     }
-    if (bv >= 0.0)
-      for (int q = tid; q < kb; q += blockDim.x) cand_data[par * kLuNB + q] = rows[(br - rb) * kPanelLd + q];
+    if (tid < P) {
+      *cl.map_shared_rank(cand_val + par * kMaxClusterCtas + bid, tid) = bv;
+      *cl.map_shared_rank(cand_row + par * kMaxClusterCtas + bid, tid) = has ? br : -1;
+    }
     if (c >= rb && c < rb + nloc)
-      for (int q = tid; q < kb; q += blockDim.x) diag_data[par * kLuNB + q] = rows[(c - rb) * kPanelLd + q];
+      for (int idx = tid; idx < P * kb; idx += blockDim.x) {
+        const int q = idx / kb, j = idx % kb;
+        *cl.map_shared_rank(diag_data + par * kLuNB + j, q) = rows[(c - rb) * kPanelLd + j];
+      }
     cl.sync();
     if (tid < 32) {
       double v = -1.0;
       int r = INT_MAX, ow = -1;
       for (int q = tid; q < P; q += 32) {
-        const double cv = *cl.map_shared_rank(cand_val + par, q);
-        const int cr = *cl.map_shared_rank(cand_row + par, q);
+        const double cv = cand_val[par * kMaxClusterCtas + q];
+        const int cr = cand_row[par * kMaxClusterCtas + q];
         if (cr >= 0 && (cv > v || (cv == v && cr < r))) { v = cv; r = cr; ow = q; }
       }
       for (int off = 16; off; off >>= 1) {
@@ -251,16 +262,11 @@ __global__ void __launch_bounds__(kPanelRows) lu_panel_cluster_kernel(T* A, int 
     }
     __syncthreads();
     const int p = s_piv, ow = s_owner;
-    const int diag_owner = c / kPanelRows;
-    const T* src = (ow >= 0) ? cl.map_shared_rank(cand_data + par * kLuNB, ow)
-                             : cl.map_shared_rank(diag_data + par * kLuNB, diag_owner);
-    for (int q = tid; q < kb; q += blockDim.x) urow[q] = src[q];
-    __syncthreads();
+    const T* urow = (ow >= 0) ? cand_data + (par * kMaxClusterCtas + ow) * kLuNB : diag_data + par * kLuNB;
+    const T* drow = diag_data + par * kLuNB;
     // the swap, each row copied by all threads of the CTA that holds it
-    if (p != c && p >= rb && p < rb + nloc) {
-      const T* dsrc = cl.map_shared_rank(diag_data + par * kLuNB, diag_owner);
-      for (int q = tid; q < kb; q += blockDim.x) rows[(p - rb) * kPanelLd + q] = dsrc[q];
-    }
+    if (p != c && p >= rb && p < rb + nloc)
+      for (int q = tid; q < kb; q += blockDim.x) rows[(p - rb) * kPanelLd + q] = drow[q];
     if (c >= rb && c < rb + nloc)
       for (int q = tid; q < kb; q += blockDim.x) rows[(c - rb) * kPanelLd + q] = urow[q];
     __syncthreads();
@@ -270,9 +276,10 @@ __global__ void __launch_bounds__(kPanelRows) lu_panel_cluster_kernel(T* A, int 
       my[c] = l;
       for (int q = c + 1; q < kb; ++q) my[q] -= l * urow[q];
     }
-    __syncthreads();
+    // the next column's block_argmax barrier orders these updates before
+    // any thread reads another thread's row
   }
-  cl.sync();  // no CTA leaves while another may still read its shared memory
+  cl.sync();
   for (int q = tid; q < nloc * kb; q += blockDim.x) {
     const int r = q / kb, c = q % kb;
     A[(long long)(k0 + rb + r) * lda + k0 + c] = rows[r * kPanelLd + c];
@@ -285,7 +292,8 @@ template <class T>
 bool launch_panel_cluster(T* A, int n, int k0, int kb, int P, int* ipiv, int* err, cudaStream_t st) {
   if (P > kMaxClusterCtas) return false;
   auto kern = lu_panel_cluster_kernel<T>;
-  const size_t smem = sizeof(T) * ((size_t)kPanelRows * kPanelLd + 5 * kLuNB) + 2 * sizeof(double) + 2 * sizeof(int);
+  const size_t smem = sizeof(T) * ((size_t)kPanelRows * kPanelLd + 2 * kMaxClusterCtas * kLuNB + 2 * kLuNB) +
+                      2 * kMaxClusterCtas * (sizeof(double) + sizeof(int));
   static int configured = 0;
   if (!configured) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
