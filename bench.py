@@ -502,19 +502,24 @@ def run_ours(args, rank, world, local_rank):
     simmx.close()
 
 
-def run_batch(args):
+def run_batch(args, rank=0, world=1, local_rank=0):
     """The 256-case seeded flapping-wing sweep (chordwise 4-16, spanwise 8-64,
     AR 2-10, k 0.1-1, heave 0.05-0.3 c, pitch 0-20 deg, 150 Euler steps per
     case) in one batch: aggregate case-steps/s over steps 1..149, device-timed
     on the batch's stream; the FP64 batch beside it and the CL error of the
-    mixed batch against it."""
+    mixed batch against it.  Under torchrun the cases are split over the ranks
+    by their N-body work (shard_cases; no data moves while stepping) and the
+    time is the maximum over ranks."""
     import torch
 
     import uvlm_b200 as U
-    from uvlm_b200.batch import draw_cases, make_batch
+    from uvlm_b200.batch import case_cost, draw_cases, make_batch, shard_cases
 
-    cases = draw_cases(256, seed=0)
+    all_cases = draw_cases(256, seed=0)
     steps = 150
+    mine = shard_cases([case_cost(d, steps) for d in all_cases], world)[rank]
+    cases = [all_cases[i] for i in mine]
+    torch.cuda.set_device(local_rank)
     warm = make_batch(cases, precision="mixed", max_steps=args.warmup + 1)
     warm.run(args.warmup + 1)  # module load, graph capture, first launches
     warm.close()
@@ -522,10 +527,14 @@ def run_batch(args):
     for prec in ("mixed", "fp64"):
         sim = make_batch(cases, precision=prec, max_steps=steps)
         sim.run(1)
-        stream = torch.cuda.ExternalStream(sim.stream(), device=0)
+        stream = torch.cuda.ExternalStream(sim.stream(), device=local_rank)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        clocks = Clocks(0) if prec == "mixed" else None
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        clocks = Clocks(local_rank) if prec == "mixed" else None
         if clocks:
             clocks.start()
         l0 = U.lib().uvlm_kernel_launch_count()
@@ -536,24 +545,33 @@ def run_batch(args):
         launches = U.lib().uvlm_kernel_launch_count() - l0
         clk = clocks.stop() if clocks else None
         ms = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
         out[prec] = dict(ms=ms, loads=sim.loads(), launches=launches, per_step=sim.launches_per_step(), clocks=clk,
                          res=sim.solve_stats()[1], factorizations=sim.factorizations())
         sim.close()
+    if rank != 0:
+        return
     L, L64 = out["mixed"]["loads"], out["fp64"]["loads"]
     cl_err = float(np.max(np.abs(L[:, :, 2] - L64[:, :, 2]).max(axis=0) / np.abs(L64[:, :, 2]).max(axis=0)))
     value = 256 * (steps - 1) / (out["mixed"]["ms"] * 1e-3)
     line = {"metric": "case-steps/s (256 seeded flapping-wing cases x 150 steps, batched, mixed)", "value": value,
-            "unit": "case-steps/s", "n_gpus": 1, "steps": steps - 1, "warmup": args.warmup,
+            "unit": "case-steps/s", "n_gpus": world, "steps": steps - 1, "warmup": args.warmup,
             "ms_per_step": out["mixed"]["ms"] / (steps - 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": "batch256: seed 0 draws, rows U{4..16}, even cols U{8..64}, AR U[2,10], "
                                    "k U[0.1,1], heave U[0.05,0.3] c, pitch U[0,20] deg, phase 90 deg, Euler, "
                                    "150 MainLoops each, all cases in one graph-replayed step",
-                       "panels_total": int(sum(d["rows"] * d["cols"] for d in cases)),
+                       "panels_total": int(sum(d["rows"] * d["cols"] for d in all_cases)),
+                       "parallelism": f"cases sharded over {world} GPU(s) by N-body work",
                        "form": "FP32 N-body, per-case FP32 LU (refactored only when refinement from the "
                                "previous step's factors stalls) + FP64 refinement (residual <= 1e-12)"},
             "plain_fp64_case_steps_per_s": 256 * (steps - 1) / (out["fp64"]["ms"] * 1e-3),
-            "cl_rel_err_max_over_cases": cl_err,
+            "cl_rel_err_max_over_cases": cl_err, "cl_err_scope": f"the {len(cases)} cases of rank 0",
             "refinement_residual_max": float(np.max(out["mixed"]["res"])),
             "factorizations": {"mixed": out["mixed"]["factorizations"], "fp64": out["fp64"]["factorizations"],
                                "case_steps": 256 * steps},
@@ -586,7 +604,21 @@ def main():
         run_profile(args)
         return
     if args.workload == "batch256":
-        run_batch(args)
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        try:
+            run_batch(args, rank, world, local_rank)
+        finally:
+            if world > 1:
+                import torch.distributed as dist
+
+                dist.destroy_process_group()
         return
     if world > 1:
         import datetime
