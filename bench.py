@@ -16,8 +16,9 @@ plain_fp64  steps/s of the plain FP64 form (fresh FP64 LU every step)
 cl_rel_err  max |CL_mixed - CL_fp64| / max |CL_fp64| over the 400-step run
 e2e         the same metric through the C-ABI, wall-clock, with the load row
             and the circulation vector copied to host memory every step
-roofline    the N-body advection kernel: 59 FLOP per (target, unique segment)
-            pair over the measured FP32 FMA peak of this GPU
+roofline    the N-body kernel: 59 FLOP per (target, unique segment) pair of
+            every N-body launch of a step over their CUDA-event time, against
+            the measured FP32 FMA peak of this GPU
 cpu_baseline the FP64 CPU oracle (restated reference) on a bounded sample
 
 --impl reference times that CPU oracle alone (the reference cannot be built
@@ -428,12 +429,18 @@ def run_ours(args, rank, world, local_rank):
     sim64.step(step0 - 1, DT)
     stage64 = [float(x) for x in sim64.stats().stage_ms]
     sim64.set_stage_timing(False)
-    pairs_advect = wl.advect_pairs()
-    adv_ms = stage_ms[5]
-    achieved = FLOP_PER_PAIR * pairs_advect / (adv_ms * 1e-3) / 1e12
-    peak = U._capi.c_double() if False else None
     import ctypes as C
 
+    # roofline of the N-body kernel: the step's algorithmic pairs (RHS, loads,
+    # advection) over the device time of its N-body launches (CUDA events
+    # around each launch on the library's stream)
+    pairs_step = C.c_double()
+    U._capi.check(U.lib().uvlm_get_last_work(simmx._h, C.byref(pairs_step), None, None))
+    nbody_ms = float(stmx.nbody_ms)
+    achieved = FLOP_PER_PAIR * pairs_step.value / (nbody_ms * 1e-3) / 1e12
+    pairs_advect = wl.advect_pairs()
+    adv_ms = stage_ms[5]
+    advect_stage_tflops = FLOP_PER_PAIR * pairs_advect / (adv_ms * 1e-3) / 1e12
     pk = C.c_double()
     U._capi.check(U.lib().uvlm_measure_fp32_peak(dev, C.byref(pk)))
     peak = pk.value
@@ -483,11 +490,13 @@ def run_ours(args, rank, world, local_rank):
             "plain_fp64_stage_ms": {"kin_shed": stage64[0], "assembly": stage64[1], "rhs": stage64[2],
                                     "solve": stage64[3], "loads": stage64[4], "advect": stage64[5],
                                     "total": stage64[7]},
-            "roofline": {"bound": "fp32_simt", "kernel": f"nbody_kernel ({wl.advection} advection stage)",
+            "roofline": {"bound": "fp32_simt", "kernel": "nbody_kernel (every N-body launch of a step: RHS, "
+                                                              f"loads, {wl.advection} advection)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "FP32 FMA probe on this GPU (uvlm_measure_fp32_peak)",
                          "per_unit": f"{FLOP_PER_PAIR} FLOP per (target, unique segment) pair",
-                         "units_per_step": pairs_advect,
+                         "units_per_step": pairs_step.value, "nbody_ms_per_step": nbody_ms,
+                         "advect_stage_tflops": advect_stage_tflops, "advect_pairs_per_step": pairs_advect,
                          "traffic": NBODY_TRAFFIC.get(wl.name),
                          "traffic_unit": "DRAM bytes per advection launch (ncu dram__bytes_read.sum + "
                                          "dram__bytes_write.sum, one launch at the held wake)"},

@@ -134,6 +134,7 @@ typedef struct {
   int32_t nbody_variant; /* N-body tile variant in use (see uvlm_nbody_variant_name) */
   int32_t pad_;
   double initial_residual; /* ||b - A g0|| / ||b|| of the GMRES initial guess */
+  double nbody_ms;         /* with stage timing: device time of the step's N-body launches */
 } uvlm_step_stats;
 
 /* ------------------------------------------------------- time-stepper */

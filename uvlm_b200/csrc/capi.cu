@@ -115,6 +115,10 @@ struct uvlm_ctx {
   uvlm_step_stats last{};
   double work_nbody = 0, work_asm = 0, work_lu = 0;
   cudaEvent_t ev[8] = {};
+  // per-launch events around the N-body evaluations of a timed step
+  static constexpr int kNbEvents = 8;
+  cudaEvent_t nbev[2 * kNbEvents] = {};
+  int nbev_n = 0;
 
   WingShape ws() const { return WingShape{num, R, C}; }
   WakeLayout wl() const { return WakeLayout{num, C, PR, wake_start, wake_nodes}; }
@@ -281,8 +285,15 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt) {
     UVLM_CUDA_TRY(cudaMemsetAsync(d_vz, 0, sizeof(double) * nt, st));
     return ok();
   }
-  return nbody_eval(blocks, nblocks, mixed() ? kNBodyFP32 : kNBodyFP64, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb,
+const bool rec = timing && nbev_n < kNbEvents;
+  if (rec) UVLM_CUDA_TRY(cudaEventRecord(nbev[2 * nbev_n], st));
+    const Error e = nbody_eval(blocks, nblocks, mixed() ? kNBodyFP32 : kNBodyFP64, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb,
                     mixed() ? variant_fp32 : variant_fp64, num_sms, st);
+  if (rec) {
+    UVLM_CUDA_TRY(cudaEventRecord(nbev[2 * nbev_n + 1], st));
+    ++nbev_n;
+  }
+  return e;
 }
 
 Error uvlm_ctx::shed(long long step) {
@@ -441,6 +452,7 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   const double t = step * dt;
   cur_dt = dt;
   work_nbody = work_asm = work_lu = 0;
+  nbev_n = 0;
   last.initial_residual = 0;
   mark(0);
   UVLM_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, st));
@@ -534,7 +546,15 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
     last.stage_ms[5] = ms[5];
     last.stage_ms[6] = 0;
     last.stage_ms[7] = ms[6];
+    double nbt = 0;
+    for (int q = 0; q < nbev_n; ++q) {
+      float m = 0;
+      cudaEventElapsedTime(&m, nbev[2 * q], nbev[2 * q + 1]);
+      nbt += m;
+    }
+    last.nbody_ms = nbt;
   }
+  nbev_n = 0;
   return ok();
 }
 
@@ -613,6 +633,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
     return set_global(fail(kErrCuda, "cudaStreamCreate failed"));
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
+  for (auto& e : c->nbev) cudaEventCreate(&e);
   if (k.nbody_variant >= 0) {
     c->tuned = true;
     if (k.nbody_variant >= nbody_num_variants()) {
@@ -635,6 +656,8 @@ int uvlm_destroy(uvlm_ctx* c) {
   cudaFree(c->d_collect_x);
   cudaFree(c->d_collect_t);
   for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->nbev)
     if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
