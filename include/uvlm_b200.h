@@ -253,6 +253,18 @@ int uvlm_rings_solve_linear_problem(const double* bound_rings, const double* bou
                                     const double* wake_rings, const double* wake_gamma, int64_t n_wake,
                                     const double freestream[3], const uvlm_kinematics* kin, double t,
                                     int32_t drop_wake_term, double* gamma_out);
+/* Impulse post-processing (src/calc_impulse_main.cpp:51-83), FP64.
+ * Sum over rings of VortexRing::Impulse() = -Normal * gamma * Area
+ * (CalcVortexImpulse, calc_impulse_main.cpp:34-41; vortex.cpp:140-143). */
+int uvlm_rings_vortex_impulse(const double* rings, const double* gammas, int64_t n, double out[3]);
+/* Sum over panels of calc_impulse::CalcLambVectorOnPanel(panel_i,
+ * node_velocities_i, freestreams_i, vortices) (calc_impulse.h:15-30, summed
+ * as calc_impulse_main.cpp:79-82): node_velocities [n_panels][4][3], one per
+ * segment in ForEachSegment order; freestreams [n_panels][3]; the induced
+ * velocity at each segment midpoint comes from every ring of `vortices`. */
+int uvlm_rings_lamb_vector(const double* panels, const double* panel_gamma, const double* node_velocities,
+                           int64_t n_panels, const double* freestreams, const double* vortices,
+                           const double* vortex_gamma, int64_t n_vortices, double out[3]);
 /* ---------------------------------------------- learned warm start (MLP) */
 /* No counterpart in the reference.  A per-panel MLP (8 features -> 3 x 256
  * GELU -> 1, BF16 weights, FP32 accumulation) predicts the correction of the

@@ -64,6 +64,10 @@ def _declare(L):
     L.orc_ring_vector.argtypes = [_P, C.c_double, C.c_int, _P]
     L.orc_ring_scalar.argtypes = [_P, C.c_int]
     L.orc_ring_scalar.restype = C.c_double
+    L.orc_vortex_impulse.argtypes = [_P, _P, _I, _P]
+    L.orc_vortex_impulse.restype = None
+    L.orc_lamb_vector.argtypes = [_P, _P, _P, _I, _P, _P, _P, _I, _P]
+    L.orc_lamb_vector.restype = None
     L.orc_ring_angle_of_attack.argtypes = [_P, _P]
     L.orc_ring_angle_of_attack.restype = C.c_double
     L.orc_rings_induced_velocity.argtypes = [_P, _P, _I, _P, C.c_int, _P]
@@ -347,3 +351,24 @@ class Simulator:
         if rc:
             raise RuntimeError("time_step_sampled failed")
         return sec
+
+
+def vortex_impulse(rings, gammas):
+    """Sum of VortexRing::Impulse() over AoS rings (calc_impulse_main.cpp:34-41)."""
+    rings = _v(rings).reshape(-1, 12)
+    out = np.zeros(3)
+    lib().orc_vortex_impulse(_p(rings), _p(_v(gammas)), rings.shape[0], _p(out))
+    return out
+
+
+def lamb_vector(panels, panel_gamma, v_nodes, freestream, vortices, vortex_gamma):
+    """Sum over panels of CalcLambVectorOnPanel (calc_impulse.h:15-30); freestream is one 3-vector or one per
+    panel (calc_impulse_main.cpp:79-82)."""
+    panels = _v(panels).reshape(-1, 12)
+    fs = np.ascontiguousarray(np.broadcast_to(_v(freestream).reshape(-1, 3), (panels.shape[0], 3)))
+    vortices = _v(vortices).reshape(-1, 12)
+    out = np.zeros(3)
+    lib().orc_lamb_vector(_p(panels), _p(_v(panel_gamma)), _p(_v(v_nodes).reshape(-1, 12)), panels.shape[0],
+                          _p(fs), _p(vortices) if vortices.size else None,
+                          _p(_v(vortex_gamma)) if vortices.size else None, vortices.shape[0], _p(out))
+    return out

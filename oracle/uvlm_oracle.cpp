@@ -844,6 +844,46 @@ double orc_ring_angle_of_attack(const double nodes[12], const double Q[3]) {
   return std::atan2(dot(V3(Q), RingNormal(r)), dot(V3(Q), RingTangent(r)));
 }
 
+void orc_vortex_impulse(const double* rings, const double* gammas, int64_t n, double out[3]) {
+  // CalcVortexImpulse (calc_impulse_main.cpp:34-41): sum of VortexRing::Impulse()
+  // = Normal() * gamma * Area() * (-1) (vortex.cpp:140-143)
+  V3 res;
+  for (int64_t k = 0; k < n; k++) {
+    Ring r = LoadRing(rings + 12 * k, gammas[k]);
+    res += RingNormal(r) * gammas[k] * RingArea(r) * (-1);
+  }
+  res.store(out);
+}
+
+void orc_lamb_vector(const double* panels, const double* panel_gamma, const double* v_nodes, int64_t n_panels,
+                     const double* freestreams, const double* vortices, const double* vortex_gamma,
+                     int64_t n_vortices, double out[3]) {
+  // CalcLambVectorOnPanel (calc_impulse.h:15-30), summed over the panels as
+  // calc_impulse_main.cpp:79-82 does: for each segment (ForEachSegment order,
+  // start = nodes[k+1], end = nodes[k]) ue = v_node[k] + u(mid) - freestream_i,
+  // res += (ue x dl) * gamma with u the velocity of every vortex
+  // (InducedVelocityByVortices, uvlm_vortex_ring.cpp:13-22).
+  std::vector<Ring> vort(n_vortices);
+  for (int64_t k = 0; k < n_vortices; k++) vort[k] = LoadRing(vortices + 12 * k, vortex_gamma[k]);
+  V3 res;
+  for (int64_t i = 0; i < n_panels; i++) {
+    Ring p = LoadRing(panels + 12 * i, panel_gamma[i]);
+    const V3 fs(freestreams + 3 * i);
+    V3 acc;
+    for (int k = 0; k < 4; k++) {
+      const V3 start = p.nodes[(k + 1) % 4], end = p.nodes[k];
+      const V3 dl = end - start;
+      const V3 pos = (start + end) / 2;
+      V3 u;
+      for (const auto& v : vort) u += RingBiotSavart(v, pos, v.gamma);
+      const V3 ue = V3(v_nodes + 12 * i + 3 * k) + u - fs;
+      acc += cross(ue, dl) * panel_gamma[i];
+    }
+    res += acc;
+  }
+  res.store(out);
+}
+
 void orc_rings_induced_velocity(const double* rings, const double* gammas, int64_t n_rings,
                                 const double pos[3], int chordwise_only, double out[3]) {
   // src/shed.inl:22-33, 66-77

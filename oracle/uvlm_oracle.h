@@ -72,6 +72,17 @@ void orc_ring_vector(const double nodes[12], double gamma, int what,
 /* what: 0 area, 1 calc_c, 2 calc_b */
 double orc_ring_scalar(const double nodes[12], int what);
 double orc_ring_angle_of_attack(const double nodes[12], const double Q[3]);
+
+/* ---- impulse post-processing: src/calc_impulse.h, calc_impulse_main.cpp -- */
+/* Sum over rings of VortexRing::Impulse() (CalcVortexImpulse,
+ * calc_impulse_main.cpp:34-41; vortex.cpp:140-143). */
+void orc_vortex_impulse(const double* rings, const double* gammas, int64_t n, double out[3]);
+/* Sum over panels of CalcLambVectorOnPanel(panel, v_nodes, freestream,
+ * vortices) (calc_impulse.h:15-30); v_nodes: 4 x 3 per panel, one per
+ * segment in ForEachSegment order; freestreams: 3 per panel. */
+void orc_lamb_vector(const double* panels, const double* panel_gamma, const double* v_nodes, int64_t n_panels,
+                     const double* freestreams, const double* vortices, const double* vortex_gamma,
+                     int64_t n_vortices, double out[3]);
 void orc_rings_induced_velocity(const double* rings, const double* gammas,
                                 int64_t n_rings, const double pos[3],
                                 int chordwise_only, double out[3]);

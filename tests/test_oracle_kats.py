@@ -326,3 +326,21 @@ def test_simulator_symmetric_and_finite():
     assert s["wake_pos"].shape == (1, 7, 9, 3)
     # steady lift at 5 degrees is positive once the start-up transient decays
     assert loads[-1, 2] > 0
+
+
+SQUARE2 = np.array([[0, 0, 0], [2, 0, 0], [2, 2, 0], [0, 2, 0]], dtype=float)  # GetSquareRing(2), testutil.h:23-30
+
+
+def test_kat_ring_impulse():  # test/vortex_test.cpp:194-199
+    np.testing.assert_allclose(o.vortex_impulse(SQUARE2[None], [10.0]), [0, 0, -40], atol=1e-12)
+
+
+@pytest.mark.parametrize("gamma, v_nodes, expect", [
+    (1.0, [[1, 0, 0], [2, 0, 0], [3, 0, 0], [4, 0, 0]], [0, 0, 4]),     # test/calc_impulse_test.cpp:6-20
+    (2.0, [[1, 0, 0], [2, 0, 0], [3, 0, 0], [4, 0, 0]], [0, 0, 8]),     # :22-36
+    (1.0, [[0, 1, 0], [0, 2, 0], [0, 3, 0], [0, 4, 0]], [0, 0, -4]),    # :38-52
+])
+def test_kat_lamb_vector_no_other_vortex(gamma, v_nodes, expect):
+    got = o.lamb_vector(SQUARE2[None], [gamma], np.array(v_nodes, float)[None], [0, 0, 0], np.zeros((0, 12)),
+                        np.zeros(0))
+    np.testing.assert_allclose(got, expect, atol=1e-12)

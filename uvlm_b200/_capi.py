@@ -121,6 +121,8 @@ SIGNATURES = [
     ("uvlm_rings_connect_trailing_edge", C.c_int, [_P, _I, _P]),
     ("uvlm_rings_solve_linear_problem", C.c_int, [_P, _P, _I, _P, _P, _I, _P, C.POINTER(Kinematics),
                                                   C.c_double, C.c_int32, _P]),
+    ("uvlm_rings_vortex_impulse", C.c_int, [_P, _P, _I, _P]),
+    ("uvlm_rings_lamb_vector", C.c_int, [_P, _P, _P, _I, _P, _P, _P, _I, _P]),
     ("uvlm_mlp_create", C.c_int, [C.c_uint64, C.POINTER(_V)]),
     ("uvlm_mlp_destroy", C.c_int, [_V]),
     ("uvlm_mlp_num_params", C.c_int64, [_V]),

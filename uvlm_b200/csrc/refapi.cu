@@ -105,6 +105,83 @@ __global__ void shift_rows_kernel(const double* src, int num, int src_rows, doub
   }
 }
 
+// ----------------------------------------------- impulse post-processing
+// Midpoints of the four segments of every panel in ForEachSegment order
+// (vortex.h:132-140: start = nodes[k+1], end = nodes[k]) as AoS targets.
+__global__ void lamb_midpoints_kernel(const double* __restrict__ panels, long long n, double* __restrict__ t) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < 4 * n; q += (long long)gridDim.x * blockDim.x) {
+    const long long i = q / 4;
+    const int k = (int)(q % 4);
+    const double* p = panels + 12 * i;
+    const d3 start = ld3(p + 3 * ((k + 1) % 4)), end = ld3(p + 3 * k);
+    st3(t + 3 * q, dvs(add(start, end), 2));
+  }
+}
+
+constexpr int kSumThreads = 256;
+
+__device__ inline d3 block_sum3(d3 v, double* sh) {
+  for (int off = 16; off; off >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, off);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, off);
+    v.z += __shfl_down_sync(0xffffffffu, v.z, off);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[3 * wid] = v.x;
+    sh[3 * wid + 1] = v.y;
+    sh[3 * wid + 2] = v.z;
+  }
+  __syncthreads();
+  d3 r = mk(0, 0, 0);
+  for (int w = 0; w < kSumThreads / 32; ++w) r = add(r, mk(sh[3 * w], sh[3 * w + 1], sh[3 * w + 2]));
+  return r;
+}
+
+// CalcLambVectorOnPanel (calc_impulse.h:15-30) summed over the panels as
+// calc_impulse_main.cpp:79-82 does, FP64, one CTA (fixed summation order):
+// ue = v_node[k] + u(mid_k) - freestream_i, res += (ue x dl) * gamma,
+// dl = end - start.
+__global__ void __launch_bounds__(kSumThreads) lamb_sum_kernel(const double* __restrict__ panels,
+                                                               const double* __restrict__ pg,
+                                                               const double* __restrict__ vnodes,
+                                                               const double* __restrict__ fs, long long n,
+                                                               const double* __restrict__ u, double* out) {
+  __shared__ double sh[3 * kSumThreads / 32];
+  d3 acc = mk(0, 0, 0);
+  for (long long i = threadIdx.x; i < n; i += kSumThreads) {
+    const double* p = panels + 12 * i;
+    const d3 f = ld3(fs + 3 * i);
+    d3 a = mk(0, 0, 0);
+    for (int k = 0; k < 4; ++k) {
+      const d3 dl = sub(ld3(p + 3 * k), ld3(p + 3 * ((k + 1) % 4)));
+      const d3 ue = sub(add(ld3(vnodes + 12 * i + 3 * k), ld3(u + 3 * (4 * i + k))), f);
+      a = add(a, scl(cross(ue, dl), pg[i]));
+    }
+    acc = add(acc, a);
+  }
+  const d3 r = block_sum3(acc, sh);
+  if (threadIdx.x == 0) st3(out, r);
+}
+
+// CalcVortexImpulse (calc_impulse_main.cpp:34-41): sum of Normal * gamma *
+// Area * (-1) (vortex.cpp:140-143; Normal :82-87, Area :132-138), one CTA.
+__global__ void __launch_bounds__(kSumThreads) vortex_impulse_kernel(const double* __restrict__ rings,
+                                                                     const double* __restrict__ g, long long n,
+                                                                     double* out) {
+  __shared__ double sh[3 * kSumThreads / 32];
+  d3 acc = mk(0, 0, 0);
+  for (long long i = threadIdx.x; i < n; i += kSumThreads) {
+    const double* r = rings + 12 * i;
+    const d3 a = ld3(r), b = ld3(r + 3), c = ld3(r + 6), d = ld3(r + 9);
+    const d3 nrm = normalized(cross(sub(b, d), sub(c, a)));
+    const double area = (norm(cross(sub(b, a), sub(d, a))) + norm(cross(sub(d, c), sub(b, c)))) / 2;
+    acc = add(acc, scl(nrm, -g[i] * area));
+  }
+  const d3 r = block_sum3(acc, sh);
+  if (threadIdx.x == 0) st3(out, r);
+}
+
 inline int gfor(long long n) { return (int)std::min<long long>(std::max<long long>((n + 255) / 256, 1), 65535); }
 
 Error velocity_at(const SheetView* views, int nv, NBodyPrec prec, const double* d_targets_aos, long long nt,
@@ -505,6 +582,79 @@ int uvlm_dense_solve(const double* A, int64_t n, const double* b, double* x, int
     lu_work_free(&lu);
     UVLM_TRY(e);
     UVLM_CUDA_TRY(cudaMemcpy(x, dx, sizeof(double) * N, cudaMemcpyDeviceToHost));
+    return ok();
+  };
+  return report(run());
+}
+
+int uvlm_rings_vortex_impulse(const double* rings, const double* gammas, int64_t n, double out[3]) {
+  if (n < 0 || !out || (n && (!rings || !gammas))) return report(fail(kErrInvalid, "invalid argument"));
+  Scratch S;
+  auto run = [&]() -> Error {
+    double *dr, *dg, *dout;
+    UVLM_TRY(S.get(&dout, 3));
+    if (n > 0) {
+      UVLM_TRY(S.up(&dr, rings, (size_t)(12 * n)));
+      UVLM_TRY(S.up(&dg, gammas, (size_t)n));
+    } else {
+      dr = dg = nullptr;
+    }
+    vortex_impulse_kernel<<<1, kSumThreads>>>(dr, dg, n, dout);
+    UVLM_LAUNCH_CHECK();
+    UVLM_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+    return ok();
+  };
+  return report(run());
+}
+
+int uvlm_rings_lamb_vector(const double* panels, const double* panel_gamma, const double* node_velocities,
+                           int64_t n_panels, const double* freestreams, const double* vortices,
+                           const double* vortex_gamma, int64_t n_vortices, double out[3]) {
+  if (n_panels < 0 || n_vortices < 0 || !out ||
+      (n_panels && (!panels || !panel_gamma || !node_velocities || !freestreams)) ||
+      (n_vortices && (!vortices || !vortex_gamma)))
+    return report(fail(kErrInvalid, "invalid argument"));
+  Scratch S;
+  auto run = [&]() -> Error {
+    double *dp, *dg, *dv, *df, *dt, *vx, *vy, *vz, *du, *dout;
+    UVLM_TRY(S.get(&dout, 3));
+    const long long nt = 4 * n_panels;
+    if (n_panels > 0) {
+      UVLM_TRY(S.up(&dp, panels, (size_t)(12 * n_panels)));
+      UVLM_TRY(S.up(&dg, panel_gamma, (size_t)n_panels));
+      UVLM_TRY(S.up(&dv, node_velocities, (size_t)(12 * n_panels)));
+      UVLM_TRY(S.up(&df, freestreams, (size_t)(3 * n_panels)));
+      UVLM_TRY(S.get(&dt, 3 * nt));
+      UVLM_TRY(S.get(&vx, nt));
+      UVLM_TRY(S.get(&vy, nt));
+      UVLM_TRY(S.get(&vz, nt));
+      UVLM_TRY(S.get(&du, 3 * nt));
+      lamb_midpoints_kernel<<<gfor(nt), 256>>>(dp, n_panels, dt);
+      UVLM_LAUNCH_CHECK();
+      if (n_vortices > 0) {
+        // velocity of every vortex ring at the midpoints (InducedVelocityByVortices)
+        double *dr, *drg, *pos, *gam;
+        UVLM_TRY(S.up(&dr, vortices, (size_t)(12 * n_vortices)));
+        UVLM_TRY(S.up(&drg, vortex_gamma, (size_t)n_vortices));
+        UVLM_TRY(S.get(&pos, 12 * n_vortices));
+        UVLM_TRY(S.get(&gam, n_vortices));
+        rings_to_sheets<<<gfor(n_vortices), 256>>>(dr, drg, n_vortices, pos, gam);
+        UVLM_LAUNCH_CHECK();
+        SheetView v{pos, 2, 0, gam, 1, 0, (int)n_vortices, 2, 1, 0};
+        UVLM_TRY(velocity_at(&v, 1, kNBodyFP64, dt, nt, vx, vy, vz, S));
+      } else {
+        UVLM_CUDA_TRY(cudaMemset(vx, 0, 8 * nt));
+        UVLM_CUDA_TRY(cudaMemset(vy, 0, 8 * nt));
+        UVLM_CUDA_TRY(cudaMemset(vz, 0, 8 * nt));
+      }
+      soa_to_aos<<<gfor(nt), 256>>>(vx, vy, vz, nt, du, nullptr, nullptr, 1.0);
+      UVLM_LAUNCH_CHECK();
+    } else {
+      dp = dg = dv = df = du = nullptr;
+    }
+    lamb_sum_kernel<<<1, kSumThreads>>>(dp, dg, dv, df, n_panels, du, dout);
+    UVLM_LAUNCH_CHECK();
+    UVLM_CUDA_TRY(cudaMemcpy(out, dout, sizeof(double) * 3, cudaMemcpyDeviceToHost));
     return ok();
   };
   return report(run());

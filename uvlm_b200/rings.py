@@ -70,3 +70,28 @@ def SolveLinearProblem(bound_rings, wake_rings, wake_gammas, freestream, morphin
                                                 _p(_f64(freestream)), C.byref(morphing.k), float(t),
                                                 int(drop_wake_term), _p(out)))
     return out
+
+
+def CalcVortexImpulse(rings, gammas) -> np.ndarray:  # noqa: N802
+    """Sum of VortexRing::Impulse() over the rings (calc_impulse_main.cpp:34-41, vortex.cpp:140-143)."""
+    r = _f64(rings).reshape(-1, 4, 3)
+    g = _f64(gammas).reshape(-1)
+    out = np.zeros(3)
+    check(lib().uvlm_rings_vortex_impulse(_p(r), _p(g), r.shape[0], out.ctypes.data_as(_P)))
+    return out
+
+
+def CalcLambVector(panels, panel_gammas, node_velocities, freestream, vortices, vortex_gammas) -> np.ndarray:  # noqa: N802
+    """Sum over panels of calc_impulse::CalcLambVectorOnPanel (calc_impulse.h:15-30), as
+    calc_impulse_main.cpp:79-82 sums it.  node_velocities: (n, 4, 3), one per segment in
+    ForEachSegment order; freestream: one 3-vector or one per panel."""
+    p = _f64(panels).reshape(-1, 4, 3)
+    g = _f64(panel_gammas).reshape(-1)
+    v = _f64(node_velocities).reshape(-1, 4, 3)
+    fs = np.ascontiguousarray(np.broadcast_to(_f64(freestream).reshape(-1, 3), (p.shape[0], 3)))
+    w = _f64(vortices).reshape(-1, 4, 3)
+    wg = _f64(vortex_gammas).reshape(-1)
+    out = np.zeros(3)
+    check(lib().uvlm_rings_lamb_vector(_p(p), _p(g), _p(v), p.shape[0], _p(fs), _p(w), _p(wg), w.shape[0],
+                                       out.ctypes.data_as(_P)))
+    return out
