@@ -48,9 +48,10 @@ DT = 2 * math.pi / OMEGA / 40
 WAKE_ROWS = 400
 FLOP_PER_PAIR = 59
 # DRAM bytes of one advection launch of the N-body kernel at the held wake,
-# from an ncu capture of the packed FP32x2 tile (bench.py --profile): about the
-# algorithmic bytes (56,115 source records x 64 B + targets + outputs).
-NBODY_TRAFFIC = {"heave_pitch": 4955648}
+# from an ncu capture of the packed FP32x2 tile with the far-field walker
+# (bench.py --profile): about the algorithmic bytes (56,115 source records x
+# 64 B + targets + outputs).
+NBODY_TRAFFIC = {"heave_pitch": 4899072}
 
 
 def make_mixed(device=0, warm_start=None, wl=None):

@@ -418,3 +418,54 @@ def test_every_fp32_tile_variant_agrees():
         rows, wpos = run("mixed", v)
         assert np.max(np.abs(rows[:, 1:] - ref[:, 1:])) <= 1e-6 * scale, names[v]
         assert np.max(np.abs(wpos - wref)) <= 1e-6, names[v]
+
+
+def _long_wake_state(rows, cols, wake_rows, span=8.0, seed=3):
+    """A wing lattice and a convected, wavy wake of `wake_rows` rows (about
+    0.157 chords apart) with smooth circulations plus noise."""
+    rng = np.random.default_rng(seed)
+    X, Y = np.meshgrid(np.linspace(0.0, 1.0, rows + 1), np.linspace(-span / 2, span / 2, cols + 1), indexing="ij")
+    wing = np.stack([X, Y, 0.04 * np.sin(3.0 * X) * np.cos(0.3 * Y)], -1)[None]
+    k = np.arange(wake_rows + 1)[:, None]
+    Yw = np.linspace(-span / 2, span / 2, cols + 1)[None, :] * (1.0 - 0.1 * np.tanh(k / 60.0))
+    wake = np.stack([1.0 + 0.157 * k + 0.0 * Yw, Yw, 0.2 * np.sin(0.3 * k) + 0.05 * np.cos(0.7 * Yw)], -1)
+    wake = wake + 0.005 * rng.standard_normal(wake.shape)
+    wing_g = (0.3 * np.cos(np.linspace(-1.4, 1.4, cols))[None, :] * np.ones((rows, 1))
+              + 0.01 * rng.standard_normal((rows, cols)))[None]
+    wake_g = (0.1 * np.sin(0.3 * np.arange(wake_rows))[:, None] * np.ones((1, cols))
+              + 0.01 * rng.standard_normal((wake_rows, cols)))[None]
+    return wing, wake[None], wing_g, wake_g
+
+
+def test_far_field_walker_matches_oracle():
+    """The far-field walker (strip-local coordinates, beyond-end form only)
+    gives per-target velocities as accurate as the near-field walker against
+    the FP64 oracle on a long wake, and it is taken (the two tiles round
+    differently)."""
+    import pyoracle as o
+
+    M = U()
+    rows, cols, wr = 6, 128, 100
+    wing, wake, wing_g, wake_g = _long_wake_state(rows, cols, wr)
+    # whole node rows of the wake as targets (consecutive, as advection uses them)
+    targets = np.ascontiguousarray(wake[0, ::4].reshape(-1, 3))
+    ref = o.sheet_induced_velocity(wing, wing_g, targets) + o.sheet_induced_velocity(wake, wake_g, targets)
+    scale = np.max(np.abs(ref))
+    names = [M.lib().uvlm_nbody_variant_name(v).decode() for v in range(64)]
+    got = {}
+    for v, name in enumerate(names):
+        if not name.startswith("fp32") or "_x2" not in name:
+            continue
+        sim = M.SimpleSimulator(precision="mixed", nbody_variant=v)
+        sim.AddWing(M.RectGenerator(), M.Morphing(), 1.0, 8.0, rows, cols)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.begin()
+        sim.set_state(wr, wing, wake, wing_g, wing_g, wake_g)
+        got[name] = sim.Velocity(targets, include_freestream=False)
+        sim.close()
+    near = np.max(np.abs(got["fp32_h3_t2_b128_x2"] - ref)) / scale
+    assert near <= 1e-5
+    for name in [n for n in got if n.endswith("_x2f")]:
+        err = np.max(np.abs(got[name] - ref)) / scale
+        assert err <= max(3 * near, 1e-7), (name, err, near)
+        assert not np.array_equal(got[name], got[name[:-1]]), name  # the far walker ran

@@ -98,7 +98,7 @@ struct uvlm_ctx {
   LuWork lu;
   GmresWork gm;
   bool have_factors = false;
-  int variant_fp64 = 9, variant_fp32 = 13;  // defaults: fp64_h2_t1_b128_m3, fp32_h3_t2_b128_x2
+  int variant_fp64 = 9, variant_fp32 = 16;  // defaults: fp64_h2_t1_b128_m3, fp32_h3_t2_b128_x2f
   bool tuned = false;  // N-body tile variant chosen (autotune or config)
   // learned warm start: network (borrowed), per-step features, collected data
   uvlm_mlp* mlp = nullptr;

@@ -366,6 +366,148 @@ __device__ __forceinline__ void walk_full_strip2(const RecF* sm, bool last_h, co
   }
 }
 
+// ------------------------------------------- far-field packed walker
+// A strip whose staged nodes all lie within rho of a local origin O (one of
+// its own nodes) is "far" from a target x when |x - O| >= 2 rho + 1e-3.  Then
+// every pair has |r| >= rho + 1e-3, so no node is cut (|r| > 1e-10) and every
+// r1.r2 > 0 (the strip subtends less than 60 degrees from x), which leaves the
+// beyond-end form of the segment factor alone, without cancellation.  With
+// node and target coordinates relative to O (FP32, rounded from the hi/lo
+// differences), r = x_O - p_O costs one subtraction per component instead of
+// three, and its error stays below ulp(rho)/2 + ulp(|x_O|)/2 <= 1.5 ulp(|r|).
+// The cut |d|^2 < 1e-10 is kept (a far target can lie on a segment's line).
+__device__ __forceinline__ Node2 node_far2(const float4 L, const float2 (&ts)[3]) {
+  Node2 n;
+  n.rx = add2(ts[0], bc2(-L.x));
+  n.ry = add2(ts[1], bc2(-L.y));
+  n.rz = add2(ts[2], bc2(-L.z));
+  const float2 q = fma2(n.rz, n.rz, fma2(n.ry, n.ry, mul2(n.rx, n.rx)));
+  n.n = mul2(q, make_float2(nb_rsqrt(q.x), nb_rsqrt(q.y)));
+  return n;
+}
+
+__device__ __forceinline__ void seg_far2(const SegV<float>& r0, const Node2& a, const Node2& b, float g, float2& vx,
+                                         float2& vy, float2& vz) {
+  const float2 dx = fma2(bc2(r0.y), a.rz, mul2(bc2(-r0.z), a.ry));
+  const float2 dy = fma2(bc2(r0.z), a.rx, mul2(bc2(-r0.x), a.rz));
+  const float2 dz = fma2(bc2(r0.x), a.ry, mul2(bc2(-r0.y), a.rx));
+  const float2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+  const float2 dot12 = fma2(a.rz, b.rz, fma2(a.ry, b.ry, mul2(a.rx, b.rx)));
+  const float2 nn = mul2(a.n, b.n);
+  const float2 den = mul2(nn, add2(nn, dot12));
+  float2 k = mul2(mul2(bc2(g), add2(a.n, b.n)), make_float2(nb_rcp(den.x), nb_rcp(den.y)));
+  k.x = d2.x >= (float)kCutD2 ? k.x : 0.f;
+  k.y = d2.y >= (float)kCutD2 ? k.y : 0.f;
+  vx = fma2(k, dx, vx);
+  vy = fma2(k, dy, vy);
+  vz = fma2(k, dz, vz);
+}
+
+// One node column of a far strip: local node coordinates and gS from `lcol`,
+// the rest of the record (gH, segment vectors) from `col`.
+template <int H, bool FIRST, bool DO_H>
+__device__ __forceinline__ void far_column2(const RecF* col, const float4* lcol, const float2 (&ts)[3],
+                                            Node2 (&prev)[H], SegV<float> (&ps0)[H], float (&pgS)[H],
+                                            float2 (&acc)[3]) {
+  Node2 cur[H + 1];
+  float gS[H], gH[H];
+  SegV<float> s0[H], h0[H];
+#pragma unroll
+  for (int r = 0; r <= H; ++r) {
+    const float4 L = lcol[r * (kStripCols + 1)];
+    if (r < H) {
+      const RecF& rec = col[r * (kStripCols + 1)];
+      const float4 sv = rec.sv;
+      gS[r] = L.w;
+      gH[r] = rec.lo.w;
+      s0[r] = SegV<float>{sv.x, sv.y, sv.z};
+      h0[r] = SegV<float>{sv.w, rec.hv.x, rec.hv.y};
+    }
+    cur[r] = node_far2(L, ts);
+  }
+  if (DO_H) {
+#pragma unroll
+    for (int r = 0; r < H; ++r) seg_far2(h0[r], cur[r], cur[r + 1], gH[r], acc[0], acc[1], acc[2]);
+  }
+  if (!FIRST) {
+#pragma unroll
+    for (int r = 0; r < H; ++r) seg_far2(ps0[r], prev[r], cur[r], pgS[r], acc[0], acc[1], acc[2]);
+  }
+#pragma unroll
+  for (int r = 0; r < H; ++r) {
+    pgS[r] = gS[r];
+    ps0[r] = s0[r];
+    prev[r] = cur[r];
+  }
+}
+
+template <int H>
+__device__ __forceinline__ void walk_far_strip2(const RecF* sm, const float4* loc, bool last_h,
+                                                const float2 (&ts)[3], float (&acc)[2][3]) {
+  Node2 prev[H];
+  SegV<float> ps0[H];
+  float pgS[H];
+  float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  far_column2<H, true, true>(sm, loc, ts, prev, ps0, pgS, a2);
+#pragma unroll 2
+  for (int j = 1; j < kStripCols; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pgS, a2);
+  if (last_h)
+    far_column2<H, false, true>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pgS, a2);
+  else
+    far_column2<H, false, false>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pgS, a2);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    acc[0][c] += a2[c].x;
+    acc[1][c] += a2[c].y;
+  }
+}
+
+// Local coordinates of a staged full strip relative to its central real node
+// O: loc[k] = (p_k - O, gS_k) for real nodes, (0, 0, 0, gS_k) for the zero
+// padding (whose segments are cut by d = 0 either way).  Returns whether all
+// of this warp's targets are far from the strip (warp-uniform) and their
+// coordinates relative to O.  `red` holds one float per warp.
+template <int H, int BLOCK>
+__device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si, float4* loc, float* red,
+                                            const Tgt<float> (&tg)[2], float2 (&ts)[3]) {
+  constexpr int kRecs = (H + 1) * (kStripCols + 1);
+  const RecF& o = sm[((si.nr - 1) >> 1) * (kStripCols + 1) + ((si.n_cols - 1) >> 1)];
+  const float4 oh = o.hi, ol = o.lo;
+  float m = 0.f;
+  for (int k = threadIdx.x; k < kRecs; k += BLOCK) {
+    const int r = k / (kStripCols + 1), j = k - r * (kStripCols + 1);
+    const float4 h = sm[k].hi, l = sm[k].lo;
+    float4 L = make_float4(0.f, 0.f, 0.f, h.w);
+    if (r < si.nr && j < si.n_cols) {
+      L.x = (h.x - oh.x) + (l.x - ol.x);
+      L.y = (h.y - oh.y) + (l.y - ol.y);
+      L.z = (h.z - oh.z) + (l.z - ol.z);
+      m = fmaxf(m, fmaf(L.z, L.z, fmaf(L.y, L.y, L.x * L.x)));
+    }
+    loc[k] = L;
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  float rho2 = red[0];
+#pragma unroll
+  for (int w = 1; w < BLOCK / 32; ++w) rho2 = fmaxf(rho2, red[w]);
+  const float lim = 2.000001f * sqrtf(rho2) + 1e-3f;
+  bool far = true;
+  float tsv[2][3];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    tsv[q][0] = (tg[q].hx - oh.x) + (tg[q].lx - ol.x);
+    tsv[q][1] = (tg[q].hy - oh.y) + (tg[q].ly - ol.y);
+    tsv[q][2] = (tg[q].hz - oh.z) + (tg[q].lz - ol.z);
+    far = far && fmaf(tsv[q][2], tsv[q][2], fmaf(tsv[q][1], tsv[q][1], tsv[q][0] * tsv[q][0])) >= lim * lim;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ts[c] = make_float2(tsv[0][c], tsv[1][c]);
+  return __all_sync(0xffffffffu, far);
+}
+
 // Targets tile0 + threadIdx.x + q BLOCK (clamped to the last one) of the
 // SoA arrays, as hi/lo FP32 pairs or FP64.
 template <class T, int TPT, int BLOCK>
@@ -391,10 +533,13 @@ __device__ __forceinline__ void load_targets(const double* __restrict__ tx, cons
 
 // Strips [s_begin, s_end) of B for the thread's targets, double-buffered
 // through shared memory; FP32 partial sums per strip, FP64 across strips.
-template <class T, class Rec, int H, int TPT, bool PAD, bool PK = false>
+// PK: 0 generic walkers, 1 packed FP32x2 walker on full strips, 2 the same
+// plus the far-field walker for strips far from all of a warp's targets
+// (`loc`, `red`: its shared-memory scratch).
+template <class T, class Rec, int H, int TPT, int BLOCK, bool PAD, int PK = 0>
 __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, long long s_end,
-                                            const Rec* __restrict__ rec, Rec* buf0, Rec* buf1,
-                                            const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3]) {
+                                            const Rec* __restrict__ rec, Rec* buf0, Rec* buf1, float4* loc,
+                                            float* red, const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3]) {
   if (s_begin >= s_end) return;
   StripInfo si = decode_strip<H>(B, s_begin);
   if constexpr (PAD)
@@ -420,9 +565,15 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
     T acc[TPT][3];
 #pragma unroll
     for (int q = 0; q < TPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = (T)0;
-    if constexpr (PAD && PK && sizeof(T) == 4 && TPT == 2)
+    if constexpr (PAD && PK == 2 && sizeof(T) == 4 && TPT == 2) {
+      float2 ts[3];
+      if (far_prepare<H, BLOCK>(cur, si, loc, red, tg, ts))
+        walk_far_strip2<H>(cur, loc, si.last_h, ts, acc);
+      else
+        walk_full_strip2<H>(cur, si.last_h, tg, acc);
+    } else if constexpr (PAD && PK == 1 && sizeof(T) == 4 && TPT == 2) {
       walk_full_strip2<H>(cur, si.last_h, tg, acc);
-    else if constexpr (PAD)
+    } else if constexpr (PAD)
       walk_full_strip<T, Rec, H, TPT>(cur, si.last_h, tg, acc);
     else
       walk_strip<T, Rec, H, TPT>(cur, si, tg, acc);
@@ -437,7 +588,7 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
   }
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, bool PK>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, int PK>
 __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
                                                        const double* __restrict__ tx, const double* __restrict__ ty,
                                                        const double* __restrict__ tz, long long n_targets,
@@ -445,6 +596,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
+  float4* loc = reinterpret_cast<float4*>(buf1 + (H + 1) * (kStripCols + 1));
+  float* red = reinterpret_cast<float*>(loc + (H + 1) * (kStripCols + 1));
 
   const long long tile0 = (long long)blockIdx.x * BLOCK * TPT;
   Tgt<T> tg[TPT];
@@ -454,7 +607,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
   const long long s_begin = (long long)blockIdx.y * strips_per_split;
   const long long s_end = min(n_strips, s_begin + strips_per_split);
-  eval_strips<T, Rec, H, TPT, PAD, PK>(B, s_begin, s_end, rec, buf0, buf1, tg, accd);
+  eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK>(B, s_begin, s_end, rec, buf0, buf1, loc, red, tg, accd);
   double* px = partial + (long long)blockIdx.y * 3 * n_targets;
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
@@ -540,7 +693,7 @@ __device__ inline int plan_search(const NBodyBatchPlan* plan, int n, long long w
   return lo;
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, bool PK>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, int PK>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBatchPlan* __restrict__ plan, int n,
                                                              const long long* __restrict__ totals,
                                                              const double* __restrict__ tx,
@@ -551,6 +704,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBat
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
+  float4* loc = reinterpret_cast<float4*>(buf1 + (H + 1) * (kStripCols + 1));
+  float* red = reinterpret_cast<float*>(loc + (H + 1) * (kStripCols + 1));
   const long long items = totals[0];
   for (long long w = blockIdx.x; w < items; w += gridDim.x) {
     const int c = plan_search(plan, n, w, [](const NBodyBatchPlan& p) { return p.item_off; });
@@ -565,7 +720,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBat
     for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
     const long long s_begin = split * kBatchStripsPerItem;
     const long long s_end = min(P.n_strips, s_begin + kBatchStripsPerItem);
-    eval_strips<T, Rec, H, TPT, PAD, PK>(P.B, s_begin, s_end, rec, buf0, buf1, tg, accd);
+    eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK>(P.B, s_begin, s_end, rec, buf0, buf1, loc, red, tg, accd);
     double* px = partial + P.part_off + split * 3 * P.n_tgt;
 #pragma unroll
     for (int q = 0; q < TPT; ++q) {
@@ -605,6 +760,7 @@ __global__ void batch_reduce_kernel(const NBodyBatchPlan* __restrict__ plan, int
 // b128, FP64 h2 t1 b128; 3 CTAs/SM each.
 constexpr int kBatchBlock = 128;
 constexpr int kBatchTptF = 2, kBatchHF = 4, kBatchHFP = 3, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
+constexpr int kBatchPadPK = 2;  // walker of the padded class (see eval_strips)
 
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, int splits, long long n, double* vx,
                                        double* vy, double* vz) {
@@ -627,7 +783,7 @@ struct Variant {
   const char* name;
   int prec;  // NBodyPrec
   int H, TPT, BLOCK, MINB;
-  int packed;  // FP32x2 walker for full strips (FP32, TPT = 2)
+  int packed;  // 1: FP32x2 walker for full strips (FP32, TPT = 2); 2: plus the far-field walker
 };
 
 // Tile shapes: H owned node rows per strip, TPT targets per thread, BLOCK
@@ -648,6 +804,9 @@ constexpr Variant kVariants[] = {
     {"fp32_h4_t2_b128_x2", kNBodyFP32, 4, 2, 128, 3, 1},
     {"fp32_h3_t2_b128_x2", kNBodyFP32, 3, 2, 128, 3, 1},
     {"fp32_h2_t2_b128_x2", kNBodyFP32, 2, 2, 128, 3, 1},
+    {"fp32_h4_t2_b128_x2f", kNBodyFP32, 4, 2, 128, 3, 2},
+    {"fp32_h3_t2_b128_x2f", kNBodyFP32, 3, 2, 128, 3, 2},
+    {"fp32_h2_t2_b128_x2f", kNBodyFP32, 2, 2, 128, 3, 2},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -663,13 +822,21 @@ bool use_padded(const Blocks& B) {
   return true;
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PK = false>
+// Dynamic shared memory of a tile: two strip buffers, plus the far-field
+// walker's local coordinates and per-warp maxima (PK == 2).
+template <class Rec, int H, int BLOCK, int PK>
+constexpr size_t strip_smem() {
+  return 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1) +
+         (PK == 2 ? sizeof(float4) * (H + 1) * (kStripCols + 1) + sizeof(float) * (BLOCK / 32) : 0);
+}
+
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, int PK = 0>
 Error launch_variant(const Blocks& B, long long n_strips, const double* tx, const double* ty, const double* tz,
                      long long n_targets, const Rec* rec, NBodyWork* work, double* vx, double* vy, double* vz,
                      int num_sms, cudaStream_t st) {
   const bool pad = use_padded(B);
   auto kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false, PK>;
-  const size_t smem = 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
+  const size_t smem = strip_smem<Rec, H, BLOCK, PK>();
   static bool attr_done[2] = {false, false};
   if (!attr_done[pad]) {
     UVLM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -770,9 +937,12 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
     case 9: return launch_variant<double, RecD, 2, 1, 128, 3>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     case 10: return launch_variant<double, RecD, 2, 1, 256, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     case 11: return launch_variant<float, RecF, 3, 2, 128, 3>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
-    case 12: return launch_variant<float, RecF, 4, 2, 128, 3, true>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
-    case 13: return launch_variant<float, RecF, 3, 2, 128, 3, true>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
-    case 14: return launch_variant<float, RecF, 2, 2, 128, 3, true>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 12: return launch_variant<float, RecF, 4, 2, 128, 3, 1>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 13: return launch_variant<float, RecF, 3, 2, 128, 3, 1>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 14: return launch_variant<float, RecF, 2, 2, 128, 3, 1>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 15: return launch_variant<float, RecF, 4, 2, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 16: return launch_variant<float, RecF, 3, 2, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 17: return launch_variant<float, RecF, 2, 2, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
     default: return fail(kErrInvalid, "bad nbody variant");
   }
 
@@ -799,14 +969,10 @@ long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in,
 }
 
 namespace {
-template <class Rec, int H>
-constexpr size_t batch_smem() {
-  return 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1);
-}
-template <class T, class Rec, int H, int TPT, bool PAD, bool PK>
+template <class T, class Rec, int H, int TPT, bool PAD, int PK>
 int batch_grid_of(int num_sms) {
   const void* k = (const void*)batch_nbody_kernel<T, Rec, H, TPT, kBatchBlock, kBatchMinB, PAD, PK>;
-  const size_t smem = batch_smem<Rec, H>();
+  const size_t smem = strip_smem<Rec, H, kBatchBlock, PK>();
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBatchBlock, smem) != cudaSuccess || occ < 1) occ = 1;
@@ -817,10 +983,10 @@ int batch_grid_of(int num_sms) {
 NBodyBatchGrids nbody_batch_grids(NBodyPrec prec, int num_sms) {
   NBodyBatchGrids g;
   if (prec == kNBodyFP32) {
-    g.general = batch_grid_of<float, RecF, kBatchHF, kBatchTptF, false, false>(num_sms);
-    g.padded = batch_grid_of<float, RecF, kBatchHFP, kBatchTptF, true, true>(num_sms);
+    g.general = batch_grid_of<float, RecF, kBatchHF, kBatchTptF, false, 0>(num_sms);
+    g.padded = batch_grid_of<float, RecF, kBatchHFP, kBatchTptF, true, kBatchPadPK>(num_sms);
   } else {
-    g.general = batch_grid_of<double, RecD, kBatchHD, kBatchTptD, false, false>(num_sms);
+    g.general = batch_grid_of<double, RecD, kBatchHD, kBatchTptD, false, 0>(num_sms);
   }
   return g;
 }
@@ -841,8 +1007,8 @@ Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const
     batch_plan_kernel<kBatchHF, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, 0, d_plan, partial_cap,
                                                                              d_totals, status);
     UVLM_LAUNCH_CHECK();
-    batch_nbody_kernel<float, RecF, kBatchHF, kBatchTptF, kBatchBlock, kBatchMinB, false, false>
-        <<<grids.general, kBatchBlock, batch_smem<RecF, kBatchHF>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
+    batch_nbody_kernel<float, RecF, kBatchHF, kBatchTptF, kBatchBlock, kBatchMinB, false, 0>
+        <<<grids.general, kBatchBlock, strip_smem<RecF, kBatchHF, kBatchBlock, 0>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
                                                                             partial);
     UVLM_LAUNCH_CHECK();
     UVLM_TRY(reduce(grids.general));
@@ -850,8 +1016,8 @@ Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const
     batch_plan_kernel<kBatchHFP, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, 1, d_plan, partial_cap,
                                                                               d_totals, status);
     UVLM_LAUNCH_CHECK();
-    batch_nbody_kernel<float, RecF, kBatchHFP, kBatchTptF, kBatchBlock, kBatchMinB, true, true>
-        <<<grids.padded, kBatchBlock, batch_smem<RecF, kBatchHFP>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
+    batch_nbody_kernel<float, RecF, kBatchHFP, kBatchTptF, kBatchBlock, kBatchMinB, true, kBatchPadPK>
+        <<<grids.padded, kBatchBlock, strip_smem<RecF, kBatchHFP, kBatchBlock, kBatchPadPK>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
                                                                             partial);
     UVLM_LAUNCH_CHECK();
     return reduce(grids.padded);
@@ -859,8 +1025,8 @@ Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const
   batch_plan_kernel<kBatchHD, kBatchBlock * kBatchTptD><<<1, 256, 0, st>>>(d_in, n, -1, d_plan, partial_cap,
                                                                            d_totals, status);
   UVLM_LAUNCH_CHECK();
-  batch_nbody_kernel<double, RecD, kBatchHD, kBatchTptD, kBatchBlock, kBatchMinB, false, false>
-      <<<grids.general, kBatchBlock, batch_smem<RecD, kBatchHD>(), st>>>(
+  batch_nbody_kernel<double, RecD, kBatchHD, kBatchTptD, kBatchBlock, kBatchMinB, false, 0>
+      <<<grids.general, kBatchBlock, strip_smem<RecD, kBatchHD, kBatchBlock, 0>(), st>>>(
           d_plan, n, d_totals, tx, ty, tz, reinterpret_cast<const RecD*>(records), partial);
   UVLM_LAUNCH_CHECK();
   return reduce(grids.general);

@@ -112,7 +112,7 @@ Error run_noalloc(const double* pos, const double* gamma, int64_t num, int64_t g
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    UVLM_TRY(nbody_eval(&blk, 1, prec, tx, ty, tz, n_targets, vx, vy, vz, &w, prec == kNBodyFP32 ? 13 : 9, sms, st));
+    UVLM_TRY(nbody_eval(&blk, 1, prec, tx, ty, tz, n_targets, vx, vy, vz, &w, prec == kNBodyFP32 ? 16 : 9, sms, st));
   } else {
     UVLM_CUDA_TRY(cudaMemsetAsync(vx, 0, 3 * vec_bytes, st));
   }

@@ -201,7 +201,7 @@ Error velocity_at(const SheetView* views, int nv, NBodyPrec prec, const double* 
   UVLM_TRY(S.get(&w.partial, (size_t)w.partial_cap));
   SourceBlock blocks[4];
   UVLM_TRY(nbody_build_sources(views, nv, prec, &w, blocks, 0));
-  const int variant = prec == kNBodyFP32 ? 13 : 9;  // fp32_h3_t2_b128_x2, fp64_h2_t1_b128_m3
+  const int variant = prec == kNBodyFP32 ? 16 : 9;  // fp32_h3_t2_b128_x2f, fp64_h2_t1_b128_m3
   UVLM_TRY(nbody_eval(blocks, nv, prec, tx, ty, tz, nt, vx, vy, vz, &w, variant, sms(), 0));
   return ok();
 }
