@@ -253,6 +253,43 @@ int uvlm_rings_solve_linear_problem(const double* bound_rings, const double* bou
                                     const double* wake_rings, const double* wake_gamma, int64_t n_wake,
                                     const double freestream[3], const uvlm_kinematics* kin, double t,
                                     int32_t drop_wake_term, double* gamma_out);
+/* UVLM::SolveLinearProblem(containers, morphings, freestream, t)
+ * (src/linear.inl:132-157): the bound rings of n_containers containers laid
+ * out one after another (container c has container_rings[c] rings and moves
+ * with kins[c], CalcRhsMorphings :87-104), then the wake rings.  FP64
+ * assembly and LU; drop_wake_term as in uvlm_rings_solve_linear_problem. */
+int uvlm_rings_solve_linear_problem_containers(const double* bound_rings, const double* bound_rings0,
+                                               const int64_t* container_rings, int32_t n_containers,
+                                               const uvlm_kinematics* kins, const double* wake_rings,
+                                               const double* wake_gamma, int64_t n_wake,
+                                               const double freestream[3], double t, int32_t drop_wake_term,
+                                               double* gamma_out);
+/* Morphing::Perfome / Morphing::Velocity (src/morphing.cpp:23-52) of n
+ * reference points x0 [n][3] at time t. */
+int uvlm_kinematics_perfome(const uvlm_kinematics* kin, const double* x0, int64_t n, double t, double* out);
+int uvlm_kinematics_velocity(const uvlm_kinematics* kin, const double* x0, int64_t n, double t, double* out);
+/* calc_load::CalcLoadKatzPlotkin(c, cp, morphing, rings, freestream, rho, t,
+ * dt) (src/calc_load/katz_plotkin.cpp:16-68) for one container of rows x
+ * cols rings (gamma: c, gamma_prev: cp).  The UVLMVortexRing `rings` is
+ * given as its bound rings (chordwise velocity, uvlm_vortex_ring.h:80-83)
+ * and wake rings (:75-78); n = 0 for the empty one the legacy simulator
+ * passes (src/simulator/simulator.cpp:37,183).  out = F.x, F.y, F.z, Pin,
+ * Pout; F starts from zero (the reference leaves it uninitialised) and Pout
+ * is 0 as in the reference. */
+int uvlm_rings_load_katz_plotkin(const double* rings, const double* gamma, const double* gamma_prev, int64_t rows,
+                                 int64_t cols, const uvlm_kinematics* kin, const double* bound_rings,
+                                 const double* bound_gamma, int64_t n_bound, const double* wake_rings,
+                                 const double* wake_gamma, int64_t n_wake, const double freestream[3], double rho,
+                                 double t, double dt, double out[5]);
+/* calc_load::CalcLoadJoukowski(vb, vb_prev, morphing, freestream, rho, t, dt)
+ * (src/calc_load/joukowski.h:24-104) for one container: rings / rings0 are
+ * its nodes() / nodes0(); the induced velocity at the segment midpoints
+ * comes from every ring of `vortices` (the container's whole ring pool).
+ * out = F.x, F.y, F.z, Pin, Pout = -F.x |freestream|. */
+int uvlm_rings_load_joukowski(const double* rings, const double* rings0, const double* gamma,
+                              const double* gamma_prev, int64_t rows, int64_t cols, const uvlm_kinematics* kin,
+                              const double* vortices, const double* vortex_gamma, int64_t n_vortices,
+                              const double freestream[3], double rho, double t, double dt, double out[5]);
 /* Impulse post-processing (src/calc_impulse_main.cpp:51-83), FP64.
  * Sum over rings of VortexRing::Impulse() = -Normal * gamma * Area
  * (CalcVortexImpulse, calc_impulse_main.cpp:34-41; vortex.cpp:140-143). */

@@ -64,6 +64,16 @@ def _declare(L):
     L.orc_ring_vector.argtypes = [_P, C.c_double, C.c_int, _P]
     L.orc_ring_scalar.argtypes = [_P, C.c_int]
     L.orc_ring_scalar.restype = C.c_double
+    L.orc_solve_linear_problem_containers.argtypes = [_P, _P, C.POINTER(C.c_int64), C.c_int,
+                                                      C.POINTER(Kinematics), _P, _P, _I, _P, C.c_double, C.c_int,
+                                                      _P]
+    L.orc_solve_linear_problem_containers.restype = C.c_int
+    L.orc_load_katz_plotkin.argtypes = [_P, _P, _P, _I, _I, C.POINTER(Kinematics), _P, _P, _I, _P, _P, _I, _P,
+                                        C.c_double, C.c_double, C.c_double, _P]
+    L.orc_load_katz_plotkin.restype = None
+    L.orc_load_joukowski_rings.argtypes = [_P, _P, _P, _P, _I, _I, C.POINTER(Kinematics), _P, _P, _I, _P,
+                                           C.c_double, C.c_double, C.c_double, _P]
+    L.orc_load_joukowski_rings.restype = None
     L.orc_vortex_impulse.argtypes = [_P, _P, _I, _P]
     L.orc_vortex_impulse.restype = None
     L.orc_lamb_vector.argtypes = [_P, _P, _P, _I, _P, _P, _P, _I, _P]
@@ -371,4 +381,53 @@ def lamb_vector(panels, panel_gamma, v_nodes, freestream, vortices, vortex_gamma
     lib().orc_lamb_vector(_p(panels), _p(_v(panel_gamma)), _p(_v(v_nodes).reshape(-1, 12)), panels.shape[0],
                           _p(fs), _p(vortices) if vortices.size else None,
                           _p(_v(vortex_gamma)) if vortices.size else None, vortices.shape[0], _p(out))
+    return out
+
+
+def _opt(a):
+    return _p(a) if a is not None and a.size else None
+
+
+def solve_linear_problem_containers(bound_rings, container_rings, kins, wake_rings, wake_gamma, freestream, t,
+                                    drop_wake_term=True, bound_rings0=None):
+    """SolveLinearProblem(containers, morphings, freestream, t) (src/linear.inl:132-157)."""
+    b = _v(bound_rings).reshape(-1, 4, 3)
+    b0 = b if bound_rings0 is None else _v(bound_rings0).reshape(-1, 4, 3)
+    w = _v(wake_rings).reshape(-1, 4, 3)
+    wg = _v(wake_gamma).reshape(-1)
+    sizes = (C.c_int64 * len(container_rings))(*[int(c) for c in container_rings])
+    karr = (Kinematics * len(kins))(*kins)
+    out = np.zeros(b.shape[0])
+    rc = lib().orc_solve_linear_problem_containers(_p(b), _p(b0), sizes, len(kins), karr, _opt(w), _opt(wg),
+                                                   w.shape[0], _p(_v(freestream)), float(t), int(drop_wake_term),
+                                                   _p(out))
+    if rc:
+        raise RuntimeError("singular matrix")
+    return out
+
+
+def load_katz_plotkin(rings, gamma, gamma_prev, rows, cols, kin, freestream, rho, t, dt, bound_rings=None,
+                      bound_gamma=None, wake_rings=None, wake_gamma=None):
+    """CalcLoadKatzPlotkin (src/calc_load/katz_plotkin.cpp:16-68) -> (F, Pin, Pout) as 5 numbers."""
+    r = _v(rings).reshape(-1, 4, 3)
+    b = np.zeros((0, 4, 3)) if bound_rings is None else _v(bound_rings).reshape(-1, 4, 3)
+    bg = np.zeros(0) if bound_gamma is None else _v(bound_gamma).reshape(-1)
+    w = np.zeros((0, 4, 3)) if wake_rings is None else _v(wake_rings).reshape(-1, 4, 3)
+    wg = np.zeros(0) if wake_gamma is None else _v(wake_gamma).reshape(-1)
+    out = np.zeros(5)
+    lib().orc_load_katz_plotkin(_p(r), _p(_v(gamma)), _p(_v(gamma_prev)), int(rows), int(cols), C.byref(kin),
+                                _opt(b), _opt(bg), b.shape[0], _opt(w), _opt(wg), w.shape[0], _p(_v(freestream)),
+                                float(rho), float(t), float(dt), _p(out))
+    return out
+
+
+def load_joukowski_rings(rings, rings0, gamma, gamma_prev, rows, cols, kin, vortices, vortex_gamma, freestream,
+                         rho, t, dt):
+    """Container CalcLoadJoukowski (src/calc_load/joukowski.h:24-104) -> (F, Pin, Pout) as 5 numbers."""
+    r = _v(rings).reshape(-1, 4, 3)
+    v = _v(vortices).reshape(-1, 4, 3)
+    out = np.zeros(5)
+    lib().orc_load_joukowski_rings(_p(r), _p(_v(rings0)), _p(_v(gamma)), _p(_v(gamma_prev)), int(rows), int(cols),
+                                   C.byref(kin), _opt(v), _opt(_v(vortex_gamma)), v.shape[0], _p(_v(freestream)),
+                                   float(rho), float(t), float(dt), _p(out))
     return out

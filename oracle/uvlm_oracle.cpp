@@ -929,12 +929,13 @@ void orc_connect_trailing_edge(const double* edge_rings, int64_t n_edge, double*
   }
 }
 
-int orc_solve_linear_problem(const double* bound_rings, const double* bound_rings0, int64_t n_bound,
-                             const double* wake_rings, const double* wake_gamma, int64_t n_wake,
-                             const double freestream[3], const orc_kinematics* mk, double t,
-                             int drop_wake_term, double* gamma_out) {
-  // src/linear.inl:14-32 (CalcMatrix), :34-45 (FreeStream), :47-61 (Wake),
-  // :63-76 (Morphing), :113-130 (SolveLinearProblem).
+// src/linear.inl:14-32 (CalcMatrix), :34-45 (FreeStream), :47-61 (Wake),
+// :63-104 (Morphing, per container), :113-157 (SolveLinearProblem).  Ring k
+// moves with morphs[kin_of[k]].
+static int SolveRings(const double* bound_rings, const double* bound_rings0, int64_t n_bound,
+                      const double* wake_rings, const double* wake_gamma, int64_t n_wake,
+                      const double freestream[3], const std::vector<Morphing>& morphs,
+                      const std::vector<int>& kin_of, double t, int drop_wake_term, double* gamma_out) {
   std::vector<Ring> b(n_bound);
   for (int64_t k = 0; k < n_bound; k++) {
     b[k] = LoadRing(bound_rings + 12 * k);
@@ -946,10 +947,9 @@ int orc_solve_linear_problem(const double* bound_rings, const double* bound_ring
   for (size_t i = 0; i < n; i++)
     for (size_t j = 0; j < n; j++)
       A[i * n + j] = dot(RingBiotSavart(b[j], RingCentroid(b[i]), 1.), RingNormal(b[i]));
-  Morphing m = MakeMorphing(mk);
   std::vector<double> rhs(n);
   for (size_t i = 0; i < n; i++) {
-    const double morph = dot(m.Velocity(RingRefCentroid(b[i]), t), RingNormal(b[i]));
+    const double morph = dot(morphs[kin_of[i]].Velocity(RingRefCentroid(b[i]), t), RingNormal(b[i]));
     const double fs = dot(V3(freestream), RingNormal(b[i]));
     rhs[i] = morph - fs;
     if (!drop_wake_term) {
@@ -963,6 +963,120 @@ int orc_solve_linear_problem(const double* bound_rings, const double* bound_ring
   if (FullPivLUSolve(A, n, rhs, x)) return 1;
   std::memcpy(gamma_out, x.data(), n * sizeof(double));
   return 0;
+}
+
+int orc_solve_linear_problem(const double* bound_rings, const double* bound_rings0, int64_t n_bound,
+                             const double* wake_rings, const double* wake_gamma, int64_t n_wake,
+                             const double freestream[3], const orc_kinematics* mk, double t,
+                             int drop_wake_term, double* gamma_out) {
+  return SolveRings(bound_rings, bound_rings0, n_bound, wake_rings, wake_gamma, n_wake, freestream,
+                    {MakeMorphing(mk)}, std::vector<int>((size_t)n_bound, 0), t, drop_wake_term, gamma_out);
+}
+
+int orc_solve_linear_problem_containers(const double* bound_rings, const double* bound_rings0,
+                                        const int64_t* container_rings, int n_containers,
+                                        const orc_kinematics* kins, const double* wake_rings,
+                                        const double* wake_gamma, int64_t n_wake, const double freestream[3],
+                                        double t, int drop_wake_term, double* gamma_out) {
+  std::vector<Morphing> morphs;
+  std::vector<int> kin_of;
+  for (int c = 0; c < n_containers; c++) {
+    morphs.push_back(MakeMorphing(kins + c));
+    kin_of.insert(kin_of.end(), (size_t)container_rings[c], c);
+  }
+  return SolveRings(bound_rings, bound_rings0, (int64_t)kin_of.size(), wake_rings, wake_gamma, n_wake,
+                    freestream, morphs, kin_of, t, drop_wake_term, gamma_out);
+}
+
+void orc_load_katz_plotkin(const double* rings, const double* gamma, const double* gamma_prev, int64_t rows,
+                           int64_t cols, const orc_kinematics* mk, const double* bound_rings,
+                           const double* bound_gamma, int64_t n_bound, const double* wake_rings,
+                           const double* wake_gamma, int64_t n_wake, const double freestream[3], double rho,
+                           double t, double dt, double out[5]) {
+  // CalcLoadKatzPlotkin (src/calc_load/katz_plotkin.cpp:16-68) with
+  // CalcLocalLiftSt / CalcLocalDragSt (katz_plotkin.h:21-34), CalcUm and
+  // CalcProjectionOperator (functions.h:14-31), DeltaGamma / Grad
+  // (vortex_container.h:87-96).  F starts from zero.
+  const Morphing m = MakeMorphing(mk);
+  const V3 fs(freestream);
+  V3 F;
+  double Pin = 0;
+  auto g = [&](int64_t i, int64_t j) { return gamma[i * cols + j]; };
+  auto gp = [&](int64_t i, int64_t j) { return gamma_prev[i * cols + j]; };
+  for (int64_t i = 0; i < rows; i++) {
+    for (int64_t j = 0; j < cols; j++) {
+      const Ring v = LoadRing(rings + 12 * (i * cols + j));
+      const V3 centroid = RingCentroid(v);
+      const double db = norm(v.nodes[0] - v.nodes[3]);
+      const double dc = norm(v.nodes[0] - v.nodes[1]);
+      const V3 Um = fs - m.Velocity(centroid, t);
+      const V3 uh = normalized(Um);
+      const V3 n = RingNormal(v);
+      const V3 Pn = n - uh * dot(uh, n);  // (I - u u^T) n
+      const double alpha = std::atan2(dot(Um, n), dot(Um, RingTangent(v)));
+      V3 Uw, Ubc;
+      for (int64_t k = 0; k < n_wake; k++)
+        Uw += RingBiotSavart(LoadRing(wake_rings + 12 * k), centroid, wake_gamma[k]);
+      for (int64_t k = 0; k < n_bound; k++)
+        Ubc += RingChordwiseBiotSavart(LoadRing(bound_rings + 12 * k), centroid, bound_gamma[k]);
+      const double dg = g(i, j) - (i == 0 ? 0.0 : g(i - 1, j));
+      const V3 grad = RingTangent(v) * dg / dc;
+      const double Lst = rho * dot(Um + Uw, grad) * db * dc * std::cos(alpha);
+      const double Dst = rho * (-dot(Um + Ubc, Pn) * dg * db);
+      double dg_dt = (g(i, j) - gp(i, j)) / dt;
+      if (i > 0) dg_dt += (g(i - 1, j) - gp(i - 1, j)) / dt;
+      dg_dt /= 2;
+      const double Lunst = rho * dg_dt * db * dc * std::cos(alpha);
+      const double Dunst = rho * dg_dt * db * dc * std::sin(alpha);
+      const V3 dF = Um / norm(Um) * (Dst + Dunst) + Pn * (Lst + Lunst);
+      F += dF;
+      Pin += (-1) * dot(Um, n) * dot(dF, n);
+    }
+  }
+  F.store(out);
+  out[3] = Pin;
+  out[4] = 0;
+}
+
+void orc_load_joukowski_rings(const double* rings, const double* rings0, const double* gamma,
+                              const double* gamma_prev, int64_t rows, int64_t cols, const orc_kinematics* mk,
+                              const double* vortices, const double* vortex_gamma, int64_t n_vortices,
+                              const double freestream[3], double rho, double t, double dt, double out[5]) {
+  // CalcLoadJoukowski (src/calc_load/joukowski.h:24-104): steady part per
+  // segment with U = u_ind(mid) + CalcUm(mid0) (the trailing-edge segment of
+  // the last row skipped), unsteady part Normal rho dG/dt B C, Pin = sum dF .
+  // Vls(reference centroid), Pout = -Fx |freestream|.
+  const Morphing m = MakeMorphing(mk);
+  const V3 fs(freestream);
+  std::vector<Ring> pool(n_vortices);
+  for (int64_t k = 0; k < n_vortices; k++) pool[k] = LoadRing(vortices + 12 * k, vortex_gamma[k]);
+  V3 F;
+  double Pin = 0;
+  for (int64_t i = 0; i < rows; i++) {
+    for (int64_t j = 0; j < cols; j++) {
+      const int64_t K = i * cols + j;
+      Ring v = LoadRing(rings + 12 * K, gamma[K]);
+      for (int q = 0; q < 4; q++) v.nodes0[q] = V3(rings0 + 12 * K + 3 * q);
+      V3 st;
+      for (int q = 0; q < 4; q++) {
+        if (i + 1 == rows && q == 1) continue;
+        const V3 a = v.nodes[(q + 1) % 4], b = v.nodes[q];
+        const V3 mid = (a + b) / 2, mid0 = (v.nodes0[(q + 1) % 4] + v.nodes0[q]) / 2;
+        V3 uind;
+        for (const auto& r : pool) uind += RingBiotSavart(r, mid, r.gamma);
+        const V3 U = uind + (fs - m.Velocity(mid0, t));
+        st += cross(U, b - a) * rho * v.gamma;
+      }
+      const double B = norm(v.nodes[0] - v.nodes[3]), Cc = norm(v.nodes[0] - v.nodes[1]);
+      const V3 unst = RingNormal(v) * rho * ((gamma[K] - gamma_prev[K]) / dt) * B * Cc;
+      const V3 dF = st + unst;
+      F += dF;
+      Pin += dot(dF, m.Velocity(RingRefCentroid(v), t));
+    }
+  }
+  F.store(out);
+  out[3] = Pin;
+  out[4] = F.x * norm(fs) * (-1);
 }
 
 void orc_calc_morphing_velocity_on_wing(const double* rings, const double* rings0, int64_t n,

@@ -100,6 +100,25 @@ int orc_solve_linear_problem(const double* bound_rings,
                              int64_t n_wake, const double freestream[3],
                              const orc_kinematics* m, double t,
                              int drop_wake_term, double* gamma_out);
+/* SolveLinearProblem(containers, morphings, freestream, t) (src/linear.inl:
+ * 132-157): container c has container_rings[c] bound rings and kins[c]. */
+int orc_solve_linear_problem_containers(const double* bound_rings, const double* bound_rings0,
+                                        const int64_t* container_rings, int n_containers,
+                                        const orc_kinematics* kins, const double* wake_rings,
+                                        const double* wake_gamma, int64_t n_wake, const double freestream[3],
+                                        double t, int drop_wake_term, double* gamma_out);
+/* calc_load::CalcLoadKatzPlotkin (src/calc_load/katz_plotkin.cpp:16-68);
+ * out = F (3), Pin, Pout. */
+void orc_load_katz_plotkin(const double* rings, const double* gamma, const double* gamma_prev, int64_t rows,
+                           int64_t cols, const orc_kinematics* m, const double* bound_rings,
+                           const double* bound_gamma, int64_t n_bound, const double* wake_rings,
+                           const double* wake_gamma, int64_t n_wake, const double freestream[3], double rho,
+                           double t, double dt, double out[5]);
+/* container calc_load::CalcLoadJoukowski (src/calc_load/joukowski.h:24-104). */
+void orc_load_joukowski_rings(const double* rings, const double* rings0, const double* gamma,
+                              const double* gamma_prev, int64_t rows, int64_t cols, const orc_kinematics* m,
+                              const double* vortices, const double* vortex_gamma, int64_t n_vortices,
+                              const double freestream[3], double rho, double t, double dt, double out[5]);
 void orc_calc_morphing_velocity_on_wing(const double* rings,
                                         const double* rings0, int64_t n,
                                         const orc_kinematics* m, double t,

@@ -344,3 +344,38 @@ def test_kat_lamb_vector_no_other_vortex(gamma, v_nodes, expect):
     got = o.lamb_vector(SQUARE2[None], [gamma], np.array(v_nodes, float)[None], [0, 0, 0], np.zeros((0, 12)),
                         np.zeros(0))
     np.testing.assert_allclose(got, expect, atol=1e-12)
+
+
+def test_katz_plotkin_flat_panel_steady():
+    """A steady flat unit panel in U = (1, 0, 0): alpha = 0, L_st = rho U G b, no drag, no Pin
+    (CalcLoadKatzPlotkin, src/calc_load/katz_plotkin.cpp:16-68)."""
+    k = o.Kinematics()
+    out = o.load_katz_plotkin(SQUARE2[None] / 2, [0.7], [0.7], 1, 1, k, [1, 0, 0], 1.0, 0.0, 0.1)
+    np.testing.assert_allclose(out, [0, 0, 0.7, 0, 0], atol=1e-14)
+
+
+def test_wing_builder_mirror_and_build():  # test/wing_builder_test.cpp:31-123
+    import legacy_oracle as L
+
+    pts = np.array([[[i, j, 0] for j in range(4)] for i in range(3)], float)  # rows 2, cols 3, p = (i, j, 0)
+    r = L.container_rings(pts, 2, 3, (0, 0, 0))
+    assert r.shape == (12, 4, 3)                              # 2 x 6 rings
+    np.testing.assert_array_equal(r[0, 0], [0, -3, 0])        # container.at(0, 0).nodes()[0]
+    np.testing.assert_array_equal(r[0, 1], [1, -3, 0])
+    np.testing.assert_array_equal(r[5, 3], [0, 3, 0])         # ring (0, 5): p(0, 6) = (0, 3, 0)
+    r2 = L.container_rings(pts, 2, 3, (0, 0, 1))
+    assert np.all(r2[..., 2] == 1)                            # add_multiple_wings: origin z = 1
+
+
+def test_legacy_loop_symmetric_and_finite():
+    import legacy_oracle as L
+
+    X, Y = np.meshgrid(np.linspace(0, 1, 3), np.linspace(0, 2, 4), indexing="ij")
+    k = o.Kinematics()
+    k.alpha, k.plug_amp, k.plug_omega = 0.1, 0.1, 1.0
+    w = dict(rows=2, cols=3, points=np.stack([X, Y, 0 * X], -1), origin=(0, 0, 0), chord=1.0, span=2.0)
+    for jouk in (False, True):
+        rows = L.start([w], [k], [1, 0, 0], 6, 0.1, use_joukowski=jouk)
+        assert rows.shape == (7, 6) and np.all(np.isfinite(rows))
+        np.testing.assert_allclose(rows[:, 2], 0, atol=1e-12)   # C_y of a symmetric wing
+        assert rows[-1, 3] > 0                                  # lift at alpha = 0.1

@@ -90,6 +90,22 @@ class Morphing:
         for i in range(3):
             self.k.origin[i] = float(origin[i])
 
+    def Perfome(self, x0, t: float) -> np.ndarray:  # noqa: N802 (reference name)
+        """Morphing::Perfome (src/morphing.cpp:23-43) of reference point(s) x0 ((3,) or (n, 3)), on the GPU."""
+        return self._eval(lib().uvlm_kinematics_perfome, x0, t)
+
+    def Velocity(self, x0, t: float) -> np.ndarray:  # noqa: N802 (reference name)
+        """Morphing::Velocity (src/morphing.cpp:45-52) of reference point(s) x0, on the GPU."""
+        return self._eval(lib().uvlm_kinematics_velocity, x0, t)
+
+    def _eval(self, fn, x0, t):
+        x = _f64(x0)
+        single = x.ndim == 1
+        x = np.ascontiguousarray(x.reshape(-1, 3))
+        out = np.zeros_like(x)
+        check(fn(C.byref(self.k), _p(x), x.shape[0], float(t), _p(out)))
+        return out[0] if single else out
+
     def Clear(self) -> None:  # noqa: N802 (reference name)
         alpha = self.k.alpha
         origin = tuple(self.k.origin)
@@ -377,6 +393,7 @@ def lu_factor_f32(A, update: str = "tf32"):
 
 
 from . import rings  # noqa: E402  (legacy AoS API)
+from . import legacy  # noqa: E402  (legacy stepper over the AoS API)
 from . import warmstart  # noqa: E402  (learned warm start)
 
 

@@ -121,6 +121,15 @@ SIGNATURES = [
     ("uvlm_rings_connect_trailing_edge", C.c_int, [_P, _I, _P]),
     ("uvlm_rings_solve_linear_problem", C.c_int, [_P, _P, _I, _P, _P, _I, _P, C.POINTER(Kinematics),
                                                   C.c_double, C.c_int32, _P]),
+    ("uvlm_rings_solve_linear_problem_containers", C.c_int, [_P, _P, C.POINTER(C.c_int64), C.c_int32,
+                                                             C.POINTER(Kinematics), _P, _P, _I, _P, C.c_double,
+                                                             C.c_int32, _P]),
+    ("uvlm_kinematics_perfome", C.c_int, [C.POINTER(Kinematics), _P, _I, C.c_double, _P]),
+    ("uvlm_kinematics_velocity", C.c_int, [C.POINTER(Kinematics), _P, _I, C.c_double, _P]),
+    ("uvlm_rings_load_katz_plotkin", C.c_int, [_P, _P, _P, _I, _I, C.POINTER(Kinematics), _P, _P, _I, _P, _P, _I,
+                                               _P, C.c_double, C.c_double, C.c_double, _P]),
+    ("uvlm_rings_load_joukowski", C.c_int, [_P, _P, _P, _P, _I, _I, C.POINTER(Kinematics), _P, _P, _I, _P,
+                                            C.c_double, C.c_double, C.c_double, _P]),
     ("uvlm_rings_vortex_impulse", C.c_int, [_P, _P, _I, _P]),
     ("uvlm_rings_lamb_vector", C.c_int, [_P, _P, _P, _I, _P, _P, _P, _I, _P]),
     ("uvlm_mlp_create", C.c_int, [C.c_uint64, C.POINTER(_V)]),

@@ -11,77 +11,13 @@
 #include "gmres.cuh"
 #include "lu.cuh"
 #include "nbody.cuh"
+#include "refapi_util.cuh"
 #include "step.cuh"
 
 using namespace uvlm;
 
 namespace {
 
-int report(const Error& e) {
-  if (e.code) set_global_error(e.msg);
-  return e.code;
-}
-
-int sms() {
-  int d = 0, v = 148;
-  cudaGetDevice(&d);
-  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
-  return v;
-}
-
-// Device buffers freed at scope exit.
-struct Scratch {
-  std::vector<void*> p;
-  ~Scratch() {
-    for (void* q : p) cudaFree(q);
-  }
-  template <class T>
-  Error get(T** out, size_t count) {
-    *out = nullptr;
-    if (count == 0) return ok();
-    UVLM_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(out), sizeof(T) * count));
-    p.push_back(*out);
-    return ok();
-  }
-  template <class T>
-  Error up(T** out, const T* host, size_t count) {
-    UVLM_TRY(get(out, count));
-    if (count) UVLM_CUDA_TRY(cudaMemcpy(*out, host, sizeof(T) * count, cudaMemcpyHostToDevice));
-    return ok();
-  }
-};
-
-__global__ void aos_to_soa(const double* a, long long n, double* x, double* y, double* z) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    x[k] = a[3 * k];
-    y[k] = a[3 * k + 1];
-    z[k] = a[3 * k + 2];
-  }
-}
-__global__ void soa_to_aos(const double* x, const double* y, const double* z, long long n, double* a, const double* add3,
-                           const double* base, double scale) {
-  // a = base + (v + add3) * scale   (base/add3 may be NULL)
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    double v[3] = {x[k], y[k], z[k]};
-    for (int d = 0; d < 3; ++d) {
-      double u = v[d] + (add3 ? add3[d] : 0.0);
-      a[3 * k + d] = base ? base[3 * k + d] + u * scale : u;
-    }
-  }
-}
-// AoS ring k (nodes n0..n3) -> 1 x 1 sheet k with p(0,0)=n0, p(0,1)=n1,
-// p(1,1)=n2, p(1,0)=n3 and circulation -g: the sheet walks n0->n1->n2->n3,
-// the AoS ring nodes[k+1]->nodes[k] (src/vortex.h:132-140).
-__global__ void rings_to_sheets(const double* rings, const double* g, long long n, double* pos, double* gam) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    const double* r = rings + 12 * k;
-    double* p = pos + 12 * k;
-    const int map[4] = {0, 1, 3, 2};  // sheet order (0,0),(0,1),(1,0),(1,1)
-    for (int q = 0; q < 4; ++q)
-      for (int d = 0; d < 3; ++d) p[3 * q + d] = r[3 * map[q] + d];
-    gam[k] = -g[k];
-  }
-}
 __global__ void connect_te_kernel(const double* edge, long long n, double* wake) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     for (int d = 0; d < 3; ++d) {
@@ -116,26 +52,6 @@ __global__ void lamb_midpoints_kernel(const double* __restrict__ panels, long lo
     const d3 start = ld3(p + 3 * ((k + 1) % 4)), end = ld3(p + 3 * k);
     st3(t + 3 * q, dvs(add(start, end), 2));
   }
-}
-
-constexpr int kSumThreads = 256;
-
-__device__ inline d3 block_sum3(d3 v, double* sh) {
-  for (int off = 16; off; off >>= 1) {
-    v.x += __shfl_down_sync(0xffffffffu, v.x, off);
-    v.y += __shfl_down_sync(0xffffffffu, v.y, off);
-    v.z += __shfl_down_sync(0xffffffffu, v.z, off);
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) {
-    sh[3 * wid] = v.x;
-    sh[3 * wid + 1] = v.y;
-    sh[3 * wid + 2] = v.z;
-  }
-  __syncthreads();
-  d3 r = mk(0, 0, 0);
-  for (int w = 0; w < kSumThreads / 32; ++w) r = add(r, mk(sh[3 * w], sh[3 * w + 1], sh[3 * w + 2]));
-  return r;
 }
 
 // CalcLambVectorOnPanel (calc_impulse.h:15-30) summed over the panels as
@@ -182,27 +98,56 @@ __global__ void __launch_bounds__(kSumThreads) vortex_impulse_kernel(const doubl
   if (threadIdx.x == 0) st3(out, r);
 }
 
-inline int gfor(long long n) { return (int)std::min<long long>(std::max<long long>((n + 255) / 256, 1), 65535); }
-
-Error velocity_at(const SheetView* views, int nv, NBodyPrec prec, const double* d_targets_aos, long long nt,
-                  double* vx, double* vy, double* vz, Scratch& S) {
-  double *tx, *ty, *tz;
-  UVLM_TRY(S.get(&tx, nt));
-  UVLM_TRY(S.get(&ty, nt));
-  UVLM_TRY(S.get(&tz, nt));
-  aos_to_soa<<<gfor(nt), 256>>>(d_targets_aos, nt, tx, ty, tz);
-  UVLM_LAUNCH_CHECK();
-  NBodyWork w;
-  long long recs = 0;
-  for (int i = 0; i < nv; ++i) recs += (long long)views[i].num * views[i].node_rows * (views[i].cols + 1);
-  w.records_cap = std::max<long long>(recs, 1) * (long long)sizeof(RecD);
-  UVLM_TRY(S.get(reinterpret_cast<char**>(&w.records), (size_t)w.records_cap));
-  w.partial_cap = 3 * std::max<long long>(nt, 1) * 64;
-  UVLM_TRY(S.get(&w.partial, (size_t)w.partial_cap));
-  SourceBlock blocks[4];
-  UVLM_TRY(nbody_build_sources(views, nv, prec, &w, blocks, 0));
-  const int variant = prec == kNBodyFP32 ? 16 : 9;  // fp32_h3_t2_b128_x2f, fp64_h2_t1_b128_m3
-  UVLM_TRY(nbody_eval(blocks, nv, prec, tx, ty, tz, nt, vx, vy, vz, &w, variant, sms(), 0));
+// SolveLinearProblem over AoS rings (src/linear.inl:113-157): FP64
+// assembly, RHS with ring i moving by kins[kin_of[i]] (kin_of NULL: kins[0]),
+// optional wake term, FP64 LU solve.
+Error solve_rings(const double* bound_rings, const double* bound_rings0, int64_t n_bound,
+                  const uvlm_kinematics* kins, int n_kins, const int* kin_of, const double* wake_rings,
+                  const double* wake_gamma, int64_t n_wake, const double freestream[3], double t,
+                  int32_t drop_wake_term, double* gamma_out) {
+  Scratch S;
+  const int n = (int)n_bound;
+  double *dr, *dr0, *A, *cen, *nrm, *b, *x, *tmp, *wv = nullptr;
+  uvlm_kinematics* dk;
+  int* dko = nullptr;
+  UVLM_TRY(S.up(&dr, bound_rings, (size_t)12 * n));
+  UVLM_TRY(S.up(&dr0, bound_rings0 ? bound_rings0 : bound_rings, (size_t)12 * n));
+  UVLM_TRY(S.up(&dk, kins, (size_t)n_kins));
+  if (kin_of) UVLM_TRY(S.up(&dko, kin_of, (size_t)n));
+  UVLM_TRY(S.get(&A, (size_t)n * n));
+  UVLM_TRY(S.get(&cen, (size_t)3 * n));
+  UVLM_TRY(S.get(&nrm, (size_t)3 * n));
+  UVLM_TRY(S.get(&b, (size_t)n));
+  UVLM_TRY(S.get(&x, (size_t)n));
+  UVLM_TRY(S.get(&tmp, (size_t)n));
+  UVLM_TRY(launch_assemble_rings(dr, n, A, cen, nrm, 0));
+  if (!drop_wake_term && n_wake > 0) {
+    double *dw, *dg, *pos, *gam, *vx, *vy, *vz;
+    UVLM_TRY(S.up(&dw, wake_rings, (size_t)12 * n_wake));
+    UVLM_TRY(S.up(&dg, wake_gamma, (size_t)n_wake));
+    UVLM_TRY(S.get(&pos, (size_t)12 * n_wake));
+    UVLM_TRY(S.get(&gam, (size_t)n_wake));
+    UVLM_TRY(S.get(&vx, n));
+    UVLM_TRY(S.get(&vy, n));
+    UVLM_TRY(S.get(&vz, n));
+    UVLM_TRY(S.get(&wv, (size_t)3 * n));
+    rings_to_sheets<<<gfor(n_wake), 256>>>(dw, dg, n_wake, pos, gam);
+    UVLM_LAUNCH_CHECK();
+    SheetView v{pos, 2, 0, gam, 1, 0, (int)n_wake, 2, 1};
+    UVLM_TRY(velocity_at(&v, 1, kNBodyFP64, cen, n, vx, vy, vz, S));
+    soa_to_aos<<<gfor(n), 256>>>(vx, vy, vz, n, wv, nullptr, nullptr, 1.0);
+    UVLM_LAUNCH_CHECK();
+  }
+  UVLM_TRY(launch_legacy_rhs(dk, dko, dr0, n, cen, nrm, freestream, t, wv, b, 0));
+  LuWork lu;
+  UVLM_TRY(lu_work_alloc(&lu, n, 8, sms()));
+  Error e = lu_factor_f64(A, n, &lu, 0);
+  if (!e.code) e = lu_check(&lu, 0);
+  if (!e.code) e = lu_solve_f64(A, n, &lu, b, x, tmp, 0);
+  if (!e.code) e = lu_check(&lu, 0);
+  lu_work_free(&lu);
+  UVLM_TRY(e);
+  UVLM_CUDA_TRY(cudaMemcpy(gamma_out, x, sizeof(double) * n, cudaMemcpyDeviceToHost));
   return ok();
 }
 
@@ -467,53 +412,29 @@ int uvlm_rings_solve_linear_problem(const double* bound_rings, const double* bou
   if (!bound_rings || n_bound < 1 || !freestream || !gamma_out || n_wake < 0 ||
       (n_wake && (!wake_rings || !wake_gamma)))
     return report(fail(kErrInvalid, "invalid argument"));
-  Scratch S;
-  auto run = [&]() -> Error {
-    const int n = (int)n_bound;
-    double *dr, *dr0, *A, *cen, *nrm, *b, *x, *tmp, *wv = nullptr;
-    uvlm_kinematics k{};
-    if (kin) k = *kin;
-    uvlm_kinematics* dk;
-    UVLM_TRY(S.up(&dr, bound_rings, (size_t)12 * n));
-    UVLM_TRY(S.up(&dr0, bound_rings0 ? bound_rings0 : bound_rings, (size_t)12 * n));
-    UVLM_TRY(S.up(&dk, &k, 1));
-    UVLM_TRY(S.get(&A, (size_t)n * n));
-    UVLM_TRY(S.get(&cen, (size_t)3 * n));
-    UVLM_TRY(S.get(&nrm, (size_t)3 * n));
-    UVLM_TRY(S.get(&b, (size_t)n));
-    UVLM_TRY(S.get(&x, (size_t)n));
-    UVLM_TRY(S.get(&tmp, (size_t)n));
-    UVLM_TRY(launch_assemble_rings(dr, n, A, cen, nrm, 0));
-    if (!drop_wake_term && n_wake > 0) {
-      double *dw, *dg, *pos, *gam, *vx, *vy, *vz;
-      UVLM_TRY(S.up(&dw, wake_rings, (size_t)12 * n_wake));
-      UVLM_TRY(S.up(&dg, wake_gamma, (size_t)n_wake));
-      UVLM_TRY(S.get(&pos, (size_t)12 * n_wake));
-      UVLM_TRY(S.get(&gam, (size_t)n_wake));
-      UVLM_TRY(S.get(&vx, n));
-      UVLM_TRY(S.get(&vy, n));
-      UVLM_TRY(S.get(&vz, n));
-      UVLM_TRY(S.get(&wv, (size_t)3 * n));
-      rings_to_sheets<<<gfor(n_wake), 256>>>(dw, dg, n_wake, pos, gam);
-      UVLM_LAUNCH_CHECK();
-      SheetView v{pos, 2, 0, gam, 1, 0, (int)n_wake, 2, 1};
-      UVLM_TRY(velocity_at(&v, 1, kNBodyFP64, cen, n, vx, vy, vz, S));
-      soa_to_aos<<<gfor(n), 256>>>(vx, vy, vz, n, wv, nullptr, nullptr, 1.0);
-      UVLM_LAUNCH_CHECK();
-    }
-    UVLM_TRY(launch_legacy_rhs(dk, dr0, n, cen, nrm, freestream, t, wv, b, 0));
-    LuWork lu;
-    UVLM_TRY(lu_work_alloc(&lu, n, 8, sms()));
-    Error e = lu_factor_f64(A, n, &lu, 0);
-    if (!e.code) e = lu_check(&lu, 0);
-    if (!e.code) e = lu_solve_f64(A, n, &lu, b, x, tmp, 0);
-    if (!e.code) e = lu_check(&lu, 0);
-    lu_work_free(&lu);
-    UVLM_TRY(e);
-    UVLM_CUDA_TRY(cudaMemcpy(gamma_out, x, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    return ok();
-  };
-  return report(run());
+  uvlm_kinematics k{};
+  if (kin) k = *kin;
+  return report(solve_rings(bound_rings, bound_rings0, n_bound, &k, 1, nullptr, wake_rings, wake_gamma, n_wake,
+                            freestream, t, drop_wake_term, gamma_out));
+}
+
+int uvlm_rings_solve_linear_problem_containers(const double* bound_rings, const double* bound_rings0,
+                                               const int64_t* container_rings, int32_t n_containers,
+                                               const uvlm_kinematics* kins, const double* wake_rings,
+                                               const double* wake_gamma, int64_t n_wake,
+                                               const double freestream[3], double t, int32_t drop_wake_term,
+                                               double* gamma_out) {
+  if (!bound_rings || n_containers < 1 || !container_rings || !kins || !freestream || !gamma_out || n_wake < 0 ||
+      (n_wake && (!wake_rings || !wake_gamma)))
+    return report(fail(kErrInvalid, "invalid argument"));
+  std::vector<int> kin_of;
+  for (int c = 0; c < n_containers; ++c) {
+    if (container_rings[c] < 0) return report(fail(kErrInvalid, "negative container size"));
+    kin_of.insert(kin_of.end(), (size_t)container_rings[c], c);
+  }
+  if (kin_of.empty()) return report(fail(kErrInvalid, "no bound rings"));
+  return report(solve_rings(bound_rings, bound_rings0, (int64_t)kin_of.size(), kins, n_containers, kin_of.data(),
+                            wake_rings, wake_gamma, n_wake, freestream, t, drop_wake_term, gamma_out));
 }
 
 int uvlm_lu_factor_f32(const float* A, int64_t n, int32_t update, float* LU, int32_t* ipiv) {

@@ -157,13 +157,14 @@ __global__ void assemble_rings_kernel(const double* rings, int n, const double* 
   }
 }
 
-__global__ void legacy_rhs_kernel(const uvlm_kinematics* __restrict__ kin, const double* rings0, int n,
-                                  const double* normal, d3 fs, double t, const double* wake_vel, double* b) {
+__global__ void legacy_rhs_kernel(const uvlm_kinematics* __restrict__ kin, const int* __restrict__ kin_of,
+                                  const double* rings0, int n, const double* normal, d3 fs, double t,
+                                  const double* wake_vel, double* b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double* r = rings0 + 12 * i;
     const d3 c0 = dvs(add(add(add(ld3(r), ld3(r + 3)), ld3(r + 6)), ld3(r + 9)), 4);  // ReferenceCentroid
     const d3 nl = ld3(normal + 3 * i);
-    double v = dot(morph_velocity(kin[0], c0, t), nl) - dot(fs, nl);
+    double v = dot(morph_velocity(kin[kin_of ? kin_of[i] : 0], c0, t), nl) - dot(fs, nl);
     if (wake_vel) v -= dot(ld3(wake_vel + 3 * i), nl);
     b[i] = v;
   }
@@ -419,11 +420,12 @@ Error launch_assemble_rings(const double* rings, int n, double* A, double* centr
   return ok();
 }
 
-Error launch_legacy_rhs(const uvlm_kinematics* d_kin, const double* rings0, int n, const double* centroid,
-                        const double* normal, const double fs[3], double t, const double* wake_vel, double* b,
-                        cudaStream_t st) {
+Error launch_legacy_rhs(const uvlm_kinematics* d_kin, const int* d_kin_of, const double* rings0, int n,
+                        const double* centroid, const double* normal, const double fs[3], double t,
+                        const double* wake_vel, double* b, cudaStream_t st) {
   (void)centroid;
-  legacy_rhs_kernel<<<grid_for(n), 256, 0, st>>>(d_kin, rings0, n, normal, mk(fs[0], fs[1], fs[2]), t, wake_vel, b);
+  legacy_rhs_kernel<<<grid_for(n), 256, 0, st>>>(d_kin, d_kin_of, rings0, n, normal, mk(fs[0], fs[1], fs[2]), t,
+                                                 wake_vel, b);
   UVLM_LAUNCH_CHECK();
   return ok();
 }

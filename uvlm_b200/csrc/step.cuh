@@ -47,9 +47,11 @@ Error launch_assemble_rings(const double* rings, int n, double* A, double* centr
                             cudaStream_t st);
 // Legacy RHS (src/linear.inl:34-76, :113-130): b_i = Vls(ref centroid_i).n_i
 // - freestream.n_i [- wake(centroid_i).n_i when the wake term is kept].
-Error launch_legacy_rhs(const uvlm_kinematics* d_kin, const double* rings0, int n, const double* centroid,
-                        const double* normal, const double fs[3], double t, const double* wake_vel, double* b,
-                        cudaStream_t st);
+// Ring i moves with d_kin[d_kin_of[i]] (d_kin_of NULL: d_kin[0]), the
+// per-container morphings of CalcRhsMorphings (src/linear.inl:87-104).
+Error launch_legacy_rhs(const uvlm_kinematics* d_kin, const int* d_kin_of, const double* rings0, int n,
+                        const double* centroid, const double* normal, const double fs[3], double t,
+                        const double* wake_vel, double* b, cudaStream_t st);
 // b_K = -(Uw - (Uls + ff)) . n_K
 Error launch_rhs(int N, const double* uw_x, const double* uw_y, const double* uw_z, const double* uls,
                  const double* normal, const double ff[3], double* b, cudaStream_t st);
