@@ -12,6 +12,8 @@
 //   UVLM::simulator::SimpleSimulator                 src/simulator/simple_simulator.h:33-108
 //   multiple_sheet::MultipleSheet<T> (layout of the missing submodule,
 //     contiguous [num][rows][cols])
+//   the legacy AoS API (VortexRing, VortexContainer, shed, linear,
+//     calc_load, WingBuilder, simulator::Start)  uvlm_b200_legacy.hpp
 // The element type of node sheets is UVLM_B200_VECTOR3 (default UVLM::Vec3);
 // any type of three packed doubles works, e.g. define it to Eigen::Vector3d
 // before including this header.  Errors throw UVLM::Error where the
@@ -183,6 +185,18 @@ class Morphing {
     for (int d = 0; d < 3; ++d) k_.origin[d] = p[d];
   }
   const uvlm_kinematics& kinematics() const { return k_; }
+  // Morphing::Perfome / Velocity (src/morphing.cpp:23-52) of one reference
+  // point, evaluated by the library's kinematics kernel.
+  void Perfome(Vector3* x, const Vector3& x0, double t) const {
+    detail::check(uvlm_kinematics_perfome(&k_, reinterpret_cast<const double*>(&x0), 1, t,
+                                          reinterpret_cast<double*>(x)),
+                  "Morphing::Perfome");
+  }
+  void Velocity(Vector3* v, const Vector3& x0, double t) const {
+    detail::check(uvlm_kinematics_velocity(&k_, reinterpret_cast<const double*>(&x0), 1, t,
+                                           reinterpret_cast<double*>(v)),
+                  "Morphing::Velocity");
+  }
 
  private:
   uvlm_kinematics k_;
@@ -341,3 +355,5 @@ class SimpleSimulator {
 
 }  // namespace simulator
 }  // namespace UVLM
+
+#include "uvlm_b200_legacy.hpp"
