@@ -302,6 +302,28 @@ int uvlm_rings_vortex_impulse(const double* rings, const double* gammas, int64_t
 int uvlm_rings_lamb_vector(const double* panels, const double* panel_gamma, const double* node_velocities,
                            int64_t n_panels, const double* freestreams, const double* vortices,
                            const double* vortex_gamma, int64_t n_vortices, double out[3]);
+/* ------------------------------------------------- per-step state output */
+/* SimpleSimulator::set_sheet_path / set_result_path
+ * (src/simulator/simple_simulator.cpp:53-66): from the next step on, every
+ * MainLoop writes the state after its solve as one AllVortexSheets record
+ * (OutputSheet :324-332) to sheet_path and one Snapshot2 record
+ * (OutputPanels :317-322) to result_path; NULL or "" writes none.  Records
+ * are the protobuf wire format of proto/uvlm.proto, each preceded by its
+ * byte length as a little-endian uint64.  The state is snapshotted on the
+ * device and written by a background thread; uvlm_flush_output waits for
+ * it, uvlm_destroy flushes and closes.  Calling again replaces the files. */
+#define UVLM_OUTPUT_SHEETS 0
+#define UVLM_OUTPUT_SNAPSHOT2 1
+int uvlm_set_output_paths(uvlm_ctx* ctx, const char* sheet_path, const char* result_path);
+int uvlm_flush_output(uvlm_ctx* ctx);
+/* One record of `kind` from host arrays in the simulator's layout (wing
+ * nodes [num][rows+1][cols+1][3], circulations [num][rows][cols], wake
+ * nodes [num][wake_rows+1][cols+1][3], circulations [num][wake_rows][cols]),
+ * appended to (append = 1) or replacing the file at path. */
+int uvlm_write_state_record(const char* path, int32_t append, int32_t kind, int64_t num, int64_t rows, int64_t cols,
+                            int64_t wake_rows, const double* wing_pos, const double* wing_gamma,
+                            const double* wake_pos, const double* wake_gamma, double t);
+
 /* ---------------------------------------------- learned warm start (MLP) */
 /* No counterpart in the reference.  A per-panel MLP (8 features -> 3 x 256
  * GELU -> 1, BF16 weights, FP32 accumulation) predicts the correction of the

@@ -304,6 +304,19 @@ class SimpleSimulator {
   void set_advection(const std::string& name) {
     detail::check(uvlm_set_advection(h_.get(), name.c_str()), "set_advection", uvlm_last_error(h_.get()));
   }
+  // set_sheet_path / set_result_path (simple_simulator.cpp:53-66): one
+  // AllVortexSheets / Snapshot2 record per step, length-prefixed protobuf.
+  void set_sheet_path(const std::string& path) {
+    sheet_path_ = path;
+    detail::check(uvlm_set_output_paths(h_.get(), sheet_path_.c_str(), result_path_.c_str()), "set_sheet_path",
+                  uvlm_last_error(h_.get()));
+  }
+  void set_result_path(const std::string& path) {
+    result_path_ = path;
+    detail::check(uvlm_set_output_paths(h_.get(), sheet_path_.c_str(), result_path_.c_str()), "set_result_path",
+                  uvlm_last_error(h_.get()));
+  }
+  void FlushOutput() { detail::check(uvlm_flush_output(h_.get()), "FlushOutput", uvlm_last_error(h_.get())); }
 
   // Run (simple_simulator.cpp:288-313): MainLoop(step, dt) for step =
   // 0..steps.  Returns the load rows t, CD_0, CL_0, CD_1, CL_1, ...
@@ -351,6 +364,7 @@ class SimpleSimulator {
   };
   std::unique_ptr<uvlm_ctx, Del> h_;
   std::size_t num_ = 0;
+  std::string sheet_path_, result_path_;
 };
 
 }  // namespace simulator

@@ -1,0 +1,127 @@
+"""Per-step state records (no GPU): the library's encoder against the protobuf runtime.
+
+`uvlm_write_state_record` writes AllVortexSheets / Snapshot2 records from
+host arrays with the same encoder the time-stepper's writer thread uses.
+The records are parsed by google.protobuf with message classes built from a
+descriptor restating proto/uvlm.proto (field numbers, types, labels), and
+re-serialised: the bytes must be identical (the encoder writes the canonical
+field order of the C++ protobuf runtime).  uvlm_b200.output decodes them to
+the same arrays.
+"""
+import numpy as np
+import pytest
+
+
+def _classes():
+    from google.protobuf import descriptor_pb2, descriptor_pool, message_factory
+
+    F = descriptor_pb2.FieldDescriptorProto
+    fd = descriptor_pb2.FileDescriptorProto(name="uvlm_test.proto", package="UVLM.proto", syntax="proto2")
+
+    def msg(name, flds, parent=None):
+        m = (parent.nested_type if parent else fd.message_type).add(name=name)
+        for fname, num, typ, label, tname in flds:
+            f = m.field.add(name=fname, number=num, type=typ, label=label)
+            if tname:
+                f.type_name = tname
+        return m
+
+    OPT, REP, REQ = F.LABEL_OPTIONAL, F.LABEL_REPEATED, F.LABEL_REQUIRED
+    D, U32, U64, M = F.TYPE_DOUBLE, F.TYPE_UINT32, F.TYPE_UINT64, F.TYPE_MESSAGE
+    # proto/uvlm.proto:4-100
+    msg("Point", [("x", 1, D, OPT, None), ("y", 2, D, OPT, None), ("z", 3, D, OPT, None)])
+    msg("VortexRing", [("gamma", 1, D, OPT, None), ("nodes", 2, M, REP, ".UVLM.proto.Point"),
+                       ("nodes0", 3, M, REP, ".UVLM.proto.Point")])
+    msg("MorphingVelocity", [("center", 1, M, OPT, ".UVLM.proto.Point"), ("nodes", 2, M, REP, ".UVLM.proto.Point"),
+                             ("freestream", 3, M, OPT, ".UVLM.proto.Point")])
+    s2 = msg("Snapshot2", [("t", 1, D, OPT, None),
+                           ("container_shapes", 2, M, REP, ".UVLM.proto.Snapshot2.ContainerShape"),
+                           ("vortices", 3, M, REP, ".UVLM.proto.VortexRing"),
+                           ("morphing_velocities", 4, M, REP, ".UVLM.proto.MorphingVelocity")])
+    msg("ContainerShape", [("rows", 1, U32, REQ, None), ("cols", 2, U32, REQ, None), ("id", 3, U32, OPT, None),
+                           ("origin", 4, M, OPT, ".UVLM.proto.Point"), ("chord", 5, D, OPT, None),
+                           ("span", 6, D, OPT, None)], parent=s2)
+    msg("VortexSheet", [("t", 1, D, OPT, None), ("num", 2, U32, REQ, None), ("rows", 3, U32, REQ, None),
+                        ("cols", 4, U32, REQ, None), ("vortices", 5, M, REP, ".UVLM.proto.VortexRing")])
+    msg("AllVortexSheets", [("t", 1, D, OPT, None), ("wing", 2, M, OPT, ".UVLM.proto.VortexSheet"),
+                            ("wake", 3, M, OPT, ".UVLM.proto.VortexSheet")])
+    del U64
+    pool = descriptor_pool.DescriptorPool()
+    pool.Add(fd)
+    get = lambda n: message_factory.GetMessageClass(pool.FindMessageTypeByName("UVLM.proto." + n))  # noqa: E731
+    return get("AllVortexSheets"), get("Snapshot2")
+
+
+def _state(rng, num, rows, cols, wr):
+    pos = rng.standard_normal((num, rows + 1, cols + 1, 3))
+    g = rng.standard_normal((num, rows, cols))
+    wpos = rng.standard_normal((num, wr + 1, cols + 1, 3))
+    wg = rng.standard_normal((num, wr, cols))
+    return pos, g, wpos, wg
+
+
+def _write(path, kind, append, st, t):
+    import ctypes as C
+
+    from uvlm_b200._capi import check, lib
+
+    pos, g, wpos, wg = [np.ascontiguousarray(a) for a in st]
+    P = C.POINTER(C.c_double)
+    num, rows, cols = g.shape
+    check(lib().uvlm_write_state_record(str(path).encode(), int(append), kind, num, rows, cols, wg.shape[1],
+                                        pos.ctypes.data_as(P), g.ctypes.data_as(P), wpos.ctypes.data_as(P),
+                                        wg.ctypes.data_as(P) if wg.size else None, float(t)))
+
+
+@pytest.mark.parametrize("wr", [0, 3])
+def test_sheet_records_parse_and_reserialise(tmp_path, wr):
+    from uvlm_b200 import output
+
+    AllVortexSheets, Snapshot2 = _classes()
+    rng = np.random.default_rng(wr)
+    st = _state(rng, 2, 3, 4, wr)
+    path = tmp_path / "sheets.rec"
+    _write(path, 0, False, st, 0.25)
+    _write(path, 0, True, st, 0.5)
+    recs = list(output.read_records(str(path)))
+    assert len(recs) == 2
+    for rec, t in zip(recs, (0.25, 0.5)):
+        m = AllVortexSheets()
+        m.ParseFromString(rec)
+        assert m.t == t and m.wing.num == 2 and m.wing.rows == 3 and m.wing.cols == 4 and m.wake.rows == wr
+        assert len(m.wing.vortices) == 24 and len(m.wake.vortices) == 2 * wr * 4
+        assert m.SerializeToString() == rec
+        pos, g, wpos, wg = st
+        v = m.wing.vortices[1 * 12 + 2 * 4 + 3]   # ring (n=1, i=2, j=3): p(i,j), p(i,j+1), p(i+1,j+1), p(i+1,j)
+        assert v.gamma == g[1, 2, 3]
+        want = [pos[1, 2, 3], pos[1, 2, 4], pos[1, 3, 4], pos[1, 3, 3]]
+        assert all([nd.x, nd.y, nd.z] == list(w) for nd, w in zip(v.nodes, want))
+        d = output.decode_all_vortex_sheets(rec)
+        assert d["t"] == t
+        p2, g2 = output.sheet_to_grid(d["wing"])
+        np.testing.assert_array_equal(p2, pos)
+        np.testing.assert_array_equal(g2, g)
+        if wr:
+            p3, g3 = output.sheet_to_grid(d["wake"])
+            np.testing.assert_array_equal(p3, wpos)
+            np.testing.assert_array_equal(g3, wg)
+
+
+def test_snapshot2_records(tmp_path):
+    from uvlm_b200 import output
+
+    _, Snapshot2 = _classes()
+    st = _state(np.random.default_rng(5), 1, 2, 3, 2)
+    path = tmp_path / "result.rec"
+    _write(path, 1, False, st, 1.0)
+    (rec,) = list(output.read_records(str(path)))
+    m = Snapshot2()
+    m.ParseFromString(rec)
+    assert not m.HasField("t") and len(m.vortices) == 6 + 6
+    assert m.SerializeToString() == rec
+    pos, g, wpos, wg = st
+    v = m.vortices[6 + 4]  # wake ring (0, 1, 1): SheetToSnapshot order p(i+1,j), p(i+1,j+1), p(i,j+1), p(i,j)
+    want = [wpos[0, 2, 1], wpos[0, 2, 2], wpos[0, 1, 2], wpos[0, 1, 1]]
+    assert v.gamma == wg[0, 1, 1] and all([nd.x, nd.y, nd.z] == list(w) for nd, w in zip(v.nodes, want))
+    d = output.decode_snapshot2(rec)
+    np.testing.assert_array_equal(d["gammas"], np.concatenate([g.ravel(), wg.ravel()]))

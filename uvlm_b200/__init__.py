@@ -194,6 +194,26 @@ class SimpleSimulator:
     def set_load_path(self, path: str) -> None:
         self._load_path = path or None
 
+    def set_sheet_path(self, path: str) -> None:
+        """SimpleSimulator::set_sheet_path (simple_simulator.cpp:61-66): an AllVortexSheets record per step
+        (read them with uvlm_b200.output.read_sheets)."""
+        self._sheet_path = path or None
+        self._set_output()
+
+    def set_result_path(self, path: str) -> None:
+        """SimpleSimulator::set_result_path (simple_simulator.cpp:53-59): a Snapshot2 record per step."""
+        self._result_path = path or None
+        self._set_output()
+
+    def _set_output(self) -> None:
+        enc = [p.encode() if p else None for p in (getattr(self, "_sheet_path", None),
+                                                     getattr(self, "_result_path", None))]
+        check(lib().uvlm_set_output_paths(self._h, enc[0], enc[1]), self._h)
+
+    def flush_output(self) -> None:
+        """Wait until every record of the steps run so far is written."""
+        check(lib().uvlm_flush_output(self._h), self._h)
+
     def Run(self, steps: int, dt: float) -> np.ndarray:  # noqa: N802
         """Run(steps, dt): steps+1 MainLoops; returns the load rows."""
         self.begin()
@@ -286,8 +306,8 @@ class SimpleSimulator:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            lib().uvlm_destroy(self._h)
-            self._h = None
+            h, self._h = self._h, None
+            check(lib().uvlm_destroy(h))
 
     def __del__(self):
         try:

@@ -130,6 +130,10 @@ SIGNATURES = [
                                                _P, C.c_double, C.c_double, C.c_double, _P]),
     ("uvlm_rings_load_joukowski", C.c_int, [_P, _P, _P, _P, _I, _I, C.POINTER(Kinematics), _P, _P, _I, _P,
                                             C.c_double, C.c_double, C.c_double, _P]),
+    ("uvlm_set_output_paths", C.c_int, [_V, C.c_char_p, C.c_char_p]),
+    ("uvlm_flush_output", C.c_int, [_V]),
+    ("uvlm_write_state_record", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _I, _I, _I, _I, _P, _P, _P, _P,
+                                          C.c_double]),
     ("uvlm_rings_vortex_impulse", C.c_int, [_P, _P, _I, _P]),
     ("uvlm_rings_lamb_vector", C.c_int, [_P, _P, _P, _I, _P, _P, _P, _I, _P]),
     ("uvlm_mlp_create", C.c_int, [C.c_uint64, C.POINTER(_V)]),

@@ -14,6 +14,7 @@
 #include "mlp.cuh"
 #include "lu.cuh"
 #include "nbody.cuh"
+#include "output.cuh"
 #include "step.cuh"
 
 using namespace uvlm;
@@ -119,6 +120,7 @@ struct uvlm_ctx {
   static constexpr int kNbEvents = 8;
   cudaEvent_t nbev[2 * kNbEvents] = {};
   int nbev_n = 0;
+  OutputWriter* out = nullptr;  // per-step AllVortexSheets / Snapshot2 records
 
   WingShape ws() const { return WingShape{num, R, C}; }
   WakeLayout wl() const { return WakeLayout{num, C, PR, wake_start, wake_nodes}; }
@@ -501,6 +503,9 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
     collect_n += N;
   }
   UVLM_CUDA_TRY(cudaMemcpyAsync(d_rhs_prev, d_rhs, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+  if (out)  // OutputPanels / OutputSheet after the solve (simple_simulator.cpp:270-277)
+    UVLM_TRY(output_enqueue(out, OutputState{num, R, C, PR, wake_start, wake_nodes, d_pos, d_gamma, d_wpos, d_wgamma},
+                            t, st));
   mark(4);
   if (cfg.compute_loads) {
     const long long lines = (long long)num * R * (2 * C + 1);
@@ -652,6 +657,8 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
 int uvlm_destroy(uvlm_ctx* c) {
   if (!c) return UVLM_OK;
   if (c->st) cudaStreamSynchronize(c->st);
+  const Error oe = output_close(c->out);
+  c->out = nullptr;
   c->free_all();
   cudaFree(c->d_collect_x);
   cudaFree(c->d_collect_t);
@@ -661,7 +668,36 @@ int uvlm_destroy(uvlm_ctx* c) {
     if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
-  return UVLM_OK;
+  return oe.code ? set_global(oe) : UVLM_OK;
+}
+
+int uvlm_set_output_paths(uvlm_ctx* c, const char* sheet_path, const char* result_path) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (c->st) cudaStreamSynchronize(c->st);
+  Error e = output_close(c->out);
+  c->out = nullptr;
+  if (e.code) return c->fail_with(e);
+  if ((sheet_path && *sheet_path) || (result_path && *result_path))
+    e = output_open(&c->out, sheet_path, result_path, c->cfg.device);
+  return c->fail_with(e);
+}
+
+int uvlm_flush_output(uvlm_ctx* c) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (!c->out) return UVLM_OK;
+  if (c->st) cudaStreamSynchronize(c->st);
+  return c->fail_with(output_flush(c->out));
+}
+
+int uvlm_write_state_record(const char* path, int32_t append, int32_t kind, int64_t num, int64_t rows, int64_t cols,
+                            int64_t wake_rows, const double* wing_pos, const double* wing_gamma,
+                            const double* wake_pos, const double* wake_gamma, double t) {
+  if (!path || (kind != UVLM_OUTPUT_SHEETS && kind != UVLM_OUTPUT_SNAPSHOT2) || num < 0 || rows < 0 || cols < 0 ||
+      wake_rows < 0 || !wing_pos || !wake_pos || (num * rows * cols > 0 && !wing_gamma) ||
+      (num * wake_rows * cols > 0 && !wake_gamma))
+    return set_global(fail(kErrInvalid, "invalid argument"));
+  return set_global(output_encode_to_file(path, append, kind, (int)num, (int)rows, (int)cols, (int)wake_rows, wing_pos,
+                                          wing_gamma, wake_pos, wake_gamma, t));
 }
 
 const char* uvlm_last_error(const uvlm_ctx* c) { return c ? c->err.c_str() : g_last_error.c_str(); }
