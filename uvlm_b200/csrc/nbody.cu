@@ -54,6 +54,30 @@ __device__ inline void stage_strip_padded(Rec* sm, const Rec* rec, const StripIn
   asm volatile("cp.async.commit_group;");
 }
 
+// Row-padded staging for the column-bounded walkers: records (r, j), j <
+// n_cols, at row stride kStripCols + 1; rows past the strip's node rows are
+// all-zero records (their segments have d = 0 and are cut); columns from
+// n_cols on are not written and never read.
+template <class Rec, int H>
+__device__ inline void stage_strip_rows(Rec* sm, const Rec* rec, const StripInfo& si) {
+  constexpr int kChunks = sizeof(Rec) / 16;
+  const int total = (H + 1) * si.n_cols * kChunks;
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int part = q % kChunks;
+    const int rj = q / kChunks;
+    const int r = rj / si.n_cols, j = rj % si.n_cols;
+    char* dst = reinterpret_cast<char*>(sm + r * (kStripCols + 1) + j) + 16 * part;
+    if (r < si.nr) {
+      const char* src = reinterpret_cast<const char*>(rec + si.first + (long long)r * si.row_stride + j) + 16 * part;
+      const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst), "l"(src));
+    } else {
+      *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  asm volatile("cp.async.commit_group;");
+}
+
 template <class T>
 struct Tgt {
   T hx, hy, hz;  // FP32: hi part; FP64: the position
@@ -462,20 +486,80 @@ __device__ __forceinline__ void walk_far_strip2(const RecF* sm, const float4* lo
   }
 }
 
-// Local coordinates of a staged full strip relative to its central real node
-// O: loc[k] = (p_k - O, gS_k) for real nodes, (0, 0, 0, gS_k) for the zero
-// padding (whose segments are cut by d = 0 either way).  Returns whether all
+// Column-bounded forms of the packed walkers: the strip's n_cols node
+// columns (row-padded staging), the chordwise segments of the last column
+// only when the strip owns them (last_h).
+template <int H>
+__device__ __forceinline__ void walk_cols2(const RecF* sm, int n_cols, bool last_h, const Tgt<float> (&tg)[2],
+                                           float (&acc)[2][3]) {
+  Node2 prev[H];
+  SegV<float> ps0[H];
+  float pgS[H];
+  float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  if (n_cols == 1) {
+    if (last_h)
+      full_column2<H, true, true>(sm, tg, prev, ps0, pgS, a2);
+    else
+      full_column2<H, true, false>(sm, tg, prev, ps0, pgS, a2);
+  } else {
+    full_column2<H, true, true>(sm, tg, prev, ps0, pgS, a2);
+#pragma unroll 2
+    for (int j = 1; j < n_cols - 1; ++j) full_column2<H, false, true>(sm + j, tg, prev, ps0, pgS, a2);
+    if (last_h)
+      full_column2<H, false, true>(sm + n_cols - 1, tg, prev, ps0, pgS, a2);
+    else
+      full_column2<H, false, false>(sm + n_cols - 1, tg, prev, ps0, pgS, a2);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    acc[0][c] += a2[c].x;
+    acc[1][c] += a2[c].y;
+  }
+}
+
+template <int H>
+__device__ __forceinline__ void walk_far_cols2(const RecF* sm, const float4* loc, int n_cols, bool last_h,
+                                               const float2 (&ts)[3], float (&acc)[2][3]) {
+  Node2 prev[H];
+  SegV<float> ps0[H];
+  float pgS[H];
+  float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  if (n_cols == 1) {
+    if (last_h)
+      far_column2<H, true, true>(sm, loc, ts, prev, ps0, pgS, a2);
+    else
+      far_column2<H, true, false>(sm, loc, ts, prev, ps0, pgS, a2);
+  } else {
+    far_column2<H, true, true>(sm, loc, ts, prev, ps0, pgS, a2);
+#pragma unroll 2
+    for (int j = 1; j < n_cols - 1; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pgS, a2);
+    if (last_h)
+      far_column2<H, false, true>(sm + n_cols - 1, loc + n_cols - 1, ts, prev, ps0, pgS, a2);
+    else
+      far_column2<H, false, false>(sm + n_cols - 1, loc + n_cols - 1, ts, prev, ps0, pgS, a2);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    acc[0][c] += a2[c].x;
+    acc[1][c] += a2[c].y;
+  }
+}
+
+// Local coordinates of a staged strip (its n_cols columns) relative to its
+// central real node O: loc[k] = (p_k - O, gS_k) for real nodes, (0, 0, 0,
+// gS_k) for the zero padding (whose segments are cut by d = 0 either way).  Returns whether all
 // of this warp's targets are far from the strip (warp-uniform) and their
 // coordinates relative to O.  `red` holds one float per warp.
 template <int H, int BLOCK>
 __device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si, float4* loc, float* red,
                                             const Tgt<float> (&tg)[2], float2 (&ts)[3]) {
-  constexpr int kRecs = (H + 1) * (kStripCols + 1);
-  const RecF& o = sm[((si.nr - 1) >> 1) * (kStripCols + 1) + ((si.n_cols - 1) >> 1)];
+  const int n_cols = si.n_cols;
+  const RecF& o = sm[((si.nr - 1) >> 1) * (kStripCols + 1) + ((n_cols - 1) >> 1)];
   const float4 oh = o.hi, ol = o.lo;
   float m = 0.f;
-  for (int k = threadIdx.x; k < kRecs; k += BLOCK) {
-    const int r = k / (kStripCols + 1), j = k - r * (kStripCols + 1);
+  for (int q = threadIdx.x; q < (H + 1) * n_cols; q += BLOCK) {
+    const int r = q / n_cols, j = q - r * n_cols;
+    const int k = r * (kStripCols + 1) + j;
     const float4 h = sm[k].hi, l = sm[k].lo;
     float4 L = make_float4(0.f, 0.f, 0.f, h.w);
     if (r < si.nr && j < si.n_cols) {
@@ -533,16 +617,19 @@ __device__ __forceinline__ void load_targets(const double* __restrict__ tx, cons
 
 // Strips [s_begin, s_end) of B for the thread's targets, double-buffered
 // through shared memory; FP32 partial sums per strip, FP64 across strips.
-// PK: 0 generic walkers, 1 packed FP32x2 walker on full strips, 2 the same
-// plus the far-field walker for strips far from all of a warp's targets
-// (`loc`, `red`: its shared-memory scratch).
+// PK: 0 generic walkers, 1 packed FP32x2 walker on full strips, 2 the packed
+// walkers bounded by each strip's column count (row-padded staging, any
+// fill) with the far-field walker for strips far from all of a warp's
+// targets (`loc`, `red`: its shared-memory scratch).
 template <class T, class Rec, int H, int TPT, int BLOCK, bool PAD, int PK = 0>
 __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, long long s_end,
                                             const Rec* __restrict__ rec, Rec* buf0, Rec* buf1, float4* loc,
                                             float* red, const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3]) {
   if (s_begin >= s_end) return;
   StripInfo si = decode_strip<H>(B, s_begin);
-  if constexpr (PAD)
+  if constexpr (PAD && PK == 2)
+    stage_strip_rows<Rec, H>(buf0, rec, si);
+  else if constexpr (PAD)
     stage_strip_padded<Rec, H>(buf0, rec, si);
   else
     stage_strip<Rec>(buf0, rec, si);
@@ -553,7 +640,9 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
     const bool has_next = s + 1 < s_end;
     if (has_next) {
       sn = decode_strip<H>(B, s + 1);
-      if constexpr (PAD)
+      if constexpr (PAD && PK == 2)
+        stage_strip_rows<Rec, H>(nxt, rec, sn);
+      else if constexpr (PAD)
         stage_strip_padded<Rec, H>(nxt, rec, sn);
       else
         stage_strip<Rec>(nxt, rec, sn);
@@ -568,9 +657,9 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
     if constexpr (PAD && PK == 2 && sizeof(T) == 4 && TPT == 2) {
       float2 ts[3];
       if (far_prepare<H, BLOCK>(cur, si, loc, red, tg, ts))
-        walk_far_strip2<H>(cur, loc, si.last_h, ts, acc);
+        walk_far_cols2<H>(cur, loc, si.n_cols, si.last_h, ts, acc);
       else
-        walk_full_strip2<H>(cur, si.last_h, tg, acc);
+        walk_cols2<H>(cur, si.n_cols, si.last_h, tg, acc);
     } else if constexpr (PAD && PK == 1 && sizeof(T) == 4 && TPT == 2) {
       walk_full_strip2<H>(cur, si.last_h, tg, acc);
     } else if constexpr (PAD)
@@ -756,8 +845,8 @@ __global__ void batch_reduce_kernel(const NBodyBatchPlan* __restrict__ plan, int
   }
 }
 
-// Batched tiles: FP32 general h4 t2 b128, FP32 padded (packed FP32x2) h3 t2
-// b128, FP64 h2 t1 b128; 3 CTAs/SM each.
+// Batched tiles: FP32 column-bounded packed FP32x2 h3 t2 b128 (every
+// problem), FP64 h2 t1 b128; 3 CTAs/SM each.
 constexpr int kBatchBlock = 128;
 constexpr int kBatchTptF = 2, kBatchHF = 4, kBatchHFP = 3, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
 constexpr int kBatchPadPK = 2;  // walker of the padded class (see eval_strips)
@@ -834,8 +923,15 @@ template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, int PK = 0>
 Error launch_variant(const Blocks& B, long long n_strips, const double* tx, const double* ty, const double* tz,
                      long long n_targets, const Rec* rec, NBodyWork* work, double* vx, double* vy, double* vz,
                      int num_sms, cudaStream_t st) {
-  const bool pad = use_padded(B);
-  auto kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false, PK>;
+  // the column-bounded walkers (PK == 2) take every sheet; the others pad only
+  // sheets that fill most of the staged columns
+  const bool pad = PK == 2 || use_padded(B);
+  void (*kern)(Blocks, long long, long long, const double*, const double*, const double*, long long, const Rec*,
+               double*);
+  if constexpr (PK == 2)
+    kern = nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK>;
+  else
+    kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false, PK>;
   const size_t smem = strip_smem<Rec, H, BLOCK, PK>();
   static bool attr_done[2] = {false, false};
   if (!attr_done[pad]) {
@@ -953,7 +1049,8 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
 namespace uvlm {
 
 int nbody_batch_rows(NBodyPrec prec, bool padded) {
-  return prec == kNBodyFP32 ? (padded ? kBatchHFP : kBatchHF) : kBatchHD;
+  (void)padded;  // one FP32 class: the column-bounded packed tile takes every sheet
+  return prec == kNBodyFP32 ? kBatchHFP : kBatchHD;
 }
 
 long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n) {
@@ -983,7 +1080,7 @@ int batch_grid_of(int num_sms) {
 NBodyBatchGrids nbody_batch_grids(NBodyPrec prec, int num_sms) {
   NBodyBatchGrids g;
   if (prec == kNBodyFP32) {
-    g.general = batch_grid_of<float, RecF, kBatchHF, kBatchTptF, false, 0>(num_sms);
+    g.general = 0;
     g.padded = batch_grid_of<float, RecF, kBatchHFP, kBatchTptF, true, kBatchPadPK>(num_sms);
   } else {
     g.general = batch_grid_of<double, RecD, kBatchHD, kBatchTptD, false, 0>(num_sms);
@@ -1003,17 +1100,8 @@ Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const
   };
   if (prec == kNBodyFP32) {
     const RecF* rf = reinterpret_cast<const RecF*>(records);
-    // general class
-    batch_plan_kernel<kBatchHF, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, 0, d_plan, partial_cap,
-                                                                             d_totals, status);
-    UVLM_LAUNCH_CHECK();
-    batch_nbody_kernel<float, RecF, kBatchHF, kBatchTptF, kBatchBlock, kBatchMinB, false, 0>
-        <<<grids.general, kBatchBlock, strip_smem<RecF, kBatchHF, kBatchBlock, 0>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
-                                                                            partial);
-    UVLM_LAUNCH_CHECK();
-    UVLM_TRY(reduce(grids.general));
-    // padded class: whole strips, packed FP32x2 walker
-    batch_plan_kernel<kBatchHFP, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, 1, d_plan, partial_cap,
+    // every problem: column-bounded packed FP32x2 tile with the far-field walker
+    batch_plan_kernel<kBatchHFP, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, -1, d_plan, partial_cap,
                                                                               d_totals, status);
     UVLM_LAUNCH_CHECK();
     batch_nbody_kernel<float, RecF, kBatchHFP, kBatchTptF, kBatchBlock, kBatchMinB, true, kBatchPadPK>
