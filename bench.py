@@ -47,6 +47,10 @@ OMEGA = 1.0  # k = 0.5, c = 1, U = 1
 DT = 2 * math.pi / OMEGA / 40
 WAKE_ROWS = 400
 FLOP_PER_PAIR = 59
+# Bounded CPU sample of one MainLoop (a few seconds of host work): the
+# N-body stages on every CPU_STRIDE-th target, the full-pivoting LU on the
+# leading CPU_LU_N^2 block, each scaled to the whole step.
+CPU_STRIDE, CPU_LU_N = 32, 2048
 # DRAM bytes of one advection launch of the N-body kernel at the held wake,
 # from an ncu capture of the packed FP32x2 tile with the far-field walker
 # (bench.py --profile): about the algorithmic bytes (56,115 source records x
@@ -287,7 +291,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     state = synthetic_state_np()
-    stride, lu_n = 128, 1024  # the same sample as the cpu_baseline of the GPU arm
+    stride, lu_n = CPU_STRIDE, CPU_LU_N  # the same sample as the cpu_baseline of the GPU arm
     for _ in range(args.warmup):
         oracle_sample(_heave_pitch(), state, stride, lu_n, threads)
     times = []
@@ -462,7 +466,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_cpu:
         state = simmx.state()
         threads = cpu_threads()
-        stride, lu_n = 128, 1024
+        stride, lu_n = CPU_STRIDE, CPU_LU_N
         tcpu, secs = oracle_sample(wl, state, stride, lu_n, threads)
         n_panels = wl.num * ROWS * COLS
         cpu = {"value": 1.0 / tcpu, "unit": "steps/s", "cores": threads, "kind": "port",
