@@ -28,6 +28,7 @@ state of the same shapes.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import math
 import os
@@ -432,9 +433,12 @@ def run_ours(args, rank, world, local_rank):
     stage_ms = [float(x) for x in stmx.stage_ms]
     sim64.set_stage_timing(True)
     sim64.step(step0 - 1, DT)
-    stage64 = [float(x) for x in sim64.stats().stage_ms]
+    st64 = sim64.stats()
+    stage64 = [float(x) for x in st64.stage_ms]
+    nbody_ms64 = float(st64.nbody_ms)
+    pairs64 = C.c_double()
+    U._capi.check(U.lib().uvlm_get_last_work(sim64._h, C.byref(pairs64), None, None))
     sim64.set_stage_timing(False)
-    import ctypes as C
 
     # roofline of the N-body kernel: the step's algorithmic pairs (RHS, loads,
     # advection) over the device time of its N-body launches (CUDA events
@@ -449,6 +453,9 @@ def run_ours(args, rank, world, local_rank):
     pk = C.c_double()
     U._capi.check(U.lib().uvlm_measure_fp32_peak(dev, C.byref(pk)))
     peak = pk.value
+    pk64 = C.c_double()
+    U._capi.check(U.lib().uvlm_measure_fp64_peak(dev, C.byref(pk64)))
+    achieved64 = FLOP_PER_PAIR * pairs64.value / (nbody_ms64 * 1e-3) / 1e12
 
     # --- end-to-end through the C-ABI with host buffers ------------------------
     e2e_t = []
@@ -498,13 +505,20 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "fp32_simt", "kernel": "nbody_kernel (every N-body launch of a step: RHS, "
                                                               f"loads, {wl.advection} advection)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "peak_source": "FP32 FMA probe on this GPU (uvlm_measure_fp32_peak)",
+                         "peak_source": "FP32 FMA probe on this GPU, the larger of scalar FFMA and packed FP32x2 "
+                                        "(uvlm_measure_fp32_peak)",
                          "per_unit": f"{FLOP_PER_PAIR} FLOP per (target, unique segment) pair",
                          "units_per_step": pairs_step.value, "nbody_ms_per_step": nbody_ms,
                          "advect_stage_tflops": advect_stage_tflops, "advect_pairs_per_step": pairs_advect,
                          "traffic": NBODY_TRAFFIC.get(wl.name),
                          "traffic_unit": "DRAM bytes per advection launch (ncu dram__bytes_read.sum + "
                                          "dram__bytes_write.sum, one launch at the held wake)"},
+            "plain_fp64_roofline": {"bound": "fp64_simt", "kernel": "nbody_kernel<double> (every N-body launch "
+                                                                     "of a plain FP64 step)",
+                                    "achieved": achieved64, "peak": pk64.value, "unit": "TFLOP/s",
+                                    "frac": achieved64 / pk64.value,
+                                    "peak_source": "FP64 FMA probe on this GPU (uvlm_measure_fp64_peak)",
+                                    "units_per_step": pairs64.value, "nbody_ms_per_step": nbody_ms64},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 8 * (1 + 2 * wl.num + wl.num * ROWS * COLS),
                     "note": "wall clock per uvlm_step + circulation download; per-step inputs are scalars"},

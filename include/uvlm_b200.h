@@ -184,9 +184,13 @@ void* uvlm_stream(uvlm_ctx* ctx);
 /* Number of CUDA kernels this library has launched in this process (all
  * contexts and entry points); differences bracket a region of interest. */
 int64_t uvlm_kernel_launch_count(void);
-/* Measured FP32 FMA throughput of the device (TFLOP/s): the denominator of
- * the N-body roofline.  No counterpart in the reference (measurement aid). */
+/* Measured FP32 FMA throughput of the device (TFLOP/s, the larger of a
+ * scalar FFMA and a packed FP32x2 probe): the denominator of the FP32
+ * N-body roofline.  No counterpart in the reference (measurement aid). */
 int uvlm_measure_fp32_peak(int32_t device, double* tflops);
+/* Measured FP64 FMA throughput (TFLOP/s): the denominator of the plain FP64
+ * form's N-body roofline. */
+int uvlm_measure_fp64_peak(int32_t device, double* tflops);
 /* Name of an N-body tile variant (e.g. "fp32_h4_t2_b128"), "?" if out of range. */
 const char* uvlm_nbody_variant_name(int32_t variant);
 /* Algorithmic work of the last step: unique-segment interactions of every

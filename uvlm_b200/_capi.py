@@ -110,6 +110,7 @@ SIGNATURES = [
     ("uvlm_velocity_at", C.c_int, [_V, _P, _I, C.c_int32, _P]),
     ("uvlm_kernel_launch_count", C.c_int64, []),
     ("uvlm_measure_fp32_peak", C.c_int, [C.c_int32, _P]),
+    ("uvlm_measure_fp64_peak", C.c_int, [C.c_int32, _P]),
     ("uvlm_nbody_variant_name", C.c_char_p, [C.c_int32]),
     ("uvlm_sheet_induced_velocity", C.c_int, [_P, _P, _I, _I, _I, _P, _I, _P, C.c_int32]),
     ("uvlm_sheet_induced_velocity_noalloc", C.c_int, [_P, _P, _I, _I, _I, _P, _I, _P, C.c_int32, _V]),

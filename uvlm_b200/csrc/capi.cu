@@ -931,6 +931,12 @@ int uvlm_measure_fp32_peak(int32_t device, double* tflops) {
   return set_global(measure_fp32_fma_peak(device_sms(device), tflops));
 }
 
+int uvlm_measure_fp64_peak(int32_t device, double* tflops) {
+  if (!tflops) return set_global(fail(kErrInvalid, "NULL argument"));
+  if (cudaSetDevice(device) != cudaSuccess) return set_global(fail(kErrCuda, "cudaSetDevice failed"));
+  return set_global(measure_fp64_fma_peak(device_sms(device), tflops));
+}
+
 int uvlm_velocity_at(uvlm_ctx* c, const double* targets, int64_t n, int32_t include_freestream, double* out) {
   if (!c || (n > 0 && (!targets || !out)) || n < 0) return set_global(fail(kErrInvalid, "NULL argument"));
   if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));

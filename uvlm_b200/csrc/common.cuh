@@ -60,6 +60,7 @@ inline Error ok() { return Error{}; }
 void note_launch(int n = 1);
 // FP32 FMA issue-rate probe (probe.cu).
 Error measure_fp32_fma_peak(int num_sms, double* tflops);
+Error measure_fp64_fma_peak(int num_sms, double* tflops);
 // Message of the last failure of a context-free C-ABI call (capi.cu).
 void set_global_error(const std::string& msg);
 inline Error fail(int code, const std::string& m) { return Error{code, m}; }
