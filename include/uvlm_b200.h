@@ -135,6 +135,8 @@ typedef struct {
   int32_t pad_;
   double initial_residual; /* ||b - A g0|| / ||b|| of the GMRES initial guess */
   double nbody_ms;         /* with stage timing: device time of the step's N-body launches */
+  double factor_ms;        /* with stage timing, mixed form: device time of this step's FP32 LU (0 if none) */
+  double inverse_ms;       /* ... and of the dense inverse of its factors (0 if none) */
 } uvlm_step_stats;
 
 /* ------------------------------------------------------- time-stepper */

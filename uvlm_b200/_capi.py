@@ -60,7 +60,8 @@ class StepStats(C.Structure):
         ("step", C.c_int64), ("t", C.c_double), ("solve_path", C.c_int32), ("gmres_iters", C.c_int32),
         ("residual", C.c_double), ("refactored", C.c_int32), ("wake_rows", C.c_int32),
         ("stage_ms", C.c_double * 8), ("nbody_variant", C.c_int32), ("pad_", C.c_int32),
-        ("initial_residual", C.c_double), ("nbody_ms", C.c_double),
+        ("initial_residual", C.c_double), ("nbody_ms", C.c_double), ("factor_ms", C.c_double),
+        ("inverse_ms", C.c_double),
     ]
 
 

@@ -120,6 +120,8 @@ struct uvlm_ctx {
   static constexpr int kNbEvents = 8;
   cudaEvent_t nbev[2 * kNbEvents] = {};
   int nbev_n = 0;
+  cudaEvent_t fev[3] = {};  // around the FP32 LU and the dense inverse of a refactorisation
+  bool fev_used = false;
   OutputWriter* out = nullptr;  // per-step AllVortexSheets / Snapshot2 records
 
   WingShape ws() const { return WingShape{num, R, C}; }
@@ -333,9 +335,15 @@ Error uvlm_ctx::solve(long long step) {
       UVLM_TRY(launch_assemble(ws(), d_pos, d_cx, d_cy, d_cz, d_normal, true, d_F32, true, st));
     else
       UVLM_CUDA_TRY(cudaMemcpyAsync(d_F32, d_A32, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToDevice, st));
+    if (timing && fev[0]) UVLM_CUDA_TRY(cudaEventRecord(fev[0], st));
     UVLM_TRY(lu_factor_f32(d_F32, N, use, &lu, st));
     UVLM_TRY(lu_check(&lu, st));
-    if (d_Minv) UVLM_TRY(lu_inverse_f32(d_F32, N, &lu, d_Minv, st));
+    if (timing && fev[1]) UVLM_CUDA_TRY(cudaEventRecord(fev[1], st));
+    if (d_Minv) UVLM_TRY(lu_inverse_f32(d_F32, N, use, &lu, d_Minv, st));
+    if (timing && fev[2]) {
+      UVLM_CUDA_TRY(cudaEventRecord(fev[2], st));
+      fev_used = true;
+    }
     have_factors = true;
     last.refactored = 1;
     work_lu += 2.0 / 3.0 * (double)N * N * N;
@@ -455,6 +463,7 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   cur_dt = dt;
   work_nbody = work_asm = work_lu = 0;
   nbev_n = 0;
+  fev_used = false;
   last.initial_residual = 0;
   mark(0);
   UVLM_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, st));
@@ -558,6 +567,14 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
       nbt += m;
     }
     last.nbody_ms = nbt;
+    last.factor_ms = last.inverse_ms = 0;
+    if (fev_used) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, fev[0], fev[1]);
+      cudaEventElapsedTime(&b, fev[1], fev[2]);
+      last.factor_ms = a;
+      last.inverse_ms = b;
+    }
   }
   nbev_n = 0;
   return ok();
@@ -639,6 +656,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
   }
   for (auto& e : c->ev) cudaEventCreate(&e);
   for (auto& e : c->nbev) cudaEventCreate(&e);
+  for (auto& e : c->fev) cudaEventCreate(&e);
   if (k.nbody_variant >= 0) {
     c->tuned = true;
     if (k.nbody_variant >= nbody_num_variants()) {
@@ -665,6 +683,8 @@ int uvlm_destroy(uvlm_ctx* c) {
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->nbev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->fev)
     if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;

@@ -739,7 +739,59 @@ __global__ void __launch_bounds__(256) apply_block_kernel(const float* __restric
 
 }  // namespace
 
-Error lu_inverse_f32(const float* LU, int n, LuWork* w, float* X, cudaStream_t st) {
+// Split-TF32 operands of the inverse's rank-kTriB updates.  With hi(a) the
+// TF32 rounding of a and lo(a) = a - hi(a) (exact in FP32), the update
+//   C -= [hi(A) lo(A) hi(A)] [hi(B) hi(B) lo(B)]^T = A B - lo(A) lo(B)
+// over K = 3 kTriB runs on the TF32 tensor cores with an error of the order
+// of FP32 rounding, so the dense inverse is as accurate as FP32 triangular
+// solves with the same factors.
+__device__ __forceinline__ float tf32_hi(float a) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
+  return __uint_as_float(r);
+}
+
+// A3[i][0:64] = hi, [64:128] = lo, [128:192] = hi of A[i][0:64] (lda), i < m.
+__global__ void split_a3_kernel(const float* __restrict__ A, int lda, int m, float* __restrict__ A3) {
+  const long long total = (long long)m * kTriB;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long i = q / kTriB;
+    const int k = (int)(q % kTriB);
+    const float a = A[i * lda + k], h = tf32_hi(a);
+    float* o = A3 + i * 3 * kTriB;
+    o[k] = h;
+    o[kTriB + k] = a - h;
+    o[2 * kTriB + k] = h;
+  }
+}
+
+// B3[j][0:64] = hi, [64:128] = hi, [128:192] = lo of X[r0 + k][j]: block row
+// r0 of X (row-major, leading dimension n) transposed, 32 x 32 tiles through
+// shared memory.
+__global__ void __launch_bounds__(256) split_b3_kernel(const float* __restrict__ X, int n, int r0,
+                                                       float* __restrict__ B3) {
+  __shared__ float t[32][33];
+  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int r = ty; r < 32; r += 8) {
+    const int j = j0 + tx;
+    t[r][tx] = j < n ? X[(long long)(r0 + k0 + r) * n + j] : 0.f;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int j = j0 + r;
+    if (j < n) {
+      const float b = t[tx][r], h = tf32_hi(b);
+      float* o = B3 + (long long)j * 3 * kTriB + k0 + tx;
+      o[0] = h;
+      o[kTriB] = h;
+      o[2 * kTriB] = b - h;
+    }
+  }
+}
+
+Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, cudaStream_t st) {
   if (n <= 0) return ok();
   const int nblk = ceil_div(n, kTriB);
   const int* perm = w->ipiv + n;
@@ -748,21 +800,36 @@ Error lu_inverse_f32(const float* LU, int n, LuWork* w, float* X, cudaStream_t s
   perm_matrix_kernel<<<std::min<long long>(ceil_div((long long)n * n, 256), 4096), 256, 0, st>>>(perm, n, X);
   UVLM_LAUNCH_CHECK();
   const int cg = ceil_div(n, 64);
-  // X = L^-1 P: block forward substitution, X_I = Linv_II (P_I - L_I,<I X_<I)
+  // Right-looking block substitution: each finished block row X_I (times the
+  // inverse of its diagonal block) is subtracted from the rows still to come
+  // in one rank-kTriB update, C -= A X_I: split-TF32 on the tensor cores when
+  // the operands are TMA-aligned (n % 4 == 0, whole 64-row blocks), else SIMT.
+  const bool tc = upd != kLuUpdateSimt && n % 4 == 0 && w->a3 != nullptr && w->b3 != nullptr;
+  auto update = [&](float* C, const float* A, int m, int r0, int nb) -> Error {
+    if (m <= 0) return ok();
+    if (tc && nb == kTriB) {
+      split_a3_kernel<<<std::min<long long>(ceil_div((long long)m * kTriB, 256), 4096), 256, 0, st>>>(A, n, m, w->a3);
+      UVLM_LAUNCH_CHECK();
+      split_b3_kernel<<<dim3(ceil_div(n, 32), kTriB / 32), 256, 0, st>>>(X, n, r0, w->b3);
+      UVLM_LAUNCH_CHECK();
+      return gemm_update_tc(C, n, w->a3, 3 * kTriB, w->b3, 3 * kTriB, m, n, 3 * kTriB, kLuUpdateTF32, w, st);
+    }
+    return gemm_update_f32_simt(C, n, A, n, X + (long long)r0 * n, n, m, n, nb, st);
+  };
+  // X = L^-1 P (L unit lower triangular): X_I = Linv_II X_I, then
+  // X_>I -= L_>I,I X_I
   for (int I = 0; I < nblk; ++I) {
-    const int r0 = I * kTriB, nb = std::min(kTriB, n - r0);
-    if (r0 > 0) UVLM_TRY(gemm_update_f32_simt(X + (long long)r0 * n, n, LU + (long long)r0 * n, n, X, n, nb, n, r0, st));
+    const int r0 = I * kTriB, nb = std::min(kTriB, n - r0), r1 = r0 + nb;
     apply_block_kernel<<<cg, 256, 0, st>>>(dl + (long long)I * kTriB * kTriB, X, n, r0, nb);
     UVLM_LAUNCH_CHECK();
+    UVLM_TRY(update(X + (long long)r1 * n, LU + (long long)r1 * n + r0, n - r1, r0, nb));
   }
-  // X = U^-1 X: block backward substitution, X_I = Uinv_II (X_I - U_I,>I X_>I)
+  // X = U^-1 X: X_I = Uinv_II X_I, then X_<I -= U_<I,I X_I
   for (int I = nblk - 1; I >= 0; --I) {
-    const int r0 = I * kTriB, nb = std::min(kTriB, n - r0), r1 = r0 + nb;
-    if (r1 < n)
-      UVLM_TRY(gemm_update_f32_simt(X + (long long)r0 * n, n, LU + (long long)r0 * n + r1, n, X + (long long)r1 * n, n,
-                                    nb, n, n - r1, st));
+    const int r0 = I * kTriB, nb = std::min(kTriB, n - r0);
     apply_block_kernel<<<cg, 256, 0, st>>>(du + (long long)I * kTriB * kTriB, X, n, r0, nb);
     UVLM_LAUNCH_CHECK();
+    UVLM_TRY(update(X, LU + r0, r0, r0, nb));
   }
   return ok();
 }
@@ -787,6 +854,8 @@ Error lu_work_alloc(LuWork* w, int n, int elem_size, int num_sms) {
   UVLM_CUDA_TRY(cudaMemset(w->err, 0, sizeof(int) * 4));
   if (elem_size == 4) {
     UVLM_CUDA_TRY(cudaMalloc(&w->ut, sizeof(float) * (size_t)n * kLuNB));
+    UVLM_CUDA_TRY(cudaMalloc(&w->a3, sizeof(float) * (size_t)n * 3 * kTriB));
+    UVLM_CUDA_TRY(cudaMalloc(&w->b3, sizeof(float) * (size_t)n * 3 * kTriB));
     UVLM_CUDA_TRY(cudaMalloc(&w->opA, 2 * (size_t)n * kLuNB));
     UVLM_CUDA_TRY(cudaMalloc(&w->opB, 2 * (size_t)n * kLuNB));
   }
@@ -806,6 +875,8 @@ void lu_work_free(LuWork* w) {
   cudaFree(w->dinv_u);
   cudaFree(w->flags);
   cudaFree(w->ut);
+  cudaFree(w->a3);
+  cudaFree(w->b3);
   cudaFree(w->opA);
   cudaFree(w->opB);
   *w = LuWork{};

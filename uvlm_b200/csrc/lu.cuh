@@ -44,6 +44,8 @@ struct LuWork {
   void* diag_data = nullptr;  // [2][kLuNB]
   void* dinv_l = nullptr;     // [nblk][kTriB][kTriB] inverses of the diagonal blocks of L
   void* dinv_u = nullptr;     // [nblk][kTriB][kTriB] inverses of the diagonal blocks of U
+  float* a3 = nullptr;        // [n][3 kTriB] split-TF32 operands of the dense inverse's updates
+  float* b3 = nullptr;        // [n][3 kTriB]
   unsigned* flags = nullptr;  // [2][nblk] solve progress flags (epoch tagged)
   unsigned epoch = 0;
   void* ut = nullptr;         // tensor-core path: U12 transposed (K-major B operand)
@@ -73,7 +75,7 @@ Error lu_solve_f32(const float* LU, int n, LuWork* w, const double* v, double* z
 // lu_factor_f32 (block forward then backward substitution on the identity
 // permuted by the pivots, GEMM updates between the diagonal-block inverses).
 // A stale preconditioner applied as one dense matrix-vector product.
-Error lu_inverse_f32(const float* LU, int n, LuWork* w, float* X, cudaStream_t st);
+Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, cudaStream_t st);
 
 // Trailing update used by the factorisation (exposed for tests/benches):
 // C[m x nc] -= A[m x k] * B[k x nc], row-major with leading dims.

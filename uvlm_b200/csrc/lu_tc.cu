@@ -5,7 +5,9 @@
 // tile: TMA loads both operand tiles (128-byte swizzle) into shared memory,
 // one thread issues the tcgen05.mma chain (kind::tf32 on the FP32 data, or
 // kind::f16 on BF16 copies) accumulating in TMEM, and four warps read the
-// accumulator with tcgen05.ld and subtract it from C.  Every wait is bounded:
+// accumulator with tcgen05.ld and subtract it from C along its rows (float4,
+// staged through shared memory).  C's rows must be 16-byte aligned (C and
+// ldc multiples of 4 floats), as the callers' TMA operands already require.  Every wait is bounded:
 // on a timeout the CTA flags the error word, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -156,7 +158,13 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const int row = m0 + warp * 32 + lane;
+    // Epilogue: each warp moves its 32 accumulator rows through a 32 x 33
+    // shared-memory slice (4 x 4.2 KB inside the operand tiles, which are
+    // free once the MMAs completed; at least 32 KB even for one K chunk) so
+    // that the read-modify-write of C runs along rows: 8 lanes per row, a
+    // float4 each, 4 rows per instruction.
+    float* stage = reinterpret_cast<float*>(sA) + warp * 32 * 33;
+    const int sub = lane >> 3, q4 = (lane & 7) * 4;
     for (int j = 0; j < kBN / 32; ++j) {
       uint32_t r[32];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32);
@@ -170,12 +178,31 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
             "=r"(r[30]), "=r"(r[31])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
-        float* crow = C + (long long)row * ldc + n0 + j * 32;
 #pragma unroll
-        for (int c = 0; c < 32; ++c)
-          if (n0 + j * 32 + c < N) crow[c] -= __uint_as_float(r[c]);
+      for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = __uint_as_float(r[c]);  // row = lane, column c
+      __syncwarp();
+      const int col = n0 + j * 32 + q4;
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int rr = p * 4 + sub;
+        const int row = m0 + warp * 32 + rr;
+        const float* srow = stage + rr * 33 + q4;
+        if (row < M) {
+          float* c4 = C + (long long)row * ldc + col;
+          if (col + 3 < N) {
+            float4 v = *reinterpret_cast<const float4*>(c4);
+            v.x -= srow[0];
+            v.y -= srow[1];
+            v.z -= srow[2];
+            v.w -= srow[3];
+            *reinterpret_cast<float4*>(c4) = v;
+          } else {
+            for (int e = 0; e < 4; ++e)
+              if (col + e < N) c4[e] -= srow[e];
+          }
+        }
       }
+      __syncwarp();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -236,8 +263,9 @@ Error gemm_update_tc(float* C, int ldc, const float* A, int lda, const float* Bt
   if (m <= 0 || nc <= 0) return ok();
   if (!load_encoder()) return fail(kErrUnsupported, "cuTensorMapEncodeTiled unavailable");
   // TMA: 16-byte aligned bases and row strides, inner coordinates on 128-byte rows
-  if ((lda % 4) || (ldbt % 4) || (k % (kind == kLuUpdateBF16 ? 64 : 32)) ||
-      (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(Bt) % 16))
+  if ((lda % 4) || (ldbt % 4) || (ldc % 4) || (k % (kind == kLuUpdateBF16 ? 64 : 32)) ||
+      (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(Bt) % 16) ||
+      (reinterpret_cast<uintptr_t>(C) % 16))
     return fail(kErrUnsupported, "operands not TMA-aligned");
   CUtensorMap ta, tb;
   int kchunks = 0, a_x0 = 0, a_y0 = 0;
