@@ -50,3 +50,27 @@ def test_sheet_and_snapshot_records_follow_the_run(tmp_path, precision):
         snap = snaps[s]
         np.testing.assert_array_equal(snap["gammas"], np.concatenate([g.ravel(), wg.ravel()]))
         np.testing.assert_array_equal(snap["rings"][0], [pos[0, 1, 0], pos[0, 1, 1], pos[0, 0, 1], pos[0, 0, 0]])
+
+
+def test_output_error_paths_and_reopen(tmp_path):
+    import uvlm_b200 as U
+    from uvlm_b200 import output
+
+    sim = U.SimpleSimulator(precision="fp64")
+    sim.AddWing(U.RectGenerator(), U.Morphing().set_plug(0.1, 1.0), 1.0, 4.0, 2, 4)
+    sim.set_forward_flight([-1.0, 0.0, 0.0])
+    with pytest.raises(U.UVLMError):
+        sim.set_sheet_path(str(tmp_path / "no_such_dir" / "x.rec"))   # cannot open: an error, no writer
+    sim._sheet_path = None
+    sim.flush_output()                                                  # nothing to flush
+    first, second = str(tmp_path / "a.rec"), str(tmp_path / "b.rec")
+    sim.set_sheet_path(first)
+    sim.begin()
+    for s in range(3):
+        sim.step(s, 0.1)
+    sim.set_sheet_path(second)                                          # closes a.rec after its 3 records
+    for s in range(3, 5):
+        sim.step(s, 0.1)
+    sim.close()                                                         # flushes b.rec
+    assert [r["t"] for r in output.read_sheets(first)] == [0.0, 0.1, 0.2]
+    assert [round(r["t"], 12) for r in output.read_sheets(second)] == [0.3, 0.4]

@@ -71,12 +71,17 @@ __device__ inline int find_case(const long long* pre, int n, long long g) {
 __device__ inline WingShape shape_of(const BCase& b) { return WingShape{1, b.R, b.C}; }
 
 // ------------------------------------------------------------ simple stages
+// Start of a step: gamma_hist <- gamma_prev <- gamma (circulations of the
+// last two steps; the loads need the last, the solve's extrapolated initial
+// guess both).
 __global__ void b_begin_kernel(const long long* __restrict__ ring_pre, int n, const double* gamma,
-                               double* gamma_prev) {
+                               double* gamma_prev, double* gamma_hist) {
   const long long total = ring_pre[n];
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-       g += (long long)gridDim.x * blockDim.x)
+       g += (long long)gridDim.x * blockDim.x) {
+    gamma_hist[g] = gamma_prev[g];
     gamma_prev[g] = gamma[g];
+  }
 }
 
 __global__ void b_kinematics_kernel(const BCase* __restrict__ cs, BPrefix P, int n, const long long* d_step,
@@ -530,6 +535,7 @@ constexpr double kStaleContraction = 0.5;
 template <class T>
 __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __restrict__ cs, double* A64, float* F32,
                                                                 int* piv_all, const double* rhs, double* gamma,
+                                                                const double* gamma_hist, const long long* d_step,
                                                                 int max_sweeps, double tol, int stale,
                                                                 int* has_factor, unsigned long long* refac,
                                                                 int* sweeps_out, double* res_out, int* status) {
@@ -572,7 +578,10 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
     };
     bool done = false;
     if (stale && has_factor[blockIdx.x]) {
-      for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = gamma[b.ring_off + i];
+      // refine from the extrapolation 2 G(s-1) - G(s-2) (from G(s-1) before step 2)
+      const bool extrap = *d_step >= 2;
+      for (int i = threadIdx.x; i < N; i += kSolveThreads)
+        x[i] = extrap ? 2.0 * gamma[b.ring_off + i] - gamma_hist[b.ring_off + i] : gamma[b.ring_off + i];
       __syncthreads();
       rel = residual();
       double prev = rel;
@@ -796,6 +805,7 @@ struct uvlm_batch {
   long long* d_pre = nullptr;  // 7 prefix arrays of n + 1
   long long* d_step = nullptr;
   double *d_pos_init = nullptr, *d_pos = nullptr, *d_gamma = nullptr, *d_gamma_prev = nullptr;
+  double* d_gamma_hist = nullptr;
   double *d_cx = nullptr, *d_cy = nullptr, *d_cz = nullptr, *d_normal = nullptr, *d_area = nullptr,
          *d_uls = nullptr, *d_rhs = nullptr;
   double *d_lx = nullptr, *d_ly = nullptr, *d_lz = nullptr, *d_line_uls = nullptr;
@@ -916,6 +926,7 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   UVLM_TRY(balloc(&d_pos, 3 * tot_nodes));
   UVLM_TRY(balloc(&d_gamma, tot_rings));
   UVLM_TRY(balloc(&d_gamma_prev, tot_rings));
+  UVLM_TRY(balloc(&d_gamma_hist, tot_rings));
   UVLM_TRY(balloc(&d_cx, tot_rings));
   UVLM_TRY(balloc(&d_cy, tot_rings));
   UVLM_TRY(balloc(&d_cz, tot_rings));
@@ -991,6 +1002,7 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   UVLM_CUDA_TRY(cudaMemset(d_step, 0, sizeof(long long)));
   UVLM_CUDA_TRY(cudaMemset(d_gamma, 0, sizeof(double) * tot_rings));
   UVLM_CUDA_TRY(cudaMemset(d_gamma_prev, 0, sizeof(double) * tot_rings));
+  UVLM_CUDA_TRY(cudaMemset(d_gamma_hist, 0, sizeof(double) * tot_rings));
   UVLM_CUDA_TRY(cudaMemset(d_wpos, 0, sizeof(double) * 3 * tot_wnode));
   UVLM_CUDA_TRY(cudaMemset(d_wgamma, 0, sizeof(double) * tot_wring));
   UVLM_CUDA_TRY(cudaMemset(d_status, 0, sizeof(int) * 4));
@@ -1028,7 +1040,7 @@ Error uvlm_batch::enqueue_step() {
     UVLM_LAUNCH_CHECK();
     return ok();
   };
-  b_begin_kernel<<<grid, 256, 0, st>>>(P.ring, n, d_gamma, d_gamma_prev);
+  b_begin_kernel<<<grid, 256, 0, st>>>(P.ring, n, d_gamma, d_gamma_prev, d_gamma_hist);
   UVLM_LAUNCH_CHECK();
   b_kinematics_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, d_step, d_pos_init, d_pos);
   UVLM_LAUNCH_CHECK();
@@ -1048,10 +1060,11 @@ Error uvlm_batch::enqueue_step() {
   const size_t smem = sizeof(double) * 2 * (size_t)max_N + panel_smem_bytes(max_N, mixed() ? 4 : 8);
   if (mixed())
     b_solve_kernel<float><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
-                                                          cfg.refine_max_iter, cfg.refine_tol, cfg.stale_factors,
+                                                          d_gamma_hist, d_step, cfg.refine_max_iter, cfg.refine_tol, cfg.stale_factors,
                                                           d_has_factor, d_refac, d_sweeps, d_res, d_status);
   else
-    b_solve_kernel<double><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma, 0, 0.0,
+    b_solve_kernel<double><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
+                                                           d_gamma_hist, d_step, 0, 0.0,
                                                            0, d_has_factor, d_refac, d_sweeps, d_res, d_status);
   UVLM_LAUNCH_CHECK();
   // loads: line velocities from the bound sheet (new circulation) and the wake
@@ -1091,7 +1104,8 @@ void uvlm_batch::release() {
   if (graph) cudaGraphDestroy(graph);
   exec = nullptr;
   graph = nullptr;
-  void* ptrs[] = {d_cases, d_pre, d_step, d_pos_init, d_pos, d_gamma, d_gamma_prev, d_cx, d_cy, d_cz, d_normal,
+  void* ptrs[] = {d_cases, d_pre, d_step, d_pos_init, d_pos, d_gamma, d_gamma_prev, d_gamma_hist, d_cx, d_cy, d_cz,
+                  d_normal,
                   d_area, d_uls, d_rhs, d_lx, d_ly, d_lz, d_line_uls, d_wpos, d_wpos2, d_k1, d_wgamma, d_wtx,
                   d_wty, d_wtz, d_vx, d_vy, d_vz, d_A64, d_F32, d_piv, d_tiles, d_rec, d_partial, d_in, d_plan,
                   d_totals, d_status, d_sweeps, d_res, d_loads, d_has_factor, d_refac};
