@@ -262,10 +262,31 @@ def synthetic_state_np():
 
 
 def run_profile(args):
-    """Mixed form only, from a synthesized full-size state: the small,
-    quick workload used for ncu captures of the per-step kernels."""
+    """The small, quick workloads used for ncu captures: the heave/pitch
+    wing's per-step kernels from a synthesized full-size state (default), its
+    step 0 alone (--profile-step0: the first TF32 factorisation and dense
+    inverse), or the 256-case sweep (--workload batch256: steps + warmup
+    batched MainLoops from the start)."""
     import uvlm_b200 as U
 
+    if args.workload == "batch256":
+        from uvlm_b200.batch import draw_cases, make_batch
+
+        sim = make_batch(draw_cases(256, seed=0), precision="mixed", max_steps=150)
+        sim.run(args.steps + args.warmup)
+        sim.close()
+        print(json.dumps({"profile": "ok", "workload": "batch256", "steps": args.steps + args.warmup,
+                          "launches": int(U.lib().uvlm_kernel_launch_count())}), flush=True)
+        return
+    if args.profile_step0:
+        sim = make_mixed(warm_start="extrapolate")
+        sim.begin()
+        sim.step(0, DT)
+        sim.synchronize()
+        sim.close()
+        print(json.dumps({"profile": "ok", "step0": True, "launches": int(U.lib().uvlm_kernel_launch_count())}),
+              flush=True)
+        return
     if args.form == "mixed":
         sim = make_mixed()
     else:
@@ -618,6 +639,8 @@ def main():
     ap.add_argument("--no-floor", action="store_true", help="skip the one-ulp FP64 rounding-floor run")
     ap.add_argument("--profile", action="store_true", help="one form on a synthesized state, for ncu")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"], help="form run by --profile")
+    ap.add_argument("--profile-step0", action="store_true",
+                    help="with --profile: only step 0 of the mixed form (first factorisation and inverse)")
     ap.add_argument("--workload", default="heave_pitch", choices=list(WORKLOADS) + ["batch256"],
                     help="heave_pitch (the metric's configuration, default), tandem4, morphing, batch256")
     args = ap.parse_args()
