@@ -395,7 +395,9 @@ __device__ __forceinline__ void walk_full_strip2(const RecF* sm, bool last_h, co
 // its own nodes) is "far" from a target x when |x - O| >= 2 rho + 1e-3.  Then
 // every pair has |r| >= rho + 1e-3, so no node is cut (|r| > 1e-10) and every
 // r1.r2 > 0 (the strip subtends less than 60 degrees from x), which leaves the
-// beyond-end form of the segment factor alone, without cancellation.  With
+// beyond-end form of the segment factor alone, without cancellation; it is
+// evaluated as 2 g (|r1|+|r2|) / (|r1||r2| ((|r1|+|r2|)^2 - |r0|^2)) with the
+// segment's |r0|^2 from its record, which needs no r1.r2.  With
 // node and target coordinates relative to O (FP32, rounded from the hi/lo
 // differences), r = x_O - p_O costs one subtraction per component instead of
 // three, and its error stays below ulp(rho)/2 + ulp(|x_O|)/2 <= 1.5 ulp(|r|).
@@ -410,16 +412,18 @@ __device__ __forceinline__ Node2 node_far2(const float4 L, const float2 (&ts)[3]
   return n;
 }
 
-__device__ __forceinline__ void seg_far2(const SegV<float>& r0, const Node2& a, const Node2& b, float g, float2& vx,
-                                         float2& vy, float2& vz) {
+__device__ __forceinline__ void seg_far2(const SegV<float>& r0, float l2, const Node2& a, const Node2& b, float g2,
+                                         float2& vx, float2& vy, float2& vz) {
   const float2 dx = fma2(bc2(r0.y), a.rz, mul2(bc2(-r0.z), a.ry));
   const float2 dy = fma2(bc2(r0.z), a.rx, mul2(bc2(-r0.x), a.rz));
   const float2 dz = fma2(bc2(r0.x), a.ry, mul2(bc2(-r0.y), a.rx));
   const float2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
-  const float2 dot12 = fma2(a.rz, b.rz, fma2(a.ry, b.ry, mul2(a.rx, b.rx)));
-  const float2 nn = mul2(a.n, b.n);
-  const float2 den = mul2(nn, add2(nn, dot12));
-  float2 k = mul2(mul2(bc2(g), add2(a.n, b.n)), make_float2(nb_rcp(den.x), nb_rcp(den.y)));
+  // 2 (|r1||r2| + r1.r2) = (|r1| + |r2|)^2 - |r0|^2 (r1 - r2 = r0): no dot
+  // product; in the far field |r1| + |r2| exceeds |r0| by a margin of the
+  // strip's size, so the difference loses at most a couple of bits
+  const float2 sn = add2(a.n, b.n);
+  const float2 den = mul2(mul2(a.n, b.n), fma2(sn, sn, bc2(-l2)));
+  float2 k = mul2(mul2(bc2(g2), sn), make_float2(nb_rcp(den.x), nb_rcp(den.y)));
   k.x = d2.x >= (float)kCutD2 ? k.x : 0.f;
   k.y = d2.y >= (float)kCutD2 ? k.y : 0.f;
   vx = fma2(k, dx, vx);
@@ -427,40 +431,46 @@ __device__ __forceinline__ void seg_far2(const SegV<float>& r0, const Node2& a, 
   vz = fma2(k, dz, vz);
 }
 
-// One node column of a far strip: local node coordinates and gS from `lcol`,
-// the rest of the record (gH, segment vectors) from `col`.
+// One node column of a far strip: local node coordinates and 2 gS from
+// `lcol`, the rest of the record (gH, segment vectors and their squared
+// lengths) from `col`.  The spanwise segments ending in this column use the
+// previous column's vectors, lengths and strengths (ps0, pl2, pgS).
 template <int H, bool FIRST, bool DO_H>
 __device__ __forceinline__ void far_column2(const RecF* col, const float4* lcol, const float2 (&ts)[3],
-                                            Node2 (&prev)[H], SegV<float> (&ps0)[H], float (&pgS)[H],
-                                            float2 (&acc)[3]) {
+                                            Node2 (&prev)[H], SegV<float> (&ps0)[H], float (&pl2)[H],
+                                            float (&pgS)[H], float2 (&acc)[3]) {
   Node2 cur[H + 1];
-  float gS[H], gH[H];
+  float gS[H], gH[H], l2S[H], l2H[H];
   SegV<float> s0[H], h0[H];
 #pragma unroll
   for (int r = 0; r <= H; ++r) {
     const float4 L = lcol[r * (kStripCols + 1)];
     if (r < H) {
       const RecF& rec = col[r * (kStripCols + 1)];
-      const float4 sv = rec.sv;
+      const float4 sv = rec.sv, hv = rec.hv;
+      const float gh = rec.lo.w;
       gS[r] = L.w;
-      gH[r] = rec.lo.w;
+      gH[r] = gh + gh;
       s0[r] = SegV<float>{sv.x, sv.y, sv.z};
-      h0[r] = SegV<float>{sv.w, rec.hv.x, rec.hv.y};
+      h0[r] = SegV<float>{sv.w, hv.x, hv.y};
+      l2S[r] = hv.z;
+      l2H[r] = hv.w;
     }
     cur[r] = node_far2(L, ts);
   }
   if (DO_H) {
 #pragma unroll
-    for (int r = 0; r < H; ++r) seg_far2(h0[r], cur[r], cur[r + 1], gH[r], acc[0], acc[1], acc[2]);
+    for (int r = 0; r < H; ++r) seg_far2(h0[r], l2H[r], cur[r], cur[r + 1], gH[r], acc[0], acc[1], acc[2]);
   }
   if (!FIRST) {
 #pragma unroll
-    for (int r = 0; r < H; ++r) seg_far2(ps0[r], prev[r], cur[r], pgS[r], acc[0], acc[1], acc[2]);
+    for (int r = 0; r < H; ++r) seg_far2(ps0[r], pl2[r], prev[r], cur[r], pgS[r], acc[0], acc[1], acc[2]);
   }
 #pragma unroll
   for (int r = 0; r < H; ++r) {
     pgS[r] = gS[r];
     ps0[r] = s0[r];
+    pl2[r] = l2S[r];
     prev[r] = cur[r];
   }
 }
@@ -470,15 +480,15 @@ __device__ __forceinline__ void walk_far_strip2(const RecF* sm, const float4* lo
                                                 const float2 (&ts)[3], float (&acc)[2][3]) {
   Node2 prev[H];
   SegV<float> ps0[H];
-  float pgS[H];
+  float pl2[H], pgS[H];
   float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-  far_column2<H, true, true>(sm, loc, ts, prev, ps0, pgS, a2);
+  far_column2<H, true, true>(sm, loc, ts, prev, ps0, pl2, pgS, a2);
 #pragma unroll 2
-  for (int j = 1; j < kStripCols; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pgS, a2);
+  for (int j = 1; j < kStripCols; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pl2, pgS, a2);
   if (last_h)
-    far_column2<H, false, true>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pgS, a2);
+    far_column2<H, false, true>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pl2, pgS, a2);
   else
-    far_column2<H, false, false>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pgS, a2);
+    far_column2<H, false, false>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pl2, pgS, a2);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     acc[0][c] += a2[c].x;
@@ -522,21 +532,21 @@ __device__ __forceinline__ void walk_far_cols2(const RecF* sm, const float4* loc
                                                const float2 (&ts)[3], float (&acc)[2][3]) {
   Node2 prev[H];
   SegV<float> ps0[H];
-  float pgS[H];
+  float pl2[H], pgS[H];
   float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   if (n_cols == 1) {
     if (last_h)
-      far_column2<H, true, true>(sm, loc, ts, prev, ps0, pgS, a2);
+      far_column2<H, true, true>(sm, loc, ts, prev, ps0, pl2, pgS, a2);
     else
-      far_column2<H, true, false>(sm, loc, ts, prev, ps0, pgS, a2);
+      far_column2<H, true, false>(sm, loc, ts, prev, ps0, pl2, pgS, a2);
   } else {
-    far_column2<H, true, true>(sm, loc, ts, prev, ps0, pgS, a2);
+    far_column2<H, true, true>(sm, loc, ts, prev, ps0, pl2, pgS, a2);
 #pragma unroll 2
-    for (int j = 1; j < n_cols - 1; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pgS, a2);
+    for (int j = 1; j < n_cols - 1; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pl2, pgS, a2);
     if (last_h)
-      far_column2<H, false, true>(sm + n_cols - 1, loc + n_cols - 1, ts, prev, ps0, pgS, a2);
+      far_column2<H, false, true>(sm + n_cols - 1, loc + n_cols - 1, ts, prev, ps0, pl2, pgS, a2);
     else
-      far_column2<H, false, false>(sm + n_cols - 1, loc + n_cols - 1, ts, prev, ps0, pgS, a2);
+      far_column2<H, false, false>(sm + n_cols - 1, loc + n_cols - 1, ts, prev, ps0, pl2, pgS, a2);
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -546,8 +556,8 @@ __device__ __forceinline__ void walk_far_cols2(const RecF* sm, const float4* loc
 }
 
 // Local coordinates of a staged strip (its n_cols columns) relative to its
-// central real node O: loc[k] = (p_k - O, gS_k) for real nodes, (0, 0, 0,
-// gS_k) for the zero padding (whose segments are cut by d = 0 either way).  Returns whether all
+// central real node O: loc[k] = (p_k - O, 2 gS_k) for real nodes, (0, 0, 0,
+// 2 gS_k) for the zero padding (whose segments are cut by d = 0 either way).  Returns whether all
 // of this warp's targets are far from the strip (warp-uniform) and their
 // coordinates relative to O.  `red` holds one float per warp.
 template <int H, int BLOCK>
@@ -561,7 +571,7 @@ __device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si,
     const int r = q / n_cols, j = q - r * n_cols;
     const int k = r * (kStripCols + 1) + j;
     const float4 h = sm[k].hi, l = sm[k].lo;
-    float4 L = make_float4(0.f, 0.f, 0.f, h.w);
+    float4 L = make_float4(0.f, 0.f, 0.f, h.w + h.w);  // 2 gS (the far segment factor's form)
     if (r < si.nr && j < si.n_cols) {
       L.x = (h.x - oh.x) + (l.x - ol.x);
       L.y = (h.y - oh.y) + (l.y - ol.y);

@@ -43,7 +43,7 @@ struct alignas(16) RecF {
   float4 hi;  // x_hi, y_hi, z_hi, gS/(4 pi)
   float4 lo;  // x_lo, y_lo, z_lo, gH/(4 pi)
   float4 sv;  // s0.x, s0.y, s0.z, h0.x
-  float4 hv;  // h0.y, h0.z, 0, 0
+  float4 hv;  // h0.y, h0.z, |s0|^2, |h0|^2 (squared lengths of the FP32 segment vectors)
 };
 struct alignas(16) RecD {
   double4 a;  // x, y, z, gS/(4 pi)
@@ -118,8 +118,11 @@ __device__ inline Rec build_record(const SheetView& v, long long k) {
     r.hi = make_float4(hx, hy, hz, (float)(gS * s));
     r.lo = make_float4((float)(p[0] - (double)hx), (float)(p[1] - (double)hy), (float)(p[2] - (double)hz),
                        (float)(gH * s));
-    r.sv = make_float4((float)s0[0], (float)s0[1], (float)s0[2], (float)h0[0]);
-    r.hv = make_float4((float)h0[1], (float)h0[2], 0.f, 0.f);
+    const float sx = (float)s0[0], sy = (float)s0[1], sz = (float)s0[2];
+    const float ex = (float)h0[0], ey = (float)h0[1], ez = (float)h0[2];
+    r.sv = make_float4(sx, sy, sz, ex);
+    r.hv = make_float4(ey, ez, (float)((double)sx * sx + (double)sy * sy + (double)sz * sz),
+                       (float)((double)ex * ex + (double)ey * ey + (double)ez * ez));
   } else {
     r.a = make_double4(p[0], p[1], p[2], gS * s);
     r.b = make_double4(gH * s, s0[0], s0[1], s0[2]);
