@@ -59,7 +59,17 @@ CPU_STRIDE, CPU_LU_N = 32, 2048
 NBODY_TRAFFIC = {"heave_pitch": 4899072}
 
 
-def make_mixed(device=0, warm_start=None, wl=None):
+def variant_index(name):
+    """Index of an N-body tile variant by name (e.g. "fp32_h3_t2_b128_x2f")."""
+    import uvlm_b200 as U
+
+    for v in range(64):
+        if U.lib().uvlm_nbody_variant_name(v).decode() == name:
+            return v
+    raise ValueError(name)
+
+
+def make_mixed(device=0, warm_start=None, wl=None, **kw):
     """The mixed-precision form: FP32 N-body, TF32 tensor-core LU factored
     once and used stale as the GMRES preconditioner (its dense inverse), FP64
     residuals, learned warm start where the workload has trained weights
@@ -68,7 +78,7 @@ def make_mixed(device=0, warm_start=None, wl=None):
     wl = wl or _heave_pitch()
     if warm_start is None:
         warm_start = "mlp" if wl.weights and os.path.exists(wl.weights) else "extrapolate"
-    sim = wl.build("mixed", device=device, solver="gmres_stale", warm_start=warm_start)
+    sim = wl.build("mixed", device=device, solver="gmres_stale", warm_start=warm_start, **kw)
     if warm_start == "mlp":
         from uvlm_b200.warmstart import MLP
 
@@ -278,8 +288,11 @@ def run_profile(args):
         print(json.dumps({"profile": "ok", "workload": "batch256", "steps": args.steps + args.warmup,
                           "launches": int(U.lib().uvlm_kernel_launch_count())}), flush=True)
         return
+    # the library's default tiles, not the autotuner (whose timings a profiler distorts)
+    pinned = dict(nbody_variant=variant_index("fp32_h3_t2_b128_x2f" if args.form == "mixed" else
+                                              "fp64_h2_t1_b128_m3"))
     if args.profile_step0:
-        sim = make_mixed(warm_start="extrapolate")
+        sim = make_mixed(warm_start="extrapolate", **pinned)
         sim.begin()
         sim.step(0, DT)
         sim.synchronize()
@@ -288,9 +301,9 @@ def run_profile(args):
               flush=True)
         return
     if args.form == "mixed":
-        sim = make_mixed()
+        sim = make_mixed(**pinned)
     else:
-        sim = make_sim("fp64")
+        sim = make_sim("fp64", **pinned)
     sim.begin()
     sim.step(0, DT)
     st = synthetic_state_np()
