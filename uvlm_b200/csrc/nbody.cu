@@ -475,27 +475,6 @@ __device__ __forceinline__ void far_column2(const RecF* col, const float4* lcol,
   }
 }
 
-template <int H>
-__device__ __forceinline__ void walk_far_strip2(const RecF* sm, const float4* loc, bool last_h,
-                                                const float2 (&ts)[3], float (&acc)[2][3]) {
-  Node2 prev[H];
-  SegV<float> ps0[H];
-  float pl2[H], pgS[H];
-  float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-  far_column2<H, true, true>(sm, loc, ts, prev, ps0, pl2, pgS, a2);
-#pragma unroll 2
-  for (int j = 1; j < kStripCols; ++j) far_column2<H, false, true>(sm + j, loc + j, ts, prev, ps0, pl2, pgS, a2);
-  if (last_h)
-    far_column2<H, false, true>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pl2, pgS, a2);
-  else
-    far_column2<H, false, false>(sm + kStripCols, loc + kStripCols, ts, prev, ps0, pl2, pgS, a2);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    acc[0][c] += a2[c].x;
-    acc[1][c] += a2[c].y;
-  }
-}
-
 // Column-bounded forms of the packed walkers: the strip's n_cols node
 // columns (row-padded staging), the chordwise segments of the last column
 // only when the strip owns them (last_h).
@@ -858,7 +837,7 @@ __global__ void batch_reduce_kernel(const NBodyBatchPlan* __restrict__ plan, int
 // Batched tiles: FP32 column-bounded packed FP32x2 h3 t2 b128 (every
 // problem), FP64 h2 t1 b128; 3 CTAs/SM each.
 constexpr int kBatchBlock = 128;
-constexpr int kBatchTptF = 2, kBatchHF = 4, kBatchHFP = 3, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
+constexpr int kBatchTptF = 2, kBatchHFP = 3, kBatchTptD = 1, kBatchHD = 2, kBatchMinB = 3;
 constexpr int kBatchPadPK = 2;  // walker of the padded class (see eval_strips)
 
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, int splits, long long n, double* vx,
