@@ -558,12 +558,36 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     // r = b - A x (FP64), returns ||r|| / ||b|| (same value in every thread)
     auto residual = [&]() -> double {
-      for (int i = wid; i < N; i += kSolveThreads / 32) {
-        const double* a = A + (long long)i * N;
-        double acc = 0;
-        for (int j = lane; j < N; j += 32) acc += a[j] * x[j];
-        for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-        if (lane == 0) r[i] = bb[i] - acc;
+      // four rows per warp at a time, so that enough loads of A are in
+      // flight for one SM to stream the matrix
+      constexpr int kW = kSolveThreads / 32;
+      for (int i0 = wid; i0 < N; i0 += 4 * kW) {
+        const double* a0 = A + (long long)i0 * N;
+        const bool v1 = i0 + kW < N, v2 = i0 + 2 * kW < N, v3 = i0 + 3 * kW < N;
+        const double* a1 = v1 ? a0 + (long long)kW * N : a0;
+        const double* a2 = v2 ? a0 + 2LL * kW * N : a0;
+        const double* a3 = v3 ? a0 + 3LL * kW * N : a0;
+        double c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+#pragma unroll 4
+        for (int j = lane; j < N; j += 32) {
+          const double xj = x[j];
+          c0 += a0[j] * xj;
+          c1 += a1[j] * xj;
+          c2 += a2[j] * xj;
+          c3 += a3[j] * xj;
+        }
+        for (int off = 16; off; off >>= 1) {
+          c0 += __shfl_down_sync(0xffffffffu, c0, off);
+          c1 += __shfl_down_sync(0xffffffffu, c1, off);
+          c2 += __shfl_down_sync(0xffffffffu, c2, off);
+          c3 += __shfl_down_sync(0xffffffffu, c3, off);
+        }
+        if (lane == 0) {
+          r[i0] = bb[i0] - c0;
+          if (v1) r[i0 + kW] = bb[i0 + kW] - c1;
+          if (v2) r[i0 + 2 * kW] = bb[i0 + 2 * kW] - c2;
+          if (v3) r[i0 + 3 * kW] = bb[i0 + 3 * kW] - c3;
+        }
       }
       __syncthreads();
       double rn = 0;
