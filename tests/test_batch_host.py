@@ -3,7 +3,6 @@ case sharding over ranks (world size 2, gloo on CPU; no GPU)."""
 import os
 
 import numpy as np
-import pytest
 
 
 def test_draw_cases_ranges_and_seed():

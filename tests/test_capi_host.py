@@ -8,7 +8,6 @@ import ctypes as C
 import os
 import re
 import subprocess
-import sys
 
 import pytest
 

@@ -17,7 +17,7 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
 
-from cases import CASES, make_gpu_sim, run_oracle  # noqa: E402
+from cases import CASES, make_gpu_sim  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 

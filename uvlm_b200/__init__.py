@@ -18,7 +18,6 @@ library built in-tree for sm_100a; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
-import math
 from dataclasses import dataclass
 
 import numpy as np
