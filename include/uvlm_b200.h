@@ -329,6 +329,18 @@ int uvlm_flush_output(uvlm_ctx* ctx);
 int uvlm_write_state_record(const char* path, int32_t append, int32_t kind, int64_t num, int64_t rows, int64_t cols,
                             int64_t wake_rows, const double* wing_pos, const double* wing_gamma,
                             const double* wake_pos, const double* wake_gamma, double t);
+/* The legacy simulator's per-step file (OutputSnapshot2,
+ * src/simulator/simulator.cpp:118-160): one Snapshot2 message, unframed
+ * (SerializeToOstream), replacing the file at path.  It holds t; one
+ * ContainerShape per container (rows, cols, id = its index, chord, span);
+ * one VortexRing per ring of the pool (rings and reference nodes rings0
+ * [n_rings][4][3], rings0 NULL writes no nodes0; gamma [n_rings]); and
+ * n_mv MorphingVelocity records (center [3], the four segment velocities
+ * [4][3], freestream [3] each). */
+int uvlm_write_legacy_snapshot2(const char* path, double t, int64_t n_containers, const int64_t* rows,
+                                const int64_t* cols, const double* chord, const double* span, const double* rings,
+                                const double* rings0, const double* gamma, int64_t n_rings, const double* mv_center,
+                                const double* mv_nodes, const double* mv_freestream, int64_t n_mv);
 
 /* ---------------------------------------------- learned warm start (MLP) */
 /* No counterpart in the reference.  A per-panel MLP (8 features -> 3 x 256

@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <fstream>
 #include <functional>
 #include <memory>
@@ -653,6 +654,58 @@ inline void ResetLegacySimulator() {
   legacy_options() = o;
 }
 
+namespace legacy_detail {
+// OutputSnapshot2 (simulator.cpp:118-160) to output_path/%08lu: the container
+// shapes, every ring of the pool with its reference nodes, and per bound ring
+// the morphing velocity at its reference centroid and at (start0 + end0) / 2
+// of each segment (ForEachSegment order), with the inlet.
+inline void OutputSnapshot2(State& s, std::size_t step, double t) {
+  std::vector<int64_t> rows, cols;
+  std::vector<double> chord, span, rings, rings0, gamma, center, nodes, free;
+  for (const auto& c : s.containers) {
+    rows.push_back((int64_t)c.rows());
+    cols.push_back((int64_t)c.cols());
+    chord.push_back(c.chord());
+    span.push_back(c.span());
+  }
+  bool all0 = true;
+  for (const auto& v : *s.vortices) {
+    gamma.push_back(v.gamma());
+    all0 = all0 && v.nodes0().size() == 4;
+    for (std::size_t q = 0; q < 4; ++q)
+      for (int d = 0; d < 3; ++d) {
+        rings.push_back(detail::c3(v.nodes()[q])[d]);
+        rings0.push_back(all0 ? detail::c3(v.nodes0()[q])[d] : 0.0);
+      }
+  }
+  for (std::size_t i = 0; i < s.containers.size(); ++i) {
+    std::vector<Vector3> x;  // per ring: reference centroid, then the four segment midpoints
+    for (const auto& v : s.containers[i]) {
+      x.push_back(v.ReferenceCentroid());
+      const auto& n0 = v.nodes0();
+      for (std::size_t q = 0; q < 4; ++q) x.push_back(detail::scale(detail::add(n0[(q + 1) % 4], n0[q]), 0.5));
+    }
+    std::vector<Vector3> vel(x.size());
+    if (!x.empty())
+      detail::check(uvlm_kinematics_velocity(&s.morphings[i].kinematics(), reinterpret_cast<const double*>(x.data()),
+                                             (int64_t)x.size(), t, reinterpret_cast<double*>(vel.data())),
+                    "OutputSnapshot2");
+    for (std::size_t k = 0; k < vel.size(); ++k)
+      for (int d = 0; d < 3; ++d) (k % 5 ? nodes : center).push_back(detail::c3(vel[k])[d]);
+    for (std::size_t k = 0; k < vel.size() / 5; ++k)
+      for (int d = 0; d < 3; ++d) free.push_back(detail::c3(s.inlet)[d]);
+  }
+  char name[32];
+  std::snprintf(name, sizeof name, "/%08lu", (unsigned long)step);
+  const std::string path = s.output_path + name;
+  detail::check(uvlm_write_legacy_snapshot2(path.c_str(), t, (int64_t)rows.size(), rows.data(), cols.data(),
+                                            chord.data(), span.data(), rings.data(), all0 ? rings0.data() : nullptr,
+                                            gamma.data(), (int64_t)gamma.size(), center.data(), nodes.data(),
+                                            free.data(), (int64_t)(center.size() / 3)),
+                "OutputSnapshot2");
+}
+}  // namespace legacy_detail
+
 inline void InitSimulator() {}
 inline void AddWing(const proto::Wing& wing, const Morphing& m) {
   auto& s = legacy_detail::state();
@@ -709,6 +762,7 @@ inline void Start(const std::size_t steps, const double dt) {
     // SolveLinearProblem (:110-116)
     const VectorX gamma = SolveLinearProblem(s.containers, s.morphings, s.inlet, t, s.options.drop_wake_term);
     for (std::size_t i = 0; i < wake_offset; i++) s.vortices->at(i).set_gamma(gamma[i]);
+    if (!s.output_path.empty()) legacy_detail::OutputSnapshot2(s, step, t);
     // CalcLoadProcess (:162-200)
     std::vector<double> row{t};
     for (std::size_t i = 0; i < s.containers.size(); i++) {

@@ -4,7 +4,8 @@
 // plus the container loads against the FP64 CPU oracle.
 //   legacy_parity cpu    containers, wing builder, ring geometry (no GPU)
 //   legacy_parity gpu    shed, linear and load checks on the GPU
-//   legacy_parity start  prints the load rows of simulator::Start
+//   legacy_parity start [dir]  prints the load rows of simulator::Start
+//                              (and writes its Snapshot2 files to dir)
 // Exit status 0 when every check passes.
 #include <cmath>
 #include <cstdio>
@@ -278,7 +279,7 @@ static void gpu_checks() {
   }
 }
 
-static void start_rows(bool joukowski) {
+static void start_rows(bool joukowski, const char* out_dir) {
   // two half wings 3 x 4 (chord 1, half span 2), the second 0.8 above
   namespace S = UVLM::simulator;
   S::ResetLegacySimulator();
@@ -307,6 +308,7 @@ static void start_rows(bool joukowski) {
     S::AddWing(wing, m);
   }
   S::SetInlet(1, 0, 0);
+  if (out_dir) S::SetOutputPath(out_dir);
   S::Start(10, 2 * 3.14159265358979323846 / 40);
   for (const auto& row : S::legacy_load_rows()) {
     for (std::size_t k = 0; k < row.size(); ++k) std::printf("%s%.17g", k ? " " : "", row[k]);
@@ -318,8 +320,9 @@ int main(int argc, char** argv) {
   const char* mode = argc > 1 ? argv[1] : "cpu";
   if (!std::strcmp(mode, "cpu")) cpu_checks();
   if (!std::strcmp(mode, "gpu")) gpu_checks();
-  if (!std::strcmp(mode, "start")) start_rows(false);
-  if (!std::strcmp(mode, "start_joukowski")) start_rows(true);
+  const char* out_dir = argc > 2 ? argv[2] : nullptr;
+  if (!std::strcmp(mode, "start")) start_rows(false, out_dir);
+  if (!std::strcmp(mode, "start_joukowski")) start_rows(true, out_dir);
   if (failures) std::printf("%d check(s) failed\n", failures);
   return failures ? 1 : 0;
 }

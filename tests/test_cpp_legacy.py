@@ -47,7 +47,11 @@ def test_cpp_legacy_start_matches_oracle(tmp_path, mode):
     import legacy_oracle as L
     import pyoracle as o
 
-    r = subprocess.run([str(_build(tmp_path)), mode], capture_output=True, text=True, timeout=300)
+    from uvlm_b200 import output, tools
+
+    out_dir = tmp_path / "result"
+    out_dir.mkdir()
+    r = subprocess.run([str(_build(tmp_path)), mode, str(out_dir)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     got = np.array([[float(x) for x in line.split()] for line in r.stdout.strip().splitlines()])
     X, Y = np.meshgrid(np.arange(4) / 3.0, np.arange(5) / 2.0, indexing="ij")
@@ -60,6 +64,19 @@ def test_cpp_legacy_start_matches_oracle(tmp_path, mode):
         k.twist_amp, k.twist_omega, k.twist_phase = 0.05, 1.0, 0.3
         k.origin[2] = 0.8 * w
         kins.append(k)
-    ref = L.start(wings, kins, [1.0, 0.0, 0.0], 10, 2 * math.pi / 40, use_joukowski=mode == "start_joukowski")
+    snaps = []
+    ref = L.start(wings, kins, [1.0, 0.0, 0.0], 10, 2 * math.pi / 40, use_joukowski=mode == "start_joukowski",
+                  snapshots=snaps)
     assert got.shape == ref.shape == (11, 11)
     np.testing.assert_allclose(got, ref, rtol=0, atol=1e-8 * np.max(np.abs(ref[:, 1:])))
+    # OutputSnapshot2 (simulator.cpp:118-160): one file per step
+    files = tools.glob_result(str(out_dir))
+    assert len(files) == 11
+    for f, s in zip(files, snaps):
+        d = output.read_snapshot2_file(f)
+        assert d["t"] == s["t"] and [c["id"] for c in d["container_shapes"]] == [0, 1]
+        np.testing.assert_allclose(d["rings"], s["rings"], rtol=0, atol=1e-10 * np.abs(s["rings"]).max())
+        np.testing.assert_array_equal(d["rings0"], s["rings0"])
+        np.testing.assert_allclose(d["gammas"], s["gammas"], rtol=0, atol=1e-8 * np.abs(s["gammas"]).max())
+        np.testing.assert_allclose(d["mv_nodes"], s["mv_nodes"], rtol=0, atol=1e-8)
+        np.testing.assert_allclose(d["mv_center"], s["mv_center"], rtol=0, atol=1e-8)

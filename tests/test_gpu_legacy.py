@@ -162,3 +162,71 @@ def test_legacy_start_matches_oracle(joukowski):
     ref = L.start(wings, oks, [1.0, 0.0, 0.0], 12, dt, use_joukowski=joukowski)
     assert got.shape == ref.shape == (13, 11)
     np.testing.assert_allclose(got, ref, rtol=0, atol=1e-8 * np.max(np.abs(ref[:, 1:])))
+
+
+def test_legacy_snapshot_files_and_calc_impulse(tmp_path):
+    """SetOutputPath / SetOutputLoadPath (simulator.cpp:118-200): one Snapshot2 file per step matching the
+    oracle's pool, nodes0 and morphing velocities; the load file's rows; then calc_impulse
+    (src/calc_impulse_main.cpp) over those files against the oracle's impulse and Lamb-vector sums."""
+    import legacy_oracle as L
+    import pyoracle as o
+
+    import uvlm_b200 as M
+    from uvlm_b200 import output, tools
+    from uvlm_b200.legacy import LegacySimulator, Wing
+
+    steps, dt = 6, 2 * math.pi / 40
+    sim = LegacySimulator()
+    w1 = Wing.rect(1.0, 2.0, 3, 4)
+    w2 = Wing.rect(1.0, 2.0, 3, 4, origin=(0.0, 0.0, 0.8))
+    m1, m2 = _kin(M, 31), _kin(M, 32)
+    sim.AddWing(w1, m1)
+    sim.AddWing(w2, m2)
+    out_dir = tmp_path / "result"
+    out_dir.mkdir()
+    load_path = str(tmp_path / "load.tsv")
+    sim.SetOutputPath(str(out_dir))
+    sim.SetOutputLoadPath(load_path)
+    rows = sim.Start(steps, dt)
+    oks = []
+    for w, m in ((w1, m1), (w2, m2)):
+        k = _okin(o, m)
+        for i in range(3):
+            k.origin[i] = w.origin[i]
+        oks.append(k)
+    wings = [dict(rows=w.rows, cols=w.cols, points=w.points, origin=w.origin, chord=w.chord, span=w.span)
+             for w in (w1, w2)]
+    ref = []
+    L.start(wings, oks, [1.0, 0.0, 0.0], steps, dt, snapshots=ref)
+    files = tools.glob_result(str(out_dir))
+    assert [f[-8:] for f in files] == [f"{s:08d}" for s in range(steps + 1)]
+    for step, (f, r) in enumerate(zip(files, ref)):
+        snap = output.read_snapshot2_file(f)
+        assert snap["t"] == dt * step
+        assert [(c["rows"], c["cols"], c["id"], c["chord"], c["span"]) for c in snap["container_shapes"]] == [
+            (3, 8, 0, 1.0, 2.0), (3, 8, 1, 1.0, 2.0)]
+        assert len(snap["rings"]) == 48 + 8 * step
+        scale = np.abs(r["rings"]).max()
+        np.testing.assert_allclose(snap["rings"], r["rings"], rtol=0, atol=1e-10 * scale)
+        np.testing.assert_array_equal(snap["rings0"], r["rings0"])
+        np.testing.assert_allclose(snap["gammas"], r["gammas"], rtol=0, atol=1e-8 * np.abs(r["gammas"]).max())
+        for k in ("mv_center", "mv_nodes"):
+            np.testing.assert_allclose(snap[k], r[k], rtol=0, atol=1e-8)  # central difference, h = 1e-6
+        np.testing.assert_array_equal(snap["mv_freestream"], r["mv_freestream"])
+        imp = tools.calc_impulse(snap)
+        want = L.calc_impulse(snap)
+        np.testing.assert_allclose(imp, want, rtol=0, atol=1e-11 * max(1.0, np.abs(want).max()))
+    pool, pool_g = sim.vortices()   # the last file holds the state after the last solve
+    last = output.read_snapshot2_file(files[-1])
+    np.testing.assert_array_equal(last["rings"], pool)
+    np.testing.assert_array_equal(last["gammas"], pool_g)
+    assert np.abs(L.calc_impulse(last)[7:]).max() > 0    # the wake carries impulse
+    text = open(load_path).read().splitlines()
+    assert len(text) == steps + 1
+    np.testing.assert_allclose([[float(x) for x in ln.split("\t")] for ln in text], rows, rtol=1e-5, atol=1e-12)
+    tsv = str(tmp_path / "impulse.tsv")
+    assert tools.main(["calc_impulse", "--input", str(out_dir), "--output", tsv]) == 0
+    got = np.array([[float(x) for x in ln.split("\t")] for ln in open(tsv).read().splitlines()])
+    want = np.array([L.calc_impulse(output.read_snapshot2_file(f)) for f in files])
+    assert got.shape == (steps + 1, 10)
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-12)

@@ -125,3 +125,70 @@ def test_snapshot2_records(tmp_path):
     assert v.gamma == wg[0, 1, 1] and all([nd.x, nd.y, nd.z] == list(w) for nd, w in zip(v.nodes, want))
     d = output.decode_snapshot2(rec)
     np.testing.assert_array_equal(d["gammas"], np.concatenate([g.ravel(), wg.ravel()]))
+
+
+def _legacy_snapshot(rng, shapes, n_wake):
+    n_bound = sum(r * c for r, c, _, _ in shapes)
+    n = n_bound + n_wake
+    return dict(rings=rng.standard_normal((n, 4, 3)), rings0=rng.standard_normal((n, 4, 3)),
+                gammas=rng.standard_normal(n), mv_center=rng.standard_normal((n_bound, 3)),
+                mv_nodes=rng.standard_normal((n_bound, 4, 3)), mv_freestream=rng.standard_normal((n_bound, 3)))
+
+
+@pytest.mark.parametrize("with_nodes0", [True, False])
+def test_legacy_snapshot2_file(tmp_path, with_nodes0):
+    """OutputSnapshot2 (src/simulator/simulator.cpp:118-160): unframed Snapshot2 with t, shapes, the pool
+    with nodes0 and the morphing velocity records, in the C++ runtime's canonical field order."""
+    from uvlm_b200 import output
+
+    _, Snapshot2 = _classes()
+    shapes = [(2, 4, 1.0, 2.0), (2, 4, 0.5, 1.5)]
+    s = _legacy_snapshot(np.random.default_rng(11), shapes, 6)
+    r0 = s["rings0"] if with_nodes0 else None
+    path = tmp_path / "00000003"
+    output.write_legacy_snapshot2(path, 0.75, shapes, s["rings"], r0, s["gammas"], s["mv_center"], s["mv_nodes"],
+                                  s["mv_freestream"])
+    raw = open(path, "rb").read()
+    m = Snapshot2()
+    m.ParseFromString(raw)
+    assert m.SerializeToString() == raw
+    assert m.t == 0.75
+    assert [(c.rows, c.cols, c.id, c.chord, c.span) for c in m.container_shapes] == [(2, 4, 0, 1.0, 2.0),
+                                                                                     (2, 4, 1, 0.5, 1.5)]
+    assert not m.container_shapes[0].HasField("origin")
+    assert len(m.vortices) == 22 and len(m.morphing_velocities) == 16
+    v = m.vortices[19]
+    assert v.gamma == s["gammas"][19]
+    assert [[p.x, p.y, p.z] for p in v.nodes] == s["rings"][19].tolist()
+    assert [[p.x, p.y, p.z] for p in v.nodes0] == (s["rings0"][19].tolist() if with_nodes0 else [])
+    mv = m.morphing_velocities[5]
+    assert [mv.center.x, mv.center.y, mv.center.z] == s["mv_center"][5].tolist()
+    assert [[p.x, p.y, p.z] for p in mv.nodes] == s["mv_nodes"][5].tolist()
+    assert [mv.freestream.x, mv.freestream.y, mv.freestream.z] == s["mv_freestream"][5].tolist()
+    d = output.read_snapshot2_file(str(path))
+    assert d["t"] == 0.75
+    for k in ("rings", "gammas", "mv_center", "mv_nodes", "mv_freestream"):
+        np.testing.assert_array_equal(d[k], s[k])
+    if with_nodes0:
+        np.testing.assert_array_equal(d["rings0"], s["rings0"])
+    else:
+        assert d["rings0"] is None
+    assert [c["offset"] for c in output.snapshot_containers(d)] == [0, 8]
+
+
+def test_legacy_snapshot2_errors(tmp_path):
+    import uvlm_b200 as U
+    from uvlm_b200 import output
+
+    s = _legacy_snapshot(np.random.default_rng(1), [(1, 2, 1.0, 1.0)], 0)
+    with pytest.raises(ValueError):
+        output.write_legacy_snapshot2(tmp_path / "x", 0.0, [(1, 2, 1.0, 1.0)], s["rings"], s["rings0"][:1],
+                                      s["gammas"], s["mv_center"], s["mv_nodes"], s["mv_freestream"])
+    with pytest.raises(U.UVLMError):
+        output.write_legacy_snapshot2(tmp_path / "no_dir" / "x", 0.0, [(1, 2, 1.0, 1.0)], s["rings"], None,
+                                      s["gammas"], s["mv_center"], s["mv_nodes"], s["mv_freestream"])
+    # an empty snapshot (no containers, rings or records) is a valid message holding only t
+    output.write_legacy_snapshot2(tmp_path / "e", 2.5, [], np.zeros((0, 4, 3)), None, [], np.zeros((0, 3)),
+                                  np.zeros((0, 4, 3)), np.zeros((0, 3)))
+    d = output.read_snapshot2_file(str(tmp_path / "e"))
+    assert d["t"] == 2.5 and d["rings"].shape == (0, 4, 3) and d["container_shapes"] == []

@@ -39,3 +39,66 @@ def test_wakefront(tmp_path):
     t, *xs = out[0]
     assert t == 0.2
     np.testing.assert_allclose(xs, [10.0, 10.01, 10.02, 10.03])  # node 1 of ring (i, j) is p(i, j+1)
+
+
+def _snapshot_file(tmp_path):
+    from uvlm_b200 import output
+
+    rng = np.random.default_rng(3)
+    shapes = [(2, 3, 1.0, 2.0), (2, 3, 1.0, 2.0)]
+    n = 12 + 3
+    rings = np.round(rng.standard_normal((n, 4, 3)), 3) * [1.0, 1e-7, 1e7]   # exercise %g's exponent form
+    g = rng.standard_normal(n)
+    path = str(tmp_path / "00000002")
+    output.write_legacy_snapshot2(path, 0.5, shapes, rings, rings, g, rng.standard_normal((12, 3)),
+                                  rng.standard_normal((12, 4, 3)), np.tile([1.0, 0.0, 0.0], (12, 1)))
+    return path, output.read_snapshot2_file(path)
+
+
+def test_dump_circulation_text(tmp_path):
+    """dump_circulation_main.cpp:23-57: 'index i j gamma x y z ...' per ring of every container, a blank line
+    per ring row and two more per container; numbers in the C++ stream default (%g)."""
+    from uvlm_b200 import tools
+
+    path, snap = _snapshot_file(tmp_path)
+    want = []
+    for index in range(2):
+        for i in range(2):
+            for j in range(3):
+                k = 6 * index + 3 * i + j
+                vals = [snap["gammas"][k], *snap["rings"][k].ravel()]
+                want.append("%d\t%d\t%d\t" % (index, i, j) + "\t".join("%g" % v for v in vals) + "\n")
+            want.append("\n")
+        want.append("\n\n")
+    assert tools.dump_circulation(snap) == "".join(want)
+    out = str(tmp_path / "circ.dat")
+    assert tools.main(["dump_circulation", "--input", path, "--output", out]) == 0
+    text = open(out).read()
+    assert text == "".join(want) and "e-07" in text and "e+0" in text
+
+
+def test_dump_centroid_files(tmp_path, capsys):
+    """dump_centroid_main.cpp:30-122: <name>_node.dat (closed ring outlines), <name>_cent.dat (centroids) and
+    <name>_vel.dat (centroid, morphing-velocity center), and the gnuplot command on stdout."""
+    from uvlm_b200 import tools
+
+    path, snap = _snapshot_file(tmp_path)
+    d = tmp_path / "dump"
+    d.mkdir()
+    assert tools.main(["dump_centroid", "--input", path, "--output", str(d)]) == 0
+    node = open(d / "00000002_node.dat").read()
+    cent = open(d / "00000002_cent.dat").read().splitlines()
+    vel = open(d / "00000002_vel.dat").read()
+    assert node.count("\n\n\n") == 12 and len(node.split("\n\n\n")[0].splitlines()) == 5
+    first = [float(x) for x in node.splitlines()[0].split("\t")]
+    np.testing.assert_allclose(first, snap["rings"][0, 0], rtol=1e-5)
+    assert len(cent) == 12
+    c = snap["rings"][7].sum(0) / 4
+    np.testing.assert_allclose([float(x) for x in cent[7].split("\t")], c, rtol=1e-5, atol=1e-12)
+    rows = vel.rstrip("\n").splitlines()
+    assert vel.endswith("\n\n\n") and len(rows) == 12
+    np.testing.assert_allclose([float(x) for x in rows[3].split("\t")][3:], snap["mv_center"][3], rtol=1e-5)
+    assert "splot" in capsys.readouterr().out
+    # one morphing record short: no velocity rows (DumpVel returns early)
+    snap["mv_center"] = snap["mv_center"][:-1]
+    assert tools.dump_centroid(snap)[2] == ""

@@ -136,6 +136,8 @@ SIGNATURES = [
     ("uvlm_flush_output", C.c_int, [_V]),
     ("uvlm_write_state_record", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, _I, _I, _I, _I, _P, _P, _P, _P,
                                           C.c_double]),
+    ("uvlm_write_legacy_snapshot2", C.c_int, [C.c_char_p, C.c_double, _I, C.POINTER(C.c_int64),
+                                              C.POINTER(C.c_int64), _P, _P, _P, _P, _P, _I, _P, _P, _P, _I]),
     ("uvlm_rings_vortex_impulse", C.c_int, [_P, _P, _I, _P]),
     ("uvlm_rings_lamb_vector", C.c_int, [_P, _P, _P, _I, _P, _P, _P, _I, _P]),
     ("uvlm_mlp_create", C.c_int, [C.c_uint64, C.POINTER(_V)]),

@@ -720,6 +720,22 @@ int uvlm_write_state_record(const char* path, int32_t append, int32_t kind, int6
                                           wing_gamma, wake_pos, wake_gamma, t));
 }
 
+int uvlm_write_legacy_snapshot2(const char* path, double t, int64_t n_containers, const int64_t* rows,
+                                const int64_t* cols, const double* chord, const double* span, const double* rings,
+                                const double* rings0, const double* gamma, int64_t n_rings, const double* mv_center,
+                                const double* mv_nodes, const double* mv_freestream, int64_t n_mv) {
+  if (!path || n_containers < 0 || n_rings < 0 || n_mv < 0 ||
+      (n_containers > 0 && (!rows || !cols || !chord || !span)) || (n_rings > 0 && (!rings || !gamma)) ||
+      (n_mv > 0 && (!mv_center || !mv_nodes || !mv_freestream)))
+    return set_global(fail(kErrInvalid, "invalid argument"));
+  for (int64_t c = 0; c < n_containers; ++c)
+    if (rows[c] < 0 || cols[c] < 0 || rows[c] > 0xFFFFFFFFll || cols[c] > 0xFFFFFFFFll)
+      return set_global(fail(kErrInvalid, "container shape out of range"));
+  const LegacySnapshot s{n_containers, rows,  cols,  chord, span,     n_rings,      rings,
+                         rings0,       gamma, n_mv, mv_center, mv_nodes, mv_freestream};
+  return set_global(output_write_legacy_snapshot2(path, t, s));
+}
+
 const char* uvlm_last_error(const uvlm_ctx* c) { return c ? c->err.c_str() : g_last_error.c_str(); }
 
 int uvlm_add_wing(uvlm_ctx* c, const uvlm_wing_desc* w, const uvlm_kinematics* kin) {

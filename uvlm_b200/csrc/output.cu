@@ -115,6 +115,17 @@ std::string encode(int kind, const SheetRef& wing, const SheetRef& wake, double 
   return o;
 }
 
+// proto::VortexRing of the legacy pool with its reference nodes
+// (VortexRingToProto, src/proto_adaptor.h:29-40): gamma, nodes, nodes0.
+void put_pool_ring(std::string& o, int field, double gamma, const double* nodes, const double* nodes0) {
+  std::string b;
+  put_double(b, 1, gamma);
+  for (int q = 0; q < 4; ++q) put_point(b, 2, nodes + 3 * q);
+  if (nodes0)
+    for (int q = 0; q < 4; ++q) put_point(b, 3, nodes0 + 3 * q);
+  put_bytes(o, field, b);
+}
+
 bool write_record(FILE* f, const std::string& msg) {
   unsigned char len[8];
   unsigned long long n = msg.size();
@@ -132,6 +143,34 @@ Error output_encode_to_file(const char* path, int append, int kind, int num, int
   const SheetRef wing{num, rows, cols, wing_pos, wing_gamma};
   const SheetRef wake{num, wake_rows, cols, wake_pos, wake_gamma};
   const bool okw = write_record(f, encode(kind, wing, wake, t));
+  const bool okc = fclose(f) == 0;
+  return okw && okc ? ok() : fail(kErrInvalid, std::string("write failed: ") + path);
+}
+
+Error output_write_legacy_snapshot2(const char* path, double t, const LegacySnapshot& s) {
+  std::string o;
+  put_double(o, 1, t);
+  for (long long c = 0; c < s.n_containers; ++c) {  // ContainerShape {rows 1, cols 2, id 3, chord 5, span 6}
+    std::string b;
+    put_uint(b, 1, (unsigned)s.rows[c]);
+    put_uint(b, 2, (unsigned)s.cols[c]);
+    put_uint(b, 3, (unsigned)c);
+    put_double(b, 5, s.chord[c]);
+    put_double(b, 6, s.span[c]);
+    put_bytes(o, 2, b);
+  }
+  for (long long r = 0; r < s.n_rings; ++r)
+    put_pool_ring(o, 3, s.gamma[r], s.rings + 12 * r, s.rings0 ? s.rings0 + 12 * r : nullptr);
+  for (long long m = 0; m < s.n_mv; ++m) {  // MorphingVelocity {center 1, nodes 2, freestream 3}
+    std::string b;
+    put_point(b, 1, s.mv_center + 3 * m);
+    for (int q = 0; q < 4; ++q) put_point(b, 2, s.mv_nodes + 12 * m + 3 * q);
+    put_point(b, 3, s.mv_freestream + 3 * m);
+    put_bytes(o, 4, b);
+  }
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(kErrInvalid, std::string("Unable to open ") + path);
+  const bool okw = fwrite(o.data(), 1, o.size(), f) == o.size();
   const bool okc = fclose(f) == 0;
   return okw && okc ? ok() : fail(kErrInvalid, std::string("write failed: ") + path);
 }

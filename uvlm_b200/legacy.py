@@ -8,8 +8,15 @@ rings and reconnection of the newest wake row to the trailing edge
 (:82-108), the circulation solve of linear.inl (:110-116), the loads of the
 chosen formulation (:162-200), then shedding and roll-up of the wake by
 AdvectParallel (:252-266).  Each stage is one call of the C-ABI (the CUDA
-kernels); the host only moves the AoS arrays.  Per-step Snapshot2 output
-(:118-160) is not written.
+kernels); the host only moves the AoS arrays.  With `SetOutputPath(dir)`
+every step writes `dir/%08d`, one unframed Snapshot2 (OutputSnapshot2,
+:118-160): the container shapes, the whole ring pool with its reference
+nodes and, per bound ring, the morphing velocity at its reference centroid
+and at the reference midpoint of each segment, with the inlet.  With
+`SetOutputLoadPath(path)` the load rows are appended to path, tab-joined
+(CalcLoadProcess :162-200).  Containers are packed one after another; this
+is the reference's layout (container c at c x rows x cols,
+src/vortex_container.h:55) when the wings share one shape.
 
 Reference behaviour that is kept:
 
@@ -75,6 +82,8 @@ class LegacySimulator:
         self.wings: list[Wing] = []
         self.morphings: list[Morphing] = []
         self.inlet = np.array([1.0, 0.0, 0.0])
+        self.output_path = ""
+        self.output_load_path = ""
 
     def AddWing(self, wing: Wing, morphing: Morphing) -> None:  # noqa: N802 (reference name)
         """simulator::AddWing (simulator.cpp:205-209): the morphing takes the wing's origin."""
@@ -86,6 +95,15 @@ class LegacySimulator:
 
     def SetInlet(self, x: float, y: float, z: float) -> None:  # noqa: N802
         self.inlet = np.array([x, y, z], dtype=np.float64)
+
+    def SetOutputPath(self, path: str) -> None:  # noqa: N802
+        """simulator::SetOutputPath (simulator.cpp:216): the directory of the per-step Snapshot2 files
+        ("" writes none)."""
+        self.output_path = str(path)
+
+    def SetOutputLoadPath(self, path: str) -> None:  # noqa: N802
+        """simulator::SetOutputLoadPath (simulator.cpp:218): the load file ("" writes none)."""
+        self.output_load_path = str(path)
 
     # -- state -----------------------------------------------------------------
     def _create_containers(self) -> None:
@@ -100,6 +118,7 @@ class LegacySimulator:
         self.bound = self.bound0.copy()
         self.bound_gamma = np.zeros(len(self.bound))
         self.wake = np.zeros((0, 4, 3))
+        self.wake0 = np.zeros((0, 4, 3))
         self.wake_gamma = np.zeros(0)
 
     def _edge(self):
@@ -110,6 +129,37 @@ class LegacySimulator:
     def vortices(self):
         """The ring pool (bound rings, then wake rings) and its circulations."""
         return np.concatenate([self.bound, self.wake]), np.concatenate([self.bound_gamma, self.wake_gamma])
+
+    def morphing_velocities(self, t: float):
+        """The MorphingVelocity records of OutputSnapshot2 (simulator.cpp:135-152), one per bound ring:
+        Morphing::Velocity at the reference centroid (VortexRing::ReferenceCentroid, src/vortex.cpp:102-104)
+        and at (start0 + end0) / 2 of each segment in ForEachSegment order (src/vortex.h:149-160:
+        start0 = nodes0[(q + 1) % 4], end0 = nodes0[q]), and the inlet.  Returns (center (n, 3),
+        nodes (n, 4, 3), freestream (n, 3))."""
+        b0 = self.bound0
+        cent = (b0[:, 0] + b0[:, 1] + b0[:, 2] + b0[:, 3]) / 4
+        mids = (np.roll(b0, -1, axis=1) + b0) / 2
+        center = np.zeros_like(cent)
+        nodes = np.zeros_like(mids)
+        for c, m in enumerate(self.morphings):
+            a, b = self.offsets[c], self.offsets[c + 1]
+            v = m.Velocity(np.concatenate([cent[a:b], mids[a:b].reshape(-1, 3)]), t)
+            center[a:b] = v[:b - a]
+            nodes[a:b] = v[b - a:].reshape(-1, 4, 3)
+        return center, nodes, np.tile(self.inlet, (len(b0), 1))
+
+    def _output_snapshot2(self, step: int, t: float) -> None:
+        """OutputSnapshot2 (simulator.cpp:118-160) to output_path/%08d."""
+        import os
+
+        from . import output
+
+        pool, pool_g = self.vortices()
+        pool0 = np.concatenate([self.bound0, self.wake0])
+        center, nodes, fs = self.morphing_velocities(t)
+        shapes = [(r, c, w.chord, w.span) for (r, c), w in zip(self.shapes, self.wings)]
+        output.write_legacy_snapshot2(os.path.join(self.output_path, f"{step:08d}"), t, shapes, pool, pool0,
+                                      pool_g, center, nodes, fs)
 
     def _morphing_process(self, t: float) -> None:
         """MorphingProcess + ConnectProcess (simulator.cpp:82-108)."""
@@ -146,6 +196,8 @@ class LegacySimulator:
         """simulator::Start (simulator.cpp:220-270).  Returns one row per step: t, then per wing
         C_x, C_y, C_z, Pin, Pout (the load file's columns)."""
         self._create_containers()
+        if self.output_load_path:
+            open(self.output_load_path, "w").close()  # CheckReady (simulator.cpp:55-65) truncates it
         out = []
         for step in range(int(steps) + 1):
             t = dt * step
@@ -154,7 +206,12 @@ class LegacySimulator:
             self.bound_gamma = rings.SolveLinearProblemContainers(
                 self.bound, self.sizes, self.morphings, self.wake, self.wake_gamma, self.inlet, t,
                 drop_wake_term=self.drop_wake_term, bound_rings0=self.bound0)
+            if self.output_path:
+                self._output_snapshot2(step, t)
             out.append([t] + self._loads(t, dt, gamma_prev))
+            if self.output_load_path:
+                with open(self.output_load_path, "a") as f:
+                    f.write("\t".join(f"{v:g}" for v in out[-1]) + "\n")
             if step == steps:
                 break
             if not self.disable_wake:
@@ -163,5 +220,6 @@ class LegacySimulator:
                 wake_next_gamma = np.concatenate([self.bound_gamma[e], self.wake_gamma])
                 pool, pool_g = self.vortices()
                 self.wake = rings.AdvectParallel(pool, pool_g, wake_next, self.inlet, dt)
+                self.wake0 = np.concatenate([self.bound0[e], self.wake0])  # shed rings keep the edge's nodes0
                 self.wake_gamma = wake_next_gamma
         return np.array(out)

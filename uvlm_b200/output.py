@@ -7,6 +7,12 @@ cols = 4, vortices = 5}, or Snapshot2 {t = 1, ..., vortices = 3}; a
 VortexRing is {gamma = 1, nodes = 2, nodes0 = 3} and a Point {x, y, z} =
 {1, 2, 3}.  The decoder here reads those fields (others are skipped), so any
 protobuf implementation of the schema reads the same bytes.
+
+The legacy simulator (uvlm_b200.legacy) writes one unframed Snapshot2 file
+per step instead (src/simulator/simulator.cpp:118-160), with t = 1,
+container_shapes = 2 {rows, cols, id, chord = 5, span = 6}, the ring pool
+with reference nodes (nodes0 = 3) and morphing_velocities = 4 {center = 1,
+nodes = 2, freestream = 3}.
 """
 from __future__ import annotations
 
@@ -75,14 +81,16 @@ def _point(b: bytes) -> list[float]:
     return p
 
 
-def _ring(b: bytes):
-    g, nodes = 0.0, []
+def _ring(b: bytes, with_nodes0: bool = False):
+    g, nodes, nodes0 = 0.0, [], []
     for f, _, v in fields(b):
         if f == 1:
             g = v
         elif f == 2:
             nodes.append(_point(v))
-    return g, nodes
+        elif f == 3 and with_nodes0:
+            nodes0.append(_point(v))
+    return (g, nodes, nodes0) if with_nodes0 else (g, nodes)
 
 
 def decode_sheet(b: bytes) -> dict:
@@ -114,15 +122,99 @@ def decode_all_vortex_sheets(b: bytes) -> dict:
     return out
 
 
-def decode_snapshot2(b: bytes) -> dict:
-    """Snapshot2 -> {rings (n, 4, 3), gammas (n,)} (the vortices field)."""
-    rings, gammas = [], []
+def _shape(b: bytes) -> dict:
+    out = dict(rows=0, cols=0, id=0, chord=0.0, span=0.0)
     for f, _, v in fields(b):
-        if f == 3:
-            g, nodes = _ring(v)
+        if 1 <= f <= 3:
+            out[("rows", "cols", "id")[f - 1]] = v
+        elif f == 5:
+            out["chord"] = v
+        elif f == 6:
+            out["span"] = v
+    return out
+
+
+def decode_snapshot2(b: bytes) -> dict:
+    """Snapshot2 -> {t, container_shapes, rings (n, 4, 3), rings0, gammas (n,), mv_center (m, 3),
+    mv_nodes (m, 4, 3), mv_freestream (m, 3)}: container_shapes are dicts {rows, cols, id, chord, span}
+    (ContainerShape), rings0 the rings' reference nodes ((n, 4, 3), or None when the rings carry none), and
+    the mv_* arrays the MorphingVelocity records {center, nodes, freestream}."""
+    out = dict(t=0.0, container_shapes=[])
+    rings, rings0, gammas, center, mv_nodes, free = [], [], [], [], [], []
+    for f, _, v in fields(b):
+        if f == 1:
+            out["t"] = v
+        elif f == 2:
+            out["container_shapes"].append(_shape(v))
+        elif f == 3:
+            g, nodes, nodes0 = _ring(v, with_nodes0=True)
             rings.append(nodes)
+            rings0.append(nodes0)
             gammas.append(g)
-    return dict(rings=np.array(rings, dtype=np.float64).reshape(-1, 4, 3), gammas=np.array(gammas))
+        elif f == 4:
+            c, nodes, fs = [0.0] * 3, [], [0.0] * 3
+            for f2, _, v2 in fields(v):
+                if f2 == 1:
+                    c = _point(v2)
+                elif f2 == 2:
+                    nodes.append(_point(v2))
+                elif f2 == 3:
+                    fs = _point(v2)
+            center.append(c)
+            mv_nodes.append(nodes)
+            free.append(fs)
+    out["rings"] = np.array(rings, dtype=np.float64).reshape(-1, 4, 3)
+    out["gammas"] = np.array(gammas, dtype=np.float64)
+    has0 = bool(rings0) and all(len(r) == 4 for r in rings0)
+    out["rings0"] = np.array(rings0, dtype=np.float64).reshape(-1, 4, 3) if has0 else None
+    out["mv_center"] = np.array(center, dtype=np.float64).reshape(-1, 3)
+    out["mv_nodes"] = np.array(mv_nodes, dtype=np.float64).reshape(len(mv_nodes), -1, 3) if mv_nodes else \
+        np.zeros((0, 4, 3))
+    out["mv_freestream"] = np.array(free, dtype=np.float64).reshape(-1, 3)
+    return out
+
+
+def read_snapshot2_file(path: str) -> dict:
+    """One unframed Snapshot2 file of the legacy simulator (LegacySimulator.SetOutputPath)."""
+    with open(path, "rb") as f:
+        return decode_snapshot2(f.read())
+
+
+def snapshot_containers(snap: dict) -> list[dict]:
+    """The VortexContainer views of a decoded Snapshot2 (Snapshot2ToContainers, src/proto_adaptor.h:75-89):
+    each shape's dict plus `offset`, the index of its first ring in the pool, id x rows x cols
+    (VortexContainer::Offset, src/vortex_container.h:55)."""
+    return [dict(c, offset=c["id"] * c["rows"] * c["cols"]) for c in snap["container_shapes"]]
+
+
+def write_legacy_snapshot2(path: str, t: float, shapes, rings, rings0, gammas, mv_center, mv_nodes,
+                           mv_freestream) -> None:
+    """Write one legacy Snapshot2 file (uvlm_write_legacy_snapshot2): shapes = [(rows, cols, chord, span)],
+    container c gets id c; rings0 None writes no reference nodes."""
+    import ctypes as C
+
+    from ._capi import check, lib
+
+    P = C.POINTER(C.c_double)
+
+    def arr(a, shape):
+        return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+
+    n_c = len(shapes)
+    rows = (C.c_int64 * max(n_c, 1))(*[int(s[0]) for s in shapes])
+    cols = (C.c_int64 * max(n_c, 1))(*[int(s[1]) for s in shapes])
+    chord = arr([s[2] for s in shapes], -1)
+    span = arr([s[3] for s in shapes], -1)
+    r = arr(rings, (-1, 4, 3))
+    r0 = None if rings0 is None else arr(rings0, (-1, 4, 3))
+    g = arr(gammas, -1)
+    c, nd, fs = arr(mv_center, (-1, 3)), arr(mv_nodes, (-1, 4, 3)), arr(mv_freestream, (-1, 3))
+    if (r0 is not None and r0.shape != r.shape) or g.shape[0] != r.shape[0] or not (
+            c.shape[0] == nd.shape[0] == fs.shape[0]):
+        raise ValueError("inconsistent snapshot arrays")
+    p = lambda a: a.ctypes.data_as(P) if a is not None and a.size else None  # noqa: E731
+    check(lib().uvlm_write_legacy_snapshot2(str(path).encode(), float(t), n_c, rows, cols, p(chord), p(span), p(r),
+                                            p(r0), p(g), r.shape[0], p(c), p(nd), p(fs), c.shape[0]))
 
 
 def read_sheets(path: str) -> list[dict]:

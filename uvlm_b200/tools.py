@@ -8,7 +8,12 @@ They post-process the per-step records of a run (uvlm_b200.output):
   ring of a Snapshot2 on a resolution x resolution grid of a coordinate plane;
 * volume_velocity (3d_velocity_main.cpp:35-126): the same on a 3-D grid plus
   the freestream (1, 0, 0), written as a VTK structured-points file;
-* wakefront (wakefront_main.cpp:17-58): the x of the nodes of one wake row.
+* wakefront (wakefront_main.cpp:17-58): the x of the nodes of one wake row;
+* calc_impulse (src/calc_impulse_main.cpp:54-107): per legacy Snapshot2 file,
+  the vortex impulse of the first wing, its Lamb-vector term and the vortex
+  impulse of the wake (GPU reductions);
+* dump_circulation / dump_centroid (dump_circulation_main.cpp:23-57,
+  dump_centroid_main.cpp:30-122): gnuplot text of one legacy Snapshot2 file.
 
 Rings are evaluated as the reference's tools evaluate them: AoS rings with
 the nodes in the order the record stores them (ProtoToVortexRing,
@@ -19,8 +24,9 @@ p(i+1,j+1), p(i+1,j), which the AoS segment order traverses opposite to the
 simulator's VORING, so its velocities have the opposite sign of the
 simulator's own; the Snapshot2 order of the grid tools matches VORING.
 
-Command line: python -m uvlm_b200.tools {velocity_at,2d_velocity,3d_velocity,wakefront} --flag=value ...
-with the reference tools' flag names.
+Command line: python -m uvlm_b200.tools {velocity_at,2d_velocity,3d_velocity,wakefront,calc_impulse,
+dump_circulation,dump_centroid} --flag=value ... with the reference tools' flag names.  The text tables of
+the last three use the reference's number format (C++ stream default, printf %g).
 """
 from __future__ import annotations
 
@@ -113,6 +119,80 @@ def wakefront(sheet_path: str, start: int = 0, wing_id: int = 0) -> list[list[fl
     return out
 
 
+def _g(values) -> str:
+    """util::join("\t", ...) of doubles with the C++ stream default (src/util.h:67-78)."""
+    return "\t".join(f"{v:g}" for v in values)
+
+
+def _containers(snap: dict):
+    return output.snapshot_containers(snap)
+
+
+def calc_impulse(snap: dict) -> np.ndarray:
+    """CalcImpulse (calc_impulse_main.cpp:54-87) of one decoded legacy Snapshot2: [t, impulse (3),
+    other_term (3), wake_impulse (3)].  impulse sums VortexRing::Impulse over the first container,
+    wake_impulse over the rings after all containers (CountTotalSize), and other_term sums
+    CalcLambVectorOnPanel over the first container's rings with morphing record i for ring i and the
+    whole pool as the inducing rings (src/calc_impulse.h:15-30)."""
+    cs = _containers(snap)
+    if not cs:
+        raise ValueError("snapshot has no container")
+    c0 = cs[0]
+    n0 = c0["rows"] * c0["cols"]
+    sel = slice(c0["offset"], c0["offset"] + n0)
+    n_bound = sum(c["rows"] * c["cols"] for c in cs)
+    R, G = snap["rings"], snap["gammas"]
+    if sel.stop > len(R) or n0 > len(snap["mv_center"]):
+        raise ValueError("snapshot holds fewer rings or morphing records than its first container")
+    impulse = rings.CalcVortexImpulse(R[sel], G[sel])
+    wake = rings.CalcVortexImpulse(R[n_bound:], G[n_bound:])
+    other = rings.CalcLambVector(R[sel], G[sel], snap["mv_nodes"][:n0], snap["mv_freestream"][:n0], R, G)
+    return np.concatenate([[snap["t"]], impulse, other, wake])
+
+
+def glob_result(path: str) -> list[str]:
+    """GlobResult (calc_impulse_main.cpp:18-32): the sorted entries of path/*."""
+    return sorted(glob.glob(os.path.join(path, "*")))
+
+
+def dump_circulation(snap: dict) -> str:
+    """Dump (dump_circulation_main.cpp:23-57): per container, per ring (i, j) one line
+    index, i, j, gamma, the xyz of its nodes; a blank line after each ring row and two after each container."""
+    out = []
+    R, G = snap["rings"], snap["gammas"]
+    for index, c in enumerate(_containers(snap)):
+        for i in range(c["rows"]):
+            for j in range(c["cols"]):
+                k = c["offset"] + j + i * c["cols"]
+                out.append(f"{index}\t{i}\t{j}\t" + _g([G[k], *R[k].ravel()]) + "\n")
+            out.append("\n")
+        out.append("\n\n")
+    return "".join(out)
+
+
+def dump_centroid(snap: dict) -> tuple[str, str, str]:
+    """Dump (dump_centroid_main.cpp:30-100): the (node, centroid, velocity) files' text.  node: per ring
+    of every container its nodes and the first again, then two blank lines; centroid: one line per ring
+    (VortexRing::Centroid, src/vortex.cpp:98-100); velocity: centroid and morphing-velocity center per ring
+    and two blank lines, written only when there is one morphing record per container ring."""
+    node, cent, pos = [], [], []
+    R = snap["rings"]
+    for c in _containers(snap):
+        for k in range(c["offset"], c["offset"] + c["rows"] * c["cols"]):
+            r = R[k]
+            node.extend(_g(p) + "\n" for p in (r[0], r[1], r[2], r[3], r[0]))
+            node.append("\n\n")
+        for k in range(c["offset"], c["offset"] + c["rows"] * c["cols"]):
+            r = R[k]
+            x = (r[0] + r[1] + r[2] + r[3]) / 4
+            pos.append(x)
+            cent.append(_g(x) + "\n")
+    vel = ""
+    if len(pos) == len(snap["mv_center"]):
+        vel = "".join(_g(p) + "\t" + _g(v) + "\n" for p, v in zip(pos, snap["mv_center"])) + "\n\n"
+    return "".join(node), "".join(cent), vel
+
+
 def _write_table(path: str, header, rows, sep: str) -> None:
     with open(path, "w") as f:
         f.write(sep.join(header) + "\n")
@@ -122,7 +202,8 @@ def _write_table(path: str, header, rows, sep: str) -> None:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m uvlm_b200.tools")
-    ap.add_argument("tool", choices=["velocity_at", "2d_velocity", "3d_velocity", "wakefront"])
+    ap.add_argument("tool", choices=["velocity_at", "2d_velocity", "3d_velocity", "wakefront", "calc_impulse",
+                                     "dump_circulation", "dump_centroid"])
     ap.add_argument("--input", default="")
     ap.add_argument("--output", default="")
     ap.add_argument("--x", type=float, default=0.0)
@@ -174,6 +255,24 @@ def main(argv=None) -> int:
                 write_vtk(a.output, vel, **grid)
                 print(f"write {len(vel)} points", file=sys.stderr)
                 break
+    elif a.tool == "calc_impulse":
+        paths = glob_result(a.input)
+        with open(a.output, "w") as f:
+            for path in paths:
+                f.write(_g(calc_impulse(output.read_snapshot2_file(path))) + "\n")
+        print(f"{len(paths)} lines are written.", file=sys.stderr)
+    elif a.tool == "dump_circulation":
+        text = dump_circulation(output.read_snapshot2_file(a.input))
+        with open(a.output, "w") as f:
+            f.write(text)
+        print(a.output, file=sys.stderr)
+    elif a.tool == "dump_centroid":
+        name = a.input[a.input.rfind("/") + 1:]  # ResultName (dump_centroid_main.cpp:64-70)
+        paths = [f"{a.output}/{name}_{kind}.dat" for kind in ("node", "cent", "vel")]
+        for path, text in zip(paths, dump_centroid(output.read_snapshot2_file(a.input))):
+            with open(path, "w") as f:
+                f.write(text)
+        print(f"splot '{paths[1]}' w p, '{paths[0]}' w l, '{paths[2]}' usi 1:2:3:4:5:6 w vec\npause -1")
     else:
         rows = wakefront(a.input, a.start, a.id)
         with open(a.output, "w") as f:
