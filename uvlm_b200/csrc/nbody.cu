@@ -534,24 +534,45 @@ __device__ __forceinline__ void walk_far_cols2(const RecF* sm, const float4* loc
   }
 }
 
-// Local coordinates of a staged strip (its n_cols columns) relative to its
+// The far test is made for the two column halves of a strip, each against
+// its own origin: a warp whose targets are far from one half only walks that
+// half with the far-field walker and the other with the near one.  Halves
+// share the middle node column c (the left half owns its spanwise segments
+// up to c, the right half the chordwise segments of c onwards); a strip of
+// fewer than 3 node columns is one part.
+//
+// Local coordinates of the part [j0, j1] of a staged strip relative to its
 // central real node O: loc[k] = (p_k - O, 2 gS_k) for real nodes, (0, 0, 0,
-// 2 gS_k) for the zero padding (whose segments are cut by d = 0 either way).  Returns whether all
-// of this warp's targets are far from the strip (warp-uniform) and their
-// coordinates relative to O.  `red` holds one float per warp.
+// 2 gS_k) for the zero padding rows (whose segments have zero strength).
+// Returns whether all of this warp's targets are far from the part
+// (warp-uniform).  Every thread of the
+// block calls it (it synchronises); `red` holds 2 floats per warp, `slot`
+// picks this part's.
+__device__ __forceinline__ const RecF& part_origin(const RecF* sm, const StripInfo& si, int j0, int j1) {
+  return sm[((si.nr - 1) >> 1) * (kStripCols + 1) + j0 + ((j1 - j0) >> 1)];
+}
+
+// The targets relative to a part's origin O (FP32, rounded from the hi/lo differences).
+__device__ __forceinline__ void part_targets(const RecF& o, const Tgt<float> (&tg)[2], float2 (&ts)[3]) {
+  const float4 oh = o.hi, ol = o.lo;
+  ts[0] = make_float2((tg[0].hx - oh.x) + (tg[0].lx - ol.x), (tg[1].hx - oh.x) + (tg[1].lx - ol.x));
+  ts[1] = make_float2((tg[0].hy - oh.y) + (tg[0].ly - ol.y), (tg[1].hy - oh.y) + (tg[1].ly - ol.y));
+  ts[2] = make_float2((tg[0].hz - oh.z) + (tg[0].lz - ol.z), (tg[1].hz - oh.z) + (tg[1].lz - ol.z));
+}
+
 template <int H, int BLOCK>
-__device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si, float4* loc, float* red,
-                                            const Tgt<float> (&tg)[2], float2 (&ts)[3]) {
-  const int n_cols = si.n_cols;
-  const RecF& o = sm[((si.nr - 1) >> 1) * (kStripCols + 1) + ((n_cols - 1) >> 1)];
+__device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si, int j0, int j1, float4* loc,
+                                            float* red, int slot, const Tgt<float> (&tg)[2]) {
+  const int w = j1 - j0 + 1;
+  const RecF& o = part_origin(sm, si, j0, j1);
   const float4 oh = o.hi, ol = o.lo;
   float m = 0.f;
-  for (int q = threadIdx.x; q < (H + 1) * n_cols; q += BLOCK) {
-    const int r = q / n_cols, j = q - r * n_cols;
+  for (int q = threadIdx.x; q < (H + 1) * w; q += BLOCK) {
+    const int r = q / w, j = j0 + (q - r * w);
     const int k = r * (kStripCols + 1) + j;
     const float4 h = sm[k].hi, l = sm[k].lo;
     float4 L = make_float4(0.f, 0.f, 0.f, h.w + h.w);  // 2 gS (the far segment factor's form)
-    if (r < si.nr && j < si.n_cols) {
+    if (r < si.nr) {
       L.x = (h.x - oh.x) + (l.x - ol.x);
       L.y = (h.y - oh.y) + (l.y - ol.y);
       L.z = (h.z - oh.z) + (l.z - ol.z);
@@ -561,24 +582,16 @@ __device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si,
   }
 #pragma unroll
   for (int off = 16; off; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  if ((threadIdx.x & 31) == 0) red[2 * (threadIdx.x >> 5) + slot] = m;
   __syncthreads();
-  float rho2 = red[0];
+  float rho2 = red[slot];
 #pragma unroll
-  for (int w = 1; w < BLOCK / 32; ++w) rho2 = fmaxf(rho2, red[w]);
+  for (int v = 1; v < BLOCK / 32; ++v) rho2 = fmaxf(rho2, red[2 * v + slot]);
   const float lim = 2.000001f * sqrtf(rho2) + 1e-3f;
-  bool far = true;
-  float tsv[2][3];
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    tsv[q][0] = (tg[q].hx - oh.x) + (tg[q].lx - ol.x);
-    tsv[q][1] = (tg[q].hy - oh.y) + (tg[q].ly - ol.y);
-    tsv[q][2] = (tg[q].hz - oh.z) + (tg[q].lz - ol.z);
-    far = far && fmaf(tsv[q][2], tsv[q][2], fmaf(tsv[q][1], tsv[q][1], tsv[q][0] * tsv[q][0])) >= lim * lim;
-  }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) ts[c] = make_float2(tsv[0][c], tsv[1][c]);
-  return __all_sync(0xffffffffu, far);
+  float2 ts[3];
+  part_targets(o, tg, ts);
+  const float2 t2 = fma2(ts[2], ts[2], fma2(ts[1], ts[1], mul2(ts[0], ts[0])));
+  return __all_sync(0xffffffffu, t2.x >= lim * lim && t2.y >= lim * lim);
 }
 
 // Targets tile0 + threadIdx.x + q BLOCK (clamped to the last one) of the
@@ -644,11 +657,25 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
 #pragma unroll
     for (int q = 0; q < TPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = (T)0;
     if constexpr (PAD && PK == 2 && sizeof(T) == 4 && TPT == 2) {
-      float2 ts[3];
-      if (far_prepare<H, BLOCK>(cur, si, loc, red, tg, ts))
-        walk_far_cols2<H>(cur, loc, si.n_cols, si.last_h, ts, acc);
-      else
-        walk_cols2<H>(cur, si.n_cols, si.last_h, tg, acc);
+      const int n = si.n_cols;
+      const int c = n >= 3 ? n >> 1 : n - 1;  // the parts [0, c] and [c, n - 1] (the second empty if c = n - 1)
+      float4* locr = loc + (H + 1) * (kStripCols + 1);
+      const bool farl = far_prepare<H, BLOCK>(cur, si, 0, c, loc, red, 0, tg);
+      const bool farr = c < n - 1 && far_prepare<H, BLOCK>(cur, si, c, n - 1, locr, red, 1, tg);
+      // one part when the strip is not split or both halves are near, else the two halves
+      const bool one = c == n - 1 || (!farl && !farr);
+#pragma unroll 1
+      for (int p = 0; p < (one ? 1 : 2); ++p) {
+        const int j0 = p ? c : 0, nc = one ? n : (p ? n - c : c + 1);
+        const bool lh = (one || p) ? si.last_h : false;
+        if (p ? farr : farl) {
+          float2 ts[3];
+          part_targets(part_origin(cur, si, j0, j0 + nc - 1), tg, ts);
+          walk_far_cols2<H>(cur + j0, (p ? locr : loc) + j0, nc, lh, ts, acc);
+        } else {
+          walk_cols2<H>(cur + j0, nc, lh, tg, acc);
+        }
+      }
     } else if constexpr (PAD && PK == 1 && sizeof(T) == 4 && TPT == 2) {
       walk_full_strip2<H>(cur, si.last_h, tg, acc);
     } else if constexpr (PAD)
@@ -675,7 +702,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
   float4* loc = reinterpret_cast<float4*>(buf1 + (H + 1) * (kStripCols + 1));
-  float* red = reinterpret_cast<float*>(loc + (H + 1) * (kStripCols + 1));
+  float* red = reinterpret_cast<float*>(loc + 2 * (H + 1) * (kStripCols + 1));
 
   const long long tile0 = (long long)blockIdx.x * BLOCK * TPT;
   Tgt<T> tg[TPT];
@@ -783,7 +810,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBat
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
   float4* loc = reinterpret_cast<float4*>(buf1 + (H + 1) * (kStripCols + 1));
-  float* red = reinterpret_cast<float*>(loc + (H + 1) * (kStripCols + 1));
+  float* red = reinterpret_cast<float*>(loc + 2 * (H + 1) * (kStripCols + 1));
   const long long items = totals[0];
   for (long long w = blockIdx.x; w < items; w += gridDim.x) {
     const int c = plan_search(plan, n, w, [](const NBodyBatchPlan& p) { return p.item_off; });
@@ -901,11 +928,12 @@ bool use_padded(const Blocks& B) {
 }
 
 // Dynamic shared memory of a tile: two strip buffers, plus the far-field
-// walker's local coordinates and per-warp maxima (PK == 2).
+// walker's local coordinates of the two halves and two per-warp maxima
+// (PK == 2).
 template <class Rec, int H, int BLOCK, int PK>
 constexpr size_t strip_smem() {
   return 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1) +
-         (PK == 2 ? sizeof(float4) * (H + 1) * (kStripCols + 1) + sizeof(float) * (BLOCK / 32) : 0);
+         (PK == 2 ? 2 * sizeof(float4) * (H + 1) * (kStripCols + 1) + 2 * sizeof(float) * (BLOCK / 32) : 0);
 }
 
 template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, int PK = 0>
