@@ -161,6 +161,28 @@ int uvlm_begin(uvlm_ctx* ctx);
  * (simple_simulator.cpp:240-286, 307-311).  load_row (host, may be NULL)
  * receives t, CD0, CL0, CD1, CL1, ... (1 + 2*num doubles, CalcLoad :226-232). */
 int uvlm_step(uvlm_ctx* ctx, int64_t step, double dt, double* load_row);
+/* The same MainLoop one stage at a time, for callers that act between the
+ * stages (read the circulations before the loads, time a stage, ...).
+ * uvlm_step is exactly these six calls, in this order; each call returns
+ * UVLM_ERR_STATE when it is not the stage expected next, and an error in a
+ * stage abandons the step (the next call must be uvlm_stage_kinematics).
+ * uvlm_step, uvlm_set_state and uvlm_erase_oldest_wake are refused while a
+ * staged step is in progress; uvlm_get_state may be called between stages.
+ *   kinematics  Morphing of every wing, Shed(step), collocation points and
+ *               normals (simple_simulator.cpp:241-262)
+ *   assemble    CalcMatrix (:76-101)
+ *   rhs         CalcRhs (:103-124)
+ *   solve       the circulation solve (:264-268) and the per-step state
+ *               output (:270-277)
+ *   loads       CalcLoad (:195-233), when loads are computed
+ *   advect      Advect(dt) (:284), the optional erase (:307-311), and the
+ *               load row (as uvlm_step's) */
+int uvlm_stage_kinematics(uvlm_ctx* ctx, int64_t step, double dt);
+int uvlm_stage_assemble(uvlm_ctx* ctx);
+int uvlm_stage_rhs(uvlm_ctx* ctx);
+int uvlm_stage_solve(uvlm_ctx* ctx);
+int uvlm_stage_loads(uvlm_ctx* ctx);
+int uvlm_stage_advect(uvlm_ctx* ctx, double* load_row);
 /* SimpleSimulator::Run(steps, dt): begin + steps+1 MainLoops; loads (host,
  * may be NULL) receives (steps+1) rows of 1 + 2*num doubles. */
 int uvlm_run(uvlm_ctx* ctx, int64_t steps, double dt, double* loads);

@@ -333,6 +333,19 @@ class SimpleSimulator {
     detail::check(uvlm_step(h_.get(), (int64_t)step, dt, row.data()), "MainLoop", uvlm_last_error(h_.get()));
     return row;
   }
+  // The same MainLoop in its six stages (uvlm_stage_*), in this order.
+  void StageKinematics(const std::size_t step, const double dt) {
+    detail::check(uvlm_stage_kinematics(h_.get(), (int64_t)step, dt), "StageKinematics", uvlm_last_error(h_.get()));
+  }
+  void StageAssemble() { detail::check(uvlm_stage_assemble(h_.get()), "StageAssemble", uvlm_last_error(h_.get())); }
+  void StageRhs() { detail::check(uvlm_stage_rhs(h_.get()), "StageRhs", uvlm_last_error(h_.get())); }
+  void StageSolve() { detail::check(uvlm_stage_solve(h_.get()), "StageSolve", uvlm_last_error(h_.get())); }
+  void StageLoads() { detail::check(uvlm_stage_loads(h_.get()), "StageLoads", uvlm_last_error(h_.get())); }
+  std::vector<double> StageAdvect() {
+    std::vector<double> row(1 + 2 * num_);
+    detail::check(uvlm_stage_advect(h_.get(), row.data()), "StageAdvect", uvlm_last_error(h_.get()));
+    return row;
+  }
   // SimpleSimulator::Velocity (simple_simulator.h:98-100): -ff + U_bound + U_wake
   // at x for the current state.
   Vector3 Velocity(const Vector3& x) const {

@@ -34,7 +34,7 @@ def _torch_reference(net, X, T):
     loss.backward()
     grads = np.concatenate([np.concatenate([p.grad.numpy().ravel() for p in params[2 * i:2 * i + 2]])
                             for i in range(4)])
-    return grads, float(loss), (y.detach().numpy() * s)
+    return grads, float(loss.detach()), (y.detach().numpy() * s)
 
 
 def test_mlp_forward_and_gradients_match_autograd():

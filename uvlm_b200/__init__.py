@@ -235,6 +235,33 @@ class SimpleSimulator:
         check(lib().uvlm_step(self._h, int(step), float(dt), _p(row)), self._h)
         return row
 
+    # MainLoop in its six stages (uvlm_stage_*): step() is exactly these calls in this order
+    def stage_kinematics(self, step: int, dt: float) -> None:
+        """Morphing of every wing, Shed(step), collocation points and normals (simple_simulator.cpp:241-262)."""
+        check(lib().uvlm_stage_kinematics(self._h, int(step), float(dt)), self._h)
+
+    def stage_assemble(self) -> None:
+        """CalcMatrix (simple_simulator.cpp:76-101)."""
+        check(lib().uvlm_stage_assemble(self._h), self._h)
+
+    def stage_rhs(self) -> None:
+        """CalcRhs (simple_simulator.cpp:103-124)."""
+        check(lib().uvlm_stage_rhs(self._h), self._h)
+
+    def stage_solve(self) -> None:
+        """The circulation solve (simple_simulator.cpp:264-268) and the per-step state output."""
+        check(lib().uvlm_stage_solve(self._h), self._h)
+
+    def stage_loads(self) -> None:
+        """CalcLoad (simple_simulator.cpp:195-233)."""
+        check(lib().uvlm_stage_loads(self._h), self._h)
+
+    def stage_advect(self) -> np.ndarray:
+        """Advect(dt) (simple_simulator.cpp:284), the optional erase, and the step's load row."""
+        row = np.zeros(1 + 2 * self._num)
+        check(lib().uvlm_stage_advect(self._h, _p(row)), self._h)
+        return row
+
     def erase_oldest_wake(self) -> None:
         check(lib().uvlm_erase_oldest_wake(self._h), self._h)
 

@@ -98,6 +98,12 @@ SIGNATURES = [
     ("uvlm_set_advection", C.c_int, [_V, C.c_char_p]),
     ("uvlm_begin", C.c_int, [_V]),
     ("uvlm_step", C.c_int, [_V, _I, C.c_double, _P]),
+    ("uvlm_stage_kinematics", C.c_int, [_V, _I, C.c_double]),
+    ("uvlm_stage_assemble", C.c_int, [_V]),
+    ("uvlm_stage_rhs", C.c_int, [_V]),
+    ("uvlm_stage_solve", C.c_int, [_V]),
+    ("uvlm_stage_loads", C.c_int, [_V]),
+    ("uvlm_stage_advect", C.c_int, [_V, _P]),
     ("uvlm_run", C.c_int, [_V, _I, C.c_double, _P]),
     ("uvlm_erase_oldest_wake", C.c_int, [_V]),
     ("uvlm_get_sizes", C.c_int, [_V, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -141,6 +142,15 @@ struct uvlm_ctx {
   Error solve(long long step);
   Error advect(double dt);
   Error step(long long step, double dt, double* row);
+  // MainLoop in stages (uvlm_step runs all six in order)
+  Error stage_kinematics(long long step, double dt);
+  Error stage_assemble();
+  Error stage_rhs();
+  Error stage_solve();
+  Error stage_loads();
+  Error stage_advect(double* row);
+  int stage_next = 0;  // the stage a staged MainLoop expects next (0: none in progress)
+  long long stage_step = 0;
   double cur_dt = 0;
   void mark(int i) {
     if (timing) cudaEventRecord(ev[i], st);
@@ -458,8 +468,19 @@ Error uvlm_ctx::warm_features(double t) {
 }
 
 Error uvlm_ctx::step(long long step, double dt, double* row) {
+  UVLM_TRY(stage_kinematics(step, dt));
+  UVLM_TRY(stage_assemble());
+  UVLM_TRY(stage_rhs());
+  UVLM_TRY(stage_solve());
+  UVLM_TRY(stage_loads());
+  return stage_advect(row);
+}
+
+// Wing motion, shed, collocation points and normals (simple_simulator.cpp:241-262).
+Error uvlm_ctx::stage_kinematics(long long step, double dt) {
   if (!built) return fail(kErrState, "uvlm_begin has not been called");
   const double t = step * dt;
+  stage_step = step;
   cur_dt = dt;
   work_nbody = work_asm = work_lu = 0;
   nbev_n = 0;
@@ -474,6 +495,10 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   UVLM_TRY(shed(step));
   UVLM_TRY(launch_panel_geometry(d_kin, ws(), d_pos, d_pos_init, t, d_cx, d_cy, d_cz, d_normal, d_area, d_uls, st));
   mark(1);
+  return ok();
+}
+
+Error uvlm_ctx::stage_assemble() {
   // influence matrix (simple_simulator.cpp:76-101)
   // Mixed form: the matrix of the FP64 residual is assembled every step, in
   // FP64 (assembly_fp64) or by the FP32 kernel; the FP32 matrix that is
@@ -488,6 +513,10 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
   }
   work_asm = (double)N * (double)N * 4.0;
   mark(2);
+  return ok();
+}
+
+Error uvlm_ctx::stage_rhs() {
   // RHS: wake normal wash at the collocation points (:103-124)
   {
     SourceBlock blocks[2];
@@ -500,6 +529,12 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
     UVLM_TRY(launch_rhs(N, d_vx, d_vy, d_vz, d_uls, d_normal, ff, d_rhs, st));
   }
   mark(3);
+  return ok();
+}
+
+Error uvlm_ctx::stage_solve() {
+  const long long step = stage_step;
+  const double t = step * cur_dt;
   UVLM_TRY(solve(step));
   UVLM_TRY(launch_check_finite(d_gamma, N, d_flags, st));
   if (collect && step >= 2 && collect_n + N <= collect_cap) {
@@ -516,6 +551,11 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
     UVLM_TRY(output_enqueue(out, OutputState{num, R, C, PR, wake_start, wake_nodes, d_pos, d_gamma, d_wpos, d_wgamma},
                             t, st));
   mark(4);
+  return ok();
+}
+
+Error uvlm_ctx::stage_loads() {
+  const double t = stage_step * cur_dt, dt = cur_dt;
   if (cfg.compute_loads) {
     const long long lines = (long long)num * R * (2 * C + 1);
     UVLM_TRY(launch_line_prep(d_kin, ws(), d_pos, d_pos_init, t, d_tx, d_ty, d_tz, d_line_uls, st));
@@ -527,6 +567,14 @@ Error uvlm_ctx::step(long long step, double dt, double* row) {
                           d_chord_span, t, dt, d_row, st));
   }
   mark(5);
+  return ok();
+}
+
+// Advect (:284), the erase of the oldest wake row, and the end of the step:
+// the load row and the error words back to the host.
+Error uvlm_ctx::stage_advect(double* row) {
+  const long long step = stage_step;
+  const double dt = cur_dt, t = step * dt;
   UVLM_TRY(advect(dt));
   mark(6);
   if (cfg.erase_wake_after > 0 && step >= cfg.erase_wake_after && wake_nodes > 0) wake_nodes -= 1;
@@ -778,6 +826,7 @@ int uvlm_begin(uvlm_ctx* c) {
   if (!c) return set_global(fail(kErrInvalid, "NULL context"));
   if (c->wings.empty()) return c->fail_with(fail(kErrState, "call uvlm_add_wing at least once"));
   cudaSetDevice(c->cfg.device);
+  c->stage_next = 0;
   c->num = (int)c->wings.size();
   c->R = (int)c->wings[0].rows;
   c->C = (int)c->wings[0].cols;
@@ -809,8 +858,33 @@ int uvlm_begin(uvlm_ctx* c) {
 int uvlm_step(uvlm_ctx* c, int64_t step, double dt, double* row) {
   if (!c) return set_global(fail(kErrInvalid, "NULL context"));
   if (!(dt > 0)) return c->fail_with(fail(kErrInvalid, "dt must be positive"));
+  if (c->stage_next) return c->fail_with(fail(kErrState, "a staged MainLoop is in progress"));
   return c->fail_with(c->step(step, dt, row));
 }
+
+// The staged MainLoop: each call checks that it is the stage expected next;
+// an error abandons the step (the next call must be uvlm_stage_kinematics).
+static int run_stage(uvlm_ctx* c, int stage, const std::function<Error()>& fn) {
+  if (!c) return set_global(fail(kErrInvalid, "NULL context"));
+  if (c->stage_next != stage) {
+    static const char* names[] = {"uvlm_stage_kinematics", "uvlm_stage_assemble", "uvlm_stage_rhs",
+                                  "uvlm_stage_solve",      "uvlm_stage_loads",    "uvlm_stage_advect"};
+    return c->fail_with(fail(kErrState, std::string("stage out of order: expected ") + names[c->stage_next]));
+  }
+  const Error e = fn();
+  c->stage_next = e.code ? 0 : (stage + 1) % 6;
+  return c->fail_with(e);
+}
+
+int uvlm_stage_kinematics(uvlm_ctx* c, int64_t step, double dt) {
+  if (c && !(dt > 0)) return c->fail_with(fail(kErrInvalid, "dt must be positive"));
+  return run_stage(c, 0, [&] { return c->stage_kinematics(step, dt); });
+}
+int uvlm_stage_assemble(uvlm_ctx* c) { return run_stage(c, 1, [&] { return c->stage_assemble(); }); }
+int uvlm_stage_rhs(uvlm_ctx* c) { return run_stage(c, 2, [&] { return c->stage_rhs(); }); }
+int uvlm_stage_solve(uvlm_ctx* c) { return run_stage(c, 3, [&] { return c->stage_solve(); }); }
+int uvlm_stage_loads(uvlm_ctx* c) { return run_stage(c, 4, [&] { return c->stage_loads(); }); }
+int uvlm_stage_advect(uvlm_ctx* c, double* row) { return run_stage(c, 5, [&] { return c->stage_advect(row); }); }
 
 int uvlm_run(uvlm_ctx* c, int64_t steps, double dt, double* loads) {
   if (!c) return set_global(fail(kErrInvalid, "NULL context"));
@@ -826,6 +900,7 @@ int uvlm_run(uvlm_ctx* c, int64_t steps, double dt, double* loads) {
 int uvlm_erase_oldest_wake(uvlm_ctx* c) {
   if (!c) return set_global(fail(kErrInvalid, "NULL context"));
   if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));
+  if (c->stage_next) return c->fail_with(fail(kErrState, "a staged MainLoop is in progress"));
   if (c->wake_nodes > 0) c->wake_nodes -= 1;
   return UVLM_OK;
 }
@@ -874,6 +949,7 @@ int uvlm_set_state(uvlm_ctx* c, int64_t wake_rows, const double* wing_pos, const
                    const double* wing_gamma, const double* wing_gamma_prev, const double* wake_gamma) {
   if (!c) return set_global(fail(kErrInvalid, "NULL context"));
   if (!c->built) return c->fail_with(fail(kErrState, "uvlm_begin has not been called"));
+  if (c->stage_next) return c->fail_with(fail(kErrState, "a staged MainLoop is in progress"));
   if (wake_rows < 0 || wake_rows + 2 > c->PR) return c->fail_with(fail(kErrCapacity, "wake_rows exceeds capacity"));
   if (!wing_pos || !wake_pos || !wing_gamma || !wing_gamma_prev || (wake_rows > 0 && !wake_gamma))
     return c->fail_with(fail(kErrInvalid, "NULL state array"));
