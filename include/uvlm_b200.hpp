@@ -17,11 +17,15 @@
 // The element type of node sheets is UVLM_B200_VECTOR3 (default UVLM::Vec3);
 // any type of three packed doubles works, e.g. define it to Eigen::Vector3d
 // before including this header.  Errors throw UVLM::Error where the
-// reference would LOG(FATAL) / CHECK-fail.
+// reference would LOG(FATAL) / CHECK-fail; defining UVLM_B200_FATAL_ON_ERROR
+// before including it makes them print the message to stderr and abort, as
+// the reference's LOG(FATAL) does.
 #pragma once
 
 #include <array>
 #include <cstddef>
+#include <cstdio>
+#include <cstdlib>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -111,7 +115,13 @@ inline void check(int rc, const char* what, const char* detail_msg = nullptr) {
   std::string m = std::string(what) + ": " + uvlm_status_string(rc);
   const char* d = detail_msg ? detail_msg : uvlm_global_last_error();
   if (d && *d) m += std::string(" (") + d + ")";
+#ifdef UVLM_B200_FATAL_ON_ERROR
+  std::fprintf(stderr, "F uvlm_b200] Check failed: %s\n", m.c_str());
+  std::fflush(stderr);
+  std::abort();
+#else
   throw Error(rc, m);
+#endif
 }
 template <class S>
 inline const double* dptr(const S& sheet) {

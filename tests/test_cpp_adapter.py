@@ -36,3 +36,23 @@ def test_cpp_adapter_matches_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("fatal", [False, True])
+def test_cpp_adapter_error_modes(tmp_path, fatal):
+    """UVLM::Error by default; with UVLM_B200_FATAL_ON_ERROR the reference's LOG(FATAL) behaviour: the
+    message on stderr, then abort."""
+    from uvlm_b200 import _capi
+
+    lib_dir = os.path.dirname(_capi.ensure_built())
+    exe = tmp_path / "fatal_mode"
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "fatal_mode.cpp"), "-L", lib_dir, "-luvlm_b200",
+           f"-Wl,-rpath,{lib_dir}", "-o", str(exe)] + (["-DUVLM_B200_FATAL_ON_ERROR"] if fatal else [])
+    subprocess.run(cmd, check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    if fatal:
+        assert r.returncode == -6  # SIGABRT
+        assert "Check failed: WriteStateRecord: invalid argument" in r.stderr
+    else:
+        assert r.returncode == 0 and r.stdout.startswith("caught 1: WriteStateRecord: invalid argument")
