@@ -102,3 +102,24 @@ def test_dump_centroid_files(tmp_path, capsys):
     # one morphing record short: no velocity rows (DumpVel returns early)
     snap["mv_center"] = snap["mv_center"][:-1]
     assert tools.dump_centroid(snap)[2] == ""
+
+
+def test_calc_impulse_rejects_incomplete_snapshots(tmp_path):
+    """calc_impulse needs a first container whose rings and morphing records are all in the file (the
+    reference indexes them unchecked); the checks run before any GPU call."""
+    import pytest
+
+    from uvlm_b200 import output, tools
+
+    empty = str(tmp_path / "e")
+    output.write_legacy_snapshot2(empty, 0.0, [], np.zeros((0, 4, 3)), None, [], np.zeros((0, 3)),
+                                  np.zeros((0, 4, 3)), np.zeros((0, 3)))
+    with pytest.raises(ValueError, match="no container"):
+        tools.calc_impulse(output.read_snapshot2_file(empty))
+    short = str(tmp_path / "s")
+    rings = np.random.default_rng(0).standard_normal((6, 4, 3))
+    output.write_legacy_snapshot2(short, 0.0, [(2, 3, 1.0, 1.0)], rings, None, np.ones(6), np.zeros((5, 3)),
+                                  np.zeros((5, 4, 3)), np.zeros((5, 3)))
+    with pytest.raises(ValueError, match="fewer rings or morphing records"):
+        tools.calc_impulse(output.read_snapshot2_file(short))
+    assert tools.glob_result(str(tmp_path)) == [empty, short]
