@@ -661,7 +661,7 @@ namespace legacy_detail {
 // of each segment (ForEachSegment order), with the inlet.
 inline void OutputSnapshot2(State& s, std::size_t step, double t) {
   std::vector<int64_t> rows, cols;
-  std::vector<double> chord, span, rings, rings0, gamma, center, nodes, free;
+  std::vector<double> chord, span, rings, rings0, gamma, center, nodes, inlet;
   for (const auto& c : s.containers) {
     rows.push_back((int64_t)c.rows());
     cols.push_back((int64_t)c.cols());
@@ -693,7 +693,7 @@ inline void OutputSnapshot2(State& s, std::size_t step, double t) {
     for (std::size_t k = 0; k < vel.size(); ++k)
       for (int d = 0; d < 3; ++d) (k % 5 ? nodes : center).push_back(detail::c3(vel[k])[d]);
     for (std::size_t k = 0; k < vel.size() / 5; ++k)
-      for (int d = 0; d < 3; ++d) free.push_back(detail::c3(s.inlet)[d]);
+      for (int d = 0; d < 3; ++d) inlet.push_back(detail::c3(s.inlet)[d]);
   }
   char name[32];
   std::snprintf(name, sizeof name, "/%08lu", (unsigned long)step);
@@ -701,7 +701,7 @@ inline void OutputSnapshot2(State& s, std::size_t step, double t) {
   detail::check(uvlm_write_legacy_snapshot2(path.c_str(), t, (int64_t)rows.size(), rows.data(), cols.data(),
                                             chord.data(), span.data(), rings.data(), all0 ? rings0.data() : nullptr,
                                             gamma.data(), (int64_t)gamma.size(), center.data(), nodes.data(),
-                                            free.data(), (int64_t)(center.size() / 3)),
+                                            inlet.data(), (int64_t)(center.size() / 3)),
                 "OutputSnapshot2");
 }
 }  // namespace legacy_detail
