@@ -192,3 +192,44 @@ def test_legacy_snapshot2_errors(tmp_path):
                                   np.zeros((0, 4, 3)), np.zeros((0, 3)))
     d = output.read_snapshot2_file(str(tmp_path / "e"))
     assert d["t"] == 2.5 and d["rings"].shape == (0, 4, 3) and d["container_shapes"] == []
+
+
+def test_snapshot2_to_containers_kat():
+    """test/proto_adaptor_test.cpp:7-50 (Snapshot2ToContainers): two shapes {id i, rows 2, cols 1} and four
+    rings carrying only their circulations 0..3; container c holds rings 2c, 2c + 1."""
+    from uvlm_b200 import output, tools
+
+    _, Snapshot2 = _classes()
+    m = Snapshot2()
+    for i in range(2):
+        sh = m.container_shapes.add()
+        sh.id, sh.rows, sh.cols = i, 2, 1
+    for i in range(4):
+        m.vortices.add().gamma = i
+    d = output.decode_snapshot2(m.SerializeToString())
+    np.testing.assert_array_equal(d["gammas"], [0, 1, 2, 3])
+    assert d["rings"] is None
+    cs = output.snapshot_containers(d)
+    assert [(c["rows"], c["cols"], c["rows"] * c["cols"]) for c in cs] == [(2, 1, 2), (2, 1, 2)]
+    assert [d["gammas"][c["offset"] + k] for c in cs for k in range(2)] == [0, 1, 2, 3]
+    # dump_circulation prints the circulation alone for rings without nodes
+    assert tools.dump_circulation(d) == "0\t0\t0\t0\n\n0\t1\t0\t1\n\n\n\n1\t0\t0\t2\n\n1\t1\t0\t3\n\n\n\n"
+    with pytest.raises(ValueError, match="no nodes"):
+        tools.dump_centroid(d)
+
+
+def test_to_vortex_sheet_kat(tmp_path):
+    """test/proto_adaptor_test.cpp:52-79 (ToVortexSheet / FromVortexSheet): a 2 x 2 x 1 sheet set with
+    circulations at(n, i, 0) = 2n + i."""
+    from uvlm_b200 import output
+
+    pos = np.zeros((2, 3, 2, 3))
+    g = np.array([[[0.0], [1.0]], [[2.0], [3.0]]])
+    path = tmp_path / "sheet.rec"
+    _write(path, 0, False, (pos, g, np.zeros((2, 1, 2, 3)), np.zeros((2, 0, 1))), 0.0)
+    (rec,) = output.read_sheets(str(path))
+    w = rec["wing"]
+    assert (w["num"], w["rows"], w["cols"]) == (2, 2, 1)
+    np.testing.assert_array_equal(w["gammas"], [0, 1, 2, 3])
+    _, g2 = output.sheet_to_grid(w)
+    np.testing.assert_array_equal(g2, g)

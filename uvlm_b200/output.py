@@ -137,8 +137,9 @@ def _shape(b: bytes) -> dict:
 def decode_snapshot2(b: bytes) -> dict:
     """Snapshot2 -> {t, container_shapes, rings (n, 4, 3), rings0, gammas (n,), mv_center (m, 3),
     mv_nodes (m, 4, 3), mv_freestream (m, 3)}: container_shapes are dicts {rows, cols, id, chord, span}
-    (ContainerShape), rings0 the rings' reference nodes ((n, 4, 3), or None when the rings carry none), and
-    the mv_* arrays the MorphingVelocity records {center, nodes, freestream}."""
+    (ContainerShape), rings None when a ring does not carry four nodes, rings0 the rings' reference nodes
+    ((n, 4, 3), or None when the rings carry none), and the mv_* arrays the MorphingVelocity records
+    {center, nodes, freestream}."""
     out = dict(t=0.0, container_shapes=[])
     rings, rings0, gammas, center, mv_nodes, free = [], [], [], [], [], []
     for f, _, v in fields(b):
@@ -163,7 +164,8 @@ def decode_snapshot2(b: bytes) -> dict:
             center.append(c)
             mv_nodes.append(nodes)
             free.append(fs)
-    out["rings"] = np.array(rings, dtype=np.float64).reshape(-1, 4, 3)
+    # rings without four nodes (a message holding circulations only) leave no ring array
+    out["rings"] = np.array(rings, dtype=np.float64).reshape(-1, 4, 3) if all(len(r) == 4 for r in rings) else None
     out["gammas"] = np.array(gammas, dtype=np.float64)
     has0 = bool(rings0) and all(len(r) == 4 for r in rings0)
     out["rings0"] = np.array(rings0, dtype=np.float64).reshape(-1, 4, 3) if has0 else None

@@ -77,7 +77,7 @@ def plane_velocity(snapshot: dict, plane: str = "xz", rng=(-1.0, -1.0, 1.0, 1.0)
                    resolution: int = 100):
     """Points and induced velocities of every ring of a decoded Snapshot2 (CalcData, :104-123)."""
     pts = plane_points(plane, rng, at, resolution)
-    return pts, rings.InducedVelocity(pts, snapshot["rings"], snapshot["gammas"])
+    return pts, rings.InducedVelocity(pts, _rings(snapshot), snapshot["gammas"])
 
 
 def volume_points(xmin=0.0, xmax=8.0, ymin=-4.0, ymax=4.0, zmin=-4.0, zmax=4.0, resolution=100) -> np.ndarray:
@@ -90,7 +90,7 @@ def volume_points(xmin=0.0, xmax=8.0, ymin=-4.0, ymax=4.0, zmin=-4.0, zmax=4.0, 
 def volume_velocity(snapshot: dict, **grid) -> tuple[np.ndarray, np.ndarray]:
     """CalcData (3d_velocity_main.cpp:68-83): induced velocity plus the freestream (1, 0, 0)."""
     pts = volume_points(**grid)
-    return pts, rings.InducedVelocity(pts, snapshot["rings"], snapshot["gammas"]) + np.array([1.0, 0.0, 0.0])
+    return pts, rings.InducedVelocity(pts, _rings(snapshot), snapshot["gammas"]) + np.array([1.0, 0.0, 0.0])
 
 
 def write_vtk(path: str, vel: np.ndarray, xmin, xmax, ymin, ymax, zmin, zmax, resolution) -> None:
@@ -128,6 +128,12 @@ def _containers(snap: dict):
     return output.snapshot_containers(snap)
 
 
+def _rings(snap: dict) -> np.ndarray:
+    if snap["rings"] is None:
+        raise ValueError("snapshot rings carry no nodes")
+    return snap["rings"]
+
+
 def calc_impulse(snap: dict) -> np.ndarray:
     """CalcImpulse (calc_impulse_main.cpp:54-87) of one decoded legacy Snapshot2: [t, impulse (3),
     other_term (3), wake_impulse (3)].  impulse sums VortexRing::Impulse over the first container,
@@ -141,7 +147,7 @@ def calc_impulse(snap: dict) -> np.ndarray:
     n0 = c0["rows"] * c0["cols"]
     sel = slice(c0["offset"], c0["offset"] + n0)
     n_bound = sum(c["rows"] * c["cols"] for c in cs)
-    R, G = snap["rings"], snap["gammas"]
+    R, G = _rings(snap), snap["gammas"]
     if sel.stop > len(R) or n0 > len(snap["mv_center"]):
         raise ValueError("snapshot holds fewer rings or morphing records than its first container")
     impulse = rings.CalcVortexImpulse(R[sel], G[sel])
@@ -164,7 +170,8 @@ def dump_circulation(snap: dict) -> str:
         for i in range(c["rows"]):
             for j in range(c["cols"]):
                 k = c["offset"] + j + i * c["cols"]
-                out.append(f"{index}\t{i}\t{j}\t" + _g([G[k], *R[k].ravel()]) + "\n")
+                nodes = [] if R is None else R[k].ravel()   # rings without nodes: the circulation alone
+                out.append(f"{index}\t{i}\t{j}\t" + _g([G[k], *nodes]) + "\n")
             out.append("\n")
         out.append("\n\n")
     return "".join(out)
@@ -176,7 +183,7 @@ def dump_centroid(snap: dict) -> tuple[str, str, str]:
     (VortexRing::Centroid, src/vortex.cpp:98-100); velocity: centroid and morphing-velocity center per ring
     and two blank lines, written only when there is one morphing record per container ring."""
     node, cent, pos = [], [], []
-    R = snap["rings"]
+    R = _rings(snap)
     for c in _containers(snap):
         for k in range(c["offset"], c["offset"] + c["rows"] * c["cols"]):
             r = R[k]
