@@ -11,7 +11,8 @@
 //   SolveLinearProblem (ring iterators and
 //     containers), internal::CalcMorphingVelocityOnWing
 //                                                src/linear.h:95-125, src/linear.inl:78-157
-//   UVLMVortexRing                               src/uvlm_vortex_ring.h:43-130
+//   UVLMVortexRing (InitWing, PlaneSymmetry,
+//     TrailingEdgeIterators, velocity queries)   src/uvlm_vortex_ring.{h,cpp}
 //   calc_load::AerodynamicLoad, CalcUm,
 //     CalcLoadKatzPlotkin, CalcLoadJoukowski     src/calc_load/{functions,katz_plotkin,joukowski}.h
 //   proto::Point / proto::Wing (the generated
@@ -416,8 +417,58 @@ class UVLMVortexRing {
   std::vector<VortexRing>& wake_vortices() { return wake_vortices_; }
   const std::vector<VortexRing>& wake_vortices() const { return wake_vortices_; }
 
+  // InitWing (src/uvlm_vortex_ring.cpp:37-72): the half-wing lattice pos
+  // ((rows + 1) x (cols + 1) points at y >= 0, index j + i (cols + 1)) as
+  // rings p(i,j), p(i+1,j), p(i+1,j+1), p(i,j+1); each row of rings is
+  // followed by its mirror image in y (PlaneSymmetry); all nodes are shifted
+  // by the origin and saved as the reference nodes.
+  void InitWing(const std::vector<Vector3>& pos, std::size_t cols) {
+    const std::size_t cp = cols + 1;
+    cols_ = cols;
+    rows_ = pos.size() / cp - 1;
+    for (std::size_t i = 0; i < rows_; ++i) {
+      for (std::size_t j = 0; j < cols_; ++j) {
+        VortexRing v;
+        for (std::size_t idx : {j + i * cp, j + (i + 1) * cp, j + 1 + (i + 1) * cp, j + 1 + i * cp})
+          v.nodes().push_back(pos[idx]);
+        bound_vortices_.push_back(v);
+      }
+      for (std::size_t j = 0; j < cols_; ++j) {
+        bound_vortices_.emplace_back();
+        bound_vortices_.back().nodes().resize(4);
+      }
+    }
+    PlaneSymmetry();
+    for (auto& v : bound_vortices_)
+      for (auto& n : v.nodes()) n = detail::add(n, origin_);
+    for (auto& v : bound_vortices_) v.SaveReferenceNode();
+  }
+  // PlaneSymmetry (src/uvlm_vortex_ring.cpp:81-94): ring (i, cols + j) of a
+  // row is the mirror of ring (i, j) in the x-z plane, its nodes reversed.
+  void PlaneSymmetry() {
+    auto mirror = [](const Vector3& p) { return detail::v3(detail::c3(p)[0], -detail::c3(p)[1], detail::c3(p)[2]); };
+    for (std::size_t i = 0; i < rows_; ++i)
+      for (std::size_t j = 0; j < cols_; ++j) {
+        const std::size_t idx = j + i * 2 * cols_;
+        auto& to = bound_vortices_[idx + cols_].nodes();
+        const auto& from = bound_vortices_[idx].nodes();
+        for (int q = 0; q < 4; ++q) to[q] = mirror(from[3 - q]);
+      }
+  }
+  // TrailingEdgeIterators (src/uvlm_vortex_ring.h:89-94): the last row of
+  // bound rings, both halves.
+  std::pair<std::vector<VortexRing>::iterator, std::vector<VortexRing>::iterator> TrailingEdgeIterators() {
+    return {bound_vortices_.begin() + (rows_ - 1) * 2 * cols_, bound_vortices_.begin() + rows_ * 2 * cols_};
+  }
+  const Vector3& origin() const { return origin_; }
+  void set_origin(const Vector3& pos) { origin_ = pos; }
+  std::size_t rows() const { return rows_; }
+  std::size_t cols() const { return cols_; }
+
  private:
   std::vector<VortexRing> bound_vortices_, wake_vortices_;
+  std::size_t cols_ = 0, rows_ = 0;
+  Vector3 origin_ = detail::v3(0, 0, 0);
 };
 
 // ------------------------------------------------------------ calc_load

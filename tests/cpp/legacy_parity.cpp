@@ -41,7 +41,41 @@ static VortexRing square(double l, double x0, double y0) {
   return r;
 }
 
+static void uvlm_vortex_ring_checks() {
+  // uvlm_vortex_ring_test.cpp:7-85: a 5 x 10 half-wing lattice of spacing 0.1
+  const double dx = 0.1;
+  const std::size_t rows = 5, cols = 10;
+  std::vector<Vector3> pos;
+  for (std::size_t i = 0; i <= rows; i++)
+    for (std::size_t j = 0; j <= cols; j++) pos.push_back(Vector3(i * dx, j * dx, 0));
+  UVLM::UVLMVortexRing rings;
+  rings.InitWing(pos, cols);
+  const auto& v = rings.bound_vortices();
+  bool ok = v.size() == 2 * rows * cols && rings.rows() == rows && rings.cols() == cols;
+  for (std::size_t i = 0; i < rows; i++) {
+    for (std::size_t j = 0; j < cols; j++) {  // y >= 0
+      const auto& n = v[j + i * (2 * cols)].nodes();
+      ok = ok && vnear(n[0], i * dx, j * dx, 0, 0) && vnear(n[1], (i + 1) * dx, j * dx, 0, 0) &&
+           vnear(n[2], (i + 1) * dx, (j + 1) * dx, 0, 0) && vnear(n[3], i * dx, (j + 1) * dx, 0, 0);
+    }
+    for (std::size_t j = 0; j < cols; j++) {  // y <= 0
+      const auto& n = v[j + cols + i * (2 * cols)].nodes();
+      ok = ok && vnear(n[3], i * dx, -1. * j * dx, 0, 0) && vnear(n[2], (i + 1) * dx, -1. * j * dx, 0, 0) &&
+           vnear(n[1], (i + 1) * dx, -1. * (j + 1) * dx, 0, 0) && vnear(n[0], i * dx, -1. * (j + 1) * dx, 0, 0);
+    }
+  }
+  expect(ok, "UVLMVortexRing::InitWing");
+  auto te = rings.TrailingEdgeIterators();
+  std::size_t i = 0;
+  bool ok2 = true;
+  for (auto it = te.first; it != te.second; ++it, ++i)
+    ok2 = ok2 && (i < cols ? near(it->nodes()[0].y(), i * dx, 0)
+                           : near(it->nodes()[3].y(), ((int)cols - (int)i) * dx, 0));
+  expect(ok2 && i == 2 * cols, "UVLMVortexRing::TrailingEdgeIterators");
+}
+
 static void cpu_checks() {
+  uvlm_vortex_ring_checks();
   // vortex_container_test.cpp:8-60: four 2 x 3 containers, gamma = running index
   auto vortices = std::make_shared<std::vector<VortexRing>>();
   for (int val = 0; val < 24; ++val) {
