@@ -3,6 +3,7 @@
 
 #include <cooperative_groups.h>
 
+#include "device_once.h"
 #include "lu.cuh"
 
 namespace uvlm {
@@ -294,17 +295,19 @@ bool launch_panel_cluster(T* A, int n, int k0, int kb, int P, int* ipiv, int* er
   auto kern = lu_panel_cluster_kernel<T>;
   const size_t smem = sizeof(T) * ((size_t)kPanelRows * kPanelLd + 2 * kMaxClusterCtas * kLuNB + 2 * kLuNB) +
                       2 * kMaxClusterCtas * (sizeof(double) + sizeof(int));
-  static int configured = 0;
-  if (!configured) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
-      cudaGetLastError();
-      configured = -1;
-    } else {
-      configured = 1;
-    }
-  }
-  if (configured < 0) return false;
+  // kernel attributes are per device: configure once on every device
+  static PerDeviceOnce configured;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (!once_on_device(configured, dev, [&] {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+          cudaGetLastError();
+          return false;
+        }
+        return true;
+      }))
+    return false;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P);
   cfg.blockDim = dim3(kPanelRows);

@@ -1,4 +1,5 @@
 // nbody.cu -- strip-tiled Biot-Savart N-body (FP32 hi/lo and FP64 forms).
+#include "device_once.h"
 #include "nbody.cuh"
 
 namespace uvlm {
@@ -950,11 +951,18 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   else
     kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false, PK>;
   const size_t smem = strip_smem<Rec, H, BLOCK, PK>();
-  static bool attr_done[2] = {false, false};
-  if (!attr_done[pad]) {
-    UVLM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_done[pad] = true;
-  }
+  // the shared-memory limit is a per-device attribute: set it once on every
+  // device this process launches on
+  static PerDeviceOnce attr_once[2];
+  int dev = 0;
+  UVLM_CUDA_TRY(cudaGetDevice(&dev));
+  cudaError_t attr_err = cudaSuccess;
+  if (!once_on_device(attr_once[pad], dev, [&] {
+        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return attr_err == cudaSuccess;
+      }))
+    return fail(kErrCuda, std::string("nbody: the shared-memory attribute could not be set on this device") +
+                              (attr_err != cudaSuccess ? std::string(": ") + cudaGetErrorString(attr_err) : ""));
   int occ = 0;
   UVLM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, BLOCK, smem));
   if (occ < 1) occ = 1;
