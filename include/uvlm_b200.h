@@ -93,7 +93,15 @@ typedef struct {
                                factored); 0: FP32 assembly serves both */
   int32_t nbody_variant;    /* -1: autotune; else a tile variant index */
   int32_t preconditioner;   /* UVLM_PRECOND_* (mixed form, GMRES solver) */
+  int32_t nbody_fp64_stages; /* mixed form: N-body stages evaluated in FP64 instead of FP32,
+                                a mask of UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT
+                                (0: all FP32) */
 } uvlm_config;
+
+/* N-body stages of a MainLoop (uvlm_config.nbody_fp64_stages). */
+#define UVLM_STAGE_RHS 1    /* wake normal wash at the collocation points (CalcRhs) */
+#define UVLM_STAGE_LOADS 2  /* velocities at the load-line midpoints (CalcLoad) */
+#define UVLM_STAGE_ADVECT 4 /* velocities at the wake nodes (Advect) */
 
 /* Closed-form kinematics of one wing (Morphing, src/morphing.h:70-92, with the
  * std::function arguments replaced by sinusoids):
@@ -150,6 +158,16 @@ const char* uvlm_status_string(int status);
 /* SimpleSimulator::AddWing (simple_simulator.cpp:126-140): all wings must
  * share rows and cols, cols even. */
 int uvlm_add_wing(uvlm_ctx* ctx, const uvlm_wing_desc* wing, const uvlm_kinematics* kin);
+/* SimpleSimulator::AddWing with any wing::WingGenerator
+ * (simple_simulator.h:50-53, simple_simulator.cpp:126-169): nodes is the
+ * whole-wing lattice the generator and WholeWing produce ((rows + 1) x
+ * (cols + 1) points of 3 doubles, [i][j][xyz], relative to the wing origin;
+ * e.g. the NACA 4-digit camber lattice of src/wing/naca4digit.cpp:29-39).
+ * The context adds `origin` to every node and sets the morphing origin to
+ * it, as BuildWing does.  chord and span scale the load coefficients
+ * (CalcLoad :227-229).  All wings share rows and cols. */
+int uvlm_add_wing_nodes(uvlm_ctx* ctx, int64_t rows, int64_t cols, const double* nodes, double chord, double span,
+                        const double origin[3], const uvlm_kinematics* kin);
 /* SimpleSimulator::set_forward_flight (simple_simulator.h:57). */
 int uvlm_set_forward_flight(uvlm_ctx* ctx, const double ff[3]);
 /* SimpleSimulator::set_advection + AdvectFactory(name). */
@@ -237,14 +255,15 @@ int uvlm_sheet_induced_velocity(const double* pos, const double* gamma, int64_t 
 
 /* No counterpart in the reference.  The same velocities as
  * uvlm_sheet_induced_velocity for callers that cannot allocate device memory
- * (inside a stream capture, in loops where cudaMalloc/cudaFree would
- * synchronise the device, or under a host framework that owns the device
- * memory budget).  pos, gamma, targets and out are DEVICE pointers owned by the
- * caller; nothing is allocated.  All scratch lives in one 32 MiB device array
- * inside the library (held by every GPU that loads it until exit); a request
- * that needs more returns UVLM_ERR_CAPACITY.  The first call on a device looks
- * up that array's address, so make it before any stream capture.  Work is
- * queued on `stream` (a cudaStream_t, NULL = legacy default stream) and is not
+ * (loops where cudaMalloc/cudaFree would synchronise the device, or a host
+ * framework that owns the device memory budget).  pos, gamma, targets and out
+ * are DEVICE pointers owned by the caller; nothing is allocated.  An empty
+ * sheet set (num, grows or gcols 0; pos and gamma may then be NULL) gives
+ * zero velocities.  All scratch lives in one 32 MiB device array inside the
+ * library (held by every GPU that loads it until exit); a request that needs
+ * more returns UVLM_ERR_CAPACITY.  The first call on a device looks up that
+ * array's address, so make it before any stream capture.  Work is queued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and is not
  * synchronised.  Calls share the array: calls that overlap on the GPU race. */
 int uvlm_sheet_induced_velocity_noalloc(const double* pos, const double* gamma, int64_t num, int64_t grows,
                                         int64_t gcols, const double* targets, int64_t n_targets, double* out,

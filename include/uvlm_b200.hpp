@@ -8,7 +8,8 @@
 //     RungeKutta4 / AdamsBashforth2, AdvectFactory   src/advect.h:48-121,
 //                                                    src/advect_factory.cpp:43-60
 //   UVLM::Morphing (closed-form sinusoid setters)    src/morphing.h:25-108
-//   UVLM::wing::RectGenerator                        src/wing/rect.h:10-30
+//   UVLM::wing::{WingGenerator, RectGenerator, NACA4digitGenerator,
+//     NACA00XXGenerator, WholeWing}, proto::Wing     src/wing/*, proto/uvlm.proto:6-30
 //   UVLM::simulator::SimpleSimulator                 src/simulator/simple_simulator.h:33-108
 //   multiple_sheet::MultipleSheet<T> (layout of the missing submodule,
 //     contiguous [num][rows][cols])
@@ -23,7 +24,10 @@
 #pragma once
 
 #include <array>
+#include <cmath>
+#include <typeinfo>
 #include <cstddef>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
@@ -269,12 +273,211 @@ inline std::unique_ptr<Advection> AdvectFactory(const std::string& name) {
 
 }  // namespace advect
 
+// ---------------------------------------------------------------- proto
+// The subset of the generated proto::Point / proto::Wing accessors that the
+// wing generators and the legacy code use (proto/uvlm.proto:6-30).
+namespace proto {
+struct Point {
+  double x_ = 0, y_ = 0, z_ = 0;
+  double x() const { return x_; }
+  double y() const { return y_; }
+  double z() const { return z_; }
+  void set_x(double v) { x_ = v; }
+  void set_y(double v) { y_ = v; }
+  void set_z(double v) { z_ = v; }
+};
+class Wing {
+ public:
+  std::uint64_t rows() const { return rows_; }
+  std::uint64_t cols() const { return cols_; }
+  void set_rows(std::uint64_t v) { rows_ = v; }
+  void set_cols(std::uint64_t v) { cols_ = v; }
+  double chord() const { return chord_; }
+  double span() const { return span_; }
+  void set_chord(double v) { chord_ = v; }
+  void set_span(double v) { span_ = v; }
+  Point* add_points() {
+    points_.emplace_back();
+    return &points_.back();
+  }
+  const std::vector<Point>& points() const { return points_; }
+  int points_size() const { return (int)points_.size(); }
+  const Point& points(int i) const { return points_[(std::size_t)i]; }
+  Point* mutable_points(int i) { return &points_[(std::size_t)i]; }
+  bool has_origin() const { return has_origin_; }
+  const Point& origin() const { return origin_; }
+  Point* mutable_origin() {
+    has_origin_ = true;
+    return &origin_;
+  }
+  void CopyFrom(const Wing& w) { *this = w; }
+  void Clear() { *this = Wing(); }
+
+ private:
+  std::uint64_t rows_ = 0, cols_ = 0;
+  double chord_ = 0, span_ = 0;
+  std::vector<Point> points_;
+  Point origin_;
+  bool has_origin_ = false;
+};
+}  // namespace proto
+
 namespace wing {
-// RectGenerator (src/wing/rect.h:10-30); Chebyshev spacing as
+
+// WingGenerator (src/wing/wing_generator.h:12-32): fills a half wing's
+// lattice; SimpleSimulator::AddWing takes ownership of any generator.
+class WingGenerator {
+ public:
+  WingGenerator() = default;
+  virtual ~WingGenerator() = default;
+  virtual void Generate(proto::Wing* wing, const double chord, const double span, const std::size_t rows,
+                        const std::size_t cols) const {
+    wing->Clear();
+    wing->set_chord(chord);
+    wing->set_span(span);
+    wing->set_cols(cols);
+    wing->set_rows(rows);
+  }
+  void operator()(proto::Wing* wing, const double chord, const double span, const std::size_t rows,
+                  const std::size_t cols) const {
+    this->Generate(wing, chord, span, rows, cols);
+  }
+};
+
+// linspace (src/util.h:36-43).
+inline std::vector<double> linspace(double a, double b, std::size_t N) {
+  const double dx = (b - a) / (N - 1);
+  std::vector<double> res;
+  for (std::size_t i = 0; i < N; i++) res.push_back(a + i * dx);
+  return res;
+}
+
 // TransformChebyshev (src/wing/rect.h:16-25).
-struct RectGenerator {
+inline void TransformChebyshev(std::vector<double>* res, std::size_t N, double xmin, double xmax) {
+  const auto theta = linspace(-M_PI_2, 0, N);
+  res->clear();
+  for (double t : theta) res->push_back(xmin + (xmax - xmin) * std::cos(t));
+  res->front() = xmin;
+  res->back() = xmax;
+}
+
+// RectGenerator (src/wing/rect.{h,cpp}): flat lattice, linspace or Chebyshev
+// spacing (the reference's --chebyshev_chord / --chebyshev_span flags are the
+// two members).  AddWing builds a plain RectGenerator wing inside the library.
+class RectGenerator : public WingGenerator {
+ public:
+  RectGenerator(bool cheb_chord = false, bool cheb_span = false)
+      : chebyshev_chord(cheb_chord), chebyshev_span(cheb_span) {}
+  void Generate(proto::Wing* wing, const double chord, const double span, const std::size_t rows,
+                const std::size_t cols) const override {
+    WingGenerator::Generate(wing, chord, span, rows, cols);
+    std::vector<double> xs, ys;
+    if (chebyshev_chord)
+      TransformChebyshev(&xs, rows + 1, 0, chord);
+    else
+      xs = linspace(0, chord, rows + 1);
+    if (chebyshev_span)
+      TransformChebyshev(&ys, cols + 1, 0, span);
+    else
+      ys = linspace(0, span, cols + 1);
+    for (const double x : xs)
+      for (const double y : ys) {
+        auto* p = wing->add_points();
+        p->set_x(x);
+        p->set_y(y);
+        p->set_z(0);
+      }
+  }
   bool chebyshev_chord = false, chebyshev_span = false;
 };
+
+// NACA4digit / NACA4digitGenerator (src/wing/naca4digit.{h,cpp}): mean camber
+// line of a 4-digit section (first digit: camber in %, second: its position
+// in tenths of the chord) on the rectangular lattice.
+inline double NACA4digit(double x, double c, int xx) {
+  const int first = xx / 10, second = xx % 10;
+  const double m = first / 100.0, p = second / 10.0;
+  double res = 0;
+  if (0 <= x && x <= p * c)
+    res = m * x / p / p * (2 * p - x / c);
+  else if (p * c <= x && x <= c)
+    res = m * (c - x) / (1 - p) / (1 - p) * (1 + x / c - 2 * p);
+  return res;
+}
+class NACA4digitGenerator : public RectGenerator {
+ public:
+  explicit NACA4digitGenerator(int digit) : RectGenerator(), digit_(digit) {}
+  void Generate(proto::Wing* wing, const double chord, const double span, const std::size_t rows,
+                const std::size_t cols) const override {
+    RectGenerator::Generate(wing, chord, span, rows, cols);
+    for (int i = 0; i < wing->points_size(); i++) {
+      auto* p = wing->mutable_points(i);
+      p->set_z(NACA4digit(p->x(), chord, digit_));
+    }
+  }
+  void set_verbose(bool) {}
+
+ private:
+  int digit_;
+};
+
+// NACA00XX / NACA00XXGenerator (src/wing/naca00XX.{h,cpp}): half thickness of
+// a symmetric 4-digit section on the rectangular lattice.
+inline double NACA00XX(double x, double c, int xx) {
+  const double t = xx * 0.01;
+  const double z = x / c;
+  return 5 * t * c *
+         (0.2969 * std::sqrt(z) + (-0.1260) * (z) + (-0.3516) * z * z + 0.2843 * z * z * z +
+          (-0.1015) * z * z * z * z);
+}
+class NACA00XXGenerator : public RectGenerator {
+ public:
+  explicit NACA00XXGenerator(int digit) : RectGenerator(), digit_(digit) {}
+  void Generate(proto::Wing* wing, const double chord, const double span, const std::size_t rows,
+                const std::size_t cols) const override {
+    RectGenerator::Generate(wing, chord, span, rows, cols);
+    for (int i = 0; i < wing->points_size(); i++) {
+      auto* p = wing->mutable_points(i);
+      p->set_z(NACA00XX(p->x(), chord, digit_));
+    }
+  }
+  void set_verbose(bool) {}
+
+ private:
+  int digit_;
+};
+
+// WholeWing (src/wing/wing.cpp:12-52): per node row, the mirror image (y ->
+// -y) of the half row in reverse order, then the half row without its first
+// point; finally + the half's origin.
+inline void WholeWing(proto::Wing* wing, const proto::Wing& half) {
+  wing->Clear();
+  wing->set_cols(half.cols() * 2);
+  wing->set_rows(half.rows());
+  *wing->mutable_origin() = half.origin();
+  wing->set_chord(half.chord());
+  wing->set_span(half.span());
+  const std::size_t COLS = half.cols() + 1;
+  const std::size_t ROWS = half.points().size() / COLS;
+  const proto::Point& o = half.origin();
+  auto put = [&](double x, double y, double z) {
+    auto* p = wing->add_points();
+    p->set_x(x + o.x());
+    p->set_y(y + o.y());
+    p->set_z(z + o.z());
+  };
+  for (std::size_t i = 0; i < ROWS; ++i) {
+    for (std::size_t q = COLS; q-- > 0;) {
+      const proto::Point& p = half.points()[i * COLS + q];
+      put(p.x(), p.y() * -1, p.z());
+    }
+    for (std::size_t q = 1; q < COLS; ++q) {
+      const proto::Point& p = half.points()[i * COLS + q];
+      put(p.x(), p.y(), p.z());
+    }
+  }
+}
+
 }  // namespace wing
 
 namespace simulator {
@@ -294,6 +497,35 @@ class SimpleSimulator {
     h_.reset(h);
   }
 
+  // AddWing (simple_simulator.cpp:126-140) with any wing::WingGenerator, as
+  // the reference's (it takes ownership of the generator): BuildWing's
+  // lattice (:155-166) is the generator's half wing (chord, span/2, rows,
+  // cols/2) through WholeWing, moved to `origin` by the library.
+  void AddWing(wing::WingGenerator* generator, const Morphing& morphing, const double chord, const double span,
+               const std::size_t rows, const std::size_t cols, const Vector3& origin) {
+    std::unique_ptr<wing::WingGenerator> gen(generator);
+    if (!gen) detail::check(UVLM_ERR_INVALID, "AddWing", "NULL wing generator");
+    if (cols & 1) detail::check(UVLM_ERR_INVALID, "AddWing", "columns must be even.");
+    if (auto* rect = dynamic_cast<wing::RectGenerator*>(gen.get()); rect && typeid(*gen) == typeid(wing::RectGenerator)) {
+      AddWing(*rect, morphing, chord, span, rows, cols, origin);
+      return;
+    }
+    proto::Wing half, whole;
+    gen->Generate(&half, chord, span / 2, rows, cols / 2);
+    wing::WholeWing(&whole, half);
+    std::vector<double> nodes;
+    nodes.reserve(whole.points().size() * 3);
+    for (const auto& p : whole.points()) {
+      nodes.push_back(p.x());
+      nodes.push_back(p.y());
+      nodes.push_back(p.z());
+    }
+    const double* o = reinterpret_cast<const double*>(&origin);
+    num_ += 1;
+    detail::check(uvlm_add_wing_nodes(h_.get(), (int64_t)rows, (int64_t)cols, nodes.data(), chord, span, o,
+                                      &morphing.kinematics()),
+                  "AddWing", uvlm_last_error(h_.get()));
+  }
   void AddWing(const wing::RectGenerator& gen, const Morphing& morphing, const double chord, const double span,
                const std::size_t rows, const std::size_t cols, const Vector3& origin) {
     uvlm_wing_desc w{};

@@ -15,8 +15,6 @@
 //     TrailingEdgeIterators, velocity queries)   src/uvlm_vortex_ring.{h,cpp}
 //   calc_load::AerodynamicLoad, CalcUm,
 //     CalcLoadKatzPlotkin, CalcLoadJoukowski     src/calc_load/{functions,katz_plotkin,joukowski}.h
-//   proto::Point / proto::Wing (the generated
-//     accessors the legacy code uses)            proto/uvlm.proto:6-30
 //   internal::TransformRow, WingBuilder          src/wing_builder.{h,cpp}
 //   simulator::{InitSimulator, AddWing, SetInlet,
 //     SetOutputPath, SetOutputLoadPath, Start}   src/simulator/simulator.{h,cpp}
@@ -529,51 +527,7 @@ inline AerodynamicLoad CalcLoadJoukowski(const VortexContainer& vb, const Vortex
 
 }  // namespace calc_load
 
-// ---------------------------------------------------------------- proto
-// The subset of the generated proto::Point / proto::Wing accessors the
-// legacy code uses (proto/uvlm.proto:6-30).
-namespace proto {
-struct Point {
-  double x_ = 0, y_ = 0, z_ = 0;
-  double x() const { return x_; }
-  double y() const { return y_; }
-  double z() const { return z_; }
-  void set_x(double v) { x_ = v; }
-  void set_y(double v) { y_ = v; }
-  void set_z(double v) { z_ = v; }
-};
-class Wing {
- public:
-  std::uint64_t rows() const { return rows_; }
-  std::uint64_t cols() const { return cols_; }
-  void set_rows(std::uint64_t v) { rows_ = v; }
-  void set_cols(std::uint64_t v) { cols_ = v; }
-  double chord() const { return chord_; }
-  double span() const { return span_; }
-  void set_chord(double v) { chord_ = v; }
-  void set_span(double v) { span_ = v; }
-  Point* add_points() {
-    points_.emplace_back();
-    return &points_.back();
-  }
-  const std::vector<Point>& points() const { return points_; }
-  bool has_origin() const { return has_origin_; }
-  const Point& origin() const { return origin_; }
-  Point* mutable_origin() {
-    has_origin_ = true;
-    return &origin_;
-  }
-  void CopyFrom(const Wing& w) { *this = w; }
-  void Clear() { *this = Wing(); }
-
- private:
-  std::uint64_t rows_ = 0, cols_ = 0;
-  double chord_ = 0, span_ = 0;
-  std::vector<Point> points_;
-  Point origin_;
-  bool has_origin_ = false;
-};
-}  // namespace proto
+// proto::Point / proto::Wing are declared in uvlm_b200.hpp (shared with the wing generators).
 
 inline Vector3 PointToVector3d(const proto::Point& p) { return Vector3(p.x(), p.y(), p.z()); }
 

@@ -109,6 +109,16 @@ def _declare(L):
     L.orc_sim_get_state.argtypes = [C.c_void_p, _P, _P, _P, _P, _P, _P]
     L.orc_sim_set_state.argtypes = [C.c_void_p, _I, _P, _P, _P, _P, _P]
     L.orc_sim_time_step_sampled.argtypes = [C.c_void_p, _I, C.c_double, _I, _I, _P]
+    L.orc_sim_add_wing_generator.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, _I, _I, _P,
+                                             C.POINTER(Kinematics), C.c_int, C.c_int]
+    L.orc_naca4digit.argtypes = [C.c_double, C.c_double, C.c_int]
+    L.orc_naca4digit.restype = C.c_double
+    L.orc_naca00xx.argtypes = [C.c_double, C.c_double, C.c_int]
+    L.orc_naca00xx.restype = C.c_double
+    L.orc_generate_wing.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _I, _I, C.c_int, C.c_int, _P]
+    L.orc_sim_set_lu_threads.argtypes = [C.c_void_p, C.c_int]
+    L.orc_sim_sliced_begin.argtypes = [C.c_void_p, _I, C.c_double, _I, C.c_int]
+    L.orc_sim_sliced_run.argtypes = [C.c_void_p, _I, _P]
 
 
 def _p(a):
@@ -300,6 +310,36 @@ class Simulator:
             raise ValueError(f"AddWing rejected the wing (code {rc})")
         self.num += 1
 
+    def add_wing_generator(self, generator, digit, chord, span, rows, cols, origin=(0, 0, 0), kin=None,
+                           cheb_chord=False, cheb_span=False):
+        """AddWing with a NACA4digitGenerator(digit) ("naca4digit"), NACA00XXGenerator(digit) ("naca00xx") or
+        RectGenerator ("rect") (simple_simulator.cpp:126-169)."""
+        kin = kin if kin is not None else Kinematics()
+        g = {"rect": 0, "naca4digit": 1, "naca00xx": 2}[generator]
+        rc = lib().orc_sim_add_wing_generator(self._h, g, int(digit), float(chord), float(span), int(rows),
+                                              int(cols), _p(_v(origin)), C.byref(kin), int(cheb_chord),
+                                              int(cheb_span))
+        if rc:
+            raise ValueError(f"AddWing rejected the wing (code {rc})")
+        self.num += 1
+
+    def set_lu_threads(self, n):
+        """Threads of the FullPivLU elimination (bit-identical for any count; 1 = Eigen's)."""
+        lib().orc_sim_set_lu_threads(self._h, int(n))
+
+    def sliced_begin(self, step, dt, slices, threads):
+        """Plans MainLoop(step, dt) as `slices` consecutive slices of about equal estimated time."""
+        rc = lib().orc_sim_sliced_begin(self._h, int(step), float(dt), int(slices), int(threads))
+        if rc:
+            raise RuntimeError(f"sliced_begin failed ({rc})")
+
+    def sliced_run(self, slice_index, row=None):
+        """Runs one slice; all slices in order perform exactly step(step, dt).  `row` (1 + 2 num doubles)
+        receives the load row when the slice finishes the loads."""
+        rc = lib().orc_sim_sliced_run(self._h, int(slice_index), _p(row))
+        if rc:
+            raise RuntimeError(f"sliced_run failed ({rc})")
+
     def set_forward_flight(self, ff):
         lib().orc_sim_set_forward_flight(self._h, _p(_v(ff)))
 
@@ -361,6 +401,25 @@ class Simulator:
         if rc:
             raise RuntimeError("time_step_sampled failed")
         return sec
+
+
+def naca4digit(x, c, xx):
+    """Mean camber of a 4-digit NACA section (src/wing/naca4digit.cpp:12-27)."""
+    return lib().orc_naca4digit(float(x), float(c), int(xx))
+
+
+def naca00xx(x, c, xx):
+    """Half thickness of a symmetric 4-digit NACA section (src/wing/naca00XX.cpp:14-19)."""
+    return lib().orc_naca00xx(float(x), float(c), int(xx))
+
+
+def generate_wing(generator, digit, chord, span, rows, cols, cheb_chord=False, cheb_span=False):
+    """WingGenerator::Generate points of "rect", "naca4digit" or "naca00xx": (rows+1, cols+1, 3)."""
+    g = {"rect": 0, "naca4digit": 1, "naca00xx": 2}[generator]
+    out = np.zeros((rows + 1, cols + 1, 3))
+    lib().orc_generate_wing(g, int(digit), float(chord), float(span), int(rows), int(cols), int(cheb_chord),
+                            int(cheb_span), _p(out))
+    return out
 
 
 def vortex_impulse(rings, gammas):

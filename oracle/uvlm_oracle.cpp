@@ -270,58 +270,124 @@ struct Morphing {
 // ------------------------------------------------------------ dense solve
 // Complete-pivoting LU with the semantics of Eigen::FullPivLU<MatrixXd>:
 // P A Q = L U, pivot = largest |a_ij| of the trailing block, solve through
-// L, U and the two permutations.  Row-major storage.
-int FullPivLUSolve(std::vector<double>& A, size_t n, const std::vector<double>& b,
-                   std::vector<double>& x) {
-  std::vector<size_t> rp(n), cp(n);
-  for (size_t i = 0; i < n; i++) rp[i] = cp[i] = i;
-  int singular = 0;
-  for (size_t k = 0; k < n; k++) {
+// L, U and the two permutations.  Row-major storage.  The elimination is
+// resumable one column at a time (Step), so that a timed run can be cut into
+// slices.  threads > 1 splits the pivot search (each thread keeps the first
+// maximum of its row block in row-major order; blocks are merged in order, so
+// the pivot is the serial one) and the row updates (independent per row):
+// the result is bit-identical to the single-threaded elimination, which is
+// the default because Eigen's FullPivLU is single-threaded.
+struct FullPivLU {
+  std::vector<double>* A = nullptr;
+  size_t n = 0;
+  std::vector<size_t> rp, cp;
+  int threads = 1;
+  bool singular = false;
+
+  void Init(std::vector<double>& a, size_t nn, int th = 1) {
+    A = &a;
+    n = nn;
+    threads = th;
+    singular = false;
+    rp.resize(n);
+    cp.resize(n);
+    for (size_t i = 0; i < n; i++) rp[i] = cp[i] = i;
+  }
+
+  // Elimination of column k; false once the trailing block is zero.
+  bool Step(size_t k) {
+    if (singular) return false;
+    std::vector<double>& M = *A;
     size_t pi = k, pj = k;
     double best = -1;
-    for (size_t i = k; i < n; i++) {
-      const double* row = &A[i * n];
-      for (size_t j = k; j < n; j++) {
-        const double a = std::fabs(row[j]);
-        if (a > best) { best = a; pi = i; pj = j; }
+    auto search = [&](size_t i0, size_t i1, double& b, size_t& bi, size_t& bj) {
+      for (size_t i = i0; i < i1; i++) {
+        const double* row = &M[i * n];
+        for (size_t j = k; j < n; j++) {
+          const double a = std::fabs(row[j]);
+          if (a > b) { b = a; bi = i; bj = j; }
+        }
       }
+    };
+#ifdef _OPENMP
+    if (threads > 1 && n - k >= 64) {
+      const int T = threads;
+      std::vector<double> tb(T, -1);
+      std::vector<size_t> ti(T, k), tj(T, k);
+#pragma omp parallel num_threads(T)
+      {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const size_t rows = n - k;
+        search(k + rows * t / nt, k + rows * (t + 1) / nt, tb[t], ti[t], tj[t]);
+      }
+      for (int t = 0; t < T; t++)
+        if (tb[t] > best) { best = tb[t]; pi = ti[t]; pj = tj[t]; }
+    } else {
+      search(k, n, best, pi, pj);
     }
-    if (best == 0) { singular = 1; break; }
+#else
+    search(k, n, best, pi, pj);
+#endif
+    if (best == 0) { singular = true; return false; }
     if (pi != k) {
-      for (size_t j = 0; j < n; j++) std::swap(A[k * n + j], A[pi * n + j]);
+      for (size_t j = 0; j < n; j++) std::swap(M[k * n + j], M[pi * n + j]);
       std::swap(rp[k], rp[pi]);
     }
     if (pj != k) {
-      for (size_t i = 0; i < n; i++) std::swap(A[i * n + k], A[i * n + pj]);
+      for (size_t i = 0; i < n; i++) std::swap(M[i * n + k], M[i * n + pj]);
       std::swap(cp[k], cp[pj]);
     }
-    const double piv = A[k * n + k];
-    const double* rowk = &A[k * n];
-    for (size_t i = k + 1; i < n; i++) {
-      double* rowi = &A[i * n];
+    const double piv = M[k * n + k];
+    const double* rowk = &M[k * n];
+    auto update = [&](size_t i) {
+      double* rowi = &M[i * n];
       const double l = rowi[k] / piv;
       rowi[k] = l;
       if (l != 0)
         for (size_t j = k + 1; j < n; j++) rowi[j] -= l * rowk[j];
+    };
+#ifdef _OPENMP
+    if (threads > 1 && n - k >= 64) {
+#pragma omp parallel for num_threads(threads) schedule(static)
+      for (long long i = (long long)k + 1; i < (long long)n; i++) update((size_t)i);
+    } else {
+      for (size_t i = k + 1; i < n; i++) update(i);
     }
+#else
+    for (size_t i = k + 1; i < n; i++) update(i);
+#endif
+    return true;
   }
-  if (singular) return 1;
-  std::vector<double> y(n);
-  for (size_t i = 0; i < n; i++) y[i] = b[rp[i]];
-  for (size_t i = 0; i < n; i++) {
-    double s = y[i];
-    const double* row = &A[i * n];
-    for (size_t j = 0; j < i; j++) s -= row[j] * y[j];
-    y[i] = s;
+
+  void Solve(const std::vector<double>& b, std::vector<double>& x) const {
+    const std::vector<double>& M = *A;
+    std::vector<double> y(n);
+    for (size_t i = 0; i < n; i++) y[i] = b[rp[i]];
+    for (size_t i = 0; i < n; i++) {
+      double s = y[i];
+      const double* row = &M[i * n];
+      for (size_t j = 0; j < i; j++) s -= row[j] * y[j];
+      y[i] = s;
+    }
+    for (size_t ii = n; ii-- > 0;) {
+      double s = y[ii];
+      const double* row = &M[ii * n];
+      for (size_t j = ii + 1; j < n; j++) s -= row[j] * y[j];
+      y[ii] = s / row[ii];
+    }
+    x.assign(n, 0);
+    for (size_t i = 0; i < n; i++) x[cp[i]] = y[i];
   }
-  for (size_t ii = n; ii-- > 0;) {
-    double s = y[ii];
-    const double* row = &A[ii * n];
-    for (size_t j = ii + 1; j < n; j++) s -= row[j] * y[j];
-    y[ii] = s / row[ii];
-  }
-  x.assign(n, 0);
-  for (size_t i = 0; i < n; i++) x[cp[i]] = y[i];
+};
+
+int FullPivLUSolve(std::vector<double>& A, size_t n, const std::vector<double>& b, std::vector<double>& x,
+                   int threads = 1) {
+  FullPivLU lu;
+  lu.Init(A, n, threads);
+  for (size_t k = 0; k < n; k++)
+    if (!lu.Step(k)) break;
+  if (lu.singular) return 1;
+  lu.Solve(b, x);
   return 0;
 }
 
@@ -491,12 +557,14 @@ std::vector<double> CalcPanelArea(const Sheet<V3>& pos, size_t n) {
 }
 
 // ------------------------------------------------------- SimpleSimulator
+// generator: 0 RectGenerator, 1 NACA4digitGenerator(digit), 2 NACA00XXGenerator(digit)
 struct WingInfo {
   double chord, span;
   size_t rows, cols;
   V3 origin;
   Morphing morphing;
   int cheb_chord, cheb_span;
+  int generator = 0, digit = 0;
 };
 
 // src/util.h:36-43
@@ -524,6 +592,43 @@ std::vector<V3> RectGenerate(double chord, double span, size_t rows, size_t cols
   std::vector<V3> pts;
   for (double x : xs)
     for (double y : ys) pts.emplace_back(x, y, 0.0);
+  return pts;
+}
+
+// src/wing/naca4digit.cpp:12-27: mean camber line of a 4-digit NACA section
+// (only the first two digits matter: m = first/100, p = second/10).
+double NACA4digit(double x, double c, int xx) {
+  const int first = xx / 10;
+  const int second = xx % 10;
+  const double m = first / 100.0;
+  const double p = second / 10.0;
+  double res = 0;
+  if (0 <= x && x <= p * c) {
+    res = m * x / p / p * (2 * p - x / c);
+  } else if (p * c <= x && x <= c) {
+    res = m * (c - x) / (1 - p) / (1 - p) * (1 + x / c - 2 * p);
+  }
+  return res;
+}
+
+// src/wing/naca00XX.cpp:14-19: half thickness of a symmetric 4-digit section.
+double NACA00XX(double x, double c, int xx) {
+  const double t = xx * 0.01;
+  const double z = x / c;
+  return 5 * t * c * (0.2969 * std::sqrt(z) + (-0.1260) * (z) + (-0.3516) * z * z + 0.2843 * z * z * z +
+                      (-0.1015) * z * z * z * z);
+}
+
+// WingGenerator::Generate of the three generators: the rectangular lattice
+// (src/wing/rect.cpp:18-45), then z = NACA4digit(x) (src/wing/naca4digit.cpp:29-39)
+// or z = NACA00XX(x) (src/wing/naca00XX.cpp:21-32) at every point.
+std::vector<V3> GenerateWing(int generator, int digit, double chord, double span, size_t rows, size_t cols, int cc,
+                             int cs) {
+  auto pts = RectGenerate(chord, span, rows, cols, cc, cs);
+  if (generator == 1)
+    for (auto& p : pts) p.z = NACA4digit(p.x, chord, digit);
+  if (generator == 2)
+    for (auto& p : pts) p.z = NACA00XX(p.x, chord, digit);
   return pts;
 }
 
@@ -574,6 +679,7 @@ struct Simulator {
   std::unique_ptr<Advection> advection;
   long long erase_after = 0;
   bool built = false;
+  int lu_threads = 1;  // FullPivLU threads (1 = Eigen's single-threaded elimination)
 
   // src/simulator/simple_simulator.cpp:126-140
   int AddWing(const WingInfo& w) {
@@ -596,7 +702,8 @@ struct Simulator {
       Morphing m = w.morphing;
       w.origin.store(m.k.origin);
       morphings.push_back(m);
-      auto half = RectGenerate(w.chord, w.span / 2, w.rows, w.cols / 2, w.cheb_chord, w.cheb_span);
+      auto half = GenerateWing(w.generator, w.digit, w.chord, w.span / 2, w.rows, w.cols / 2, w.cheb_chord,
+                               w.cheb_span);
       auto pts = WholeWing(half, w.cols / 2, V3());
       for (auto& p : pts) p = p + w.origin;
       std::copy(pts.begin(), pts.end(), wing_pos_init.sheet_begin(n));
@@ -677,6 +784,38 @@ struct Simulator {
   }
 
   // src/simulator/simple_simulator.cpp:195-233
+  V3 LoadLineVelocity(const VortexLine& line, size_t n, double t) const {
+    const V3 mp = (line.p0 + line.p1) / 2;
+    const V3 mp_init = (line.p0_init + line.p1_init) / 2;
+    return Velocity(mp) - morphings[n].Velocity(mp_init, t);
+  }
+  // JoukowskiSteady + JoukowskiUnsteady of wing n from its line velocities U.
+  void LoadSums(size_t n, const std::vector<VortexLine>& lines, const V3* U, const std::vector<V3>& normal,
+                double dt, double* row) const {
+    const auto area = CalcPanelArea(wing_pos, n);
+    // JoukowskiSteady (src/calc_load/joukowski.cpp:36-53)
+    double Fx = 0, Fy = 0, Fz = 0;
+    for (size_t i = 0; i < lines.size(); i++) {
+      const V3 df = cross(U[i], lines[i].p1 - lines[i].p0) * lines[i].gamma;
+      Fx += df.x; Fy += df.y; Fz += df.z;
+    }
+    // JoukowskiUnsteady range form (src/calc_load/joukowski.h:132-148)
+    double Gx = 0, Gy = 0, Gz = 0;
+    const size_t off = wing_gamma.index(n, 0, 0);
+    const size_t cnt = wing_gamma.rows() * wing_gamma.cols();
+    for (size_t k = 0; k < cnt; k++) {
+      const double g = wing_gamma[off + k], gp = wing_gamma_prev[off + k];
+      const double dg_dt = (g - gp) / dt;
+      const V3 df = normal[off + k] * dg_dt * area[k];
+      Gx += df.x; Gy += df.y; Gz += df.z;
+    }
+    const V3 F = V3(Fx, Fy, Fz) + V3(Gx, Gy, Gz);
+    const double Q = norm(ff);
+    const double S = info[n].chord * info[n].span;
+    const V3 C = F / (0.5 * Q * Q * S);
+    if (row) { row[1 + 2 * n] = C.x; row[2 + 2 * n] = C.z; }
+  }
+
   void CalcLoad(const std::vector<V3>& normal, double t, double dt, double* row,
                 size_t stride = 1) const {
     if (row) row[0] = t;
@@ -684,34 +823,9 @@ struct Simulator {
       const auto lines = GetLines(wing_pos, wing_pos_init, wing_gamma, n);
       std::vector<V3> U(lines.size());
 #pragma omp parallel for schedule(dynamic, 8)
-      for (long long i = 0; i < (long long)lines.size(); i += (long long)stride) {
-        const auto& line = lines[i];
-        const V3 mp = (line.p0 + line.p1) / 2;
-        const V3 mp_init = (line.p0_init + line.p1_init) / 2;
-        U[i] = Velocity(mp) - morphings[n].Velocity(mp_init, t);
-      }
-      const auto area = CalcPanelArea(wing_pos, n);
-      // JoukowskiSteady (src/calc_load/joukowski.cpp:36-53)
-      double Fx = 0, Fy = 0, Fz = 0;
-      for (size_t i = 0; i < lines.size(); i++) {
-        const V3 df = cross(U[i], lines[i].p1 - lines[i].p0) * lines[i].gamma;
-        Fx += df.x; Fy += df.y; Fz += df.z;
-      }
-      // JoukowskiUnsteady range form (src/calc_load/joukowski.h:132-148)
-      double Gx = 0, Gy = 0, Gz = 0;
-      const size_t off = wing_gamma.index(n, 0, 0);
-      const size_t cnt = wing_gamma.rows() * wing_gamma.cols();
-      for (size_t k = 0; k < cnt; k++) {
-        const double g = wing_gamma[off + k], gp = wing_gamma_prev[off + k];
-        const double dg_dt = (g - gp) / dt;
-        const V3 df = normal[off + k] * dg_dt * area[k];
-        Gx += df.x; Gy += df.y; Gz += df.z;
-      }
-      const V3 F = V3(Fx, Fy, Fz) + V3(Gx, Gy, Gz);
-      const double Q = norm(ff);
-      const double S = info[n].chord * info[n].span;
-      const V3 C = F / (0.5 * Q * Q * S);
-      if (row) { row[1 + 2 * n] = C.x; row[2 + 2 * n] = C.z; }
+      for (long long i = 0; i < (long long)lines.size(); i += (long long)stride)
+        U[i] = LoadLineVelocity(lines[i], n, t);
+      LoadSums(n, lines, U.data(), normal, dt, row);
     }
   }
 
@@ -732,7 +846,7 @@ struct Simulator {
     auto A = CalcMatrix(cpos, normal);
     auto rhs = CalcRhs(cpos, cpos_init, normal, t);
     std::vector<double> g;
-    if (FullPivLUSolve(A, rhs.size(), rhs, g)) return 5;
+    if (FullPivLUSolve(A, rhs.size(), rhs, g, lu_threads)) return 5;
     for (size_t K = 0; K < wing_gamma.size(); K++) wing_gamma[K] = g[K];
     CalcLoad(normal, t, dt, row);
     advection->Advect(&wake_pos, wing_pos, wing_gamma, wake_pos, wake_gamma, ff, dt);
@@ -740,6 +854,251 @@ struct Simulator {
       wake_pos.erase_last_row();
       wake_gamma.erase_last_row();
     }
+    return 0;
+  }
+  // ---- MainLoop(step, dt) cut into slices ------------------------------------
+  // The CPU reference timing runs one MainLoop at full size as a sequence of
+  // slices of about equal estimated time (one slice per timed bench step).
+  // The loop is broken into work items -- the kinematics and shed, row ranges
+  // of CalcMatrix and CalcRhs, single columns of the FullPivLU elimination,
+  // its substitutions, ranges of load lines, ranges of wake nodes of each
+  // advection stage, the updates -- which evaluate the same expressions as
+  // MainLoop for every output element, so running all slices in order is
+  // exactly MainLoop(step, dt).  Euler and RK2 advection are cut into node
+  // ranges; RK4 and AB2 run as one item.
+  enum SliceKind { kKin, kMat, kRhs, kLu, kLuSolve, kLoadPrep, kLoadVel, kLoadFin, kAdvPrep, kAdvVel1, kAdvMid,
+                   kAdvVel2, kAdvEnd, kAdvAll, kErase };
+  struct SliceItem {
+    int kind;
+    size_t a, b;
+    double cost;
+  };
+  struct SlicedLoop {
+    size_t step = 0;
+    double dt = 0, t = 0;
+    int scheme = 0;  // 0 Euler, 1 RK2, 2 other (one item)
+    size_t rk_ignore = 5;
+    std::vector<SliceItem> items;
+    std::vector<size_t> first;  // first item of every slice, then items.size()
+    size_t next_slice = 0;
+    std::vector<V3> cpos, cpos_init, normal;
+    std::vector<double> A, rhs, g;
+    FullPivLU lu;
+    std::vector<std::vector<VortexLine>> lines;
+    std::vector<size_t> line_off;
+    std::vector<V3> U;
+    Sheet<V3> k1, k2, pos2;
+    double* row = nullptr;
+    bool failed = false;
+  } sl;
+
+  // Plans MainLoop(step, dt) in `slices` slices; `threads` is the OpenMP
+  // thread count the N-body items run with (for the time estimate only).
+  int SlicedBegin(size_t step, double dt, size_t slices, int threads) {
+    if (!built || slices < 1) return 4;
+    SlicedLoop& L = sl;
+    L = SlicedLoop();
+    L.step = step;
+    L.dt = dt;
+    L.t = step * dt;
+    if (auto* e = dynamic_cast<Euler*>(advection.get())) { (void)e; L.scheme = 0; }
+    else if (auto* r = dynamic_cast<RK2*>(advection.get())) { L.scheme = 1; L.rk_ignore = r->ignore; }
+    else L.scheme = 2;
+    // sizes after the shed of this step
+    const size_t num = wing_gamma.num(), N = wing_gamma.size();
+    const size_t wake_rings = num * (wake_gamma.rows() + (step > 0 ? 1 : 0)) * wing_gamma.cols();
+    const size_t wake_nodes = num * (wake_pos.rows() + 1) * wake_pos.cols();
+    const size_t lines = num * (4 * wing_gamma.rows() * wing_gamma.cols() - wing_gamma.cols());
+    // estimated seconds: one FP64 segment evaluation ~18 ns on one thread;
+    // one elimination element (pivot search + update) ~1.2 ns on one thread
+    const double seg = 18e-9 / std::max(threads, 1), elem = 1.2e-9 / std::max(lu_threads, 1);
+    auto add = [&](int kind, size_t a, size_t b, double cost) { L.items.push_back(SliceItem{kind, a, b, cost}); };
+    auto ranges = [&](int kind, size_t n, size_t chunk, double per) {
+      for (size_t a = 0; a < n; a += chunk) add(kind, a, std::min(n, a + chunk), per * (double)(std::min(n, a + chunk) - a));
+    };
+    add(kKin, 0, 0, 1e-4);
+    ranges(kMat, N, 16, seg * 4.0 * N);
+    ranges(kRhs, N, 64, seg * 4.0 * wake_rings);
+    for (size_t k = 0; k < N; k++) add(kLu, k, k + 1, elem * (double)(N - k) * (double)(N - k));
+    add(kLuSolve, 0, 0, 2e-9 * (double)N * (double)N);
+    add(kLoadPrep, 0, 0, 1e-4);
+    ranges(kLoadVel, lines, 64, seg * 4.0 * (N + wake_rings));
+    add(kLoadFin, 0, 0, 1e-4);
+    const double per_node = seg * 4.0 * (N + wake_rings);
+    if (L.scheme == 2) {
+      add(kAdvAll, 0, 0, per_node * wake_nodes * 4.0);
+    } else {
+      add(kAdvPrep, 0, 0, 1e-5);
+      ranges(kAdvVel1, wake_nodes, 64, per_node);
+      add(kAdvMid, 0, 0, 1e-5);
+      if (L.scheme == 1) ranges(kAdvVel2, wake_nodes, 64, per_node);
+      add(kAdvEnd, 0, 0, 1e-5);
+    }
+    add(kErase, 0, 0, 1e-6);
+    double total = 0;
+    for (const auto& it : L.items) total += it.cost;
+    L.first.push_back(0);
+    double acc = 0;
+    for (size_t q = 0; q < L.items.size(); q++) {
+      acc += L.items[q].cost;
+      if (L.first.size() < slices && acc >= total * (double)L.first.size() / (double)slices && q + 1 < L.items.size())
+        L.first.push_back(q + 1);
+    }
+    while (L.first.size() < slices) L.first.push_back(L.items.size());
+    L.first.push_back(L.items.size());
+    return 0;
+  }
+
+  void SliceItemRun(const SliceItem& it) {
+    SlicedLoop& L = sl;
+    const size_t N = wing_gamma.size();
+    switch (it.kind) {
+      case kKin: {
+        wing_gamma_prev = wing_gamma;
+        for (size_t n = 0; n < wing_pos.num(); n++) {
+          const V3* src = wing_pos_init.sheet_begin(n);
+          V3* dst = wing_pos.sheet_begin(n);
+          const size_t cnt = wing_pos.rows() * wing_pos.cols();
+          for (size_t k = 0; k < cnt; k++) dst[k] = morphings[n].Perfome(src[k], L.t);
+        }
+        Shed(L.step);
+        L.cpos = CollocationPoints(wing_pos);
+        L.cpos_init = CollocationPoints(wing_pos_init);
+        L.normal = Normals(wing_pos);
+        L.A.assign(N * N, 0.0);
+        L.rhs.assign(N, 0.0);
+        break;
+      }
+      case kMat: {  // CalcMatrix rows (src/simulator/simple_simulator.cpp:76-101)
+        Sheet<double> gamma(wing_gamma);
+        std::fill(gamma.data().begin(), gamma.data().end(), 1.0);
+#pragma omp parallel for schedule(dynamic, 4)
+        for (long long K = (long long)it.a; K < (long long)it.b; K++) {
+          size_t Lc = 0;
+          for (size_t nn = 0; nn < gamma.num(); nn++)
+            for (size_t ii = 0; ii < gamma.rows(); ii++)
+              for (size_t jj = 0; jj < gamma.cols(); jj++, Lc++)
+                L.A[K * N + Lc] = dot(VORING(L.cpos[K], wing_pos, gamma, nn, ii, jj), L.normal[K]);
+        }
+        break;
+      }
+      case kRhs: {  // CalcRhs rows (:103-124)
+        const size_t per = wing_gamma.rows() * wing_gamma.cols();
+#pragma omp parallel for schedule(dynamic, 4)
+        for (long long K = (long long)it.a; K < (long long)it.b; K++) {
+          const size_t n = (size_t)K / per;
+          const V3 Uw = InducedVelocity(L.cpos[K], wake_pos, wake_gamma);
+          const V3 Uls = morphings[n].Velocity(L.cpos_init[K], L.t);
+          const V3 u = Uw - (Uls + ff);
+          L.rhs[K] = -dot(u, L.normal[K]);
+        }
+        break;
+      }
+      case kLu:
+        if (it.a == 0) L.lu.Init(L.A, N, lu_threads);
+        L.lu.Step(it.a);
+        break;
+      case kLuSolve:
+        if (L.lu.singular) { L.failed = true; break; }
+        L.lu.Solve(L.rhs, L.g);
+        for (size_t K = 0; K < N; K++) wing_gamma[K] = L.g[K];
+        break;
+      case kLoadPrep: {
+        L.lines.clear();
+        L.line_off.assign(1, 0);
+        for (size_t n = 0; n < wing_pos.num(); n++) {
+          L.lines.push_back(GetLines(wing_pos, wing_pos_init, wing_gamma, n));
+          L.line_off.push_back(L.line_off.back() + L.lines.back().size());
+        }
+        L.U.assign(L.line_off.back(), V3());
+        break;
+      }
+      case kLoadVel: {
+#pragma omp parallel for schedule(dynamic, 8)
+        for (long long q = (long long)it.a; q < (long long)it.b; q++) {
+          size_t n = 0;
+          while ((size_t)q >= L.line_off[n + 1]) n++;
+          L.U[q] = LoadLineVelocity(L.lines[n][q - L.line_off[n]], n, L.t);
+        }
+        break;
+      }
+      case kLoadFin:
+        if (L.row) L.row[0] = L.t;
+        for (size_t n = 0; n < wing_pos.num(); n++) LoadSums(n, L.lines[n], L.U.data() + L.line_off[n], L.normal, L.dt, L.row);
+        break;
+      case kAdvPrep:
+        L.k1.resize(wake_pos);
+        break;
+      case kAdvVel1: {  // advect::Velocity of the wake nodes (src/advect.h:26-46)
+#pragma omp parallel for schedule(dynamic, 16)
+        for (long long K = (long long)it.a; K < (long long)it.b; K++)
+          L.k1[K] = -ff + InducedVelocity(wake_pos[K], wing_pos, wing_gamma) +
+                    InducedVelocity(wake_pos[K], wake_pos, wake_gamma);
+        break;
+      }
+      case kAdvMid: {
+        for (size_t n = 0; n < L.k1.num(); n++)
+          if (L.k1.rows() > 0)
+            for (size_t j = 0; j < L.k1.cols(); j++) L.k1.at(n, 0, j) = -ff;
+        if (L.scheme == 1) {  // RK2 (src/advect.cpp:24-80): the whole wake moved to pos2
+          L.pos2.resize(wake_pos);
+          for (size_t K = 0; K < wake_pos.size(); K++) L.pos2[K] = wake_pos[K] + L.k1[K] * L.dt;
+          L.k2.resize(L.pos2);
+        }
+        break;
+      }
+      case kAdvVel2: {
+#pragma omp parallel for schedule(dynamic, 16)
+        for (long long K = (long long)it.a; K < (long long)it.b; K++)
+          L.k2[K] = -ff + InducedVelocity(L.pos2[K], wing_pos, wing_gamma) +
+                    InducedVelocity(L.pos2[K], L.pos2, wake_gamma);
+        break;
+      }
+      case kAdvEnd: {
+        if (L.scheme == 0) {  // Euler (src/advect.cpp:11-22)
+          for (size_t K = 0; K < wake_pos.size(); K++) wake_pos[K] = wake_pos[K] + L.k1[K] * L.dt;
+          break;
+        }
+        for (size_t n = 0; n < L.k2.num(); n++)
+          if (L.k2.rows() > 0)
+            for (size_t j = 0; j < L.k2.cols(); j++) L.k2.at(n, 0, j) = -ff;
+        for (size_t n = 0; n < wake_pos.num(); n++)
+          for (size_t i = 0; i < wake_pos.rows(); i++)
+            for (size_t j = 0; j < wake_pos.cols(); j++) {
+              const size_t K = wake_pos.index(n, i, j);
+              if (i > L.rk_ignore)
+                wake_pos[K] = wake_pos[K] + (L.k1[K] + L.k2[K]) * L.dt / 2;
+              else
+                wake_pos[K] = wake_pos[K] + L.k1[K] * L.dt;
+            }
+        break;
+      }
+      case kAdvAll:
+        advection->Advect(&wake_pos, wing_pos, wing_gamma, wake_pos, wake_gamma, ff, L.dt);
+        break;
+      case kErase:
+        if (erase_after > 0 && (long long)L.step >= erase_after) {
+          wake_pos.erase_last_row();
+          wake_gamma.erase_last_row();
+        }
+        break;
+      default:
+        break;
+    }
+  }
+
+  // Runs slice `s` (slices run in order 0, 1, ...); the load row is written
+  // by the slice that finishes the loads.  0, or 5 if the matrix is singular,
+  // 6 if out of order.
+  int SlicedRun(size_t s, double* row) {
+    SlicedLoop& L = sl;
+    if (s != L.next_slice || s + 1 >= L.first.size()) return 6;
+    L.row = row;
+    for (size_t q = L.first[s]; q < L.first[s + 1]; q++) {
+      SliceItemRun(L.items[q]);
+      if (L.failed) return 5;
+    }
+    L.next_slice++;
     return 0;
   }
 };
@@ -1136,6 +1495,32 @@ int orc_sim_add_wing(void* s, double chord, double span, int64_t rows, int64_t c
                      const orc_kinematics* m, int cc, int cs) {
   WingInfo w{chord, span, (size_t)rows, (size_t)cols, V3(origin), MakeMorphing(m), cc, cs};
   return static_cast<Simulator*>(s)->AddWing(w);
+}
+
+int orc_sim_add_wing_generator(void* s, int generator, int digit, double chord, double span, int64_t rows,
+                               int64_t cols, const double origin[3], const orc_kinematics* m, int cc, int cs) {
+  if (generator < 0 || generator > 2) return 1;
+  WingInfo w{chord, span, (size_t)rows, (size_t)cols, V3(origin), MakeMorphing(m), cc, cs, generator, digit};
+  return static_cast<Simulator*>(s)->AddWing(w);
+}
+
+double orc_naca4digit(double x, double c, int xx) { return NACA4digit(x, c, xx); }
+double orc_naca00xx(double x, double c, int xx) { return NACA00XX(x, c, xx); }
+
+void orc_generate_wing(int generator, int digit, double chord, double span, int64_t rows, int64_t cols, int cc,
+                       int cs, double* out) {
+  auto v = GenerateWing(generator, digit, chord, span, rows, cols, cc, cs);
+  for (size_t k = 0; k < v.size(); k++) v[k].store(out + 3 * k);
+}
+
+void orc_sim_set_lu_threads(void* s, int threads) { static_cast<Simulator*>(s)->lu_threads = threads > 1 ? threads : 1; }
+
+int orc_sim_sliced_begin(void* s, int64_t step, double dt, int64_t slices, int threads) {
+  return static_cast<Simulator*>(s)->SlicedBegin((size_t)step, dt, (size_t)std::max<int64_t>(slices, 1), threads);
+}
+
+int orc_sim_sliced_run(void* s, int64_t slice, double* load_row) {
+  return static_cast<Simulator*>(s)->SlicedRun((size_t)slice, load_row);
 }
 
 void orc_sim_set_forward_flight(void* s, const double ff[3]) { static_cast<Simulator*>(s)->ff = V3(ff); }

@@ -141,6 +141,15 @@ void orc_rect_generate(double chord, double span, int64_t rows, int64_t cols,
 void orc_whole_wing(const double* half, int64_t rows, int64_t half_cols,
                     const double origin[3], double* out);
 
+/* NACA4digit (src/wing/naca4digit.cpp:12-27) and NACA00XX
+ * (src/wing/naca00XX.cpp:14-19) at x for chord c and digits xx. */
+double orc_naca4digit(double x, double c, int xx);
+double orc_naca00xx(double x, double c, int xx);
+/* WingGenerator::Generate of RectGenerator (generator 0), NACA4digitGenerator
+ * (1) or NACA00XXGenerator (2) with `digit`: (rows+1)*(cols+1)*3 points. */
+void orc_generate_wing(int generator, int digit, double chord, double span, int64_t rows, int64_t cols, int cc,
+                       int cs, double* out);
+
 /* ---- dense solve: Eigen::FullPivLU<MatrixXd>(A).solve(b) ---------------- */
 /* A is row-major n x n and is overwritten.  Returns 0, or 1 if singular. */
 int orc_fullpiv_lu_solve(double* A, int64_t n, const double* b, double* x);
@@ -151,6 +160,14 @@ void orc_sim_destroy(void* sim);
 int orc_sim_add_wing(void* sim, double chord, double span, int64_t rows,
                      int64_t cols, const double origin[3],
                      const orc_kinematics* m, int cheb_chord, int cheb_span);
+/* AddWing with a NACA4digitGenerator (generator 1) or NACA00XXGenerator (2)
+ * of the given digits; generator 0 is RectGenerator (= orc_sim_add_wing). */
+int orc_sim_add_wing_generator(void* sim, int generator, int digit, double chord, double span, int64_t rows,
+                               int64_t cols, const double origin[3], const orc_kinematics* m, int cheb_chord,
+                               int cheb_span);
+/* Threads of the FullPivLU elimination (default 1, as Eigen's).  The result
+ * is bit-identical for any count. */
+void orc_sim_set_lu_threads(void* sim, int threads);
 void orc_sim_set_forward_flight(void* sim, const double ff[3]);
 /* names as AdvectFactory: "euler", "RK2", "RK4", "AB2" */
 int orc_sim_set_advection(void* sim, const char* name);
@@ -173,6 +190,15 @@ void orc_sim_get_state(void* sim, double* wing_pos, double* wing_pos_init,
 int orc_sim_set_state(void* sim, int64_t wake_rows, const double* wing_pos,
                       const double* wake_pos, const double* wing_gamma,
                       const double* wing_gamma_prev, const double* wake_gamma);
+/* MainLoop(step, dt) cut into `slices` consecutive slices of about equal
+ * estimated time (threads: the OpenMP threads the N-body loops run with, used
+ * for the estimate only).  Running every slice in order (orc_sim_sliced_run
+ * with slice = 0, 1, ..., slices-1) performs exactly orc_sim_step(step, dt):
+ * the same expressions for every output element.  load_row is written by the
+ * slice that finishes the loads (pass it to every call).  Returns 0, 4 before
+ * begin, 5 singular, 6 for a slice out of order. */
+int orc_sim_sliced_begin(void* sim, int64_t step, double dt, int64_t slices, int threads);
+int orc_sim_sliced_run(void* sim, int64_t slice, double* load_row);
 /* Timing helper for the CPU baseline: runs every stage of MainLoop(step) on a
  * copy of the state, evaluating the N-body stages on every stride-th target
  * only and the FullPivLU on the leading lu_n x lu_n block.  Writes per-stage

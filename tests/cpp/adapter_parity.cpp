@@ -92,7 +92,47 @@ int main() {
     for (int d = 0; d < 3; ++d) e3 = std::fmax(e3, std::fabs(next[q][d] - inplace[q][d]));
   expect(e3 == 0.0 && next.size() == wake_pos.size(), "Advection::Advect aliasing next == wake_pos", e3);
 
-  // 4. errors surface as UVLM::Error (the reference aborts)
+  // 4. the set-up of src/multiple_flapping_wings_main.cpp:40-73 with its flag
+  // defaults: three NACA 83 wings (AddWing takes the generator, as the
+  // reference's does), flap -pi/4 cos(w t) = pi/4 sin(w t - pi/2), alpha 5 deg,
+  // w = 2 U k / c with k = 0.1, 6 x 20 rings, Euler; 30 steps
+  {
+    const double w = 2 * 1.0 * 0.1 / 1.0, dtw = 2 * PI / w / 40, alpha = 5 * PI / 180;
+    const double origins[3][3] = {{0, 0, 0}, {3, 6, 0}, {3, -6, 0}};
+    UVLM::simulator::SimpleSimulator ms;
+    UVLM::Morphing mf;
+    mf.set_flap(PI / 4, w, -PI / 2);
+    mf.set_alpha(alpha);
+    for (auto& og : origins)
+      ms.AddWing(new UVLM::wing::NACA4digitGenerator(83), mf, 1.0, 6.0, 6, 20, Vector3(og[0], og[1], og[2]));
+    ms.set_forward_flight(Vector3(-1, 0, 0));
+    ms.set_advection("euler");
+    const auto mrows = ms.Run(30, dtw);
+
+    orc_kinematics kf{};
+    kf.alpha = alpha;
+    kf.flap_amp = PI / 4;
+    kf.flap_omega = w;
+    kf.flap_phase = -PI / 2;
+    void* om = orc_sim_create();
+    for (auto& og : origins) orc_sim_add_wing_generator(om, 1, 83, 1.0, 6.0, 6, 20, og, &kf, 0, 0);
+    orc_sim_set_forward_flight(om, ff);
+    orc_sim_set_advection(om, "euler");
+    orc_sim_begin(om);
+    double e4 = 0, s4 = 0;
+    for (int s = 0; s <= 30; ++s) {
+      double row[7];
+      orc_sim_step(om, s, dtw, row);
+      for (int q = 1; q < 7; ++q) {
+        e4 = std::fmax(e4, std::fabs(mrows[s][q] - row[q]));
+        s4 = std::fmax(s4, std::fabs(row[q]));
+      }
+    }
+    orc_sim_destroy(om);
+    expect(e4 <= 1e-8 * s4, "NACA 83 three-wing flap loads vs oracle", e4);
+  }
+
+  // 5. errors surface as UVLM::Error (the reference aborts)
   bool threw = false;
   try {
     UVLM::advect::AdvectFactory("RK3");

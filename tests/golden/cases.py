@@ -63,6 +63,15 @@ CASES = {
         wings=[dict(chord=1.0, span=8.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0),
                     kin=dict(bend_cx=0.05, bend_cy=0.1, bend_omega=0.6))],
         ff=(-1.0, 0.0, 0.0), advection="euler", dt=2 * math.pi / 0.6 / 40, steps=16),
+    # src/multiple_flapping_wings_main.cpp:40-73 with its flag defaults: NACA 83 camber lattice
+    # (NACA4digitGenerator(83)), AR 6, alpha 5 deg, flap -pi/4 cos(w t) = pi/4 sin(w t - pi/2) with
+    # w = 2 U k / c, k = 0.1, --lines 2 (the leading wing and two wings at (3, +-6, 0)), 6 x 20 rings,
+    # 40 steps per cycle, Euler; 30 of its 50 steps
+    "naca83_flap_3wings_6x20": dict(
+        wings=[dict(chord=1.0, span=6.0, rows=6, cols=20, origin=o, generator=("naca4digit", 83),
+                    kin=dict(alpha=5 * DEG, flap_amp=math.pi / 4, flap_omega=0.2, flap_phase=-math.pi / 2))
+               for o in [(0.0, 0.0, 0.0), (3.0, 6.0, 0.0), (3.0, -6.0, 0.0)]],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=2 * math.pi / 0.2 / 40, steps=30),
     "chebyshev_euler_4x8": dict(
         wings=[dict(chord=1.0, span=4.0, rows=4, cols=8, origin=(0.0, 0.0, 0.0), cheb_chord=True, cheb_span=True,
                     kin=dict(alpha=6 * DEG, plug_amp=0.05, plug_omega=1.5))],
@@ -77,8 +86,10 @@ def run_oracle(case: dict):
 
     sim = o.Simulator()
     for w in case["wings"]:
-        sim.add_wing(w["chord"], w["span"], w["rows"], w["cols"], origin=w["origin"], kin=o.kinematics(**w["kin"]),
-                     cheb_chord=w.get("cheb_chord", False), cheb_span=w.get("cheb_span", False))
+        gen, digit = w.get("generator", ("rect", 0))
+        sim.add_wing_generator(gen, digit, w["chord"], w["span"], w["rows"], w["cols"], origin=w["origin"],
+                               kin=o.kinematics(**w["kin"]), cheb_chord=w.get("cheb_chord", False),
+                               cheb_span=w.get("cheb_span", False))
     sim.set_forward_flight(case["ff"])
     sim.set_advection(case["advection"])
     if case.get("erase_wake_after"):
@@ -101,8 +112,42 @@ def make_gpu_sim(case: dict, **kw):
         m.set_twist(k.get("twist_amp", 0.0), k.get("twist_omega", 0.0), k.get("twist_phase", 0.0),
                     k.get("twist_span_slope", 0.0))
         m.set_bend(k.get("bend_cx", 0.0), k.get("bend_cy", 0.0), k.get("bend_omega", 0.0), k.get("bend_phase", 0.0))
-        sim.AddWing(U.RectGenerator(w.get("cheb_chord", False), w.get("cheb_span", False)), m, w["chord"], w["span"],
-                    w["rows"], w["cols"], w["origin"])
+        gen, digit = w.get("generator", ("rect", 0))
+        cheb = (w.get("cheb_chord", False), w.get("cheb_span", False))
+        g = {"rect": lambda: U.RectGenerator(*cheb), "naca4digit": lambda: U.NACA4digitGenerator(digit, *cheb),
+             "naca00xx": lambda: U.NACA00XXGenerator(digit, *cheb)}[gen]()
+        sim.AddWing(g, m, w["chord"], w["span"], w["rows"], w["cols"], w["origin"])
     sim.set_forward_flight(case["ff"])
     sim.set_advection(case["advection"])
     return sim
+
+
+# The benchmark workloads at full size (the same set-ups as bench.py's
+# heave_pitch, tandem4 and morphing workloads; tests/test_oracle_golden.py
+# checks that they agree), for the oracle-pinned full-size fixtures made by
+# tests/golden/make_fullsize.py.  `steps` is the window the fixture covers:
+# from step 0 while the FP64 form's own one-ulp sensitivity stays far below
+# the tolerances of the parity tests.
+def _fullsize():
+    hp_w = 1.0
+    heave_pitch = dict(
+        wings=[dict(chord=1.0, span=8.0, rows=32, cols=128, origin=(0.0, 0.0, 0.0),
+                    kin=dict(plug_amp=0.2, plug_omega=hp_w, twist_amp=10 * DEG, twist_omega=hp_w,
+                             twist_phase=math.pi / 2))],
+        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / hp_w / 40, steps=40)
+    tw = 0.8
+    tandem = dict(
+        wings=[dict(chord=1.0, span=4.0, rows=16, cols=64, origin=(x, 0.0, z),
+                    kin=dict(plug_amp=0.15, plug_omega=tw, plug_phase=q * math.pi / 2, twist_amp=15 * DEG,
+                             twist_omega=tw, twist_phase=q * math.pi / 2 + math.pi / 2))
+               for q, (x, z) in enumerate([(0.0, 0.0), (0.0, 0.5), (1.5, 0.0), (1.5, 0.5)])],
+        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / tw / 40, steps=20)
+    mw = 0.6
+    morphing = dict(
+        wings=[dict(chord=1.0, span=8.0, rows=24, cols=96, origin=(0.0, 0.0, 0.0),
+                    kin=dict(bend_cx=0.05, bend_cy=0.1, bend_omega=mw))],
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=2 * math.pi / mw / 40, steps=50)
+    return {"heave_pitch_32x128": heave_pitch, "tandem4_16x64": tandem, "morphing_24x96": morphing}
+
+
+FULLSIZE = _fullsize()

@@ -6,6 +6,7 @@ with the same inputs, expected values and tolerances.  The oracle
 are the pins that make it trustworthy.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -379,3 +380,37 @@ def test_legacy_loop_symmetric_and_finite():
         assert rows.shape == (7, 6) and np.all(np.isfinite(rows))
         np.testing.assert_allclose(rows[:, 2], 0, atol=1e-12)   # C_y of a symmetric wing
         assert rows[-1, 3] > 0                                  # lift at alpha = 0.1
+
+
+# ---- wing generators: test/naca4digit_test.cpp, test/naca00XX_test.cpp ----
+# The published section tables the reference's tests read (test/wing/data/)
+# are kept in tests/golden/naca_tables.npz (tests/golden/make_naca_tables.py).
+_NACA = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "naca_tables.npz"))
+
+
+def test_naca4digit_table():  # naca4digit_test.cpp:31-43 (mean square error below 1e-6)
+    d = _NACA["naca62xx"]
+    err = np.mean([(y - o.naca4digit(x, 100, 62)) ** 2 for x, y in d])
+    assert 1e-6 > err
+
+
+def test_naca4digit_generator():  # naca4digit_test.cpp:45-55
+    pts = o.generate_wing("naca4digit", 83, 3, 2, 10, 10)
+    for p in pts.reshape(-1, 3):
+        assert p[2] == o.naca4digit(p[0], 3, 83)
+
+
+def test_naca00xx_table():  # naca00XX_test.cpp:29-38 (sum of squares below 1e-10)
+    d = _NACA["naca0012"]
+    err = sum((z - o.naca00xx(x, 1.0, 12)) ** 2 for x, z in d)
+    assert 1e-10 > err
+
+
+@pytest.mark.parametrize("digit", [12, 0])
+def test_naca00xx_generator(digit):  # naca00XX_test.cpp:40-68 (Generate, GenerateRect)
+    pts = o.generate_wing("naca00xx", digit, 2, 2, 2, 2).reshape(-1, 3)
+    z1, z2 = (o.naca00xx(1.0, 2.0, 12), o.naca00xx(2.0, 2.0, 12)) if digit else (0.0, 0.0)
+    expect = [(0, 0, 0), (0, 1, 0), (0, 2, 0), (1, 0, z1), (1, 1, z1), (1, 2, z1), (2, 0, z2), (2, 1, z2),
+              (2, 2, z2)]
+    for p, e in zip(pts, expect):
+        np.testing.assert_array_equal(p, e)

@@ -6,7 +6,8 @@ The Python classes mirror the reference's C++ API for the per-step hot path
   SimpleSimulator  src/simulator/simple_simulator.h:36-108
   Morphing         src/morphing.h:25-108 (closed-form sinusoids instead of
                    std::function; see ``Morphing``)
-  RectGenerator    src/wing/rect.h:28-35
+  RectGenerator, NACA4digitGenerator, NACA00XXGenerator, WholeWing
+                   src/wing/* (host-side lattice generators, uvlm_b200.wing)
   AdvectFactory    src/advect_factory.cpp:43-60 -> ``Advection`` objects
                    whose ``Advect`` matches src/advect.h:48-59
   InducedVelocity  src/velocity.h:14-24
@@ -24,9 +25,11 @@ import numpy as np
 
 from ._capi import (ADVECT, LU_PREC, PRECISION, SOLVER, WARM, Config, Kinematics, StepStats, UVLMError, WingDesc,
                     check, lib)
+from .wing import NACA00XXGenerator, NACA4digitGenerator, RectGenerator, WholeWing, WingGenerator
 
-__all__ = ["SimpleSimulator", "Morphing", "RectGenerator", "AdvectFactory", "Advection", "InducedVelocity",
-           "UVLMError", "dense_solve", "rings", "lib"]
+__all__ = ["SimpleSimulator", "Morphing", "WingGenerator", "RectGenerator", "NACA4digitGenerator",
+           "NACA00XXGenerator", "WholeWing", "AdvectFactory", "Advection", "InducedVelocity", "UVLMError",
+           "dense_solve", "rings", "lib"]
 
 _P = C.POINTER(C.c_double)
 
@@ -113,14 +116,6 @@ class Morphing:
         self.set_origin(origin)
 
 
-class RectGenerator:
-    """Flat rectangular half-wing lattice (src/wing/rect.cpp:18-45)."""
-
-    def __init__(self, chebyshev_chord: bool = False, chebyshev_span: bool = False):
-        self.chebyshev_chord = bool(chebyshev_chord)
-        self.chebyshev_span = bool(chebyshev_span)
-
-
 class SimpleSimulator:
     """The UVLM time-stepper (src/simulator/simple_simulator.{h,cpp}) on a B200.
 
@@ -133,13 +128,15 @@ class SimpleSimulator:
       preconditioner  "inverse" (dense (LU)^-1 of the stale factors, one
                   matrix-vector product per GMRES iteration) or "triangular"
                   (forward/backward solves with the factors)
+      fp64_stages mixed form: N-body stages evaluated in FP64, any of
+                  "rhs", "loads", "advect"
     """
 
     def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
                  lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
                  gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
                  assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True,
-                 preconditioner: str = "inverse"):
+                 preconditioner: str = "inverse", fp64_stages=()):
         cfg = Config()
         lib().uvlm_config_default(C.byref(cfg))
         cfg.precision = PRECISION[precision]
@@ -159,6 +156,7 @@ class SimpleSimulator:
         cfg.nbody_variant = int(nbody_variant)
         cfg.compute_loads = int(bool(compute_loads))
         cfg.preconditioner = {"inverse": 0, "triangular": 1}[preconditioner]
+        cfg.nbody_fp64_stages = sum({"rhs": 1, "loads": 2, "advect": 4}[s] for s in set(fp64_stages))
         self._cfg = cfg
         h = C.c_void_p()
         check(lib().uvlm_create(C.byref(cfg), C.byref(h)))
@@ -169,15 +167,25 @@ class SimpleSimulator:
         self._built = False
 
     # -- reference API ------------------------------------------------------
-    def AddWing(self, generator: RectGenerator, morphing: Morphing, chord: float, span: float, rows: int,  # noqa: N802
+    def AddWing(self, generator: WingGenerator, morphing: Morphing, chord: float, span: float, rows: int,  # noqa: N802
                 cols: int, origin=(0.0, 0.0, 0.0)) -> None:
-        w = WingDesc()
-        w.chord, w.span, w.rows, w.cols = float(chord), float(span), int(rows), int(cols)
-        for i in range(3):
-            w.origin[i] = float(origin[i])
+        """SimpleSimulator::AddWing (simple_simulator.cpp:126-140, BuildWing :142-169) with any
+        WingGenerator: the half wing (chord, span/2, rows, cols/2) from the generator, mirrored by
+        WholeWing, moved to `origin`.  A plain RectGenerator wing is generated by the library itself."""
         gen = generator or RectGenerator()
-        w.chebyshev_chord, w.chebyshev_span = int(gen.chebyshev_chord), int(gen.chebyshev_span)
-        check(lib().uvlm_add_wing(self._h, C.byref(w), C.byref(morphing.k)), self._h)
+        if int(cols) % 2:
+            raise UVLMError(1, "columns must be even.")
+        if type(gen) is RectGenerator:
+            w = WingDesc()
+            w.chord, w.span, w.rows, w.cols = float(chord), float(span), int(rows), int(cols)
+            for i in range(3):
+                w.origin[i] = float(origin[i])
+            w.chebyshev_chord, w.chebyshev_span = int(gen.chebyshev_chord), int(gen.chebyshev_span)
+            check(lib().uvlm_add_wing(self._h, C.byref(w), C.byref(morphing.k)), self._h)
+        else:
+            nodes = _f64(WholeWing(gen.Generate(float(chord), float(span) / 2, int(rows), int(cols) // 2)))
+            check(lib().uvlm_add_wing_nodes(self._h, int(rows), int(cols), _p(nodes), float(chord), float(span),
+                                            _p(_f64(origin)), C.byref(morphing.k)), self._h)
         self._num += 1
         self._wings.append((chord, span, rows, cols))
 

@@ -31,7 +31,7 @@ class Config(C.Structure):
         ("max_wake_rows", C.c_int64), ("erase_wake_after", C.c_int64),
         ("gmres_restart", C.c_int32), ("gmres_max_iter", C.c_int32), ("gmres_tol", C.c_double),
         ("device", C.c_int32), ("compute_loads", C.c_int32), ("assembly_fp64", C.c_int32),
-        ("nbody_variant", C.c_int32), ("preconditioner", C.c_int32),
+        ("nbody_variant", C.c_int32), ("preconditioner", C.c_int32), ("nbody_fp64_stages", C.c_int32),
     ]
 
 
@@ -94,6 +94,7 @@ SIGNATURES = [
     ("uvlm_global_last_error", C.c_char_p, []),
     ("uvlm_status_string", C.c_char_p, [C.c_int]),
     ("uvlm_add_wing", C.c_int, [_V, C.POINTER(WingDesc), C.POINTER(Kinematics)]),
+    ("uvlm_add_wing_nodes", C.c_int, [_V, _I, _I, _P, C.c_double, C.c_double, _P, C.POINTER(Kinematics)]),
     ("uvlm_set_forward_flight", C.c_int, [_V, _P]),
     ("uvlm_set_advection", C.c_int, [_V, C.c_char_p]),
     ("uvlm_begin", C.c_int, [_V]),

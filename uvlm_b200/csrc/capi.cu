@@ -62,6 +62,7 @@ Mlp* mlp_of(uvlm_mlp* h);
 struct uvlm_ctx {
   uvlm_config cfg{};
   std::vector<uvlm_wing_desc> wings;
+  std::vector<std::vector<double>> wing_nodes;  // per wing: the caller's lattice, or empty (RectGenerator)
   std::vector<uvlm_kinematics> kins;
   double ff[3] = {0, 0, 0};
   std::string err;
@@ -136,8 +137,13 @@ struct uvlm_ctx {
   }
   void free_all();
   Error alloc_all();
-  Error build_sources(bool with_bound, const double* wake_pos_buf, SourceBlock* blocks, int* nb_out);
-  Error eval(const SourceBlock* blocks, int nblocks, long long nt);
+  // precision of an N-body stage (UVLM_STAGE_* bit): the context's, or FP64
+  // where the mixed form is told to evaluate that stage in FP64
+  NBodyPrec stage_prec(int stage_bit) const {
+    return (!mixed() || (cfg.nbody_fp64_stages & stage_bit)) ? kNBodyFP64 : kNBodyFP32;
+  }
+  Error build_sources(bool with_bound, const double* wake_pos_buf, NBodyPrec prec, SourceBlock* blocks, int* nb_out);
+  Error eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec);
   Error shed(long long step);
   Error solve(long long step);
   Error advect(double dt);
@@ -251,7 +257,8 @@ Error uvlm_ctx::alloc_all() {
 }
 
 // Source records: [bound sheets][wake sheets (positions from wake_pos_buf)].
-Error uvlm_ctx::build_sources(bool with_bound, const double* wake_pos_buf, SourceBlock* blocks, int* nb_out) {
+Error uvlm_ctx::build_sources(bool with_bound, const double* wake_pos_buf, NBodyPrec prec, SourceBlock* blocks,
+                              int* nb_out) {
   SheetView views[2];
   int nv = 0;
   if (with_bound) views[nv++] = SheetView{d_pos, R + 1, 0, d_gamma, R, 0, num, R + 1, C};
@@ -259,17 +266,17 @@ Error uvlm_ctx::build_sources(bool with_bound, const double* wake_pos_buf, Sourc
     views[nv++] = SheetView{wake_pos_buf, PR, wake_start, d_wgamma, PR, wake_start, num, wake_nodes, C};
   *nb_out = nv;
   if (nv == 0) return ok();
-  return nbody_build_sources(views, nv, mixed() ? kNBodyFP32 : kNBodyFP64, &nb, blocks, st);
+  return nbody_build_sources(views, nv, prec, &nb, blocks, st);
 }
 
-Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt) {
+Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec) {
   const double pairs = (double)nt * (double)nbody_unique_segments(blocks, nblocks);
   work_nbody += pairs;
-  if (!tuned && nblocks > 0 && pairs >= 2e9) {
+  const NBodyPrec main_prec = mixed() ? kNBodyFP32 : kNBodyFP64;
+  if (!tuned && prec == main_prec && nblocks > 0 && pairs >= 2e9) {
     // Tile autotune on the first large evaluation: time every compiled variant
     // of this precision on the real sources and targets, keep the fastest
     // (the default unless another is more than 3% faster).
-    const NBodyPrec prec = mixed() ? kNBodyFP32 : kNBodyFP64;
     int& chosen = mixed() ? variant_fp32 : variant_fp64;
     float best_ms = 1e30f;
     int best = chosen;
@@ -301,8 +308,8 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt) {
   }
 const bool rec = timing && nbev_n < kNbEvents;
   if (rec) UVLM_CUDA_TRY(cudaEventRecord(nbev[2 * nbev_n], st));
-    const Error e = nbody_eval(blocks, nblocks, mixed() ? kNBodyFP32 : kNBodyFP64, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb,
-                    mixed() ? variant_fp32 : variant_fp64, num_sms, st);
+  const Error e = nbody_eval(blocks, nblocks, prec, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb,
+                             prec == kNBodyFP32 ? variant_fp32 : variant_fp64, num_sms, st);
   if (rec) {
     UVLM_CUDA_TRY(cudaEventRecord(nbev[2 * nbev_n + 1], st));
     ++nbev_n;
@@ -399,11 +406,12 @@ Error uvlm_ctx::advect(double dt) {
   const long long nt = (long long)num * (wake_nodes - 1) * (C + 1);
   SourceBlock blocks[2];
   int nbk = 0;
+  const NBodyPrec prec = stage_prec(UVLM_STAGE_ADVECT);
   auto velocity_at = [&](const double* pos_buf, bool rebuild) -> Error {
-    if (rebuild) UVLM_TRY(build_sources(true, pos_buf, blocks, &nbk));
+    if (rebuild) UVLM_TRY(build_sources(true, pos_buf, prec, blocks, &nbk));
     if (nt > 0) {
       UVLM_TRY(launch_gather_wake(L, pos_buf, d_tx, d_ty, d_tz, st));
-      UVLM_TRY(eval(blocks, nbk, nt));
+      UVLM_TRY(eval(blocks, nbk, nt, prec));
     }
     return ok();
   };
@@ -521,11 +529,12 @@ Error uvlm_ctx::stage_rhs() {
   {
     SourceBlock blocks[2];
     int nbk = 0;
-    UVLM_TRY(build_sources(false, d_wpos, blocks, &nbk));
+    const NBodyPrec prec = stage_prec(UVLM_STAGE_RHS);
+    UVLM_TRY(build_sources(false, d_wpos, prec, blocks, &nbk));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_tx, d_cx, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_ty, d_cy, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_tz, d_cz, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-    UVLM_TRY(eval(blocks, nbk, N));
+    UVLM_TRY(eval(blocks, nbk, N, prec));
     UVLM_TRY(launch_rhs(N, d_vx, d_vy, d_vz, d_uls, d_normal, ff, d_rhs, st));
   }
   mark(3);
@@ -561,8 +570,9 @@ Error uvlm_ctx::stage_loads() {
     UVLM_TRY(launch_line_prep(d_kin, ws(), d_pos, d_pos_init, t, d_tx, d_ty, d_tz, d_line_uls, st));
     SourceBlock blocks[2];
     int nbk = 0;
-    UVLM_TRY(build_sources(true, d_wpos, blocks, &nbk));
-    UVLM_TRY(eval(blocks, nbk, lines));
+    const NBodyPrec prec = stage_prec(UVLM_STAGE_LOADS);
+    UVLM_TRY(build_sources(true, d_wpos, prec, blocks, &nbk));
+    UVLM_TRY(eval(blocks, nbk, lines, prec));
     UVLM_TRY(launch_loads(ws(), d_pos, d_gamma, d_gamma_prev, d_normal, d_area, d_vx, d_vy, d_vz, d_line_uls, ff,
                           d_chord_span, t, dt, d_row, st));
   }
@@ -683,7 +693,8 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
     return set_global(fail(kErrInvalid, "unknown precision"));
   }
   if (k.advection < 0 || k.advection > 3 || k.max_wake_rows < 1 || k.gmres_restart < 1 || k.gmres_max_iter < 1 ||
-      !(k.gmres_tol > 0) || k.preconditioner < 0 || k.preconditioner > 1) {
+      !(k.gmres_tol > 0) || k.preconditioner < 0 || k.preconditioner > 1 || k.nbody_fp64_stages < 0 ||
+      k.nbody_fp64_stages > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT)) {
     delete c;
     return set_global(fail(kErrInvalid, "invalid configuration"));
   }
@@ -794,10 +805,37 @@ int uvlm_add_wing(uvlm_ctx* c, const uvlm_wing_desc* w, const uvlm_kinematics* k
   if (!c->wings.empty() && (c->wings.back().rows != w->rows || c->wings.back().cols != w->cols))
     return c->fail_with(fail(kErrInvalid, "all wings must have the same rows and cols"));
   c->wings.push_back(*w);
+  c->wing_nodes.emplace_back();
   uvlm_kinematics k{};
   if (kin) k = *kin;
   // BuildWing sets the morphing origin to the wing origin (simple_simulator.cpp:157)
   for (int d = 0; d < 3; ++d) k.origin[d] = w->origin[d];
+  c->kins.push_back(k);
+  return UVLM_OK;
+}
+
+int uvlm_add_wing_nodes(uvlm_ctx* c, int64_t rows, int64_t cols, const double* nodes, double chord, double span,
+                        const double origin[3], const uvlm_kinematics* kin) {
+  if (!c || !nodes || !origin) return set_global(fail(kErrInvalid, "NULL argument"));
+  if (c->built) return c->fail_with(fail(kErrState, "wings are added before uvlm_begin"));
+  if (rows < 1 || cols < 1 || rows > (1 << 20) || cols > (1 << 20) || !(chord > 0) || !(span > 0))
+    return c->fail_with(fail(kErrInvalid, "rows >= 1, cols >= 1 and positive chord/span are required"));
+  if (!c->wings.empty() && (c->wings.back().rows != rows || c->wings.back().cols != cols))
+    return c->fail_with(fail(kErrInvalid, "all wings must have the same rows and cols"));
+  const size_t cnt = (size_t)(rows + 1) * (size_t)(cols + 1) * 3;
+  for (size_t q = 0; q < cnt; ++q)
+    if (!std::isfinite(nodes[q])) return c->fail_with(fail(kErrInvalid, "non-finite wing node"));
+  uvlm_wing_desc w{};
+  w.chord = chord;
+  w.span = span;
+  w.rows = rows;
+  w.cols = cols;
+  for (int d = 0; d < 3; ++d) w.origin[d] = origin[d];
+  c->wings.push_back(w);
+  c->wing_nodes.emplace_back(nodes, nodes + cnt);
+  uvlm_kinematics k{};
+  if (kin) k = *kin;
+  for (int d = 0; d < 3; ++d) k.origin[d] = origin[d];
   c->kins.push_back(k);
   return UVLM_OK;
 }
@@ -835,9 +873,17 @@ int uvlm_begin(uvlm_ctx* c) {
   Error e = c->alloc_all();
   if (e.code) return c->fail_with(e);
   std::vector<double> nodes;
-  for (auto& w : c->wings) {
-    auto v = whole_wing_nodes(w);
-    nodes.insert(nodes.end(), v.begin(), v.end());
+  for (size_t q = 0; q < c->wings.size(); ++q) {
+    const auto& w = c->wings[q];
+    if (c->wing_nodes[q].empty()) {
+      auto v = whole_wing_nodes(w);
+      nodes.insert(nodes.end(), v.begin(), v.end());
+    } else {
+      // the caller's lattice (points of WholeWing) moved to the wing origin
+      // (simple_simulator.cpp:162-166)
+      const auto& v = c->wing_nodes[q];
+      for (size_t k = 0; k < v.size(); ++k) nodes.push_back(v[k] + w.origin[k % 3]);
+    }
   }
   if (cudaMemcpy(c->d_pos_init, nodes.data(), sizeof(double) * nodes.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_pos, nodes.data(), sizeof(double) * nodes.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -1057,7 +1103,8 @@ int uvlm_velocity_at(uvlm_ctx* c, const double* targets, int64_t n, int32_t incl
   auto run = [&]() -> Error {
     SourceBlock blocks[2];
     int nbk = 0;
-    UVLM_TRY(c->build_sources(true, c->d_wpos, blocks, &nbk));
+    const NBodyPrec prec = c->mixed() ? kNBodyFP32 : kNBodyFP64;
+    UVLM_TRY(c->build_sources(true, c->d_wpos, prec, blocks, &nbk));
     std::vector<double> sx, sy, sz;
     for (int64_t k0 = 0; k0 < n; k0 += c->tcap) {
       const long long cnt = std::min<long long>(c->tcap, n - k0);
@@ -1072,7 +1119,7 @@ int uvlm_velocity_at(uvlm_ctx* c, const double* targets, int64_t n, int32_t incl
       UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_tx, sx.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_ty, sy.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_tz, sz.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
-      UVLM_TRY(c->eval(blocks, nbk, cnt));
+      UVLM_TRY(c->eval(blocks, nbk, cnt, prec));
       UVLM_CUDA_TRY(cudaMemcpyAsync(sx.data(), c->d_vx, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(sy.data(), c->d_vy, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(sz.data(), c->d_vz, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
