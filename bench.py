@@ -22,8 +22,8 @@ roofline    the N-body kernel: 59 FLOP per (target, unique segment) pair of
 cpu_baseline the FP64 CPU oracle (restated reference) on a bounded sample
 
 --impl reference times that CPU oracle alone (the reference cannot be built
-here: its third-party libraries and submodules are absent) on a synthetic
-state of the same shapes.
+here: its third-party libraries and submodules are absent): one complete
+MainLoop at the held-wake state, cut into --steps timed slices.
 """
 from __future__ import annotations
 
@@ -321,26 +321,66 @@ def cpu_threads():
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
 
+def headline_config(wl, world):
+    """The `config` of the headline line, shared by both arms."""
+    learned = bool(wl.weights and os.path.exists(wl.weights))
+    return dict(wl.config(), parallelism=f"replicas x{world}",
+                form=("mixed+learned" if learned else "mixed") + ": FP32 N-body, TF32 tcgen05 LU factored once (dense "
+                     "inverse as the GMRES preconditioner), FP64 matrix and residuals, " +
+                     ("MLP warm start" if learned else "warm start 2 g_n - g_{n-1}"))
+
+
 def run_reference(args, rank, world):
+    """The reference's CPU method (the FP64 oracle restating it; the reference itself cannot be built here),
+    timed on one complete, unsampled MainLoop at the held-wake state of the headline workload, with every
+    host thread on the loops the reference parallelises and the FullPivLU single-threaded as Eigen's.  The
+    MainLoop is cut into --steps consecutive slices of about equal estimated time (every slice runs part of
+    the same loop; all of them together are exactly one MainLoop), one slice per timed step, so the whole
+    run stays within a few minutes: value = 1 MainLoop / (sum of the slice times).  Warm-up: the first
+    --warmup slices of a second MainLoop on a copy of the state, untimed."""
     threads = cpu_threads()
     if rank != 0:
         return
-    state = synthetic_state_np()
-    stride, lu_n = CPU_STRIDE, CPU_LU_N  # the same sample as the cpu_baseline of the GPU arm
-    for _ in range(args.warmup):
-        oracle_sample(_heave_pitch(), state, stride, lu_n, threads)
+    wl = WORKLOADS[args.workload]()
+    state = synthetic_state_np() if wl.name == "heave_pitch" else None
+    if state is None:
+        raise SystemExit("--impl reference runs the headline workload (heave_pitch)")
+
+    def prepared():
+        sim = wl.oracle()
+        sim.set_threads(threads)
+        sim.set_erase_wake_after(wl.wake_rows)
+        sim.begin()
+        sim.set_state(wl.wake_rows, state["wing_pos"], state["wake_pos"], state["wing_gamma"],
+                      state["wing_gamma_prev"], state["wake_gamma"])
+        return sim
+
+    step = wl.wake_rows + 1
+    k = max(1, args.steps)
+    warm = prepared()
+    warm.sliced_begin(step, wl.dt, k, threads)
+    for q in range(min(args.warmup, k)):
+        warm.sliced_run(q, np.zeros(1 + 2 * wl.num))
+    del warm
+    sim = prepared()
+    sim.sliced_begin(step, wl.dt, k, threads)
+    row = np.zeros(1 + 2 * wl.num)
     times = []
-    for _ in range(args.steps):
-        t, _ = oracle_sample(_heave_pitch(), state, stride, lu_n, threads)
-        times.append(t)
-    value = args.steps / float(np.sum(times))
-    sample = (f"one MainLoop per step at the 51,200-ring state: N-body stages (assembly, RHS, loads, RK2 advection) on "
-              f"every {stride}th target scaled x{stride}, FullPivLU on the leading {lu_n}x{lu_n} block scaled by "
-              f"(4096/{lu_n})^3; OpenMP {threads} threads; synthetic convected wake")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+    for q in range(k):
+        t0 = time.perf_counter()
+        sim.sliced_run(q, row)
+        times.append(time.perf_counter() - t0)
+    total = float(np.sum(times))
+    value = 1.0 / total
+    sample = (f"one complete FP64 MainLoop (no sampling, no scaling) at the {wl.num * wl.wake_rows * wl.cols:,}-ring "
+              f"state, cut into {k} consecutive slices timed as the {k} steps (kinematics+shed, CalcMatrix rows, "
+              f"CalcRhs rows, FullPivLU columns single-threaded, load lines, RK2 wake-node ranges); value = 1 "
+              f"MainLoop / sum of slice times ({total:.1f} s); OpenMP {threads} threads; synthetic convected wake")
+    line = {"impl": "reference", "metric": wl.metric, "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * total / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(),
+            "config": headline_config(wl, world),
+            "mainloop_s": total, "slice_s": [round(t, 3) for t in times], "load_row": [float(x) for x in row],
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -521,10 +561,7 @@ def run_ours(args, rank, world, local_rank):
             "metric": wl.metric, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_mx / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": dict(wl.config(), parallelism=f"replicas x{world}",
-                           form=("mixed+learned" if learned else "mixed") + ": FP32 N-body, TF32 tcgen05 LU "
-                                "factored once (dense inverse as the GMRES preconditioner), FP64 matrix and "
-                                "residuals, " + ("MLP warm start" if learned else "warm start 2 g_n - g_{n-1}")),
+            "config": headline_config(wl, world),
             "plain_fp64_steps_per_s": plain, "speedup_vs_plain_fp64": value / world / plain,
             "cl_rel_err": cl_err, "cd_rel_err": cd_err,
             "cl_err_reference": f"plain FP64 GPU form, same {WAKE_ROWS} steps",
@@ -575,7 +612,7 @@ def run_batch(args, rank=0, world=1, local_rank=0):
     import torch
 
     import uvlm_b200 as U
-    from uvlm_b200.batch import case_cost, draw_cases, make_batch, shard_cases
+    from uvlm_b200.batch import case_cost, draw_cases, gather_case_rows, make_batch, shard_cases
 
     all_cases = draw_cases(256, seed=0)
     steps = 150
@@ -613,7 +650,12 @@ def run_batch(args, rank=0, world=1, local_rank=0):
             t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        out[prec] = dict(ms=ms, loads=sim.loads(), launches=launches, per_step=sim.launches_per_step(), clocks=clk,
+        dist_mod = None
+        if world > 1:
+            import torch.distributed as dist_mod
+        # every rank's per-case load rows, gathered into case order (no data moves while stepping)
+        loads_all = gather_case_rows(sim.loads(), mine, len(all_cases), dist_mod)
+        out[prec] = dict(ms=ms, loads=loads_all, launches=launches, per_step=sim.launches_per_step(), clocks=clk,
                          res=sim.solve_stats()[1], factorizations=sim.factorizations())
         sim.close()
     if rank != 0:
@@ -633,7 +675,8 @@ def run_batch(args, rank=0, world=1, local_rank=0):
                        "form": "FP32 N-body, per-case FP32 LU (refactored only when refinement from the "
                                "previous step's factors stalls) + FP64 refinement (residual <= 1e-12)"},
             "plain_fp64_case_steps_per_s": 256 * (steps - 1) / (out["fp64"]["ms"] * 1e-3),
-            "cl_rel_err_max_over_cases": cl_err, "cl_err_scope": f"the {len(cases)} cases of rank 0",
+            "cl_rel_err_max_over_cases": cl_err, "cl_err_scope": f"all {len(all_cases)} cases, gathered from "
+                                                                  f"{world} rank(s)",
             "refinement_residual_max": float(np.max(out["mixed"]["res"])),
             "factorizations": {"mixed": out["mixed"]["factorizations"], "fp64": out["fp64"]["factorizations"],
                                "case_steps": 256 * steps},

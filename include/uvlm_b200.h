@@ -233,6 +233,19 @@ int uvlm_measure_fp32_peak(int32_t device, double* tflops);
 /* Measured FP64 FMA throughput (TFLOP/s): the denominator of the plain FP64
  * form's N-body roofline. */
 int uvlm_measure_fp64_peak(int32_t device, double* tflops);
+/* Every bounded device-side wait of the library (the triangular solves'
+ * block-row flags, the cooperative grid barrier, the tensor-core kernels'
+ * mbarriers) gives up after `cycles` SM clock cycles on `device` (0 restores
+ * the default, about one second), flags the error word and returns; the call
+ * that launched it returns UVLM_ERR_TIMEOUT.  No counterpart in the reference;
+ * a knob for tests of the timeout path. */
+int uvlm_set_wait_limit(int32_t device, int64_t cycles);
+/* Check of the timeout path: one CTA waits (as a triangular-solve block row
+ * waits for the rows before it) for a flag that nothing sets, with a limit of
+ * `cycles`; the wait gives up and this returns UVLM_ERR_TIMEOUT.  The default
+ * limit is restored afterwards and the device stays usable.  No counterpart
+ * in the reference. */
+int uvlm_check_bounded_wait(int32_t device, int64_t cycles);
 /* Name of an N-body tile variant (e.g. "fp32_h4_t2_b128"), "?" if out of range. */
 const char* uvlm_nbody_variant_name(int32_t variant);
 /* Algorithmic work of the last step: unique-segment interactions of every
@@ -401,6 +414,12 @@ int uvlm_mlp_set_params(uvlm_mlp* mlp, const float* params);
 int uvlm_mlp_set_normalization(uvlm_mlp* mlp, const float* mean, const float* stdev, float out_scale);
 /* Host arrays: x [n][8], y [n]. */
 int uvlm_mlp_forward(uvlm_mlp* mlp, const float* x, int64_t n, float* y);
+/* The same network on the tcgen05 tensor cores (the inference the time-
+ * stepper uses for UVLM_WARM_MLP): the hidden layers take BF16 activations
+ * and BF16 weights with FP32 accumulation in TMEM, so y differs from
+ * uvlm_mlp_forward (FP32 activations) at the BF16 level.  UVLM_ERR_UNSUPPORTED
+ * off sm_100 devices. */
+int uvlm_mlp_forward_tc(uvlm_mlp* mlp, const float* x, int64_t n, float* y);
 /* Mean-square loss on (prediction - target)/out_scale and its gradient with
  * respect to every parameter (same layout as the parameters). */
 int uvlm_mlp_gradients(uvlm_mlp* mlp, const float* x, const float* target, int64_t n, float* grads, double* loss);

@@ -37,7 +37,7 @@ def test_shard_cases_balances_work():
 def _rank(rank, world, port, out_dir):
     import torch.distributed as dist
 
-    from uvlm_b200.batch import case_cost, draw_cases, shard_cases
+    from uvlm_b200.batch import case_cost, draw_cases, gather_case_rows, shard_cases
 
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     cases = draw_cases(256, seed=0)
@@ -47,10 +47,16 @@ def _rank(rank, world, port, out_dir):
     # the union is the whole sweep exactly once
     got = [None] * world
     dist.all_gather_object(got, (mine, sum(costs[i] for i in mine)))
+    # per-case load rows (t, CD, CL) of this rank's cases, as a batch returns
+    # them ([steps][cases][3]), gathered into case order on every rank
+    steps = 5
+    rows = np.array([[[s * 0.1, 1e-3 * c + s, -c - 1e-4 * s] for c in mine] for s in range(steps)])
+    full = gather_case_rows(rows, mine, 256, dist)
     if rank == 0:
         seen = sorted(i for m, _ in got for i in m)
         np.save(os.path.join(out_dir, "seen.npy"), np.array(seen))
         np.save(os.path.join(out_dir, "work.npy"), np.array([w for _, w in got]))
+        np.save(os.path.join(out_dir, "rows.npy"), full)
     dist.barrier()
     dist.destroy_process_group()
 
@@ -68,3 +74,18 @@ def test_case_sharding_world_size_two(tmp_path):
     work = np.load(tmp_path / "work.npy")
     assert list(seen) == list(range(256))
     assert abs(work[0] - work[1]) / work.sum() < 0.02
+    rows = np.load(tmp_path / "rows.npy")
+    c = np.arange(256)
+    expect = np.array([np.stack([np.full(256, s * 0.1), 1e-3 * c + s, -c - 1e-4 * s], -1) for s in range(5)])
+    np.testing.assert_array_equal(rows, expect)
+
+
+def test_gather_case_rows_single_process_needs_every_case():
+    import pytest
+
+    from uvlm_b200.batch import gather_case_rows
+
+    rows = np.arange(12.0).reshape(2, 2, 3)
+    np.testing.assert_array_equal(gather_case_rows(rows, [1, 0], 2), rows[:, ::-1])
+    with pytest.raises(ValueError):
+        gather_case_rows(rows, [0, 1], 3)

@@ -1,0 +1,81 @@
+"""The benchmark workloads at full size against the FP64 oracle (needs a B200).
+
+The fixtures (tests/golden/{heave_pitch_32x128,tandem4_16x64,morphing_24x96}.npz,
+made by tests/golden/make_fullsize.py) hold the oracle's load rows of every
+step of a window from step 0, its circulations every 10 steps and its final
+wake.  The plain FP64 form must reproduce them to rounding; the mixed form
+(FP32 N-body, TF32 tensor-core LU as the stale preconditioner of an FP64
+GMRES, learned warm start where the workload has trained weights) is held to
+the north-star bound, CL and CD within 1e-6 of max |C| over the window.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(HERE, "golden"))
+sys.path.insert(0, ROOT)
+
+from cases import FULLSIZE, make_gpu_sim  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+NAMES = [n for n in FULLSIZE if os.path.exists(os.path.join(HERE, "golden", f"{n}.npz"))]
+WEIGHTS = {"heave_pitch_32x128": "warmstart_heave_pitch_32x128.npz", "morphing_24x96": "warmstart_morphing_24x96.npz"}
+
+
+def rel_to_max(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _run(name, **kw):
+    case = FULLSIZE[name]
+    fx = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    sim = make_gpu_sim(case, max_wake_rows=case["steps"] + 8, **kw)
+    sim.begin()
+    rows, gammas = [], {}
+    keep = set(int(s) for s in fx["gamma_steps"])
+    for s in range(case["steps"]):
+        rows.append(sim.step(s, case["dt"]))
+        if s in keep:
+            gammas[s] = sim.state()["wing_gamma"]
+    st = sim.state()
+    sim.close()
+    return fx, np.array(rows), gammas, st
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fullsize_fp64_matches_oracle(name):
+    fx, rows, gammas, st = _run(name)
+    np.testing.assert_array_equal(rows[:, 0], fx["loads"][:, 0])
+    err = rel_to_max(rows[:, 1:], fx["loads"][:, 1:])
+    gerr = max(rel_to_max(gammas[int(s)], g) for s, g in zip(fx["gamma_steps"], fx["gammas"]))
+    werr = float(np.max(np.abs(st["wake_pos"] - fx["wake_pos"])))
+    print(f"{name} FP64 vs oracle: loads {err:.2e}, circulation {gerr:.2e}, wake nodes {werr:.2e}")
+    assert err < 1e-8
+    assert gerr < 1e-9
+    assert st["wake_pos"].shape == fx["wake_pos"].shape and werr < 1e-9
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fullsize_mixed_within_1e6_of_oracle(name):
+    from uvlm_b200.warmstart import MLP
+
+    wts = WEIGHTS.get(name)
+    kw = dict(precision="mixed", solver="gmres_stale", warm_start="mlp" if wts else "extrapolate")
+    case = FULLSIZE[name]
+    fx = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    sim = make_gpu_sim(case, max_wake_rows=case["steps"] + 8, **kw)
+    if wts:
+        sim.set_mlp(MLP.load(os.path.join(ROOT, "uvlm_b200", "weights", wts)))
+    sim.begin()
+    rows = np.array([sim.step(s, case["dt"]) for s in range(case["steps"])])
+    sim.close()
+    num = len(case["wings"])
+    cl = max(rel_to_max(rows[:, 2 + 2 * n], fx["loads"][:, 2 + 2 * n]) for n in range(num))
+    cd = max(rel_to_max(rows[:, 1 + 2 * n], fx["loads"][:, 1 + 2 * n]) for n in range(num))
+    print(f"{name} mixed vs oracle over steps 0-{case['steps'] - 1}: CL {cl:.2e}, CD {cd:.2e}")
+    assert cl <= 1e-6 and cd <= 1e-6

@@ -53,6 +53,45 @@ def test_mlp_forward_and_gradients_match_autograd():
     assert np.max(np.abs(g - g_ref)) <= 1e-4 * np.max(np.abs(g_ref))
 
 
+def _torch_forward_bf16_activations(net, X):
+    """FP64 forward of the same network with the BF16 rounding the tensor cores see: BF16 weights of every
+    layer, and the hidden layers' inputs (the GELU outputs of layers 1 and 2) rounded to BF16."""
+    import torch
+
+    h = (torch.tensor(X, dtype=torch.float64) - torch.tensor(net.mean, dtype=torch.float64)) / torch.tensor(
+        net.std, dtype=torch.float64)
+    for i, (W, b) in enumerate(net.layers()):
+        if i in (1, 2):
+            h = h.to(torch.float32).to(torch.bfloat16).to(torch.float64)
+        z = h @ torch.tensor(W).to(torch.bfloat16).to(torch.float64) + torch.tensor(b, dtype=torch.float64)
+        h = 0.5 * z * (1 + torch.erf(z / math.sqrt(2))) if i < 3 else z
+    return h[:, 0].numpy() * net.out_scale
+
+
+@pytest.mark.parametrize("n", [1, 128, 1000, 4096])
+def test_mlp_tensor_core_inference_matches_fp64_reference(n):
+    """The tcgen05 inference (BF16 activations, FP32 accumulation in TMEM) against FP64 autograd-free
+    references: with the same BF16 roundings to 2e-3 of max |y|, and against the FP32-activation network (the
+    SIMT forward and FP64 with exact activations) to the BF16 activation level, 2e-2 of max |y|."""
+    import os
+
+    from uvlm_b200.warmstart import MLP
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    net = MLP.load(os.path.join(root, "uvlm_b200", "weights", "warmstart_heave_pitch_32x128.npz"))
+    rng = np.random.default_rng(n)
+    X = (net.mean + net.std * rng.standard_normal((n, 8))).astype(np.float32)
+    y_tc = net.forward_tc(X)
+    y_simt = net.forward(X)
+    y_bf = _torch_forward_bf16_activations(net, X)
+    _, _, y_fp = _torch_reference(net, X, np.zeros(n, np.float32))
+    scale = max(np.max(np.abs(y_fp)), 1e-30)
+    assert np.all(np.isfinite(y_tc))
+    assert np.max(np.abs(y_tc - y_bf)) <= 2e-3 * scale
+    assert np.max(np.abs(y_tc - y_fp)) <= 2e-2 * scale
+    assert np.max(np.abs(y_tc - y_simt)) <= 2e-2 * scale
+
+
 def test_mlp_training_fits_a_smooth_target():
     from uvlm_b200.warmstart import MLP
 

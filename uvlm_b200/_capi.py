@@ -95,6 +95,8 @@ SIGNATURES = [
     ("uvlm_status_string", C.c_char_p, [C.c_int]),
     ("uvlm_add_wing", C.c_int, [_V, C.POINTER(WingDesc), C.POINTER(Kinematics)]),
     ("uvlm_add_wing_nodes", C.c_int, [_V, _I, _I, _P, C.c_double, C.c_double, _P, C.POINTER(Kinematics)]),
+    ("uvlm_set_wait_limit", C.c_int, [C.c_int32, _I]),
+    ("uvlm_check_bounded_wait", C.c_int, [C.c_int32, _I]),
     ("uvlm_set_forward_flight", C.c_int, [_V, _P]),
     ("uvlm_set_advection", C.c_int, [_V, C.c_char_p]),
     ("uvlm_begin", C.c_int, [_V]),
@@ -154,6 +156,7 @@ SIGNATURES = [
     ("uvlm_mlp_set_params", C.c_int, [_V, C.POINTER(C.c_float)]),
     ("uvlm_mlp_set_normalization", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float]),
     ("uvlm_mlp_forward", C.c_int, [_V, C.POINTER(C.c_float), _I, C.POINTER(C.c_float)]),
+    ("uvlm_mlp_forward_tc", C.c_int, [_V, C.POINTER(C.c_float), _I, C.POINTER(C.c_float)]),
     ("uvlm_mlp_gradients", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.POINTER(C.c_float),
                                      _P]),
     ("uvlm_mlp_train", C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.c_int32, C.c_int32,

@@ -197,6 +197,27 @@ def shard_cases(costs, world: int) -> list[list[int]]:
     return [sorted(p) for p in parts]
 
 
+def gather_case_rows(rows, mine, n_cases: int, dist=None):
+    """Per-case result rows of every rank in case order.  rows: [steps][len(mine)][...] of this rank's
+    cases `mine` (from shard_cases); returns [steps][n_cases][...] on every rank (the all-gather of
+    torch.distributed when `dist` is given and initialised, else this rank's rows alone must cover
+    every case)."""
+    rows = np.asarray(rows)
+    parts = [(list(mine), rows)]
+    if dist is not None and dist.is_initialized() and dist.get_world_size() > 1:
+        got = [None] * dist.get_world_size()
+        dist.all_gather_object(got, (list(mine), rows))
+        parts = got
+    out = np.zeros((rows.shape[0], n_cases) + rows.shape[2:], dtype=rows.dtype)
+    seen = np.zeros(n_cases, dtype=bool)
+    for idx, r in parts:
+        out[:, idx] = r
+        seen[idx] = True
+    if not seen.all():
+        raise ValueError("the gathered shards do not cover every case")
+    return out
+
+
 def make_batch(cases: list[dict], precision: str = "mixed", advection: str = "euler", max_steps: int = 151,
                device: int = 0, use_graph: bool = True, stale_factors: bool = True) -> BatchSimulator:
     sim = BatchSimulator(precision=precision, advection=advection, max_steps=max_steps, device=device,

@@ -114,7 +114,9 @@ struct uvlm_ctx {
   long long collect_cap = 0, collect_n = 0;
   float* d_collect_x = nullptr;
   float* d_collect_t = nullptr;
+  Error warm_phase(double t);
   Error warm_features(double t);
+  bool mlp_tc_used = false;  // this step's guess came from the tensor-core inference
   uvlm_step_stats last{};
   double work_nbody = 0, work_asm = 0, work_lu = 0;
   cudaEvent_t ev[8] = {};
@@ -229,7 +231,7 @@ Error uvlm_ctx::alloc_all() {
   UVLM_CUDA_TRY(cudaMemset(d_rhs_prev, 0, sizeof(double) * N));
   UVLM_TRY(dalloc(&d_flags, 4));
   UVLM_CUDA_TRY(cudaMallocHost(&h_row, sizeof(double) * (1 + 2 * num)));
-  UVLM_CUDA_TRY(cudaMallocHost(&h_flags, sizeof(int) * 8));
+  UVLM_CUDA_TRY(cudaMallocHost(&h_flags, sizeof(int) * 12));
   // N-body scratch: records for bound + wake sheets, per-split partial sums
   nb.records_cap = (long long)(nn + wn) * (long long)sizeof(RecD);
   UVLM_CUDA_TRY(cudaMalloc(&nb.records, nb.records_cap));
@@ -374,9 +376,18 @@ Error uvlm_ctx::solve(long long step) {
     UVLM_TRY(launch_extrapolate(d_gamma, d_gamma_prev, d_gamma_hist, N, st));
   if (cfg.warm_start == UVLM_WARM_MLP && step >= 2) {
     if (!mlp) return fail(kErrState, "warm_start MLP needs uvlm_set_mlp");
-    UVLM_TRY(warm_features(step * cur_dt));
-    UVLM_TRY(mlp_forward(mlp_of(mlp), d_feat, N, d_mlp_y, st));
-    UVLM_TRY(mlp_apply_guess(N, d_gamma_prev, d_gamma_hist, d_mlp_y, d_gamma, st));
+    if (mlp_tc_available()) {
+      // features, the three hidden layers on the tensor cores, the head and
+      // the guess in one kernel
+      UVLM_TRY(warm_phase(step * cur_dt));
+      UVLM_TRY(mlp_guess_tc(mlp_of(mlp), num, R, C, d_gamma_prev, d_gamma_hist, d_rhs, d_rhs_prev, d_phase, d_gamma,
+                            st));
+      mlp_tc_used = true;
+    } else {
+      UVLM_TRY(warm_features(step * cur_dt));
+      UVLM_TRY(mlp_forward(mlp_of(mlp), d_feat, N, d_mlp_y, st));
+      UVLM_TRY(mlp_apply_guess(N, d_gamma_prev, d_gamma_hist, d_mlp_y, d_gamma, st));
+    }
   }
   const float* A32 = cfg.assembly_fp64 ? nullptr : d_A32;
   const double* A64 = cfg.assembly_fp64 ? d_A64 : nullptr;
@@ -459,7 +470,7 @@ Error uvlm_ctx::advect(double dt) {
 // previous solution), G_{n-1}, the new and the previous RHS and the phase of
 // each wing's dominant motion (first non-zero angular frequency of plug,
 // flap, twist, bend).
-Error uvlm_ctx::warm_features(double t) {
+Error uvlm_ctx::warm_phase(double t) {
   for (int n = 0; n < num; ++n) {
     const uvlm_kinematics& k = kins[n];
     const double om[4] = {k.plug_omega, k.flap_omega, k.twist_omega, k.bend_omega};
@@ -472,6 +483,11 @@ Error uvlm_ctx::warm_features(double t) {
     h_phase[n] = w * t;
   }
   UVLM_CUDA_TRY(cudaMemcpyAsync(d_phase, h_phase, sizeof(double) * num, cudaMemcpyHostToDevice, st));
+  return ok();
+}
+
+Error uvlm_ctx::warm_features(double t) {
+  UVLM_TRY(warm_phase(t));
   return mlp_features(num, R, C, d_gamma_prev, d_gamma_hist, d_rhs, d_rhs_prev, d_phase, d_feat, st);
 }
 
@@ -592,9 +608,18 @@ Error uvlm_ctx::stage_advect(double* row) {
   UVLM_CUDA_TRY(cudaMemcpyAsync(h_row, d_row, sizeof(double) * (1 + 2 * num), cudaMemcpyDeviceToHost, st));
   UVLM_CUDA_TRY(cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
   UVLM_CUDA_TRY(cudaMemcpyAsync(h_flags + 4, lu.err, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  h_flags[8] = 0;
+  Mlp* tcm = mlp_tc_used && mlp ? mlp_of(mlp) : nullptr;
+  if (tcm && tcm->tc_err)
+    UVLM_CUDA_TRY(cudaMemcpyAsync(h_flags + 8, tcm->tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  mlp_tc_used = false;
   mark(7);
   UVLM_CUDA_TRY(cudaStreamSynchronize(st));
   if (h_flags[4]) return fail(kErrTimeout, "a bounded device wait in the dense solve gave up");
+  if (h_flags[8]) {
+    UVLM_CUDA_TRY(cudaMemset(tcm->tc_err, 0, sizeof(int)));
+    return fail(kErrTimeout, "a bounded device wait of the tensor-core warm start gave up");
+  }
   if (h_flags[5]) return fail(kErrSingular, "zero pivot in the LU factorisation");
   if (h_flags[0]) return fail(kErrNonFinite, "non-finite circulation after the solve");
   if (!cfg.compute_loads) {
@@ -1087,6 +1112,25 @@ int uvlm_measure_fp32_peak(int32_t device, double* tflops) {
   if (!tflops) return set_global(fail(kErrInvalid, "NULL argument"));
   if (cudaSetDevice(device) != cudaSuccess) return set_global(fail(kErrCuda, "cudaSetDevice failed"));
   return set_global(measure_fp32_fma_peak(device_sms(device), tflops));
+}
+
+int uvlm_set_wait_limit(int32_t device, int64_t cycles) {
+  if (cycles < 0) return set_global(fail(kErrInvalid, "negative wait limit"));
+  if (cudaSetDevice(device) != cudaSuccess) return set_global(fail(kErrCuda, "cudaSetDevice failed"));
+  Error e = lu_set_wait_limit((long long)cycles);
+  if (!e.code) e = tc_set_wait_limit((long long)cycles);
+  if (!e.code) e = mlp_tc_set_wait_limit((long long)cycles);
+  return set_global(e);
+}
+
+int uvlm_check_bounded_wait(int32_t device, int64_t cycles) {
+  if (cycles <= 0) return set_global(fail(kErrInvalid, "the wait limit must be positive"));
+  if (cudaSetDevice(device) != cudaSuccess) return set_global(fail(kErrCuda, "cudaSetDevice failed"));
+  bool gave_up = false;
+  const Error e = lu_wait_probe((long long)cycles, &gave_up);
+  if (e.code) return set_global(e);
+  if (gave_up) return set_global(fail(kErrTimeout, "a bounded device wait gave up (as intended by the check)"));
+  return UVLM_OK;
 }
 
 int uvlm_measure_fp64_peak(int32_t device, double* tflops) {

@@ -89,7 +89,19 @@ __host__ __device__ inline d3 normalized(d3 a) {
 __device__ inline d3 ld3(const double* p) { return d3{p[0], p[1], p[2]}; }
 __device__ inline void st3(double* p, d3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
 
-// Bounded wait used by every spin loop: gives up after ~kSpinLimitCycles.
-constexpr long long kSpinLimitCycles = 4000000000LL;  // ~2 s at 2 GHz
+// Bounded waits: every spin loop and mbarrier wait of the library gives up
+// after g_wait_limit clock cycles (default ~1 s at 2 GHz), sets an error word
+// that the host turns into UVLM_ERR_TIMEOUT, and leaves the kernel.  The
+// library is built without relocatable device code, so each translation unit
+// holds its own copy of the limit; uvlm_set_wait_limit updates all of them
+// through the per-unit setters below.
+constexpr long long kDefaultWaitCycles = 2000000000LL;
+static __device__ long long g_wait_limit = kDefaultWaitCycles;
+// This translation unit's copy of the limit, on the current device.
+static inline Error set_wait_limit_here(long long cycles) {
+  const long long v = cycles > 0 ? cycles : kDefaultWaitCycles;
+  UVLM_CUDA_TRY(cudaMemcpyToSymbol(g_wait_limit, &v, sizeof(v)));
+  return ok();
+}
 
 }  // namespace uvlm

@@ -10,7 +10,7 @@ namespace uvlm {
 namespace {
 
 // Grid-wide barrier for cooperative launches.  bar[0] = arrival count,
-// bar[1] = generation.  The wait is bounded: after kSpinLimitCycles the
+// bar[1] = generation.  The wait is bounded: after g_wait_limit cycles the
 // waiter sets err[0] (abort) and every CTA leaves at its next barrier.
 __device__ bool grid_sync(unsigned* bar, unsigned nblocks, int* err) {
   __shared__ int s_ok;
@@ -27,10 +27,10 @@ __device__ bool grid_sync(unsigned* bar, unsigned nblocks, int* err) {
       __threadfence();
       atomicAdd(bar + 1, 1u);
     } else {
-      const long long t0 = clock64();
+      const long long t0 = clock64(), lim = g_wait_limit;
       while (*vgen == g) {
         if (verr[0]) { okv = 0; break; }
-        if (clock64() - t0 > kSpinLimitCycles) { atomicExch(err, 1); okv = 0; break; }
+        if (clock64() - t0 > lim) { atomicExch(err, 1); okv = 0; break; }
         __nanosleep(32);
       }
     }
@@ -494,11 +494,11 @@ __device__ int wait_ready(const unsigned* flags, int first, int left, bool lower
   if (threadIdx.x == 0) {
     const volatile unsigned* vf = flags;
     const int b0 = lower ? first : nblk - 1 - first;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), lim = g_wait_limit;
     int cnt = 1;
     while (vf[b0] != epoch) {
       if (((volatile int*)err)[0]) { cnt = 0; break; }
-      if (clock64() - t0 > kSpinLimitCycles) { atomicExch(err + 2, 1); atomicExch(err, 1); cnt = 0; break; }
+      if (clock64() - t0 > lim) { atomicExch(err + 2, 1); atomicExch(err, 1); cnt = 0; break; }
       __nanosleep(32);
     }
     if (cnt) {
@@ -589,6 +589,11 @@ __global__ void __launch_bounds__(256) trsv_kernel(const T* __restrict__ LU, int
   __syncthreads();
   if (tid == 0) atomicExch(flags + I, epoch);
 }
+
+// Check of the bounded waits: one CTA waits, as a block row of the
+// triangular solves waits for the rows before it, for a flag that nothing
+// publishes; the wait must give up and report through err.
+__global__ void wait_probe_kernel(const unsigned* flags, int* err) { wait_ready(flags, 0, 1, true, 1, 1u, err); }
 
 template <class T>
 Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
@@ -925,6 +930,37 @@ Error gemm_update_f32_simt(float* C, int ldc, const float* A, int lda, const flo
   dim3 grid(ceil_div(nc, 64), ceil_div(m, 64));
   gemm_update_kernel<float><<<grid, 256, 0, st>>>(C, ldc, A, lda, B, ldb, m, nc, k);
   UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+Error lu_set_wait_limit(long long cycles) { return set_wait_limit_here(cycles); }
+
+Error lu_wait_probe(long long cycles, bool* gave_up) {
+  unsigned* flags = nullptr;
+  int* err = nullptr;
+  UVLM_CUDA_TRY(cudaMalloc(&flags, 64 * sizeof(unsigned)));
+  const cudaError_t e = cudaMalloc(&err, 4 * sizeof(int));
+  if (e != cudaSuccess) {
+    cudaFree(flags);
+    return fail(kErrCuda, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  int h[4] = {0, 0, 0, 0};
+  Error r = set_wait_limit_here(cycles);
+  if (!r.code) {
+    cudaMemset(flags, 0, 64 * sizeof(unsigned));
+    cudaMemset(err, 0, 4 * sizeof(int));
+    wait_probe_kernel<<<1, 64>>>(flags, err);
+    note_launch();
+    cudaError_t k = cudaGetLastError();
+    if (k == cudaSuccess) k = cudaMemcpy(h, err, sizeof(h), cudaMemcpyDeviceToHost);
+    if (k != cudaSuccess) r = fail(kErrCuda, std::string("wait probe: ") + cudaGetErrorString(k));
+  }
+  const Error restore = set_wait_limit_here(0);
+  cudaFree(flags);
+  cudaFree(err);
+  if (r.code) return r;
+  if (restore.code) return restore;
+  *gave_up = h[0] != 0 && h[2] != 0;
   return ok();
 }
 

@@ -88,5 +88,11 @@ Error gemm_update_f32_simt(float* C, int ldc, const float* A, int lda, const flo
 Error gemm_update_tc(float* C, int ldc, const float* A, int lda, const float* Bt, int ldbt, int m, int nc, int k,
                      LuUpdate kind, LuWork* w, cudaStream_t st);
 bool gemm_tc_available();
+// The bounded-wait limit of this unit's kernels (0 = default), and a check
+// that a wait on a flag nothing sets gives up after `cycles` (restores the
+// default limit afterwards).
+Error lu_set_wait_limit(long long cycles);
+Error tc_set_wait_limit(long long cycles);
+Error lu_wait_probe(long long cycles, bool* gave_up);
 
 }  // namespace uvlm

@@ -16,6 +16,7 @@
 #include <mutex>
 
 #include "lu.cuh"
+#include "tc_common.cuh"
 
 namespace uvlm {
 namespace {
@@ -23,54 +24,6 @@ namespace {
 constexpr int kBM = 128;
 constexpr int kBN = 128;
 constexpr int kRowBytes = 128;  // one swizzle row: 32 FP32 / 64 BF16 elements of K
-constexpr long long kWaitCycles = 2000000000LL;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// Bounded wait on an mbarrier phase; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles) return false;
-  }
-  return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// Shared-memory descriptor of a K-major operand tile in the canonical
-// 128-byte-swizzle layout: 8-row atoms of 1024 B (stride byte offset), SM100
-// descriptor version 1, layout type 2 (SWIZZLE_128B).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset: next 8-row group
-  d |= (uint64_t)1 << 46;              // version
-  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
-  return d;
-}
 
 // Instruction descriptor: FP32 accumulator, A/B format (2 = TF32, 1 = BF16),
 // both K-major, N = kBN, M = kBM.
@@ -220,8 +173,12 @@ __global__ void to_bf16_rows(const float* src, int ld, int rows, int k, __nv_bfl
   }
 }
 
+}  // namespace
+
+namespace {
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
+}  // namespace
 
 bool load_encoder() {
   std::call_once(g_encode_once, [] {
@@ -248,7 +205,8 @@ Error encode_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dt, int 
   return ok();
 }
 
-}  // namespace
+
+Error tc_set_wait_limit(long long cycles) { return set_wait_limit_here(cycles); }
 
 bool gemm_tc_available() {
   int dev = 0, major = 0, minor = 0;

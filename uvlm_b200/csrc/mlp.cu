@@ -263,6 +263,8 @@ void mlp_free(Mlp* m) {
   cudaFree(m->dact);
   cudaFree(m->y);
   cudaFree(m->dy);
+  cudaFree(m->wT);
+  cudaFree(m->tc_err);
   *m = Mlp{};
 }
 
@@ -285,6 +287,7 @@ Error mlp_reserve(Mlp* m, long long B) {
 }
 
 Error mlp_sync_bf16(Mlp* m, cudaStream_t st) {
+  m->version += 1;
   to_bf16<<<g1((long long)m->n_params), 256, 0, st>>>(m->master, m->n_params, m->wbf);
   UVLM_LAUNCH_CHECK();
   return ok();
@@ -360,6 +363,7 @@ Error mlp_loss_backward(Mlp* m, const float* x, const float* target, long long B
 
 Error mlp_adam_step(Mlp* m, float lr, cudaStream_t st) {
   m->adam_t += 1;
+  m->version += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - (float)std::pow(b1, (double)m->adam_t);
   const float c2 = 1.f - (float)std::pow(b2, (double)m->adam_t);

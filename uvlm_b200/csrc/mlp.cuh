@@ -10,6 +10,7 @@
 // and Adam are hand-written kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -46,6 +47,13 @@ struct Mlp {
   float* y = nullptr;     // [cap]
   float* dy = nullptr;    // [cap]
   double* loss = nullptr; // [1]
+  // tensor-core inference (mlp_tc.cu): K-major BF16 copies of the two hidden
+  // 256 x 256 weight matrices and their TMA maps, rebuilt when the weights
+  // change (version counts the changes of wbf)
+  long long version = 0, wT_version = -1;
+  __nv_bfloat16* wT = nullptr;  // [2][256][256]
+  CUtensorMap tmap[2];
+  int* tc_err = nullptr;        // a bounded wait of the inference kernel gave up
 };
 
 Error mlp_create(Mlp* m, unsigned long long seed);
@@ -58,6 +66,19 @@ Error mlp_loss_backward(Mlp* m, const float* x, const float* target, long long B
                         cudaStream_t st);
 Error mlp_adam_step(Mlp* m, float lr, cudaStream_t st);
 Error mlp_sync_bf16(Mlp* m, cudaStream_t st);
+
+// Tensor-core inference (tcgen05, BF16 operands, FP32 accumulation), fused:
+// y = out_scale * net((x - mean)/std) for feature rows x [B][kMlpIn] ...
+Error mlp_forward_tc(Mlp* m, const float* x, long long B, float* y, cudaStream_t st);
+// ... or straight from the solver state (the features of mlp_features) to
+// the initial guess x0 = 2 g_n - g_{n-1} + y of every panel.
+Error mlp_guess_tc(Mlp* m, int num, int R, int C, const double* g_n, const double* g_nm1, const double* b_np1,
+                   const double* b_n, const double* phase, double* x0, cudaStream_t st);
+// UVLM_ERR_TIMEOUT if a bounded wait of the inference kernel gave up since
+// the last check (synchronises the stream).
+Error mlp_tc_check(Mlp* m, cudaStream_t st);
+bool mlp_tc_available();
+Error mlp_tc_set_wait_limit(long long cycles);
 
 // Features of all N panels for predicting step n+1 (see the header comment),
 // written as [N][kMlpIn] FP32.  phase[n] = phase of wing n at t_{n+1}.

@@ -2,6 +2,8 @@
 // normalisation, forward, gradients (for checks against autograd) and
 // training on (features, target) pairs collected from the solver.
 #include <algorithm>
+#include <climits>
+#include <cstdint>
 #include <numeric>
 #include <random>
 #include <vector>
@@ -100,6 +102,23 @@ int uvlm_mlp_forward(uvlm_mlp* h, const float* x, int64_t n, float* y) {
     UVLM_CUDA_TRY(cudaMalloc(&dy.p, sizeof(float) * n));
     UVLM_CUDA_TRY(cudaMemcpy(dx.p, x, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice));
     UVLM_TRY(mlp_forward(&h->m, (const float*)dx.p, n, (float*)dy.p, 0));
+    UVLM_CUDA_TRY(cudaMemcpy(y, dy.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    return ok();
+  };
+  return report(run());
+}
+
+int uvlm_mlp_forward_tc(uvlm_mlp* h, const float* x, int64_t n, float* y) {
+  if (!h || !x || !y || n < 0 || n > INT32_MAX) return report(fail(kErrInvalid, "invalid argument"));
+  if (n == 0) return UVLM_OK;
+  if (!mlp_tc_available()) return report(fail(kErrUnsupported, "tcgen05 inference needs an sm_100 device"));
+  auto run = [&]() -> Error {
+    DevBuf dx, dy;
+    UVLM_CUDA_TRY(cudaMalloc(&dx.p, sizeof(float) * n * kMlpIn));
+    UVLM_CUDA_TRY(cudaMalloc(&dy.p, sizeof(float) * n));
+    UVLM_CUDA_TRY(cudaMemcpy(dx.p, x, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice));
+    UVLM_TRY(mlp_forward_tc(&h->m, (const float*)dx.p, n, (float*)dy.p, 0));
+    UVLM_TRY(mlp_tc_check(&h->m, 0));
     UVLM_CUDA_TRY(cudaMemcpy(y, dy.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
     return ok();
   };

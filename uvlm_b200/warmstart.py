@@ -80,6 +80,14 @@ class MLP:
         check(lib().uvlm_mlp_forward(self._h, _pf(X), X.shape[0], _pf(y)))
         return y
 
+    def forward_tc(self, X) -> np.ndarray:
+        """The same network on the tcgen05 tensor cores (BF16 activations in the hidden layers): the inference
+        the time-stepper uses for its learned warm start."""
+        X = _f32(X).reshape(-1, N_FEATURES)
+        y = np.zeros(X.shape[0], np.float32)
+        check(lib().uvlm_mlp_forward_tc(self._h, _pf(X), X.shape[0], _pf(y)))
+        return y
+
     def gradients(self, X, T):
         X = _f32(X).reshape(-1, N_FEATURES)
         T = _f32(T).reshape(-1)
