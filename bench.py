@@ -438,8 +438,6 @@ def run_ours(args, rank, world, local_rank):
                 st_ = sm.stats()
                 abl[name][0].append(st_.initial_residual)
                 abl[name][1].append(st_.gmres_iters)
-    if simex:
-        simex.close()
     preroll_s = time.time() - t0
     warm_ablation = {k: {"initial_residual_mean": float(np.mean(v[0])), "gmres_iters_total": int(np.sum(v[1])),
                          "steps": len(v[1])} for k, v in abl.items() if v[1]}
@@ -473,9 +471,12 @@ def run_ours(args, rank, world, local_rank):
     # --- warm-up and timed steps ---------------------------------------------
     s_mx = torch.cuda.ExternalStream(simmx.stream(), device=dev)
     s_64 = torch.cuda.ExternalStream(sim64.stream(), device=dev)
+    s_ex = torch.cuda.ExternalStream(simex.stream(), device=dev) if simex else None
     for i in range(args.warmup):
         simmx.step(step0 + i, DT)
         sim64.step(step0 + i, DT)
+        if simex:
+            simex.step(step0 + i, DT)
     step0 += args.warmup
     if world > 1:
         dist.barrier()
@@ -487,6 +488,10 @@ def run_ours(args, rank, world, local_rank):
     launches = U.lib().uvlm_kernel_launch_count() - launches0
     clk = clocks.stop()
     t_64, _ = timed_steps(sim64, step0, args.steps, flush, torch, s_64)
+    # the same steps without the network (warm start 2 g_n - g_{n-1}), timed alike
+    t_ex = timed_steps(simex, step0, args.steps, flush, torch, s_ex)[0] if simex else None
+    if simex:
+        simex.close()
     st = simmx.stats()
     total_mx = float(np.sum(t_mx))
     if world > 1:
@@ -530,6 +535,13 @@ def run_ours(args, rank, world, local_rank):
     pk64 = C.c_double()
     U._capi.check(U.lib().uvlm_measure_fp64_peak(dev, C.byref(pk64)))
     achieved64 = FLOP_PER_PAIR * pairs64.value / (nbody_ms64 * 1e-3) / 1e12
+    # assembly (CalcMatrix): N collocation points x the wing lattices' unique
+    # segments, 59 FLOP each, over the stage's device time; the mixed form
+    # assembles its residual matrix in FP64 every step (the FP32 matrix only
+    # when it factors), so the FP64 probe is the denominator
+    n_panels = wl.num * ROWS * COLS
+    asm_pairs = n_panels * wl.num * ((ROWS + 1) * COLS + ROWS * (COLS + 1))
+    asm_tflops = FLOP_PER_PAIR * asm_pairs / (stage_ms[1] * 1e-3) / 1e12
 
     # --- end-to-end through the C-ABI with host buffers ------------------------
     e2e_t = []
@@ -541,6 +553,27 @@ def run_ours(args, rank, world, local_rank):
         e2e_t.append(time.perf_counter() - t1)
     step0 += args.steps
     e2e_value = world * args.steps / float(np.sum(e2e_t))
+
+    # --- the fine-grained drop-in: advect::Advection::Advect with host sheets ----
+    # (the call a reference caller swaps first), at the held wake, mixed form:
+    # every call copies the wing and wake sheets in and the advected wake out
+    st_adv = simmx.state()
+    adv = U.AdvectFactory(wl.advection, precision="mixed")
+    nxt = np.empty_like(st_adv["wake_pos"])
+    ff = np.array([-1.0, 0.0, 0.0])
+    for _ in range(2):
+        adv.Advect(st_adv["wing_pos"], st_adv["wing_gamma"], st_adv["wake_pos"], st_adv["wake_gamma"], ff, DT, nxt)
+    adv_t = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        adv.Advect(st_adv["wing_pos"], st_adv["wing_gamma"], st_adv["wake_pos"], st_adv["wake_gamma"], ff, DT, nxt)
+        adv_t.append(time.perf_counter() - t1)
+    del adv
+    adv_in = sum(st_adv[k].nbytes for k in ("wing_pos", "wing_gamma", "wake_pos", "wake_gamma"))
+    e2e_advect = {"value": args.steps / float(np.sum(adv_t)), "unit": "Advect calls/s",
+                  "h2d_bytes_per_step": int(adv_in), "d2h_bytes_per_step": int(nxt.nbytes),
+                  "note": f"advect::Advection::Advect ({wl.advection}, mixed form) through uvlm_advection_advect "
+                          f"with host MultipleSheet arrays at the held wake, wall clock per call"}
 
     # --- CPU baseline (rank 0 only) --------------------------------------------
     cpu = None
@@ -563,6 +596,9 @@ def run_ours(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": headline_config(wl, world),
             "plain_fp64_steps_per_s": plain, "speedup_vs_plain_fp64": value / world / plain,
+            "mixed_extrapolate_steps_per_s": (args.steps / (float(np.sum(t_ex)) * 1e-3)) if t_ex is not None else None,
+            "learned_warm_start_speedup": ((value / world) / (args.steps / (float(np.sum(t_ex)) * 1e-3))
+                                           if t_ex is not None else None),
             "cl_rel_err": cl_err, "cd_rel_err": cd_err,
             "cl_err_reference": f"plain FP64 GPU form, same {WAKE_ROWS} steps",
             "accuracy": accuracy, "warm_start_ablation": warm_ablation,
@@ -590,9 +626,18 @@ def run_ours(args, rank, world, local_rank):
                                     "frac": achieved64 / pk64.value,
                                     "peak_source": "FP64 FMA probe on this GPU (uvlm_measure_fp64_peak)",
                                     "units_per_step": pairs64.value, "nbody_ms_per_step": nbody_ms64},
+            "assembly_roofline": {"bound": "fp64_simt", "kernel": "assemble_kernel<double> (the FP64 residual "
+                                                                   "matrix, every step)",
+                                  "achieved": asm_tflops, "peak": pk64.value, "unit": "TFLOP/s",
+                                  "frac": asm_tflops / pk64.value,
+                                  "per_unit": f"{FLOP_PER_PAIR} FLOP per (collocation point, unique wing segment) pair",
+                                  "units_per_step": asm_pairs, "stage_ms": stage_ms[1],
+                                  "note": "the kernel evaluates each ring's 4 segments (about 2x the unique "
+                                          "segments), which is not credited"},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 8 * (1 + 2 * wl.num + wl.num * ROWS * COLS),
                     "note": "wall clock per uvlm_step + circulation download; per-step inputs are scalars"},
+            "e2e_advect": e2e_advect,
             "gpu_launches": int(launches), "clocks": clk, "preroll_s": preroll_s,
             "cpu_baseline": cpu,
         }

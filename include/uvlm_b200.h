@@ -84,7 +84,8 @@ typedef struct {
   int64_t max_wake_rows;    /* capacity in ring rows */
   int64_t erase_wake_after; /* --erase_wake_after (0 = never) */
   int32_t gmres_restart;    /* Krylov dimension before a restart */
-  int32_t gmres_max_iter;   /* above this a fresh LU is factored (the fallback) */
+  int32_t gmres_max_iter;   /* above this the plain fresh FP64 LU solve is taken (the fallback), and
+                               the FP32 factors of the preconditioner are refreshed */
   double gmres_tol;         /* relative residual ||b - A g|| / ||b|| */
   int32_t device;           /* CUDA device ordinal */
   int32_t compute_loads;    /* 1: Joukowski loads every step (CalcLoad) */
@@ -133,7 +134,9 @@ typedef struct {
 typedef struct {
   int64_t step;
   double t;
-  int32_t solve_path;   /* 0 fresh LU, 1 GMRES with stale LU, 2 GMRES then fresh-LU fallback */
+  int32_t solve_path;   /* 0 fresh LU, 1 GMRES with stale LU, 2 the fallback: GMRES stopped at
+                           gmres_max_iter (or its initial guess was non-finite) and the plain
+                           fresh FP64 LU solve of the step's FP64 matrix gave the circulation */
   int32_t gmres_iters;
   double residual;      /* final ||b - A g|| / ||b|| (FP64), 0 for the plain LU path */
   int32_t refactored;   /* a factorisation ran in this step */

@@ -469,3 +469,36 @@ def test_far_field_walker_matches_oracle():
         err = np.max(np.abs(got[name] - ref)) / scale
         assert err <= max(3 * near, 1e-7), (name, err, near)
         assert not np.array_equal(got[name], got[name[:-1]]), name  # the far walker ran
+
+
+def test_fp64_far_field_walker_matches_oracle():
+    """The FP64 far-field tiles (the far-field algebra of the FP32 form on FP64
+    records) give per-target velocities within FP64 rounding of the oracle on
+    a long wake, like the FP64 near-field tile, and they are taken."""
+    import pyoracle as o
+
+    M = U()
+    rows, cols, wr = 6, 128, 100
+    wing, wake, wing_g, wake_g = _long_wake_state(rows, cols, wr)
+    targets = np.ascontiguousarray(wake[0, ::4].reshape(-1, 3))
+    ref = o.sheet_induced_velocity(wing, wing_g, targets) + o.sheet_induced_velocity(wake, wake_g, targets)
+    scale = np.max(np.abs(ref))
+    names = [M.lib().uvlm_nbody_variant_name(v).decode() for v in range(64)]
+    got = {}
+    for v, name in enumerate(names):
+        if not name.startswith("fp64"):
+            continue
+        sim = M.SimpleSimulator(precision="fp64", nbody_variant=v)
+        sim.AddWing(M.RectGenerator(), M.Morphing(), 1.0, 8.0, rows, cols)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.begin()
+        sim.set_state(wr, wing, wake, wing_g, wing_g, wake_g)
+        got[name] = sim.Velocity(targets, include_freestream=False)
+        sim.close()
+    far = [n for n in got if n.endswith("f")]
+    assert far
+    for name, v in got.items():
+        err = np.max(np.abs(v - ref)) / scale
+        assert err <= 1e-12, (name, err)
+    for name in far:
+        assert not np.array_equal(got[name], got["fp64_h2_t1_b128_m3"]), name  # the far walker ran

@@ -92,6 +92,8 @@ struct uvlm_ctx {
   float* d_A32 = nullptr;    // FP32 matrix of the mixed form
   float* d_F32 = nullptr;    // FP32 factors of the mixed form
   float* d_Minv = nullptr;   // dense (LU)^-1 P of those factors (UVLM_PRECOND_INVERSE)
+  double* d_F64 = nullptr;   // mixed form: FP64 factors of the fallback solve (a copy of d_A64)
+  LuWork lu64;               // ... and its pivots and scratch
   double* d_tmp = nullptr;   // [N] scratch
   double* d_row = nullptr;   // [1+2num] load row
   int* d_flags = nullptr;    // [4] non-finite etc.
@@ -177,6 +179,9 @@ void uvlm_ctx::free_all() {
   cudaFree(d_F32);
   cudaFree(d_Minv);
   d_Minv = nullptr;
+  cudaFree(d_F64);
+  d_F64 = nullptr;
+  lu_work_free(&lu64);
   cudaFree(d_rhs_prev);
   cudaFree(d_phase);
   cudaFree(d_feat);
@@ -246,6 +251,10 @@ Error uvlm_ctx::alloc_all() {
       UVLM_CUDA_TRY(cudaMalloc(&d_Minv, sizeof(float) * (size_t)N * N));
     UVLM_TRY(lu_work_alloc(&lu, N, 4, num_sms));
     UVLM_TRY(gmres_work_alloc(&gm, N, std::max(2, cfg.gmres_restart)));
+    if (cfg.assembly_fp64) {  // the plain fresh-LU solve that backs up the GMRES solve
+      UVLM_TRY(dalloc(&d_F64, (size_t)N * N));
+      UVLM_TRY(lu_work_alloc(&lu64, N, 8, num_sms));
+    }
   } else {
     UVLM_TRY(lu_work_alloc(&lu, N, 8, num_sms));
   }
@@ -394,20 +403,38 @@ Error uvlm_ctx::solve(long long step) {
   GmresResult r;
   UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_Minv, d_rhs, d_gamma, cfg.gmres_tol, cfg.gmres_max_iter, &gm, &r, st));
   last.solve_path = fresh ? 0 : 1;
-  if (!r.converged && !fresh) {
-    // fresh-LU fallback: factor the current matrix and solve again
-    UVLM_TRY(factor());
+  last.gmres_iters = r.iters;
+  last.initial_residual = r.initial_relres;
+  if (!r.converged) {
+    // More than gmres_max_iter iterations (or a non-finite initial guess):
+    // the plain fresh-LU solve, an FP64 LU of the FP64 matrix of this step,
+    // gives the circulation (the plain form's own solve, which also judges
+    // the error of the accelerated path); the FP32 factors are refreshed so
+    // that the next steps' GMRES is preconditioned by this step's matrix.
+    last.solve_path = 2;
+    if (!fresh) UVLM_TRY(factor());
+    if (d_F64) {
+      UVLM_CUDA_TRY(cudaMemcpyAsync(d_F64, d_A64, sizeof(double) * (size_t)N * N, cudaMemcpyDeviceToDevice, st));
+      UVLM_TRY(lu_factor_f64(d_F64, N, &lu64, st));
+      UVLM_TRY(lu_check(&lu64, st));
+      UVLM_TRY(lu_solve_f64(d_F64, N, &lu64, d_rhs, d_gamma, d_tmp, st));
+      UVLM_TRY(lu_check(&lu64, st));
+      work_lu += 2.0 / 3.0 * (double)N * N * N;
+      // residual of the plain solve (zero GMRES iterations from its answer)
+      GmresResult rp;
+      UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_Minv, d_rhs, d_gamma, 1.0, 0, &gm, &rp, st));
+      last.residual = rp.relres;
+      return ok();
+    }
+    // FP32 assembly only (no FP64 matrix): a fresh FP32 factorisation and GMRES again
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_gamma, d_gamma_prev, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     GmresResult r2;
     UVLM_TRY(gmres_solve(A32, A64, N, d_F32, &lu, d_Minv, d_rhs, d_gamma, cfg.gmres_tol, 4 * cfg.gmres_max_iter, &gm, &r2,
                          st));
-    r2.iters += r.iters;
+    last.gmres_iters += r2.iters;
     r = r2;
-    last.solve_path = 2;
   }
-  last.gmres_iters = r.iters;
   last.residual = r.relres;
-  last.initial_residual = r.initial_relres;
   if (!r.converged) return fail(kErrNonFinite, "GMRES did not converge after a fresh factorisation");
   return ok();
 }

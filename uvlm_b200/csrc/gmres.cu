@@ -115,6 +115,7 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
   const int m = g->m;
   res->iters = 0;
   res->converged = false;
+  res->nonfinite_guess = false;
   auto matvec_res = [&](const double* xin, double* out) -> Error {
     if (A32)
       matvec_kernel<float><<<ceil_div(n, 8), 256, 0, st>>>(A32, n, xin, b, out);
@@ -149,7 +150,16 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
     UVLM_TRY(norm2(g->V, &beta));
     res->relres = beta / bnorm;
     if (total == 0) res->initial_relres = res->relres;
-    if (!std::isfinite(beta)) return fail(kErrNonFinite, "non-finite GMRES residual");
+    if (!std::isfinite(beta)) {
+      // a non-finite initial guess (the RHS is finite): not converged, so the
+      // caller can take its fallback; later it is an error of the iteration
+      if (total == 0) {
+        res->converged = false;
+        res->nonfinite_guess = true;
+        return ok();
+      }
+      return fail(kErrNonFinite, "non-finite GMRES residual");
+    }
     if (beta <= tol * bnorm) {
       res->converged = true;
       break;

@@ -28,6 +28,7 @@ struct GmresResult {
   double relres = 0;
   double initial_relres = 0;  // ||b - A x0|| / ||b|| of the initial guess
   bool converged = false;
+  bool nonfinite_guess = false;  // the initial guess gave a non-finite residual (nothing iterated)
 };
 
 Error gmres_work_alloc(GmresWork* g, int n, int m);

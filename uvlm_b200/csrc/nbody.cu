@@ -1,4 +1,6 @@
 // nbody.cu -- strip-tiled Biot-Savart N-body (FP32 hi/lo and FP64 forms).
+#include <type_traits>
+
 #include "device_once.h"
 #include "nbody.cuh"
 
@@ -595,6 +597,137 @@ __device__ __forceinline__ bool far_prepare(const RecF* sm, const StripInfo& si,
   return __all_sync(0xffffffffu, t2.x >= lim * lim && t2.y >= lim * lim);
 }
 
+// ------------------------------------------------ far-field FP64 walker
+// The far-field algebra for the FP64 form: a warp whose targets are at least
+// 2 rho + 1e-3 from a part's central node O (rho: the part's radius about O)
+// sees every node beyond rho + 1e-3 (none is cut) and every r1.r2 > 0, so the
+// segment factor takes the single form 2 g (|r1|+|r2|) / (|r1||r2|
+// ((|r1|+|r2|)^2 - |r0|^2)) (no r1.r2, no select); the |d|^2 < 1e-10 cut
+// stays.  FP64 positions need no O-relative coordinates: r = x - p directly.
+template <class T>
+__device__ __forceinline__ void seg_far(const SegV<T>& r0, T l2, const NodeV<T>& a, const NodeV<T>& b, T g, T& vx,
+                                        T& vy, T& vz) {
+  const T dx = r0.y * a.rz - r0.z * a.ry;
+  const T dy = r0.z * a.rx - r0.x * a.rz;
+  const T dz = r0.x * a.ry - r0.y * a.rx;
+  const T d2 = dx * dx + dy * dy + dz * dz;
+  const T sn = a.n + b.n;
+  const T den = a.n * b.n * (sn * sn - l2);
+  T k = (g + g) * sn * __drcp_rn(den);
+  k = d2 >= (T)kCutD2 ? k : (T)0;
+  vx += k * dx;
+  vy += k * dy;
+  vz += k * dz;
+}
+
+template <class T, class Rec, int H, int TPT, bool FIRST, bool DO_H>
+__device__ __forceinline__ void far_column(const Rec* col, const Tgt<T> (&tg)[TPT], NodeV<T> (&prev)[TPT][H],
+                                           SegV<T> (&ps0)[H], T (&pl2)[H], T (&pgS)[H], T (&acc)[TPT][3]) {
+  NodeV<T> cur[TPT][H + 1];
+  T gS[H], gH[H], l2S[H], l2H[H];
+  SegV<T> s0[H], h0[H];
+#pragma unroll
+  for (int r = 0; r <= H; ++r) {
+    const Rec rec = col[r * (kStripCols + 1)];
+    if (r < H) {
+      rec_fields<T, Rec>(rec, gS[r], gH[r], s0[r], h0[r]);
+      l2S[r] = s0[r].x * s0[r].x + s0[r].y * s0[r].y + s0[r].z * s0[r].z;
+      l2H[r] = h0[r].x * h0[r].x + h0[r].y * h0[r].y + h0[r].z * h0[r].z;
+    }
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) cur[q][r] = node_from<T, Rec>(rec, tg[q]);
+  }
+  if (DO_H) {
+#pragma unroll
+    for (int r = 0; r < H; ++r)
+#pragma unroll
+      for (int q = 0; q < TPT; ++q)
+        seg_far<T>(h0[r], l2H[r], cur[q][r], cur[q][r + 1], gH[r], acc[q][0], acc[q][1], acc[q][2]);
+  }
+  if (!FIRST) {
+#pragma unroll
+    for (int r = 0; r < H; ++r)
+#pragma unroll
+      for (int q = 0; q < TPT; ++q)
+        seg_far<T>(ps0[r], pl2[r], prev[q][r], cur[q][r], pgS[r], acc[q][0], acc[q][1], acc[q][2]);
+  }
+#pragma unroll
+  for (int r = 0; r < H; ++r) {
+    pgS[r] = gS[r];
+    ps0[r] = s0[r];
+    pl2[r] = l2S[r];
+#pragma unroll
+    for (int q = 0; q < TPT; ++q) prev[q][r] = cur[q][r];
+  }
+}
+
+// Column-bounded generic walkers over row-padded staging (record stride
+// kStripCols + 1): the near-field one (full_column) or the far-field one.
+template <class T, class Rec, int H, int TPT, bool FAR>
+__device__ __forceinline__ void walk_cols(const Rec* sm, int n_cols, bool last_h, const Tgt<T> (&tg)[TPT],
+                                          T (&acc)[TPT][3]) {
+  NodeV<T> prev[TPT][H];
+  SegV<T> ps0[H];
+  T pl2[H], pgS[H];
+  auto col = [&](const Rec* c, auto first, auto do_h) {
+    constexpr bool kFirst = decltype(first)::value, kDoH = decltype(do_h)::value;
+    if constexpr (FAR)
+      far_column<T, Rec, H, TPT, kFirst, kDoH>(c, tg, prev, ps0, pl2, pgS, acc);
+    else
+      full_column<T, Rec, H, TPT, kFirst, kDoH>(c, tg, prev, ps0, pgS, acc);
+  };
+  using Yes = std::true_type;
+  using No = std::false_type;
+  if (n_cols == 1) {
+    if (last_h)
+      col(sm, Yes{}, Yes{});
+    else
+      col(sm, Yes{}, No{});
+    return;
+  }
+  col(sm, Yes{}, Yes{});
+#pragma unroll 2
+  for (int j = 1; j < n_cols - 1; ++j) col(sm + j, No{}, Yes{});
+  if (last_h)
+    col(sm + n_cols - 1, No{}, Yes{});
+  else
+    col(sm + n_cols - 1, No{}, No{});
+}
+
+// Far test of the part [j0, j1] of a staged FP64 strip (every thread of the
+// block calls it: it synchronises): the part's radius about its central node
+// by a block max, then whether all of this warp's targets are far from it.
+template <class Rec, int H, int BLOCK, int TPT>
+__device__ __forceinline__ bool far_prepare_d(const Rec* sm, const StripInfo& si, int j0, int j1, float* red,
+                                              int slot, const Tgt<double> (&tg)[TPT]) {
+  const int w = j1 - j0 + 1;
+  const Rec& o = sm[((si.nr - 1) >> 1) * (kStripCols + 1) + j0 + ((j1 - j0) >> 1)];
+  const double ox = o.a.x, oy = o.a.y, oz = o.a.z;
+  double m = 0.0;
+  for (int q = threadIdx.x; q < si.nr * w; q += BLOCK) {
+    const int r = q / w, j = j0 + (q - r * w);
+    const Rec& p = sm[r * (kStripCols + 1) + j];
+    const double dx = p.a.x - ox, dy = p.a.y - oy, dz = p.a.z - oz;
+    m = fmax(m, dx * dx + dy * dy + dz * dz);
+  }
+  float mf = __double2float_ru(m);
+#pragma unroll
+  for (int off = 16; off; off >>= 1) mf = fmaxf(mf, __shfl_xor_sync(0xffffffffu, mf, off));
+  if ((threadIdx.x & 31) == 0) red[2 * (threadIdx.x >> 5) + slot] = mf;
+  __syncthreads();
+  float rho2 = red[slot];
+#pragma unroll
+  for (int v = 1; v < BLOCK / 32; ++v) rho2 = fmaxf(rho2, red[2 * v + slot]);
+  const double lim = 2.000001 * sqrt((double)rho2) + 1e-3;
+  bool far = true;
+#pragma unroll
+  for (int q = 0; q < TPT; ++q) {
+    const double dx = tg[q].hx - ox, dy = tg[q].hy - oy, dz = tg[q].hz - oz;
+    far = far && (dx * dx + dy * dy + dz * dz >= lim * lim);
+  }
+  return __all_sync(0xffffffffu, far);
+}
+
 // Targets tile0 + threadIdx.x + q BLOCK (clamped to the last one) of the
 // SoA arrays, as hi/lo FP32 pairs or FP64.
 template <class T, int TPT, int BLOCK>
@@ -677,6 +810,23 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
           walk_cols2<H>(cur + j0, nc, lh, tg, acc);
         }
       }
+    } else if constexpr (PAD && PK == 2 && sizeof(T) == 8) {
+      // FP64 form: the two column halves of the strip, each walked by the
+      // far-field walker when every target of the warp is far from it
+      const int n = si.n_cols;
+      const int c = n >= 3 ? n >> 1 : n - 1;
+      const bool farl = far_prepare_d<Rec, H, BLOCK, TPT>(cur, si, 0, c, red, 0, tg);
+      const bool farr = c < n - 1 && far_prepare_d<Rec, H, BLOCK, TPT>(cur, si, c, n - 1, red, 1, tg);
+      const bool one = c == n - 1 || (!farl && !farr);
+#pragma unroll 1
+      for (int p = 0; p < (one ? 1 : 2); ++p) {
+        const int j0 = p ? c : 0, nc = one ? n : (p ? n - c : c + 1);
+        const bool lh = (one || p) ? si.last_h : false;
+        if (!one && (p ? farr : farl))
+          walk_cols<T, Rec, H, TPT, true>(cur + j0, nc, lh, tg, acc);
+        else
+          walk_cols<T, Rec, H, TPT, false>(cur + j0, nc, lh, tg, acc);
+      }
     } else if constexpr (PAD && PK == 1 && sizeof(T) == 4 && TPT == 2) {
       walk_full_strip2<H>(cur, si.last_h, tg, acc);
     } else if constexpr (PAD)
@@ -703,7 +853,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
   float4* loc = reinterpret_cast<float4*>(buf1 + (H + 1) * (kStripCols + 1));
-  float* red = reinterpret_cast<float*>(loc + 2 * (H + 1) * (kStripCols + 1));
+  // the FP32 far-field walker's local coordinates (none in the FP64 form), then the per-warp maxima
+  float* red = reinterpret_cast<float*>(loc + (sizeof(Rec) == sizeof(RecF) ? 2 * (H + 1) * (kStripCols + 1) : 0));
 
   const long long tile0 = (long long)blockIdx.x * BLOCK * TPT;
   Tgt<T> tg[TPT];
@@ -811,7 +962,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBat
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
   float4* loc = reinterpret_cast<float4*>(buf1 + (H + 1) * (kStripCols + 1));
-  float* red = reinterpret_cast<float*>(loc + 2 * (H + 1) * (kStripCols + 1));
+  // the FP32 far-field walker's local coordinates (none in the FP64 form), then the per-warp maxima
+  float* red = reinterpret_cast<float*>(loc + (sizeof(Rec) == sizeof(RecF) ? 2 * (H + 1) * (kStripCols + 1) : 0));
   const long long items = totals[0];
   for (long long w = blockIdx.x; w < items; w += gridDim.x) {
     const int c = plan_search(plan, n, w, [](const NBodyBatchPlan& p) { return p.item_off; });
@@ -913,6 +1065,9 @@ constexpr Variant kVariants[] = {
     {"fp32_h4_t2_b128_x2f", kNBodyFP32, 4, 2, 128, 3, 2},
     {"fp32_h3_t2_b128_x2f", kNBodyFP32, 3, 2, 128, 3, 2},
     {"fp32_h2_t2_b128_x2f", kNBodyFP32, 2, 2, 128, 3, 2},
+    {"fp64_h2_t1_b128_m3f", kNBodyFP64, 2, 1, 128, 3, 2},
+    {"fp64_h3_t1_b128_m2f", kNBodyFP64, 3, 1, 128, 2, 2},
+    {"fp64_h2_t2_b128_f", kNBodyFP64, 2, 2, 128, 1, 2},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -933,8 +1088,10 @@ bool use_padded(const Blocks& B) {
 // (PK == 2).
 template <class Rec, int H, int BLOCK, int PK>
 constexpr size_t strip_smem() {
+  constexpr bool fp32 = sizeof(Rec) == sizeof(RecF);
   return 2 * sizeof(Rec) * (H + 1) * (kStripCols + 1) +
-         (PK == 2 ? 2 * sizeof(float4) * (H + 1) * (kStripCols + 1) + 2 * sizeof(float) * (BLOCK / 32) : 0);
+         (PK == 2 ? (fp32 ? 2 * sizeof(float4) * (H + 1) * (kStripCols + 1) : 0) + 2 * sizeof(float) * (BLOCK / 32)
+                  : 0);
 }
 
 template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, int PK = 0>
@@ -1064,6 +1221,9 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
     case 15: return launch_variant<float, RecF, 4, 2, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
     case 16: return launch_variant<float, RecF, 3, 2, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
     case 17: return launch_variant<float, RecF, 2, 2, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rf, work, vx, vy, vz, num_sms, st);
+    case 18: return launch_variant<double, RecD, 2, 1, 128, 3, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 19: return launch_variant<double, RecD, 3, 1, 128, 2, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
+    case 20: return launch_variant<double, RecD, 2, 2, 128, 1, 2>(B_, strips, tx, ty, tz, n_targets, rd, work, vx, vy, vz, num_sms, st);
     default: return fail(kErrInvalid, "bad nbody variant");
   }
 
