@@ -482,6 +482,9 @@ typedef struct {
   int32_t use_graph;       /* 1: capture one step as a CUDA graph and replay it */
   int32_t stale_factors;   /* MIXED, 1: a case refines from its previous circulation with the FP32 factors
                               of an earlier step and is factored again only when that does not converge */
+  int32_t nbody_tile;      /* MIXED: -1 (default) the tile autotuner picks the N-body tile at creation, timing
+                              every compiled FP32 tile on the last step's advection over a synthetic wake;
+                              0..2 pins a tile (see uvlm_batch_nbody_tile_name) */
 } uvlm_batch_config;
 
 int uvlm_batch_config_default(uvlm_batch_config* cfg);
@@ -505,6 +508,8 @@ int uvlm_batch_get_solve_stats(const uvlm_batch* b, int32_t* sweeps, double* res
 int uvlm_batch_factorizations(const uvlm_batch* b, int64_t* count);
 /* Kernels one step launches (nodes of the captured graph). */
 int uvlm_batch_launches_per_step(const uvlm_batch* b, int64_t* launches);
+/* Name of the N-body tile the batch runs (chosen by the autotuner or pinned). */
+const char* uvlm_batch_nbody_tile_name(const uvlm_batch* b);
 /* The batch's CUDA stream (a cudaStream_t), for events around uvlm_batch_run. */
 void* uvlm_batch_stream(const uvlm_batch* b);
 

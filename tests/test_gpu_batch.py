@@ -193,3 +193,52 @@ def test_batch_stale_factors_same_answer_fewer_factorizations():
     assert np.all(out[True][2] <= 1e-12)
     scale = np.max(np.abs(out[False][0][:, :, 1:]))
     assert np.max(np.abs(out[True][0][:, :, 1:] - out[False][0][:, :, 1:])) <= 1e-9 * scale
+
+
+def test_batch_tile_autotuner_is_fixed_under_graph_replay():
+    """The tile autotuner picks one compiled FP32 tile at creation; every
+    graph-replayed step runs it: the autotuned batch equals, bit for bit, a
+    batch pinned to the tile it chose, with and without graph replay."""
+    from uvlm_b200.batch import draw_cases, make_batch
+
+    cases = draw_cases(12, seed=4)
+    auto = make_batch(cases, precision="mixed", max_steps=30)
+    name = auto.nbody_tile()
+    assert name.startswith("fp32_") and name.endswith("_x2f"), name
+    auto.run(20)
+    tiles = ["fp32_h3_t2_b128_x2f", "fp32_h2_t2_b128_x2f", "fp32_h4_t2_b128_x2f"]
+    outs = []
+    for graph in (True, False):
+        from uvlm_b200.batch import BatchSimulator, case_morphing
+
+        sim = BatchSimulator(precision="mixed", max_steps=30, use_graph=graph, nbody_tile=tiles.index(name))
+        for d in cases:
+            sim.add_case(case_morphing(d), d["chord"], d["span"], d["rows"], d["cols"], d["dt"])
+        assert sim.nbody_tile() == name
+        sim.run(20)
+        outs.append(sim.loads())
+        sim.close()
+    np.testing.assert_array_equal(auto.loads(), outs[0])
+    np.testing.assert_array_equal(outs[0], outs[1])
+    auto.close()
+
+
+def test_every_batch_tile_agrees_with_the_fp64_batch():
+    from uvlm_b200.batch import BatchSimulator, case_morphing, draw_cases
+
+    cases = draw_cases(6, seed=9)
+
+    def run(precision, tile=-1):
+        sim = BatchSimulator(precision=precision, max_steps=16, nbody_tile=tile)
+        for d in cases:
+            sim.add_case(case_morphing(d), d["chord"], d["span"], d["rows"], d["cols"], d["dt"])
+        sim.run(15)
+        out = sim.loads()
+        sim.close()
+        return out
+
+    ref = run("fp64")
+    scale = np.max(np.abs(ref[:, :, 1:]))
+    for t in range(3):
+        got = run("mixed", t)
+        assert np.max(np.abs(got[:, :, 1:] - ref[:, :, 1:])) <= 1e-6 * scale, t

@@ -77,7 +77,7 @@ class BatchConfig(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("advection", C.c_int32), ("rk_ignore_rows", C.c_int32),
         ("refine_max_iter", C.c_int32), ("refine_tol", C.c_double), ("max_steps", C.c_int64),
-        ("device", C.c_int32), ("use_graph", C.c_int32), ("stale_factors", C.c_int32),
+        ("device", C.c_int32), ("use_graph", C.c_int32), ("stale_factors", C.c_int32), ("nbody_tile", C.c_int32),
     ]
 
 
@@ -169,6 +169,7 @@ SIGNATURES = [
     ("uvlm_dense_solve", C.c_int, [_P, _I, _P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     ("uvlm_batch_config_default", C.c_int, [C.POINTER(BatchConfig)]),
     ("uvlm_batch_create", C.c_int, [C.POINTER(BatchConfig), C.POINTER(BatchCase), C.c_int32, C.POINTER(_V)]),
+    ("uvlm_batch_nbody_tile_name", C.c_char_p, [_V]),
     ("uvlm_batch_destroy", C.c_int, [_V]),
     ("uvlm_batch_last_error", C.c_char_p, [_V]),
     ("uvlm_batch_run", C.c_int, [_V, _I]),

@@ -41,7 +41,7 @@ class BatchSimulator:
 
     def __init__(self, precision: str = "mixed", advection: str = "euler", max_steps: int = 151, device: int = 0,
                  use_graph: bool = True, refine_tol: float = 1e-12, refine_max_iter: int = 10,
-                 rk_ignore_rows: int = 5, stale_factors: bool = True):
+                 rk_ignore_rows: int = 5, stale_factors: bool = True, nbody_tile: int = -1):
         cfg = BatchConfig()
         check(lib().uvlm_batch_config_default(C.byref(cfg)))
         cfg.precision = PRECISION[precision]
@@ -53,6 +53,7 @@ class BatchSimulator:
         cfg.refine_max_iter = int(refine_max_iter)
         cfg.rk_ignore_rows = int(rk_ignore_rows)
         cfg.stale_factors = int(bool(stale_factors))
+        cfg.nbody_tile = int(nbody_tile)  # -1: the tile autotuner chooses at creation
         self._cfg = cfg
         self._cases = []
         self._h = None
@@ -96,6 +97,12 @@ class BatchSimulator:
         v = C.c_int64()
         _check(lib().uvlm_batch_steps_done(self._h, C.byref(v)), self._h)
         return v.value
+
+    def nbody_tile(self) -> str:
+        """Name of the N-body tile the batch runs (autotuned or pinned)."""
+        if self._h is None:
+            self.begin()
+        return lib().uvlm_batch_nbody_tile_name(self._h).decode()
 
     def loads(self) -> np.ndarray:
         """[steps_done][n_cases][3] = (t, CD, CL)."""

@@ -800,6 +800,25 @@ __global__ void b_advect_kernel(const BCase* __restrict__ cs, BPrefix P, int n, 
   }
 }
 
+// Synthetic wake of the tile autotuner: every case's trailing edge convected
+// by its forward flight for s steps with a gentle vertical wave (node rows
+// 0..s of the layout above), the shape of a late step's wake.
+__global__ void b_synth_wake_kernel(const BCase* __restrict__ cs, BPrefix P, int n, int cap, long long s,
+                                    const double* pos_init, double* wpos) {
+  const long long total = P.wnode[n];
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const BCase& b = cs[find_case(P.wnode, n, g)];
+    const long long local = g - b.wnode_off;
+    const long long i = local / (b.C + 1) - (cap - 1 - s);
+    if (i < 0) continue;
+    const int j = (int)(local % (b.C + 1));
+    const d3 te = ld3(pos_init + 3 * (b.node_off + (long long)b.R * (b.C + 1) + j));
+    const double t = (double)i * b.dt;
+    st3(wpos + 3 * g, add(te, mk(-b.ff[0] * t, -b.ff[1] * t, -b.ff[2] * t + 0.05 * sin(0.3 * (double)i))));
+  }
+}
+
 __global__ void b_step_end_kernel(long long* d_step) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_step += 1;
 }
@@ -866,6 +885,8 @@ struct uvlm_batch {
     return e.code;
   }
   Error alloc(const uvlm_batch_case* cases);
+  Error build_records(int with_bound, const double* wsrc);
+  Error tune_tiles();
   Error enqueue_step();
   Error nbody(int stage, const double* tx, const double* ty, const double* tz);
   void release();
@@ -1052,18 +1073,75 @@ Error uvlm_batch::nbody(int stage, const double* tx, const double* ty, const dou
                           d_totals, d_status, nb_grids, st);
 }
 
+Error uvlm_batch::build_records(int with_bound, const double* wsrc) {
+  const BPrefix P = prefixes();
+  if (mixed())
+    b_records_kernel<RecF><<<grid, 256, 0, st>>>(d_cases, P, n, cap, d_step, with_bound, d_pos, d_gamma, wsrc,
+                                                d_wgamma, reinterpret_cast<RecF*>(d_rec));
+  else
+    b_records_kernel<RecD><<<grid, 256, 0, st>>>(d_cases, P, n, cap, d_step, with_bound, d_pos, d_gamma, wsrc,
+                                                d_wgamma, reinterpret_cast<RecD*>(d_rec));
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
+
+// Tile autotuner of the batched N-body (before the first step, outside any
+// graph capture): the advection stage of the last step the batch can run,
+// on a synthetic wake of that length (b_synth_wake_kernel), is timed with
+// every compiled FP32 tile; the fastest is kept (the default unless another
+// is more than 3% faster) and every later step, captured once as a graph,
+// runs it.  The wake buffers and the step counter are cleared afterwards.
+Error uvlm_batch::tune_tiles() {
+  if (!mixed()) return ok();
+  if (cfg.nbody_tile >= 0) {
+    nb_grids.tile = cfg.nbody_tile;
+    return ok();
+  }
+  const long long s = cfg.max_steps - 1;
+  if (s < 2) return ok();
+  const BPrefix P = prefixes();
+  b_synth_wake_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, cap, s, d_pos_init, d_wpos);
+  UVLM_LAUNCH_CHECK();
+  UVLM_CUDA_TRY(cudaMemcpyAsync(d_step, &s, sizeof(s), cudaMemcpyHostToDevice, st));
+  UVLM_TRY(build_records(1, d_wpos));
+  b_gather_wake_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, cap, d_step, d_wpos, d_wtx, d_wty, d_wtz);
+  UVLM_LAUNCH_CHECK();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  UVLM_CUDA_TRY(cudaEventCreate(&e0));
+  UVLM_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int chosen = 0;
+  Error err = ok();
+  for (int t = 0; t < kNumBatchTilesF && !err.code; ++t) {
+    nb_grids.tile = t;
+    float ms = 0;
+    for (int rep = 0; rep < 3 && !err.code; ++rep) {  // the first run warms caches and module state
+      cudaEventRecord(e0, st);
+      err = nbody(kStageAdvect, d_wtx, d_wty, d_wtz);
+      cudaEventRecord(e1, st);
+      if (!err.code && cudaEventSynchronize(e1) != cudaSuccess) err = fail(kErrCuda, "tile autotune");
+      if (!err.code) cudaEventElapsedTime(&ms, e0, e1);
+    }
+    const float score = t == 0 ? ms / 1.03f : ms;
+    if (!err.code && score < best) {
+      best = score;
+      chosen = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  nb_grids.tile = chosen;
+  UVLM_TRY(err);
+  const long long zero = 0;
+  UVLM_CUDA_TRY(cudaMemsetAsync(d_wpos, 0, sizeof(double) * 3 * (size_t)tot_wnode, st));
+  UVLM_CUDA_TRY(cudaMemcpyAsync(d_step, &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+  UVLM_CUDA_TRY(cudaStreamSynchronize(st));
+  return ok();
+}
+
 Error uvlm_batch::enqueue_step() {
   const BPrefix P = prefixes();
-  auto records = [&](int with_bound, const double* wsrc) -> Error {
-    if (mixed())
-      b_records_kernel<RecF><<<grid, 256, 0, st>>>(d_cases, P, n, cap, d_step, with_bound, d_pos, d_gamma, wsrc,
-                                                  d_wgamma, reinterpret_cast<RecF*>(d_rec));
-    else
-      b_records_kernel<RecD><<<grid, 256, 0, st>>>(d_cases, P, n, cap, d_step, with_bound, d_pos, d_gamma, wsrc,
-                                                  d_wgamma, reinterpret_cast<RecD*>(d_rec));
-    UVLM_LAUNCH_CHECK();
-    return ok();
-  };
+  auto records = [&](int with_bound, const double* wsrc) -> Error { return build_records(with_bound, wsrc); };
   b_begin_kernel<<<grid, 256, 0, st>>>(P.ring, n, d_gamma, d_gamma_prev, d_gamma_hist);
   UVLM_LAUNCH_CHECK();
   b_kinematics_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, d_step, d_pos_init, d_pos);
@@ -1153,7 +1231,12 @@ int uvlm_batch_config_default(uvlm_batch_config* c) {
   c->device = 0;
   c->use_graph = 1;
   c->stale_factors = 1;
+  c->nbody_tile = -1;
   return UVLM_OK;
+}
+
+const char* uvlm_batch_nbody_tile_name(const uvlm_batch* b) {
+  return b ? nbody_batch_tile_name(b->prec(), b->nb_grids.tile) : "?";
 }
 
 int uvlm_batch_create(const uvlm_batch_config* cfg, const uvlm_batch_case* cases, int32_t n_cases,
@@ -1165,7 +1248,8 @@ int uvlm_batch_create(const uvlm_batch_config* cfg, const uvlm_batch_case* cases
   *out = nullptr;
   if ((cfg->precision != UVLM_PRECISION_FP64 && cfg->precision != UVLM_PRECISION_MIXED) ||
       (cfg->advection != UVLM_ADVECT_EULER && cfg->advection != UVLM_ADVECT_RK2) || cfg->max_steps < 1 ||
-      cfg->refine_max_iter < 0 || !(cfg->refine_tol > 0)) {
+      cfg->refine_max_iter < 0 || !(cfg->refine_tol > 0) || cfg->nbody_tile < -1 ||
+      cfg->nbody_tile >= kNumBatchTilesF) {
     set_global_error("uvlm_batch_create: invalid configuration (precision, advection Euler/RK2, max_steps)");
     return UVLM_ERR_INVALID;
   }
@@ -1192,6 +1276,7 @@ int uvlm_batch_create(const uvlm_batch_config* cfg, const uvlm_batch_case* cases
   Error e{};
   if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) e = fail(kErrCuda, "stream");
   if (!e.code) e = b->alloc(cases);
+  if (!e.code) e = b->tune_tiles();
   if (e.code) {
     set_global_error(e.msg);
     b->release();

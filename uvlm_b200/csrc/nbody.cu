@@ -1233,21 +1233,38 @@ Error nbody_eval(const SourceBlock* blocks, int n_blocks, NBodyPrec prec, const 
 
 namespace uvlm {
 
+// FP32 batch tiles the batch autotuner chooses from: column-bounded packed
+// FP32x2 walkers with the far-field walker, H node rows per strip.
+constexpr int kBatchTileH[kNumBatchTilesF] = {3, 2, 4};
+
 int nbody_batch_rows(NBodyPrec prec, bool padded) {
   (void)padded;  // one FP32 class: the column-bounded packed tile takes every sheet
   return prec == kNBodyFP32 ? kBatchHFP : kBatchHD;
 }
 
+const char* nbody_batch_tile_name(NBodyPrec prec, int tile) {
+  static const char* names[kNumBatchTilesF] = {"fp32_h3_t2_b128_x2f", "fp32_h2_t2_b128_x2f", "fp32_h4_t2_b128_x2f"};
+  if (prec != kNBodyFP32) return "fp64_h2_t1_b128";
+  return (tile >= 0 && tile < kNumBatchTilesF) ? names[tile] : "?";
+}
+
 long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n) {
-  long long total = 0;
-  for (int c = 0; c < n; ++c) {
-    const int H = nbody_batch_rows(prec, prec == kNBodyFP32 && batch_input_padded(in[c]));
-    Blocks B{};
-    const long long strips = fill_blocks(B, in[c].blocks, in[c].n_blocks, H);
-    const long long splits = (strips + kBatchStripsPerItem - 1) / kBatchStripsPerItem;
-    total += splits * 3 * in[c].n_tgt;
+  // the bound of every tile the batch may run (the fewest rows per strip
+  // make the most strips, hence the most source splits)
+  long long worst = 0;
+  const int tiles = prec == kNBodyFP32 ? kNumBatchTilesF : 1;
+  for (int t = 0; t < tiles; ++t) {
+    const int H = prec == kNBodyFP32 ? kBatchTileH[t] : kBatchHD;
+    long long total = 0;
+    for (int c = 0; c < n; ++c) {
+      Blocks B{};
+      const long long strips = fill_blocks(B, in[c].blocks, in[c].n_blocks, H);
+      const long long splits = (strips + kBatchStripsPerItem - 1) / kBatchStripsPerItem;
+      total += splits * 3 * in[c].n_tgt;
+    }
+    worst = std::max(worst, total);
   }
-  return total;
+  return worst;
 }
 
 namespace {
@@ -1260,13 +1277,30 @@ int batch_grid_of(int num_sms) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBatchBlock, smem) != cudaSuccess || occ < 1) occ = 1;
   return num_sms * occ;
 }
+
+template <int H>
+Error batch_eval_f32(const NBodyBatchInput* d_in, int n, const double* tx, const double* ty, const double* tz,
+                     const RecF* rf, double* partial, long long partial_cap, NBodyBatchPlan* d_plan,
+                     long long* d_totals, int* status, int grid, cudaStream_t st) {
+  batch_plan_kernel<H, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, -1, d_plan, partial_cap, d_totals,
+                                                                    status);
+  UVLM_LAUNCH_CHECK();
+  batch_nbody_kernel<float, RecF, H, kBatchTptF, kBatchBlock, kBatchMinB, true, kBatchPadPK>
+      <<<grid, kBatchBlock, strip_smem<RecF, H, kBatchBlock, kBatchPadPK>(), st>>>(d_plan, n, d_totals, tx, ty, tz,
+                                                                                 rf, partial);
+  UVLM_LAUNCH_CHECK();
+  return ok();
+}
 }  // namespace
 
 NBodyBatchGrids nbody_batch_grids(NBodyPrec prec, int num_sms) {
   NBodyBatchGrids g;
   if (prec == kNBodyFP32) {
     g.general = 0;
-    g.padded = batch_grid_of<float, RecF, kBatchHFP, kBatchTptF, true, kBatchPadPK>(num_sms);
+    g.tiles[0] = batch_grid_of<float, RecF, 3, kBatchTptF, true, kBatchPadPK>(num_sms);
+    g.tiles[1] = batch_grid_of<float, RecF, 2, kBatchTptF, true, kBatchPadPK>(num_sms);
+    g.tiles[2] = batch_grid_of<float, RecF, 4, kBatchTptF, true, kBatchPadPK>(num_sms);
+    g.padded = g.tiles[0];
   } else {
     g.general = batch_grid_of<double, RecD, kBatchHD, kBatchTptD, false, 0>(num_sms);
   }
@@ -1284,16 +1318,17 @@ Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const
     return ok();
   };
   if (prec == kNBodyFP32) {
+    // every problem: the column-bounded packed FP32x2 tile with the far-field
+    // walker, in the height the batch's autotuner chose
     const RecF* rf = reinterpret_cast<const RecF*>(records);
-    // every problem: column-bounded packed FP32x2 tile with the far-field walker
-    batch_plan_kernel<kBatchHFP, kBatchBlock * kBatchTptF><<<1, 256, 0, st>>>(d_in, n, -1, d_plan, partial_cap,
-                                                                              d_totals, status);
-    UVLM_LAUNCH_CHECK();
-    batch_nbody_kernel<float, RecF, kBatchHFP, kBatchTptF, kBatchBlock, kBatchMinB, true, kBatchPadPK>
-        <<<grids.padded, kBatchBlock, strip_smem<RecF, kBatchHFP, kBatchBlock, kBatchPadPK>(), st>>>(d_plan, n, d_totals, tx, ty, tz, rf,
-                                                                            partial);
-    UVLM_LAUNCH_CHECK();
-    return reduce(grids.padded);
+    const int t = (grids.tile >= 0 && grids.tile < kNumBatchTilesF) ? grids.tile : 0;
+    const int grid = grids.tiles[t];
+    switch (t) {
+      case 1: UVLM_TRY(batch_eval_f32<2>(d_in, n, tx, ty, tz, rf, partial, partial_cap, d_plan, d_totals, status, grid, st)); break;
+      case 2: UVLM_TRY(batch_eval_f32<4>(d_in, n, tx, ty, tz, rf, partial, partial_cap, d_plan, d_totals, status, grid, st)); break;
+      default: UVLM_TRY(batch_eval_f32<3>(d_in, n, tx, ty, tz, rf, partial, partial_cap, d_plan, d_totals, status, grid, st)); break;
+    }
+    return reduce(grid);
   }
   batch_plan_kernel<kBatchHD, kBatchBlock * kBatchTptD><<<1, 256, 0, st>>>(d_in, n, -1, d_plan, partial_cap,
                                                                            d_totals, status);

@@ -234,10 +234,15 @@ __host__ __device__ inline bool batch_input_padded(const NBodyBatchInput& x) {
 int nbody_batch_rows(NBodyPrec prec, bool padded);
 // Upper bound of the partial-sum doubles for the given inputs (host copy).
 long long nbody_batch_partial_doubles(NBodyPrec prec, const NBodyBatchInput* in, int n);
-// Persistent grid sizes used by nbody_batch_eval on this device.
+// Persistent grid sizes used by nbody_batch_eval on this device, and the
+// FP32 tile (strip height) the batch runs: tiles[t] is the grid of tile t.
+constexpr int kNumBatchTilesF = 3;
 struct NBodyBatchGrids {
   int general = 0, padded = 0;
+  int tiles[kNumBatchTilesF] = {0, 0, 0};
+  int tile = 0;
 };
+const char* nbody_batch_tile_name(NBodyPrec prec, int tile);
 NBodyBatchGrids nbody_batch_grids(NBodyPrec prec, int num_sms);
 
 // d_in: n problems on the device.  Plans on the device (one CTA), evaluates
