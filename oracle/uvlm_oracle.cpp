@@ -300,12 +300,19 @@ struct FullPivLU {
     std::vector<double>& M = *A;
     size_t pi = k, pj = k;
     double best = -1;
+    // The first maximum of |a_ij| in row-major order: per row a vectorised
+    // max (as Eigen's packet maxCoeff), then the first column attaining it
+    // when the row beats every earlier row (the same pivot as a scalar scan).
     auto search = [&](size_t i0, size_t i1, double& b, size_t& bi, size_t& bj) {
       for (size_t i = i0; i < i1; i++) {
         const double* row = &M[i * n];
-        for (size_t j = k; j < n; j++) {
-          const double a = std::fabs(row[j]);
-          if (a > b) { b = a; bi = i; bj = j; }
+        double m = -1;
+#pragma omp simd reduction(max : m)
+        for (size_t j = k; j < n; j++) m = std::max(m, std::fabs(row[j]));
+        if (m > b) {
+          size_t j = k;
+          while (std::fabs(row[j]) != m) j++;
+          b = m; bi = i; bj = j;
         }
       }
     };
@@ -343,8 +350,10 @@ struct FullPivLU {
       double* rowi = &M[i * n];
       const double l = rowi[k] / piv;
       rowi[k] = l;
-      if (l != 0)
+      if (l != 0) {
+#pragma omp simd
         for (size_t j = k + 1; j < n; j++) rowi[j] -= l * rowk[j];
+      }
     };
 #ifdef _OPENMP
     if (threads > 1 && n - k >= 64) {
