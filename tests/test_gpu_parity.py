@@ -502,3 +502,35 @@ def test_fp64_far_field_walker_matches_oracle():
         assert err <= 1e-12, (name, err)
     for name in far:
         assert not np.array_equal(got[name], got["fp64_h2_t1_b128_m3"]), name  # the far walker ran
+
+
+def test_fp64_near_field_option_of_the_mixed_form():
+    """near_fp64: the pairs the far-field test leaves to the near-field walker
+    are evaluated in FP64 (FP64 records, FP64 accumulation).  The velocities
+    stay within the FP32 far field's error of the oracle and are at least as
+    accurate as the all-FP32 walk; a pinned tile without the far-field walker
+    is refused."""
+    import pyoracle as o
+
+    M = U()
+    rows, cols, wr = 6, 128, 100
+    wing, wake, wing_g, wake_g = _long_wake_state(rows, cols, wr)
+    targets = np.ascontiguousarray(wake[0, ::4].reshape(-1, 3))
+    ref = o.sheet_induced_velocity(wing, wing_g, targets) + o.sheet_induced_velocity(wake, wake_g, targets)
+    scale = np.max(np.abs(ref))
+    got = {}
+    for near in (False, True):
+        sim = M.SimpleSimulator(precision="mixed", near_fp64=near)
+        sim.AddWing(M.RectGenerator(), M.Morphing(), 1.0, 8.0, rows, cols)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.begin()
+        sim.set_state(wr, wing, wake, wing_g, wing_g, wake_g)
+        got[near] = sim.Velocity(targets, include_freestream=False)
+        sim.close()
+    e32 = np.max(np.abs(got[False] - ref)) / scale
+    e64 = np.max(np.abs(got[True] - ref)) / scale
+    print("FP32 near field", e32, "FP64 near field", e64)
+    assert e64 <= e32 and e64 <= 1e-6
+    names = [M.lib().uvlm_nbody_variant_name(v).decode() for v in range(64)]
+    with pytest.raises(M.UVLMError):
+        M.SimpleSimulator(precision="mixed", near_fp64=True, nbody_variant=names.index("fp32_h3_t2_b128_x2"))

@@ -194,6 +194,7 @@ void uvlm_ctx::free_all() {
   cudaFree(d_flags);
   cudaFree(nb.records);
   cudaFree(nb.partial);
+  cudaFree(nb.records64);
   d_A32 = d_F32 = nullptr;
   d_kin = nullptr;
   d_flags = nullptr;
@@ -242,6 +243,11 @@ Error uvlm_ctx::alloc_all() {
   UVLM_CUDA_TRY(cudaMalloc(&nb.records, nb.records_cap));
   nb.partial_cap = 3LL * std::max<long long>(64LL * N, 16LL * tcap);
   UVLM_CUDA_TRY(cudaMalloc(&nb.partial, sizeof(double) * nb.partial_cap));
+  if (mixed() && cfg.nbody_near_fp64) {
+    nb.near64 = true;
+    nb.records64_cap = (long long)(nn + wn) * (long long)sizeof(RecD);
+    UVLM_CUDA_TRY(cudaMalloc(&nb.records64, nb.records64_cap));
+  }
   // dense matrices
   if (!mixed() || cfg.assembly_fp64) UVLM_TRY(dalloc(&d_A64, (size_t)N * N));
   if (mixed()) {
@@ -293,6 +299,7 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBody
     int best = chosen;
     for (int v = 0; v < nbody_num_variants(); ++v) {
       if (nbody_variant_prec(v) != prec) continue;
+      if (prec == kNBodyFP32 && nb.near64 && !nbody_variant_near64(v)) continue;  // keep the FP64 near field
       float ms = 0;
       for (int rep = 0; rep < 2; ++rep) {
         UVLM_CUDA_TRY(cudaEventRecord(ev[0], st));
@@ -746,7 +753,8 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
   }
   if (k.advection < 0 || k.advection > 3 || k.max_wake_rows < 1 || k.gmres_restart < 1 || k.gmres_max_iter < 1 ||
       !(k.gmres_tol > 0) || k.preconditioner < 0 || k.preconditioner > 1 || k.nbody_fp64_stages < 0 ||
-      k.nbody_fp64_stages > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT)) {
+      k.nbody_fp64_stages > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT) || k.nbody_near_fp64 < 0 ||
+      k.nbody_near_fp64 > 1) {
     delete c;
     return set_global(fail(kErrInvalid, "invalid configuration"));
   }
@@ -773,6 +781,10 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
     if (k.nbody_variant >= nbody_num_variants()) {
       uvlm_destroy(c);
       return set_global(fail(kErrInvalid, "nbody_variant out of range"));
+    }
+    if (k.precision == UVLM_PRECISION_MIXED && k.nbody_near_fp64 && !nbody_variant_near64(k.nbody_variant)) {
+      uvlm_destroy(c);
+      return set_global(fail(kErrInvalid, "nbody_near_fp64 needs a packed far-field FP32 tile (\"fp32_*_t2_*_x2f\")"));
     }
     if (k.precision == UVLM_PRECISION_MIXED)
       c->variant_fp32 = k.nbody_variant;

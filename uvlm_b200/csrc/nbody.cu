@@ -728,6 +728,73 @@ __device__ __forceinline__ bool far_prepare_d(const Rec* sm, const StripInfo& si
   return __all_sync(0xffffffffu, far);
 }
 
+// ------------------------------------------------ FP64 near field
+// The mixed form's near pairs (those the far-field test leaves to the
+// near-field walker) in FP64 when the context asks for it: the plain FP64
+// form's near-field arithmetic (seg<double>) on the FP64 records of the same
+// sheets, read from global memory (they stay in L1/L2), for the thread's
+// targets one at a time, accumulated in FP64.  Rows past the strip's loaded
+// rows read as zero records, as the row-padded staging does.
+template <int H, bool FIRST, bool DO_H>
+__device__ __forceinline__ void near64_column(const RecD* __restrict__ col, int stride, int nr,
+                                              const Tgt<double> (&tg)[1], NodeV<double> (&prev)[1][H],
+                                              SegV<double> (&ps0)[H], double (&pgS)[H], double (&acc)[1][3]) {
+  NodeV<double> cur[1][H + 1];
+  double gS[H], gH[H];
+  SegV<double> s0[H], h0[H];
+#pragma unroll
+  for (int r = 0; r <= H; ++r) {
+    RecD rec;
+    if (r < nr) {
+      rec = col[(long long)r * stride];
+    } else {
+      rec.a = make_double4(0, 0, 0, 0);
+      rec.b = rec.a;
+      rec.c = rec.a;
+    }
+    if (r < H) rec_fields<double, RecD>(rec, gS[r], gH[r], s0[r], h0[r]);
+    cur[0][r] = node_from<double, RecD>(rec, tg[0]);
+  }
+  if (DO_H) {
+#pragma unroll
+    for (int r = 0; r < H; ++r) seg<double>(h0[r], cur[0][r], cur[0][r + 1], gH[r], acc[0][0], acc[0][1], acc[0][2]);
+  }
+  if (!FIRST) {
+#pragma unroll
+    for (int r = 0; r < H; ++r) seg<double>(ps0[r], prev[0][r], cur[0][r], pgS[r], acc[0][0], acc[0][1], acc[0][2]);
+  }
+#pragma unroll
+  for (int r = 0; r < H; ++r) {
+    pgS[r] = gS[r];
+    ps0[r] = s0[r];
+    prev[0][r] = cur[0][r];
+  }
+}
+
+// Columns [0, n_cols) of a part starting at `base` (record of its first
+// row); the chordwise segments of the last column only when owned.
+template <int H>
+__device__ __forceinline__ void walk_near64(const RecD* __restrict__ base, int stride, int nr, int n_cols, bool last_h,
+                                            const Tgt<double> (&tg)[1], double (&acc)[1][3]) {
+  NodeV<double> prev[1][H];
+  SegV<double> ps0[H];
+  double pgS[H];
+  if (n_cols == 1) {
+    if (last_h)
+      near64_column<H, true, true>(base, stride, nr, tg, prev, ps0, pgS, acc);
+    else
+      near64_column<H, true, false>(base, stride, nr, tg, prev, ps0, pgS, acc);
+    return;
+  }
+  near64_column<H, true, true>(base, stride, nr, tg, prev, ps0, pgS, acc);
+#pragma unroll 1
+  for (int j = 1; j < n_cols - 1; ++j) near64_column<H, false, true>(base + j, stride, nr, tg, prev, ps0, pgS, acc);
+  if (last_h)
+    near64_column<H, false, true>(base + n_cols - 1, stride, nr, tg, prev, ps0, pgS, acc);
+  else
+    near64_column<H, false, false>(base + n_cols - 1, stride, nr, tg, prev, ps0, pgS, acc);
+}
+
 // Targets tile0 + threadIdx.x + q BLOCK (clamped to the last one) of the
 // SoA arrays, as hi/lo FP32 pairs or FP64.
 template <class T, int TPT, int BLOCK>
@@ -757,10 +824,11 @@ __device__ __forceinline__ void load_targets(const double* __restrict__ tx, cons
 // walkers bounded by each strip's column count (row-padded staging, any
 // fill) with the far-field walker for strips far from all of a warp's
 // targets (`loc`, `red`: its shared-memory scratch).
-template <class T, class Rec, int H, int TPT, int BLOCK, bool PAD, int PK = 0>
+template <class T, class Rec, int H, int TPT, int BLOCK, bool PAD, int PK = 0, bool NEAR64 = false>
 __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, long long s_end,
                                             const Rec* __restrict__ rec, Rec* buf0, Rec* buf1, float4* loc,
-                                            float* red, const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3]) {
+                                            float* red, const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3],
+                                            const RecD* __restrict__ rec64 = nullptr) {
   if (s_begin >= s_end) return;
   StripInfo si = decode_strip<H>(B, s_begin);
   if constexpr (PAD && PK == 2)
@@ -806,6 +874,21 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
           float2 ts[3];
           part_targets(part_origin(cur, si, j0, j0 + nc - 1), tg, ts);
           walk_far_cols2<H>(cur + j0, (p ? locr : loc) + j0, nc, lh, ts, acc);
+        } else if constexpr (NEAR64) {
+          // near part in FP64 from the FP64 records, one target at a time
+#pragma unroll 1
+          for (int q = 0; q < 2; ++q) {
+            Tgt<double> td[1];
+            td[0].hx = (double)tg[q].hx + (double)tg[q].lx;
+            td[0].hy = (double)tg[q].hy + (double)tg[q].ly;
+            td[0].hz = (double)tg[q].hz + (double)tg[q].lz;
+            td[0].lx = td[0].ly = td[0].lz = 0.0;
+            double a64[1][3] = {{0.0, 0.0, 0.0}};
+            walk_near64<H>(rec64 + si.first + j0, si.row_stride, si.nr, nc, lh, td, a64);
+            accd[q][0] += a64[0][0];
+            accd[q][1] += a64[0][1];
+            accd[q][2] += a64[0][2];
+          }
         } else {
           walk_cols2<H>(cur + j0, nc, lh, tg, acc);
         }
@@ -822,7 +905,7 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
       for (int p = 0; p < (one ? 1 : 2); ++p) {
         const int j0 = p ? c : 0, nc = one ? n : (p ? n - c : c + 1);
         const bool lh = (one || p) ? si.last_h : false;
-        if (!one && (p ? farr : farl))
+        if (p ? farr : farl)
           walk_cols<T, Rec, H, TPT, true>(cur + j0, nc, lh, tg, acc);
         else
           walk_cols<T, Rec, H, TPT, false>(cur + j0, nc, lh, tg, acc);
@@ -844,11 +927,12 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
   }
 }
 
-template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, int PK>
+template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, int PK, bool NEAR64 = false>
 __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
                                                        const double* __restrict__ tx, const double* __restrict__ ty,
                                                        const double* __restrict__ tz, long long n_targets,
-                                                       const Rec* __restrict__ rec, double* __restrict__ partial) {
+                                                       const Rec* __restrict__ rec, double* __restrict__ partial,
+                                                       const RecD* __restrict__ rec64) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Rec* buf0 = reinterpret_cast<Rec*>(smem_raw);
   Rec* buf1 = buf0 + (H + 1) * (kStripCols + 1);
@@ -864,7 +948,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
   const long long s_begin = (long long)blockIdx.y * strips_per_split;
   const long long s_end = min(n_strips, s_begin + strips_per_split);
-  eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK>(B, s_begin, s_end, rec, buf0, buf1, loc, red, tg, accd);
+  eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK, NEAR64>(B, s_begin, s_end, rec, buf0, buf1, loc, red, tg, accd,
+                                                      rec64);
   double* px = partial + (long long)blockIdx.y * 3 * n_targets;
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
@@ -1101,20 +1186,28 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   // the column-bounded walkers (PK == 2) take every sheet; the others pad only
   // sheets that fill most of the staged columns
   const bool pad = PK == 2 || use_padded(B);
+  // the mixed form's near pairs in FP64 (packed FP32x2 tiles with the far-field walker)
+  constexpr bool kCanNear64 = PK == 2 && sizeof(T) == 4 && TPT == 2;
+  const RecD* rec64 = (kCanNear64 && work->near64) ? reinterpret_cast<const RecD*>(work->records64) : nullptr;
+  if (kCanNear64 && work->near64 && !rec64) return fail(kErrInvalid, "FP64 near field without FP64 records");
   void (*kern)(Blocks, long long, long long, const double*, const double*, const double*, long long, const Rec*,
-               double*);
-  if constexpr (PK == 2)
+               double*, const RecD*);
+  if constexpr (kCanNear64)
+    kern = rec64 ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK, true>
+                 : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK, false>;
+  else if constexpr (PK == 2)
     kern = nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK>;
   else
     kern = pad ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK> : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, false, PK>;
   const size_t smem = strip_smem<Rec, H, BLOCK, PK>();
   // the shared-memory limit is a per-device attribute: set it once on every
-  // device this process launches on
-  static PerDeviceOnce attr_once[2];
+  // device this process launches on (per kernel instance)
+  static PerDeviceOnce attr_once[4];
+  const int inst = (pad ? 1 : 0) + (rec64 ? 2 : 0);
   int dev = 0;
   UVLM_CUDA_TRY(cudaGetDevice(&dev));
   cudaError_t attr_err = cudaSuccess;
-  if (!once_on_device(attr_once[pad], dev, [&] {
+  if (!once_on_device(attr_once[inst], dev, [&] {
         attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return attr_err == cudaSuccess;
       }))
@@ -1136,7 +1229,7 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   const long long need = splits * 3 * n_targets;
   if (work->partial_cap < need) return fail(kErrCapacity, "nbody partial buffer too small");
   dim3 grid((unsigned)tiles, (unsigned)splits);
-  kern<<<grid, BLOCK, smem, st>>>(B, n_strips, sps, tx, ty, tz, n_targets, rec, work->partial);
+  kern<<<grid, BLOCK, smem, st>>>(B, n_strips, sps, tx, ty, tz, n_targets, rec, work->partial, rec64);
   UVLM_LAUNCH_CHECK();
   const int rb = 256;
   const int rg = (int)std::min<long long>((n_targets + rb - 1) / rb, (long long)num_sms * 8);
@@ -1149,6 +1242,10 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
 
 int nbody_num_variants() { return kNumVariants; }
 int nbody_variant_prec(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].prec : -1; }
+bool nbody_variant_near64(int v) {
+  return v >= 0 && v < kNumVariants && kVariants[v].prec == kNBodyFP32 && kVariants[v].packed == 2 &&
+         kVariants[v].TPT == 2;
+}
 const char* nbody_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
 
 long long nbody_unique_segments(const SourceBlock* blocks, int n_blocks) {
@@ -1178,6 +1275,13 @@ Error nbody_build_sources(const SheetView* views, int n_views, NBodyPrec prec, N
       else
         build_records_kernel<RecD><<<gs, bs, 0, st>>>(v, reinterpret_cast<RecD*>(work->records) + off);
       UVLM_LAUNCH_CHECK();
+      if (prec == kNBodyFP32 && work->near64) {
+        // FP64 records of the same nodes for the FP64 near field
+        if ((off + cnt) * (long long)sizeof(RecD) > work->records64_cap)
+          return fail(kErrCapacity, "nbody FP64 record buffer too small");
+        build_records_kernel<RecD><<<gs, bs, 0, st>>>(v, reinterpret_cast<RecD*>(work->records64) + off);
+        UVLM_LAUNCH_CHECK();
+      }
     }
     off += cnt;
   }

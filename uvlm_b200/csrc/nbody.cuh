@@ -83,6 +83,11 @@ struct NBodyWork {
   double* partial = nullptr;  // [splits][3][targets]
   long long partial_cap = 0;  // doubles
   long long max_splits = 0;   // > 0: at most this many source splits (bounded scratch)
+  // FP32 form: the near pairs in FP64 (packed tiles with the far-field test),
+  // which needs the FP64 records of the same sheets as well
+  bool near64 = false;
+  void* records64 = nullptr;  // RecD array, same indices as records
+  long long records64_cap = 0;
 };
 
 // ------------------------------------------------------------ record build
@@ -256,6 +261,8 @@ Error nbody_batch_eval(NBodyPrec prec, const NBodyBatchInput* d_in, int n, const
 
 int nbody_num_variants();
 int nbody_variant_prec(int v);
+// Whether a variant evaluates the FP32 form's near pairs in FP64 when NBodyWork::near64 is set.
+bool nbody_variant_near64(int v);
 const char* nbody_variant_name(int v);
 
 // Build the source records of `n_views` sheets into work.records (blocks are
