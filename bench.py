@@ -289,7 +289,8 @@ def run_profile(args):
                           "launches": int(U.lib().uvlm_kernel_launch_count())}), flush=True)
         return
     # the library's default tiles, not the autotuner (whose timings a profiler distorts)
-    pinned = dict(nbody_variant=variant_index("fp32_h3_t2_b128_x2f" if args.form == "mixed" else
+    pinned = dict(nbody_variant=variant_index(args.variant) if args.variant else
+                  variant_index("fp32_h3_t2_b128_x2f" if args.form == "mixed" else
                                               "fp64_h2_t1_b128_m3"))
     if args.profile_step0:
         sim = make_mixed(warm_start="extrapolate", **pinned)
@@ -740,6 +741,7 @@ def main():
     ap.add_argument("--no-floor", action="store_true", help="skip the one-ulp FP64 rounding-floor run")
     ap.add_argument("--profile", action="store_true", help="one form on a synthesized state, for ncu")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"], help="form run by --profile")
+    ap.add_argument("--variant", default=None, help="N-body tile pinned by --profile (default: the form's default)")
     ap.add_argument("--profile-step0", action="store_true",
                     help="with --profile: only step 0 of the mixed form (first factorisation and inverse)")
     ap.add_argument("--workload", default="heave_pitch", choices=list(WORKLOADS) + ["batch256"],
