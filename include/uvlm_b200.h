@@ -97,9 +97,10 @@ typedef struct {
   int32_t nbody_fp64_stages; /* mixed form: N-body stages evaluated in FP64 instead of FP32,
                                 a mask of UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT
                                 (0: all FP32) */
-  int32_t nbody_near_fp64;   /* mixed form, 1: in the FP32 N-body stages, the pairs the far-field test
-                                leaves to the near-field walker (source strips close to the targets)
-                                are evaluated in FP64 from FP64 records and accumulated in FP64 */
+  int32_t nbody_near_fp64;   /* mixed form: FP32 N-body stages (a mask of UVLM_STAGE_*) whose pairs the
+                                far-field test leaves to the near-field walker (source strips close to
+                                the targets) are evaluated in FP64 from FP64 records and accumulated in
+                                FP64; 0: none */
 } uvlm_config;
 
 /* N-body stages of a MainLoop (uvlm_config.nbody_fp64_stages). */

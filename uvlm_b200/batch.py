@@ -226,9 +226,10 @@ def gather_case_rows(rows, mine, n_cases: int, dist=None):
 
 
 def make_batch(cases: list[dict], precision: str = "mixed", advection: str = "euler", max_steps: int = 151,
-               device: int = 0, use_graph: bool = True, stale_factors: bool = True) -> BatchSimulator:
+               device: int = 0, use_graph: bool = True, stale_factors: bool = True,
+               nbody_tile: int = -1) -> BatchSimulator:
     sim = BatchSimulator(precision=precision, advection=advection, max_steps=max_steps, device=device,
-                         use_graph=use_graph, stale_factors=stale_factors)
+                         use_graph=use_graph, stale_factors=stale_factors, nbody_tile=nbody_tile)
     for d in cases:
         sim.add_case(case_morphing(d), d["chord"], d["span"], d["rows"], d["cols"], d["dt"])
     return sim

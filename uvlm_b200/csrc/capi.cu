@@ -146,6 +146,8 @@ struct uvlm_ctx {
   NBodyPrec stage_prec(int stage_bit) const {
     return (!mixed() || (cfg.nbody_fp64_stages & stage_bit)) ? kNBodyFP64 : kNBodyFP32;
   }
+  // whether the FP32 evaluation of a stage takes its near pairs in FP64
+  bool stage_near64(int stage_bit) const { return mixed() && (cfg.nbody_near_fp64 & stage_bit) != 0; }
   Error build_sources(bool with_bound, const double* wake_pos_buf, NBodyPrec prec, SourceBlock* blocks, int* nb_out);
   Error eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec);
   Error shed(long long step);
@@ -244,7 +246,6 @@ Error uvlm_ctx::alloc_all() {
   nb.partial_cap = 3LL * std::max<long long>(64LL * N, 16LL * tcap);
   UVLM_CUDA_TRY(cudaMalloc(&nb.partial, sizeof(double) * nb.partial_cap));
   if (mixed() && cfg.nbody_near_fp64) {
-    nb.near64 = true;
     nb.records64_cap = (long long)(nn + wn) * (long long)sizeof(RecD);
     UVLM_CUDA_TRY(cudaMalloc(&nb.records64, nb.records64_cap));
   }
@@ -299,7 +300,7 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBody
     int best = chosen;
     for (int v = 0; v < nbody_num_variants(); ++v) {
       if (nbody_variant_prec(v) != prec) continue;
-      if (prec == kNBodyFP32 && nb.near64 && !nbody_variant_near64(v)) continue;  // keep the FP64 near field
+      if (prec == kNBodyFP32 && cfg.nbody_near_fp64 && !nbody_variant_near64(v)) continue;  // keep the FP64 near field
       float ms = 0;
       for (int rep = 0; rep < 2; ++rep) {
         UVLM_CUDA_TRY(cudaEventRecord(ev[0], st));
@@ -452,6 +453,7 @@ Error uvlm_ctx::advect(double dt) {
   SourceBlock blocks[2];
   int nbk = 0;
   const NBodyPrec prec = stage_prec(UVLM_STAGE_ADVECT);
+  nb.near64 = stage_near64(UVLM_STAGE_ADVECT);
   auto velocity_at = [&](const double* pos_buf, bool rebuild) -> Error {
     if (rebuild) UVLM_TRY(build_sources(true, pos_buf, prec, blocks, &nbk));
     if (nt > 0) {
@@ -580,6 +582,7 @@ Error uvlm_ctx::stage_rhs() {
     SourceBlock blocks[2];
     int nbk = 0;
     const NBodyPrec prec = stage_prec(UVLM_STAGE_RHS);
+    nb.near64 = stage_near64(UVLM_STAGE_RHS);
     UVLM_TRY(build_sources(false, d_wpos, prec, blocks, &nbk));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_tx, d_cx, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_ty, d_cy, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
@@ -621,6 +624,7 @@ Error uvlm_ctx::stage_loads() {
     SourceBlock blocks[2];
     int nbk = 0;
     const NBodyPrec prec = stage_prec(UVLM_STAGE_LOADS);
+    nb.near64 = stage_near64(UVLM_STAGE_LOADS);
     UVLM_TRY(build_sources(true, d_wpos, prec, blocks, &nbk));
     UVLM_TRY(eval(blocks, nbk, lines, prec));
     UVLM_TRY(launch_loads(ws(), d_pos, d_gamma, d_gamma_prev, d_normal, d_area, d_vx, d_vy, d_vz, d_line_uls, ff,
@@ -754,7 +758,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
   if (k.advection < 0 || k.advection > 3 || k.max_wake_rows < 1 || k.gmres_restart < 1 || k.gmres_max_iter < 1 ||
       !(k.gmres_tol > 0) || k.preconditioner < 0 || k.preconditioner > 1 || k.nbody_fp64_stages < 0 ||
       k.nbody_fp64_stages > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT) || k.nbody_near_fp64 < 0 ||
-      k.nbody_near_fp64 > 1) {
+      k.nbody_near_fp64 > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT)) {
     delete c;
     return set_global(fail(kErrInvalid, "invalid configuration"));
   }
@@ -1187,6 +1191,7 @@ int uvlm_velocity_at(uvlm_ctx* c, const double* targets, int64_t n, int32_t incl
     SourceBlock blocks[2];
     int nbk = 0;
     const NBodyPrec prec = c->mixed() ? kNBodyFP32 : kNBodyFP64;
+    c->nb.near64 = c->stage_near64(UVLM_STAGE_ADVECT);  // a query sees what the wake nodes see
     UVLM_TRY(c->build_sources(true, c->d_wpos, prec, blocks, &nbk));
     std::vector<double> sx, sy, sz;
     for (int64_t k0 = 0; k0 < n; k0 += c->tcap) {

@@ -1223,6 +1223,8 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   if (splits > n_strips) splits = n_strips;
   if (splits > 64) splits = 64;
   if (work->max_splits > 0 && splits > work->max_splits) splits = work->max_splits;
+  // never more splits than the partial-sum buffer holds for these targets
+  if (splits > work->partial_cap / (3 * n_targets)) splits = work->partial_cap / (3 * n_targets);
   if (splits < 1) splits = 1;
   const long long sps = (n_strips + splits - 1) / splits;
   splits = (n_strips + sps - 1) / sps;
