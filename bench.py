@@ -605,6 +605,7 @@ def run_ours(args, rank, world, local_rank):
             "accuracy": accuracy, "warm_start_ablation": warm_ablation,
             "gmres_iters_last": int(st.gmres_iters), "solve_path_last": int(st.solve_path),
             "nbody_variant": U.lib().uvlm_nbody_variant_name(int(st.nbody_variant)).decode(),
+            "plain_fp64_nbody_variant": U.lib().uvlm_nbody_variant_name(int(st64.nbody_variant)).decode(),
             "stage_ms": {"kin_shed": stage_ms[0], "assembly": stage_ms[1], "rhs": stage_ms[2], "solve": stage_ms[3],
                          "loads": stage_ms[4], "advect": stage_ms[5], "total": stage_ms[7]},
             "plain_fp64_stage_ms": {"kin_shed": stage64[0], "assembly": stage64[1], "rhs": stage64[2],
