@@ -100,7 +100,7 @@ typedef struct {
   int32_t nbody_near_fp64;   /* mixed form: FP32 N-body stages (a mask of UVLM_STAGE_*) whose pairs the
                                 far-field test leaves to the near-field walker (source strips close to
                                 the targets) are evaluated in FP64 from FP64 records and accumulated in
-                                FP64; 0: none */
+                                FP64; 0: none; uvlm_config_default sets UVLM_STAGE_RHS */
 } uvlm_config;
 
 /* N-body stages of a MainLoop (uvlm_config.nbody_fp64_stages). */

@@ -135,7 +135,9 @@ def _fullsize():
         wings=[dict(chord=1.0, span=8.0, rows=32, cols=128, origin=(0.0, 0.0, 0.0),
                     kin=dict(plug_amp=0.2, plug_omega=hp_w, twist_amp=10 * DEG, twist_omega=hp_w,
                              twist_phase=math.pi / 2))],
-        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / hp_w / 40, steps=40)
+        ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / hp_w / 40, steps=40,
+        # the mixed form as configured by default (RHS near field in FP64): CL/CD bound per window end
+        mixed=dict(kw={}, windows={40: 1e-6}))
     tw = 0.8
     tandem = dict(
         wings=[dict(chord=1.0, span=4.0, rows=16, cols=64, origin=(x, 0.0, z),
@@ -145,12 +147,21 @@ def _fullsize():
         ff=(-1.0, 0.0, 0.0), advection="RK2", dt=2 * math.pi / tw / 40, steps=20,
         # the front wings' wakes pass through the rear wings' lattices: a wake node that
         # passes a bound segment closely amplifies rounding in its own position
-        gamma_tol=1e-8, wake_pos_tol=1e-4)
+        gamma_tol=1e-8, wake_pos_tol=1e-4,
+        # the near field of every stage in FP64 (the default's 2.6e-6 misses 1e-6 here)
+        mixed=dict(kw=dict(near_fp64=True), windows={20: 1e-6}))
     mw = 0.6
     morphing = dict(
         wings=[dict(chord=1.0, span=8.0, rows=24, cols=96, origin=(0.0, 0.0, 0.0),
                     kin=dict(bend_cx=0.05, bend_cy=0.1, bend_omega=mw))],
-        ff=(-1.0, 0.0, 0.0), advection="euler", dt=2 * math.pi / mw / 40, steps=50)
+        ff=(-1.0, 0.0, 0.0), advection="euler", dt=2 * math.pi / mw / 40, steps=50,
+        # the span bend lifts the tips by up to 1.6 chords: the rolled-up tip wake
+        # passes its own segments closely, which amplifies rounding in those nodes
+        wake_pos_tol=1e-4,
+        # near field of every stage in FP64; after step 40 the tip wake's roll-up amplifies
+        # the FP32 far field's rounding (the FP64 form's own one-ulp sensitivity grows from
+        # 2e-14 to 1.4e-10 between steps 40 and 50)
+        mixed=dict(kw=dict(near_fp64=True), windows={40: 1e-6, 50: 1e-5}))
     return {"heave_pitch_32x128": heave_pitch, "tandem4_16x64": tandem, "morphing_24x96": morphing}
 
 

@@ -65,11 +65,16 @@ def test_fullsize_fp64_matches_oracle(name):
 
 @pytest.mark.parametrize("name", NAMES)
 def test_fullsize_mixed_within_1e6_of_oracle(name):
+    """The mixed form against the oracle, CL and CD relative to max |C| of each
+    wing, within the bound of each window of the case (1e-6, the north-star
+    bound, except where a case states a looser one for a later, chaotic
+    window)."""
     from uvlm_b200.warmstart import MLP
 
+    case = FULLSIZE[name]
     wts = WEIGHTS.get(name)
     kw = dict(precision="mixed", solver="gmres_stale", warm_start="mlp" if wts else "extrapolate")
-    case = FULLSIZE[name]
+    kw.update(case["mixed"]["kw"])
     fx = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
     sim = make_gpu_sim(case, max_wake_rows=case["steps"] + 8, **kw)
     if wts:
@@ -78,7 +83,10 @@ def test_fullsize_mixed_within_1e6_of_oracle(name):
     rows = np.array([sim.step(s, case["dt"]) for s in range(case["steps"])])
     sim.close()
     num = len(case["wings"])
-    cl = max(rel_to_max(rows[:, 2 + 2 * n], fx["loads"][:, 2 + 2 * n]) for n in range(num))
-    cd = max(rel_to_max(rows[:, 1 + 2 * n], fx["loads"][:, 1 + 2 * n]) for n in range(num))
-    print(f"{name} mixed vs oracle over steps 0-{case['steps'] - 1}: CL {cl:.2e}, CD {cd:.2e}")
-    assert cl <= 1e-6 and cd <= 1e-6
+    for end, tol in sorted(case["mixed"]["windows"].items()):
+        cl = max(float(np.max(np.abs(rows[:end, 2 + 2 * n] - fx["loads"][:end, 2 + 2 * n])) /
+                       np.max(np.abs(fx["loads"][:, 2 + 2 * n]))) for n in range(num))
+        cd = max(float(np.max(np.abs(rows[:end, 1 + 2 * n] - fx["loads"][:end, 1 + 2 * n])) /
+                       np.max(np.abs(fx["loads"][:, 1 + 2 * n]))) for n in range(num))
+        print(f"{name} mixed {case['mixed']['kw']} vs oracle over steps 0-{end - 1}: CL {cl:.2e}, CD {cd:.2e}")
+        assert cl <= tol and cd <= tol, (end, cl, cd, tol)

@@ -399,7 +399,7 @@ def test_every_fp32_tile_variant_agrees():
 
     dt = 2 * math.pi / 40
     def run(precision, v=-1):
-        sim = U.SimpleSimulator(precision=precision, nbody_variant=v)
+        sim = U.SimpleSimulator(precision=precision, nbody_variant=v, near_fp64=())  # every tile's own walk
         m = U.Morphing().set_plug(0.2, 1.0).set_twist(math.radians(10), 1.0, math.pi / 2)
         sim.AddWing(U.RectGenerator(), m, 1.0, 8.0, 6, 128)
         sim.set_forward_flight([-1.0, 0.0, 0.0])
@@ -456,7 +456,7 @@ def test_far_field_walker_matches_oracle():
     for v, name in enumerate(names):
         if not name.startswith("fp32") or "_x2" not in name:
             continue
-        sim = M.SimpleSimulator(precision="mixed", nbody_variant=v)
+        sim = M.SimpleSimulator(precision="mixed", nbody_variant=v, near_fp64=())
         sim.AddWing(M.RectGenerator(), M.Morphing(), 1.0, 8.0, rows, cols)
         sim.set_forward_flight([-1.0, 0.0, 0.0])
         sim.begin()

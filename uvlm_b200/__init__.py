@@ -132,14 +132,15 @@ class SimpleSimulator:
                   "rhs", "loads", "advect"
       near_fp64   mixed form: the near-field pairs of the FP32 N-body stages
                   in FP64 (FP64 records, FP64 accumulation): True for every
-                  stage, or any of "rhs", "loads", "advect"
+                  stage, or any of "rhs", "loads", "advect"; None (default)
+                  takes the library's default, the RHS stage
     """
 
     def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
                  lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
                  gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
                  assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True,
-                 preconditioner: str = "inverse", fp64_stages=(), near_fp64=()):
+                 preconditioner: str = "inverse", fp64_stages=(), near_fp64=None):
         cfg = Config()
         lib().uvlm_config_default(C.byref(cfg))
         cfg.precision = PRECISION[precision]
@@ -163,7 +164,8 @@ class SimpleSimulator:
         stages = {"rhs": 1, "loads": 2, "advect": 4}
         if near_fp64 is True:
             near_fp64 = tuple(stages)
-        cfg.nbody_near_fp64 = sum(stages[s] for s in set(near_fp64 or ()))
+        if near_fp64 is not None:
+            cfg.nbody_near_fp64 = sum(stages[s] for s in set(near_fp64 or ()))
         self._cfg = cfg
         h = C.c_void_p()
         check(lib().uvlm_create(C.byref(cfg), C.byref(h)))

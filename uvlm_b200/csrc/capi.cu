@@ -711,6 +711,10 @@ void uvlm_config_default(uvlm_config* c) {
   c->solver = UVLM_SOLVER_LU;
   c->warm_start = UVLM_WARM_PREVIOUS;
   c->lu_precision = UVLM_LU_TF32;
+  // mixed form: the RHS stage's near pairs in FP64 (the wake's newest rows sit
+  // next to the trailing-edge collocation points; their FP32 rounding is the
+  // largest source of circulation error, for about 4 % of the step's time)
+  c->nbody_near_fp64 = UVLM_STAGE_RHS;
   c->advection = UVLM_ADVECT_EULER;
   c->rk_ignore_rows = 5;
   c->max_wake_rows = 1024;
