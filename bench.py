@@ -69,6 +69,14 @@ def variant_index(name):
     raise ValueError(name)
 
 
+def stage_variant_names(st):
+    """The N-body tile each stage ran with in the step whose stats are st."""
+    import uvlm_b200 as U
+
+    return {name: U.lib().uvlm_nbody_variant_name(int(st.stage_variant[i])).decode()
+            for i, name in enumerate(("rhs", "loads", "advect"))}
+
+
 def make_mixed(device=0, warm_start=None, wl=None, **kw):
     """The mixed-precision form: FP32 N-body, TF32 tensor-core LU factored
     once and used stale as the GMRES preconditioner (its dense inverse), FP64
@@ -606,6 +614,8 @@ def run_ours(args, rank, world, local_rank):
             "gmres_iters_last": int(st.gmres_iters), "solve_path_last": int(st.solve_path),
             "nbody_variant": U.lib().uvlm_nbody_variant_name(int(st.nbody_variant)).decode(),
             "plain_fp64_nbody_variant": U.lib().uvlm_nbody_variant_name(int(st64.nbody_variant)).decode(),
+            "nbody_stage_variants": stage_variant_names(st),
+            "plain_fp64_nbody_stage_variants": stage_variant_names(st64),
             "stage_ms": {"kin_shed": stage_ms[0], "assembly": stage_ms[1], "rhs": stage_ms[2], "solve": stage_ms[3],
                          "loads": stage_ms[4], "advect": stage_ms[5], "total": stage_ms[7]},
             "plain_fp64_stage_ms": {"kin_shed": stage64[0], "assembly": stage64[1], "rhs": stage64[2],

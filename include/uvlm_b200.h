@@ -152,6 +152,8 @@ typedef struct {
   double nbody_ms;         /* with stage timing: device time of the step's N-body launches */
   double factor_ms;        /* with stage timing, mixed form: device time of this step's FP32 LU (0 if none) */
   double inverse_ms;       /* ... and of the dense inverse of its factors (0 if none) */
+  int32_t stage_variant[4]; /* N-body tile of the rhs, loads and advect stages ([3] = -1); nbody_variant
+                               is the advect stage's in the context's precision */
 } uvlm_step_stats;
 
 /* ------------------------------------------------------- time-stepper */

@@ -296,8 +296,10 @@ def _influence_like(n, seed):
     return A
 
 
-@pytest.mark.parametrize("n", [5, 64, 200, 700])
+@pytest.mark.parametrize("n", [5, 64, 200, 700, 701, 1030])
 def test_dense_solve_fp64(n):
+    # even n: the pipelined 128 x 128 FP64 trailing update (700, 1030: ragged
+    # edge tiles); odd n: rows not 16-byte aligned, the 64 x 64 update
     A = _influence_like(n, n)
     b = np.random.default_rng(1).standard_normal(n)
     x, _ = U().dense_solve(A, b, "fp64")

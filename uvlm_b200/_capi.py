@@ -62,7 +62,7 @@ class StepStats(C.Structure):
         ("residual", C.c_double), ("refactored", C.c_int32), ("wake_rows", C.c_int32),
         ("stage_ms", C.c_double * 8), ("nbody_variant", C.c_int32), ("pad_", C.c_int32),
         ("initial_residual", C.c_double), ("nbody_ms", C.c_double), ("factor_ms", C.c_double),
-        ("inverse_ms", C.c_double),
+        ("inverse_ms", C.c_double), ("stage_variant", C.c_int32 * 4),
     ]
 
 

@@ -91,7 +91,7 @@ struct uvlm_ctx {
   double* d_A64 = nullptr;   // FP64 matrix (plain: factored in place; mixed: residual matrix if assembly_fp64)
   float* d_A32 = nullptr;    // FP32 matrix of the mixed form
   float* d_F32 = nullptr;    // FP32 factors of the mixed form
-  float* d_Minv = nullptr;   // dense (LU)^-1 P of those factors (UVLM_PRECOND_INVERSE)
+  float* d_Minv = nullptr;   // dense (LU)^-1 of those factors, applied after their row permutation (UVLM_PRECOND_INVERSE)
   double* d_F64 = nullptr;   // mixed form: FP64 factors of the fallback solve (a copy of d_A64)
   LuWork lu64;               // ... and its pivots and scratch
   double* d_tmp = nullptr;   // [N] scratch
@@ -103,8 +103,12 @@ struct uvlm_ctx {
   LuWork lu;
   GmresWork gm;
   bool have_factors = false;
-  int variant_fp64 = 9, variant_fp32 = 16;  // defaults: fp64_h2_t1_b128_m3, fp32_h3_t2_b128_x2f
-  bool tuned = false;  // N-body tile variant chosen (autotune or config)
+  // N-body tile variant per stage (kStageRhs, kStageLoads, kStageAdvect) and
+  // precision ([0] FP32, [1] FP64); defaults fp32_h3_t2_b128_x2f and
+  // fp64_h2_t1_b128_m3, each autotuned on that stage's first large evaluation
+  // unless the configuration pins one
+  int stage_variant[3][2] = {{16, 9}, {16, 9}, {16, 9}};
+  bool stage_tuned[3][2] = {};
   // learned warm start: network (borrowed), per-step features, collected data
   uvlm_mlp* mlp = nullptr;
   double* d_rhs_prev = nullptr;
@@ -149,7 +153,8 @@ struct uvlm_ctx {
   // whether the FP32 evaluation of a stage takes its near pairs in FP64
   bool stage_near64(int stage_bit) const { return mixed() && (cfg.nbody_near_fp64 & stage_bit) != 0; }
   Error build_sources(bool with_bound, const double* wake_pos_buf, NBodyPrec prec, SourceBlock* blocks, int* nb_out);
-  Error eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec);
+  static constexpr int kStageRhs = 0, kStageLoads = 1, kStageAdvect = 2;
+  Error eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec, int stage);
   Error shed(long long step);
   Error solve(long long step);
   Error advect(double dt);
@@ -287,15 +292,17 @@ Error uvlm_ctx::build_sources(bool with_bound, const double* wake_pos_buf, NBody
   return nbody_build_sources(views, nv, prec, &nb, blocks, st);
 }
 
-Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec) {
+Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBodyPrec prec, int stage) {
   const double pairs = (double)nt * (double)nbody_unique_segments(blocks, nblocks);
   work_nbody += pairs;
-  const NBodyPrec main_prec = mixed() ? kNBodyFP32 : kNBodyFP64;
-  if (!tuned && prec == main_prec && nblocks > 0 && pairs >= 2e9) {
-    // Tile autotune on the first large evaluation: time every compiled variant
-    // of this precision on the real sources and targets, keep the fastest
-    // (the default unless another is more than 3% faster).
-    int& chosen = mixed() ? variant_fp32 : variant_fp64;
+  const int pi = prec == kNBodyFP64 ? 1 : 0;
+  int& chosen = stage_variant[stage][pi];
+  if (!stage_tuned[stage][pi] && nblocks > 0 && pairs >= 2e9) {
+    // Tile autotune on the stage's first large evaluation: time every
+    // compiled variant of this precision on the real sources and targets,
+    // keep the fastest (the default unless another is more than 3% faster).
+    // The stages differ in their targets (collocation points, load lines,
+    // wake nodes), and so in the share of far strips the walkers skip.
     float best_ms = 1e30f;
     int best = chosen;
     for (int v = 0; v < nbody_num_variants(); ++v) {
@@ -317,7 +324,7 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBody
       }
     }
     chosen = best;
-    tuned = true;
+    stage_tuned[stage][pi] = true;
   }
   if (nblocks == 0) {
     UVLM_CUDA_TRY(cudaMemsetAsync(d_vx, 0, sizeof(double) * nt, st));
@@ -328,7 +335,7 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBody
 const bool rec = timing && nbev_n < kNbEvents;
   if (rec) UVLM_CUDA_TRY(cudaEventRecord(nbev[2 * nbev_n], st));
   const Error e = nbody_eval(blocks, nblocks, prec, d_tx, d_ty, d_tz, nt, d_vx, d_vy, d_vz, &nb,
-                             prec == kNBodyFP32 ? variant_fp32 : variant_fp64, num_sms, st);
+                             chosen, num_sms, st);
   if (rec) {
     UVLM_CUDA_TRY(cudaEventRecord(nbev[2 * nbev_n + 1], st));
     ++nbev_n;
@@ -458,7 +465,7 @@ Error uvlm_ctx::advect(double dt) {
     if (rebuild) UVLM_TRY(build_sources(true, pos_buf, prec, blocks, &nbk));
     if (nt > 0) {
       UVLM_TRY(launch_gather_wake(L, pos_buf, d_tx, d_ty, d_tz, st));
-      UVLM_TRY(eval(blocks, nbk, nt, prec));
+      UVLM_TRY(eval(blocks, nbk, nt, prec, kStageAdvect));
     }
     return ok();
   };
@@ -587,7 +594,7 @@ Error uvlm_ctx::stage_rhs() {
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_tx, d_cx, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_ty, d_cy, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     UVLM_CUDA_TRY(cudaMemcpyAsync(d_tz, d_cz, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-    UVLM_TRY(eval(blocks, nbk, N, prec));
+    UVLM_TRY(eval(blocks, nbk, N, prec, kStageRhs));
     UVLM_TRY(launch_rhs(N, d_vx, d_vy, d_vz, d_uls, d_normal, ff, d_rhs, st));
   }
   mark(3);
@@ -626,7 +633,7 @@ Error uvlm_ctx::stage_loads() {
     const NBodyPrec prec = stage_prec(UVLM_STAGE_LOADS);
     nb.near64 = stage_near64(UVLM_STAGE_LOADS);
     UVLM_TRY(build_sources(true, d_wpos, prec, blocks, &nbk));
-    UVLM_TRY(eval(blocks, nbk, lines, prec));
+    UVLM_TRY(eval(blocks, nbk, lines, prec, kStageLoads));
     UVLM_TRY(launch_loads(ws(), d_pos, d_gamma, d_gamma_prev, d_normal, d_area, d_vx, d_vy, d_vz, d_line_uls, ff,
                           d_chord_span, t, dt, d_row, st));
   }
@@ -668,7 +675,15 @@ Error uvlm_ctx::stage_advect(double* row) {
   last.step = step;
   last.t = t;
   last.wake_rows = wake_rings();
-  last.nbody_variant = mixed() ? variant_fp32 : variant_fp64;
+  {
+    const int pm = mixed() ? 0 : 1;
+    last.nbody_variant = stage_variant[kStageAdvect][pm];
+    last.stage_variant[0] = stage_variant[kStageRhs][stage_prec(UVLM_STAGE_RHS) == kNBodyFP64 ? 1 : 0];
+    last.stage_variant[1] = stage_variant[kStageLoads][stage_prec(UVLM_STAGE_LOADS) == kNBodyFP64 ? 1 : 0];
+    last.stage_variant[2] = stage_variant[kStageAdvect][stage_prec(UVLM_STAGE_ADVECT) == kNBodyFP64 ? 1 : 0];
+    last.stage_variant[3] = -1;
+    (void)pm;
+  }
   if (timing) {
     float ms[8] = {0};
     const int map[7][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {0, 7}};
@@ -785,7 +800,6 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
   for (auto& e : c->nbev) cudaEventCreate(&e);
   for (auto& e : c->fev) cudaEventCreate(&e);
   if (k.nbody_variant >= 0) {
-    c->tuned = true;
     if (k.nbody_variant >= nbody_num_variants()) {
       uvlm_destroy(c);
       return set_global(fail(kErrInvalid, "nbody_variant out of range"));
@@ -794,10 +808,12 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
       uvlm_destroy(c);
       return set_global(fail(kErrInvalid, "nbody_near_fp64 needs a packed far-field FP32 tile (\"fp32_*_t2_*_x2f\")"));
     }
-    if (k.precision == UVLM_PRECISION_MIXED)
-      c->variant_fp32 = k.nbody_variant;
-    else
-      c->variant_fp64 = k.nbody_variant;
+    // the pinned tile serves every stage of its precision
+    const int pi = nbody_variant_prec(k.nbody_variant) == kNBodyFP64 ? 1 : 0;
+    for (int st = 0; st < 3; ++st) {
+      c->stage_variant[st][pi] = k.nbody_variant;
+      c->stage_tuned[st][pi] = true;
+    }
   }
   *out = c;
   return UVLM_OK;
@@ -1211,7 +1227,7 @@ int uvlm_velocity_at(uvlm_ctx* c, const double* targets, int64_t n, int32_t incl
       UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_tx, sx.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_ty, sy.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(c->d_tz, sz.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st));
-      UVLM_TRY(c->eval(blocks, nbk, cnt, prec));
+      UVLM_TRY(c->eval(blocks, nbk, cnt, prec, uvlm_ctx::kStageAdvect));
       UVLM_CUDA_TRY(cudaMemcpyAsync(sx.data(), c->d_vx, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(sy.data(), c->d_vy, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));
       UVLM_CUDA_TRY(cudaMemcpyAsync(sz.data(), c->d_vz, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st));

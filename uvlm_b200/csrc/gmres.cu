@@ -71,6 +71,11 @@ __global__ void update_kernel(const double* Z, int n, int cnt, const double* y, 
   }
 }
 
+// y[i] = x[perm[i]]
+__global__ void gather_kernel(const double* __restrict__ x, const int* __restrict__ perm, int n, double* y) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) y[k] = x[perm[k]];
+}
+
 inline int grid_n(int n) { return std::max(1, std::min(ceil_div(n, 256), 1184)); }
 
 }  // namespace
@@ -179,9 +184,12 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
     for (; j < m && total < max_iter; ++j) {
       double* Vj = g->V + (size_t)j * n;
       double* Zj = g->Z + (size_t)j * n;
-      if (Minv)
-        UVLM_TRY(matvec(Minv, nullptr, n, Vj, Zj, st));
-      else
+      if (Minv) {
+        // Z_j = (LU)^-1 P V_j: the row permutation of the factors, then the dense inverse
+        gather_kernel<<<grid_n(n), 256, 0, st>>>(Vj, lu->ipiv + n, n, g->w);
+        UVLM_LAUNCH_CHECK();
+        UVLM_TRY(matvec(Minv, nullptr, n, g->w, Zj, st));
+      } else
         UVLM_TRY(lu_solve_f32(LU, n, lu, Vj, Zj, g->ptmp, st));
       UVLM_TRY(matvec(A32, A64, n, Zj, g->w, st));
       // classical Gram-Schmidt, applied twice (CGS2)

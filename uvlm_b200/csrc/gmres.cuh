@@ -36,8 +36,9 @@ void gmres_work_free(GmresWork* g);
 
 // Solves A x = b.  Exactly one of A32 / A64 is non-null (the residual matrix,
 // read with FP64 accumulation).  LU/lu are FP32 factors (lu_factor_f32) of a
-// nearby matrix.  Minv, when non-null, is (LU)^-1 P as a dense FP32 matrix
-// (lu_inverse_f32) and replaces the triangular solves.  x holds the initial
+// nearby matrix.  Minv, when non-null, is (LU)^-1 as a dense FP32 matrix
+// (lu_inverse_f32), applied after the row permutation of the factors (perm =
+// lu->ipiv + n) in place of the triangular solves.  x holds the initial
 // guess on entry.
 Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, LuWork* lu, const float* Minv,
                   const double* b, double* x, double tol, int max_iter, GmresWork* g, GmresResult* res,

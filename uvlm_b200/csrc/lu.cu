@@ -333,6 +333,407 @@ bool launch_panel_cluster(T* A, int n, int k0, int kb, int P, int* ipiv, int* er
   return true;
 }
 
+// ------------------------------------------------ tournament-pivoting panel
+// The panel of kLuNB = 64 columns and m = n - k0 rows in one thread-block
+// cluster of P = ceil(m / 256) CTAs (<= 16), with a few cluster barriers per
+// panel instead of one per column.  The pivot rows are chosen by a tournament
+// (communication-avoiding LU): each CTA factors its 256 rows with partial
+// pivoting and keeps the 64 rows it picks, in pivot order; groups of up to
+// four candidate sets are then merged by factoring their ORIGINAL rows
+// (gathered from A, which the tournament does not modify) and keeping the 64
+// rows picked, in a 4-ary tree over the cluster (the partners' lists are read
+// through distributed shared memory).  The root's factorisation is the
+// panel's top block L11\U11 in the root's pivot order.  The chosen rows are
+// then brought to the top (LAPACK-style swap sequence in ipiv, replayed by
+// every CTA for its own rows), and every other row r gets L21(r) from
+// l U11 = a(r) (forward substitution on its original row).  The remaining
+// columns are swapped by laswp and updated as before.  The pivots differ from
+// column-by-column partial pivoting only where the candidates' magnitudes are
+// close; the factorisation is of the same quality for the influence matrices
+// of the path (and it backs a GMRES solve with FP64 residuals in the mixed
+// form).
+//
+// Each factorisation keeps one row per thread in registers.  Column loop:
+// blocks of 8 columns unrolled (compile-time register indices), a run-time
+// loop over the blocks, and the row shifted left by 8 columns after each
+// block (v[k] is column c0 + k), which keeps the code small and the row in
+// registers.  Per column: a block argmax of (|a|, row id) packed into one
+// 64-bit key (two warp max-reductions per level; ties go to the smaller row
+// id, NaN counts as largest, a finished row has key 0 and never wins; for
+// FP64 the 13 lowest mantissa bits make way for the id, so values within
+// 2^-39 of each other count as tied); the pivot row's owner publishes its
+// U part in shared memory; every other live row stores its multiplier in its
+// shared-memory row of L (Lrow) and eliminates against the pivot row.  Two
+// block barriers per column: a published row from one lane (one warp) costs
+// less than every warp's candidate row before a single barrier.
+constexpr int kTspRows = 256;  // rows per CTA = threads per CTA
+constexpr int kTspMaxCtas = 16;
+constexpr int kTspMaxRows = kTspRows * kTspMaxCtas;
+constexpr int kTspLd = kLuNB + 1;  // Lrow stride: a column of Lrow is conflict-free
+constexpr int kTspTop = kLuNB * kLuNB;
+
+struct TspScratch {
+  unsigned khi[2][kTspRows / 32];  // per-warp argmax keys, by step parity
+  unsigned klo[2][kTspRows / 32];
+  int list[kLuNB];    // this CTA's candidate ids (rows relative to k0), in pivot order
+  int pivrow[kLuNB];  // the thread (Lrow row) of each pivot of the last factorisation
+  int seq[kLuNB];     // the swap sequence (positions relative to k0)
+  int cnt[4];         // [0] this CTA's candidate count; [1..3] partners' counts while merging
+  short at[kTspMaxRows];   // original row (relative to k0) at each position
+  short pos[kTspMaxRows];  // position of each original row
+};
+
+template <class T>
+constexpr size_t tsp_smem() {
+  return sizeof(T) * ((size_t)kTspTop + (size_t)kTspRows * kTspLd) + sizeof(TspScratch);
+}
+
+// One row of the panel (64 values from column k0) from A into registers;
+// vector loads when the row start is 16-byte aligned.
+template <class T>
+__device__ __forceinline__ void tsp_load_row(const T* __restrict__ A, long long off, T (&v)[kLuNB]) {
+  const T* src = A + off;
+  if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    constexpr int kPer = 16 / sizeof(T);
+#pragma unroll
+    for (int q = 0; q < kLuNB / kPer; ++q) {
+      if constexpr (sizeof(T) == 8) {
+        const double2 t = reinterpret_cast<const double2*>(src)[q];
+        v[2 * q] = t.x;
+        v[2 * q + 1] = t.y;
+      } else {
+        const float4 t = reinterpret_cast<const float4*>(src)[q];
+        v[4 * q] = t.x;
+        v[4 * q + 1] = t.y;
+        v[4 * q + 2] = t.z;
+        v[4 * q + 3] = t.w;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kLuNB; ++j) v[j] = src[j];
+  }
+}
+
+// Argmax key of a row: (hi, lo) compared lexicographically; 0 for a finished row.
+template <class T>
+__device__ __forceinline__ void tsp_key(T a, int id, bool alive, unsigned& hi, unsigned& lo) {
+  hi = 0u;
+  lo = 0u;
+  if (!alive) return;
+  const unsigned tag = 0x1000u - (unsigned)id;  // ids < 4096: 1 .. 0x1000, larger for smaller ids
+  if constexpr (sizeof(T) == 4) {
+    const float x = fabsf(a);
+    hi = x != x ? 0xFFFFFFFFu : __float_as_uint(x);
+    lo = tag;
+  } else {
+    const double x = fabs(a);
+    const unsigned long long b = x != x ? ~0ull : (unsigned long long)__double_as_longlong(x);
+    hi = (unsigned)(b >> 32);
+    lo = ((unsigned)b & ~0x1FFFu) | tag;
+  }
+}
+
+// Eight consecutive values at a 32-byte aligned address (vector accesses).
+template <class T>
+__device__ __forceinline__ void tsp_ld8(const T* p, T (&o)[8]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+    o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w, o[4] = b.x, o[5] = b.y, o[6] = b.z, o[7] = b.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 a = reinterpret_cast<const double2*>(p)[q];
+      o[2 * q] = a.x;
+      o[2 * q + 1] = a.y;
+    }
+  }
+}
+
+// uc[8 jc + t] = v[8 jc + t] (column c0 + 8 jc + t) for the 8-column chunks
+// that reach column c (= c0 + k) and lie left of column 64 (the shifted row's
+// entries past column 63 are dead); the chunk holding column c also writes
+// the columns left of it, which no reader uses.
+template <class T>
+__device__ __forceinline__ void tsp_publish(T* uc, int c0, int k, const T (&v)[kLuNB]) {
+#pragma unroll
+  for (int jc = 0; jc < 8; ++jc) {
+    if (8 * jc + 7 < k) continue;
+    if (c0 + 8 * jc < kLuNB) {
+      T* p = uc + 8 * jc;
+      if constexpr (sizeof(T) == 4) {
+        reinterpret_cast<float4*>(p)[0] = make_float4(v[8 * jc], v[8 * jc + 1], v[8 * jc + 2], v[8 * jc + 3]);
+        reinterpret_cast<float4*>(p)[1] = make_float4(v[8 * jc + 4], v[8 * jc + 5], v[8 * jc + 6], v[8 * jc + 7]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          reinterpret_cast<double2*>(p)[q] = make_double2(v[8 * jc + 2 * q], v[8 * jc + 2 * q + 1]);
+      }
+    }
+  }
+}
+
+// The elimination of step c = c0 + k against the pivot row uc (column c0 + j
+// at uc[j]): l = v[k] / uc[k] into *lk, v[j] -= l uc[j] for the live columns
+// right of c, chunk by chunk.  A zero pivot leaves the row as it is and
+// returns v[k] as its multiplier.
+template <class T>
+__device__ __forceinline__ void tsp_eliminate(T (&v)[kLuNB], const T* uc, int c0, int k, T* lk) {
+  const T piv = uc[k];
+  if (piv == (T)0) {
+    *lk = v[k];
+    return;
+  }
+  const T l = v[k] / piv;
+  *lk = l;
+#pragma unroll
+  for (int jc = 0; jc < 8; ++jc) {
+    if (8 * jc + 7 < k + 1) continue;
+    if (c0 + 8 * jc < kLuNB) {
+      T t8[8];
+      tsp_ld8<T>(uc + 8 * jc, t8);
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (8 * jc + t >= k + 1) v[8 * jc + t] -= l * t8[t];
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void tsp_shift8(T (&v)[kLuNB]) {
+#pragma unroll
+  for (int j = 0; j < kLuNB - 8; ++j) v[j] = v[j + 8];
+}
+
+// Partial-pivoting elimination of the R <= 256 rows held by threads
+// 0 .. R-1 (v, original id myid).  Picks min(64, R) pivot rows: their ids go
+// to out[] in pivot order, the owning threads to sc.pivrow[]; step c leaves
+// the pivot row's U part in Top[c] (columns c .. 63) and every other row's
+// multiplier in Lrow[thread][c].  Per column: the per-warp keys (of the
+// step's parity: a slow reader of step c may still read them while a fast
+// warp writes those of step c + 1) and a barrier; the block key; the owner
+// publishes its row and a barrier; the others eliminate.  The operations on
+// each row are those of a column-by-column factorisation, in the same order.
+// Every thread of the CTA calls it.
+template <class T>
+__device__ int tsp_factor(T (&v)[kLuNB], bool alive, int myid, int R, T* Top, T* Lrow, TspScratch& sc,
+                          int* out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int steps = min(kLuNB, R);
+  T* lrow = Lrow + tid * kTspLd;
+#pragma unroll 1
+  for (int c0 = 0; c0 < steps; c0 += 8) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int c = c0 + k;
+      if (c < steps) {  // uniform
+        const int par = c & 1;
+        unsigned hi, lo;
+        tsp_key<T>(v[k], myid, alive, hi, lo);
+        const unsigned whi = __reduce_max_sync(0xffffffffu, hi);
+        const unsigned wlo = __reduce_max_sync(0xffffffffu, hi == whi ? lo : 0u);
+        if (lane == 0) {
+          sc.khi[par][warp] = whi;
+          sc.klo[par][warp] = wlo;
+        }
+        __syncthreads();
+        const unsigned ph = lane < kTspRows / 32 ? sc.khi[par][lane] : 0u;
+        const unsigned pl = lane < kTspRows / 32 ? sc.klo[par][lane] : 0u;
+        const unsigned bhi = __reduce_max_sync(0xffffffffu, ph);
+        const unsigned blo = __reduce_max_sync(0xffffffffu, ph == bhi ? pl : 0u);
+        T* u = Top + c * kLuNB + c0;  // column c0 + j at u[j]
+        if (alive && hi == bhi && lo == blo) {
+          out[c] = 0x1000 - (int)(blo & 0x1FFFu);
+          sc.pivrow[c] = tid;
+          tsp_publish<T>(u, c0, k, v);
+          alive = false;
+        }
+        __syncthreads();
+        if (alive) tsp_eliminate<T>(v, u, c0, k, lrow + c);
+      }
+    }
+    tsp_shift8<T>(v);
+  }
+  __syncthreads();  // Top, Lrow, out and pivrow complete for every thread
+  return steps;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTspRows, 1) lu_panel_tsp_kernel(T* A, int lda, int n, int k0, int* ipiv,
+                                                                   int* err) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* Top = reinterpret_cast<T*>(smraw);  // [64][64]: the pivot rows' U parts (columns c .. 63 of row c)
+  T* Lrow = Top + kTspTop;               // [256][kTspLd]: multipliers of each thread's row
+  TspScratch& sc = *reinterpret_cast<TspScratch*>(Lrow + kTspRows * kTspLd);
+  const int P = (int)cl.num_blocks(), bid = (int)cl.block_rank(), tid = threadIdx.x;
+  const int m = n - k0;
+  const int rb = bid * kTspRows;
+  const int nloc = max(0, min(kTspRows, m - rb));
+  T v[kLuNB];
+
+  // ---- phase 1: this CTA's rows
+  {
+    const bool alive = tid < nloc;
+    if (alive) tsp_load_row<T>(A, (long long)(k0 + rb + tid) * lda + k0, v);
+    const int k = tsp_factor<T>(v, alive, rb + tid, nloc, Top, Lrow, sc, sc.list);
+    if (tid == 0) sc.cnt[0] = k;
+  }
+
+  // ---- phase 2: 4-ary tournament tree over the cluster; the merges factor
+  // the candidates' original rows
+  for (int step = 1; step < P; step *= 4) {
+    cl.sync();  // the candidate lists of this level are final
+    if ((bid % (4 * step)) == 0 && bid + step < P) {
+      if (tid == 0)
+        for (int g = 1; g < 4; ++g) {
+          const int src = bid + g * step;
+          sc.cnt[g] = src < P ? *cl.map_shared_rank(&sc.cnt[0], src) : 0;
+        }
+      __syncthreads();
+      int R = 0, myid = INT_MAX;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const int c = sc.cnt[g];
+        if (tid >= R && tid < R + c)
+          myid = g == 0 ? sc.list[tid - R] : *cl.map_shared_rank(&sc.list[tid - R], bid + g * step);
+        R += c;
+      }
+      const bool alive = tid < R;
+      if (alive) tsp_load_row<T>(A, (long long)(k0 + myid) * lda + k0, v);
+      const int k = tsp_factor<T>(v, alive, myid, R, Top, Lrow, sc, sc.list);
+      if (tid == 0) sc.cnt[0] = k;
+    }
+  }
+  cl.sync();  // the root's Top, Lrow, pivrow and list are final
+
+  // ---- phase 3: the swap sequence (CTA 0), sent to every CTA; the row map
+  for (int q = tid; q < m; q += kTspRows) {
+    sc.at[q] = (short)q;
+    sc.pos[q] = (short)q;
+  }
+  __syncthreads();
+  const int kb = kLuNB;  // m >= 64: the launcher's condition
+  if (bid == 0 && tid == 0) {
+    for (int i = 0; i < kb; ++i) {
+      const int r = sc.list[i];
+      const int qn = sc.pos[r];
+      const int ri = sc.at[i];
+      sc.at[i] = (short)r;
+      sc.pos[r] = (short)i;
+      sc.at[qn] = (short)ri;
+      sc.pos[ri] = (short)qn;
+      sc.seq[i] = qn;
+      ipiv[k0 + i] = k0 + qn;
+    }
+  }
+  __syncthreads();
+  if (bid == 0)
+    for (int q = tid; q < (P - 1) * kb; q += kTspRows) {
+      const int c = 1 + q / kb, i = q - (c - 1) * kb;
+      *cl.map_shared_rank(&sc.seq[i], c) = sc.seq[i];
+    }
+  cl.sync();
+  if (bid > 0) {
+    if (tid == 0)
+      for (int i = 0; i < kb; ++i) {
+        const int qn = sc.seq[i];
+        const short t = sc.at[i];
+        sc.at[i] = sc.at[qn];
+        sc.at[qn] = t;
+      }
+    // U11 from the root
+    const T* root = cl.map_shared_rank(Top, 0);
+    for (int q = tid; q < kLuNB * kLuNB; q += kTspRows) Top[q] = root[q];
+  }
+  __syncthreads();
+  // this CTA's rows below the top block: original values by new position
+  const int p = rb + tid;
+  const bool mine = tid < nloc && p >= kb;
+  if (mine) tsp_load_row<T>(A, (long long)(k0 + sc.at[p]) * lda + k0, v);
+  cl.sync();  // every CTA holds its original rows before any row of A is overwritten
+
+  // ---- phase 4: the top block L11\U11 from the root, then L21 from l U11 = a
+  if (bid == 0) {
+    for (int q = tid; q < kb * kLuNB; q += kTspRows) {
+      const int i = q / kLuNB, c = q - i * kLuNB;
+      A[(long long)(k0 + i) * lda + k0 + c] = c < i ? Lrow[sc.pivrow[i] * kTspLd + c] : Top[q];
+    }
+    if (tid < kb && Top[tid * kLuNB + tid] == (T)0) atomicExch(err + 1, 1);
+    __syncthreads();  // the root's Lrow is read before the substitution below overwrites it
+  }
+  if (mine) {
+    // by columns: the operations, in order, of eliminating this row against
+    // the pivot rows in a column-by-column factorisation
+    T* lrow = Lrow + tid * kTspLd;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kLuNB; c0 += 8) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int c = c0 + k;
+        tsp_eliminate<T>(v, Top + c * kLuNB + c0, c0, k, lrow + c);
+        if (Top[c * kLuNB + c] == (T)0) lrow[c] = (T)0;  // a zero pivot: multiplier 0 (the factor is singular)
+      }
+      tsp_shift8<T>(v);
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < nloc * kLuNB; q += kTspRows) {
+    const int r = q >> 6, c = q & (kLuNB - 1);
+    if (rb + r >= kb) A[(long long)(k0 + rb + r) * lda + k0 + c] = Lrow[r * kTspLd + c];
+  }
+  // every access to another CTA's shared memory came before the last cluster
+  // barrier, so the CTAs may leave independently
+}
+
+// Launches the tournament panel; false when it cannot run (a panel narrower
+// than 64 columns, too many rows for one cluster, or the cluster cannot be
+// formed).
+template <class T>
+bool launch_panel_tsp(T* A, int n, int k0, int kb, int* ipiv, int* err, cudaStream_t st) {
+  const int m = n - k0;
+  const int P = ceil_div(m, kTspRows);
+  if (P > kTspMaxCtas || kb != kLuNB || m < kLuNB) return false;
+  auto kern = lu_panel_tsp_kernel<T>;
+  const size_t smem = tsp_smem<T>();
+  static PerDeviceOnce configured;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (!once_on_device(configured, dev, [&] {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+          cudaGetLastError();
+          return false;
+        }
+        return true;
+      }))
+    return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P);
+  cfg.blockDim = dim3(kTspRows);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = P;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaLaunchKernelEx(&cfg, kern, A, n, n, k0, ipiv, err) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  note_launch();
+  return true;
+}
+
 // Row swaps of one panel applied to the columns outside the panel.
 template <class T>
 __global__ void laswp_kernel(T* A, int lda, int n, int k0, int kb, const int* __restrict__ ipiv) {
@@ -430,6 +831,126 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(T* C, int ldc, const T
     for (int j = 0; j < 4; ++j) {
       const int c = col0 + tx * 4 + j;
       if (c < nc) C[(long long)r * ldc + c] -= acc[i][j];
+    }
+  }
+}
+
+// FP64 trailing update C -= A B of the plain form's LU (K = the panel width):
+// 128 x 128 output tiles, 256 threads each holding an 8 x 8 register block
+// (rows ty*4 + i and 64 + ty*4 + i, columns tx*4 + j and 64 + tx*4 + j), K
+// in steps of 16 through a three-stage cp.async pipeline.  Each product is
+// accumulated over k in order with FMAs and subtracted from C once, as in
+// gemm_update_kernel, so both kernels give the same bits.  The 16-byte copies
+// need 16-byte aligned rows: even leading dimensions and aligned bases.
+constexpr int kG64BM = 128, kG64BN = 128, kG64BK = 16, kG64Stages = 3;
+constexpr int kG64ALd = kG64BK + 2;  // 144-byte rows of the A tile: the 4-row strides fall on other banks
+constexpr int kG64StageA = kG64BM * kG64ALd;
+constexpr int kG64StageB = kG64BK * kG64BN;
+constexpr size_t kG64Smem = sizeof(double) * kG64Stages * (kG64StageA + kG64StageB);
+
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 1) gemm_update_f64_kernel(double* C, int ldc, const double* __restrict__ A,
+                                                                 int lda, const double* __restrict__ B, int ldb,
+                                                                 int m, int nc, int k) {
+  extern __shared__ __align__(16) double g64_smem[];
+  double* sA = g64_smem;                                // [stages][128][18]
+  double* sB = g64_smem + kG64Stages * kG64StageA;     // [stages][16][128]
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int row0 = blockIdx.y * kG64BM, col0 = blockIdx.x * kG64BN;
+  const int steps = (k + kG64BK - 1) / kG64BK;
+
+  // 16-byte chunks (two doubles) of one K step; a chunk past the matrix is
+  // zero-filled (the source address is then clamped to a valid one)
+  auto load_step = [&](int t, int slot) {
+    const int kk0 = t * kG64BK;
+    double* a = sA + slot * kG64StageA;
+    double* b = sB + slot * kG64StageB;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int q = tid + 256 * i;
+      const int r = q >> 3, c2 = (q & 7) * 2;
+      const int gr = row0 + r, gk = kk0 + c2;
+      const int bytes = gr < m ? 8 * max(0, min(2, k - gk)) : 0;
+      const double* src = bytes ? A + (long long)gr * lda + gk : A;
+      cp_async16_zfill(a + r * kG64ALd + c2, src, bytes);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int q = tid + 256 * i;
+      const int r = q >> 6, c2 = (q & 63) * 2;
+      const int gk = kk0 + r, gc = col0 + c2;
+      const int bytes = gk < k ? 8 * max(0, min(2, nc - gc)) : 0;
+      const double* src = bytes ? B + (long long)gk * ldb + gc : B;
+      cp_async16_zfill(b + r * kG64BN + c2, src, bytes);
+    }
+  };
+
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < kG64Stages - 1; ++s) {
+    if (s < steps) load_step(s, s);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  for (int t = 0; t < steps; ++t) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kG64Stages - 2) : "memory");
+    __syncthreads();  // step t landed for every thread; slot (t - 1) % stages is free
+    if (t + kG64Stages - 1 < steps) load_step(t + kG64Stages - 1, (t + kG64Stages - 1) % kG64Stages);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const double* a = sA + (t % kG64Stages) * kG64StageA;
+    const double* b = sB + (t % kG64Stages) * kG64StageB;
+#pragma unroll
+    for (int kk = 0; kk < kG64BK; ++kk) {
+      double av[8], bv[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        av[i] = a[(ty * 4 + i) * kG64ALd + kk];
+        av[4 + i] = a[(64 + ty * 4 + i) * kG64ALd + kk];
+      }
+      const double2 b0 = *reinterpret_cast<const double2*>(b + kk * kG64BN + tx * 4);
+      const double2 b1 = *reinterpret_cast<const double2*>(b + kk * kG64BN + tx * 4 + 2);
+      const double2 b2 = *reinterpret_cast<const double2*>(b + kk * kG64BN + 64 + tx * 4);
+      const double2 b3 = *reinterpret_cast<const double2*>(b + kk * kG64BN + 64 + tx * 4 + 2);
+      bv[0] = b0.x, bv[1] = b0.y, bv[2] = b1.x, bv[3] = b1.y;
+      bv[4] = b2.x, bv[5] = b2.y, bv[6] = b3.x, bv[7] = b3.y;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = row0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+    if (r >= m) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = col0 + h * 64 + tx * 4;
+      double* cp = C + (long long)r * ldc + c;
+      if (c + 3 < nc) {
+        double2 v0 = *reinterpret_cast<double2*>(cp);
+        double2 v1 = *reinterpret_cast<double2*>(cp + 2);
+        v0.x -= acc[i][h * 4 + 0];
+        v0.y -= acc[i][h * 4 + 1];
+        v1.x -= acc[i][h * 4 + 2];
+        v1.y -= acc[i][h * 4 + 3];
+        *reinterpret_cast<double2*>(cp) = v0;
+        *reinterpret_cast<double2*>(cp + 2) = v1;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (c + j < nc) cp[j] -= acc[i][h * 4 + j];
+      }
     }
   }
 }
@@ -619,7 +1140,10 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
     unsigned* bar = w->bar;
     int* err = w->err;
     int nn = n, kk0 = k0, kkb = kb, rr = rpc;
-    if (!launch_panel_cluster<T>(A, n, k0, kb, P, ipiv, err, st)) {
+    // tournament pivoting in one cluster; else the column-by-column cluster
+    // panel; else the cooperative kernel
+    if (!(w->tournament && launch_panel_tsp<T>(A, n, k0, kb, ipiv, err, st)) &&
+        !launch_panel_cluster<T>(A, n, k0, kb, P, ipiv, err, st)) {
       void* args[] = {&A, &lda, &nn, &kk0, &kkb, &ipiv, &cv, &cr, &cd, &dd, &bar, &err, &rr};
       UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(kPanelRows), args, smem, st));
       note_launch();
@@ -696,20 +1220,20 @@ Error tri_solve(const T* LU, int n, LuWork* w, const double* vin, V* y, V* z, do
 }
 
 // Y = P (the row permutation of the factorisation as a dense matrix).
-__global__ void perm_matrix_kernel(const int* __restrict__ perm, int n, float* Y) {
+__global__ void identity_kernel(int n, float* Y) {
   const long long total = (long long)n * n;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
        q += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(q / n), c = (int)(q % n);
-    Y[q] = (c == perm[r]) ? 1.f : 0.f;
+    Y[q] = (c == r) ? 1.f : 0.f;
   }
 }
 
-// Y[rows r0 .. r0+nb) = D * Y[rows r0 .. r0+nb), D a kTriB x kTriB block
-// (rows/cols >= nb are identity padding), in place: each CTA owns 64 columns
-// and reads its whole tile before writing.
+// Y[rows r0 .. r0+nb) = D * Y[rows r0 .. r0+nb) on the columns below ncols,
+// D a kTriB x kTriB block (rows/cols >= nb are identity padding), in place:
+// each CTA owns 64 columns and reads its whole tile before writing.
 __global__ void __launch_bounds__(256) apply_block_kernel(const float* __restrict__ D, float* Y, int n, int r0,
-                                                          int nb) {
+                                                          int nb, int ncols) {
   __shared__ float Ds[kTriB][kTriB + 1];
   __shared__ float Ts[kTriB][kTriB];
   const int c0 = blockIdx.x * 64;
@@ -717,7 +1241,7 @@ __global__ void __launch_bounds__(256) apply_block_kernel(const float* __restric
   for (int q = tid; q < kTriB * kTriB; q += 256) {
     const int i = q / kTriB, j = q % kTriB;
     Ds[i][j] = D[q];
-    Ts[i][j] = (i < nb && c0 + j < n) ? Y[(long long)(r0 + i) * n + c0 + j] : 0.f;
+    Ts[i][j] = (i < nb && c0 + j < ncols) ? Y[(long long)(r0 + i) * n + c0 + j] : 0.f;
   }
   __syncthreads();
   const int tx = tid & 15, ty = tid >> 4;
@@ -740,7 +1264,7 @@ __global__ void __launch_bounds__(256) apply_block_kernel(const float* __restric
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int c = c0 + tx * 4 + j;
-      if (c < n) Y[(long long)(r0 + r) * n + c] = acc[i][j];
+      if (c < ncols) Y[(long long)(r0 + r) * n + c] = acc[i][j];
     }
   }
 }
@@ -774,22 +1298,22 @@ __global__ void split_a3_kernel(const float* __restrict__ A, int lda, int m, flo
   }
 }
 
-// B3[j][0:64] = hi, [64:128] = hi, [128:192] = lo of X[r0 + k][j]: block row
-// r0 of X (row-major, leading dimension n) transposed, 32 x 32 tiles through
-// shared memory.
-__global__ void __launch_bounds__(256) split_b3_kernel(const float* __restrict__ X, int n, int r0,
+// B3[j][0:64] = hi, [64:128] = hi, [128:192] = lo of X[r0 + k][j], j < ncols:
+// block row r0 of X (row-major, leading dimension n) transposed, 32 x 32
+// tiles through shared memory.
+__global__ void __launch_bounds__(256) split_b3_kernel(const float* __restrict__ X, int n, int ncols, int r0,
                                                        float* __restrict__ B3) {
   __shared__ float t[32][33];
   const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (int r = ty; r < 32; r += 8) {
     const int j = j0 + tx;
-    t[r][tx] = j < n ? X[(long long)(r0 + k0 + r) * n + j] : 0.f;
+    t[r][tx] = j < ncols ? X[(long long)(r0 + k0 + r) * n + j] : 0.f;
   }
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
     const int j = j0 + r;
-    if (j < n) {
+    if (j < ncols) {
       const float b = t[tx][r], h = tf32_hi(b);
       float* o = B3 + (long long)j * 3 * kTriB + k0 + tx;
       o[0] = h;
@@ -802,42 +1326,43 @@ __global__ void __launch_bounds__(256) split_b3_kernel(const float* __restrict__
 Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, cudaStream_t st) {
   if (n <= 0) return ok();
   const int nblk = ceil_div(n, kTriB);
-  const int* perm = w->ipiv + n;
   const float* dl = reinterpret_cast<const float*>(w->dinv_l);
   const float* du = reinterpret_cast<const float*>(w->dinv_u);
-  perm_matrix_kernel<<<std::min<long long>(ceil_div((long long)n * n, 256), 4096), 256, 0, st>>>(perm, n, X);
+  identity_kernel<<<std::min<long long>(ceil_div((long long)n * n, 256), 4096), 256, 0, st>>>(n, X);
   UVLM_LAUNCH_CHECK();
-  const int cg = ceil_div(n, 64);
   // Right-looking block substitution: each finished block row X_I (times the
   // inverse of its diagonal block) is subtracted from the rows still to come
-  // in one rank-kTriB update, C -= A X_I: split-TF32 on the tensor cores when
-  // the operands are TMA-aligned (n % 4 == 0, whole 64-row blocks), else SIMT.
+  // in one rank-kTriB update, C -= A X_I, on the columns X_I can be non-zero
+  // in: split-TF32 on the tensor cores when the operands are TMA-aligned
+  // (n % 4 == 0, whole 64-row blocks), else SIMT.
   const bool tc = upd != kLuUpdateSimt && n % 4 == 0 && w->a3 != nullptr && w->b3 != nullptr;
-  auto update = [&](float* C, const float* A, int m, int r0, int nb) -> Error {
-    if (m <= 0) return ok();
+  auto update = [&](float* C, const float* A, int m, int ncols, int r0, int nb) -> Error {
+    if (m <= 0 || ncols <= 0) return ok();
     if (tc && nb == kTriB) {
       split_a3_kernel<<<std::min<long long>(ceil_div((long long)m * kTriB, 256), 4096), 256, 0, st>>>(A, n, m, w->a3);
       UVLM_LAUNCH_CHECK();
-      split_b3_kernel<<<dim3(ceil_div(n, 32), kTriB / 32), 256, 0, st>>>(X, n, r0, w->b3);
+      split_b3_kernel<<<dim3(ceil_div(ncols, 32), kTriB / 32), 256, 0, st>>>(X, n, ncols, r0, w->b3);
       UVLM_LAUNCH_CHECK();
-      return gemm_update_tc(C, n, w->a3, 3 * kTriB, w->b3, 3 * kTriB, m, n, 3 * kTriB, kLuUpdateTF32, w, st);
+      return gemm_update_tc(C, n, w->a3, 3 * kTriB, w->b3, 3 * kTriB, m, ncols, 3 * kTriB, kLuUpdateTF32, w, st);
     }
-    return gemm_update_f32_simt(C, n, A, n, X + (long long)r0 * n, n, m, n, nb, st);
+    return gemm_update_f32_simt(C, n, A, n, X + (long long)r0 * n, n, m, ncols, nb, st);
   };
-  // X = L^-1 P (L unit lower triangular): X_I = Linv_II X_I, then
-  // X_>I -= L_>I,I X_I
+  // X = L^-1 (L unit lower triangular, so X is too: block row I is non-zero
+  // only in the columns below r1): X_I = Linv_II X_I, then
+  // X_>I -= L_>I,I X_I on those columns
   for (int I = 0; I < nblk; ++I) {
     const int r0 = I * kTriB, nb = std::min(kTriB, n - r0), r1 = r0 + nb;
-    apply_block_kernel<<<cg, 256, 0, st>>>(dl + (long long)I * kTriB * kTriB, X, n, r0, nb);
+    apply_block_kernel<<<ceil_div(r1, 64), 256, 0, st>>>(dl + (long long)I * kTriB * kTriB, X, n, r0, nb, r1);
     UVLM_LAUNCH_CHECK();
-    UVLM_TRY(update(X + (long long)r1 * n, LU + (long long)r1 * n + r0, n - r1, r0, nb));
+    UVLM_TRY(update(X + (long long)r1 * n, LU + (long long)r1 * n + r0, n - r1, r1, r0, nb));
   }
-  // X = U^-1 X: X_I = Uinv_II X_I, then X_<I -= U_<I,I X_I
+  // X = U^-1 X (dense): X_I = Uinv_II X_I, then X_<I -= U_<I,I X_I
+  const int cg = ceil_div(n, 64);
   for (int I = nblk - 1; I >= 0; --I) {
     const int r0 = I * kTriB, nb = std::min(kTriB, n - r0);
-    apply_block_kernel<<<cg, 256, 0, st>>>(du + (long long)I * kTriB * kTriB, X, n, r0, nb);
+    apply_block_kernel<<<cg, 256, 0, st>>>(du + (long long)I * kTriB * kTriB, X, n, r0, nb, n);
     UVLM_LAUNCH_CHECK();
-    UVLM_TRY(update(X, LU + r0, r0, r0, nb));
+    UVLM_TRY(update(X, LU + r0, r0, n, r0, nb));
   }
   return ok();
 }
@@ -918,6 +1443,20 @@ Error lu_solve_f32(const float* LU, int n, LuWork* w, const double* v, double* z
 Error gemm_update_f64(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int m, int nc, int k,
                       cudaStream_t st) {
   if (m <= 0 || nc <= 0 || k <= 0) return ok();
+  const bool aligned = lda % 2 == 0 && ldb % 2 == 0 && ldc % 2 == 0 &&
+                       ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) |
+                         reinterpret_cast<uintptr_t>(C)) % 16) == 0;
+  static PerDeviceOnce attr_once;
+  int dev = 0;
+  if (aligned && cudaGetDevice(&dev) == cudaSuccess && once_on_device(attr_once, dev, [] {
+        return cudaFuncSetAttribute(gemm_update_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kG64Smem) == cudaSuccess;
+      })) {
+    dim3 grid(ceil_div(nc, kG64BN), ceil_div(m, kG64BM));
+    gemm_update_f64_kernel<<<grid, 256, kG64Smem, st>>>(C, ldc, A, lda, B, ldb, m, nc, k);
+    UVLM_LAUNCH_CHECK();
+    return ok();
+  }
   dim3 grid(ceil_div(nc, 64), ceil_div(m, 64));
   gemm_update_kernel<double><<<grid, 256, 0, st>>>(C, ldc, A, lda, B, ldb, m, nc, k);
   UVLM_LAUNCH_CHECK();

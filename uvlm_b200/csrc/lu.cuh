@@ -10,9 +10,12 @@
 //
 // Layout: A is row-major n x n (row K = collocation point, column L = ring).
 // Factor: per panel of kLuNB columns
-//   1. lu_panel   -- one cooperative kernel; every CTA keeps a slice of the
-//                    panel rows in shared memory; per column a grid barrier
-//                    (bounded wait) selects the pivot from per-CTA candidates;
+//   1. lu_panel   -- one thread-block cluster (<= 16 CTAs of 256 rows): the
+//                    pivot rows chosen by a tournament (each CTA factors its
+//                    rows, candidate sets merged in a 4-ary tree through
+//                    distributed shared memory), then L21 by substitution;
+//                    else a cluster with one barrier per column; else one
+//                    cooperative kernel with a bounded grid barrier per column;
 //   2. laswp      -- the panel's row swaps applied to the other columns;
 //   3. trsm       -- U12 = L11^-1 A12;
 //   4. update     -- A22 -= L21 U12: FP64 SIMT GEMM (plain form) or a tcgen05
@@ -53,6 +56,7 @@ struct LuWork {
   void* opB = nullptr;
   int elem_size = 8;
   int num_sms = 148;
+  bool tournament = true;     // panel pivots by a tournament (one cluster per panel) where it fits
 };
 
 constexpr int kLuMaxCtas = 148;
@@ -71,10 +75,13 @@ Error lu_solve_f64(const double* LU, int n, LuWork* w, const double* b, double* 
 // z = (LU)^-1 v with FP32 factors: FP64 in/out, FP32 arithmetic (preconditioner).
 Error lu_solve_f32(const float* LU, int n, LuWork* w, const double* v, double* z, float* tmp, cudaStream_t st);
 
-// X = (LU)^-1 P = A^-1 as a dense row-major FP32 matrix from the factors of
-// lu_factor_f32 (block forward then backward substitution on the identity
-// permuted by the pivots, GEMM updates between the diagonal-block inverses).
-// A stale preconditioner applied as one dense matrix-vector product.
+// X = (LU)^-1 = U^-1 L^-1 as a dense row-major FP32 matrix from the factors
+// of lu_factor_f32 (block forward then backward substitution on the identity,
+// GEMM updates between the diagonal-block inverses; the forward pass updates
+// only the lower-triangular part it can fill).  A^-1 = X P: applied to v as
+// X (P v) with (P v)[i] = v[perm[i]], perm = ipiv + n of the same LuWork.
+// A stale preconditioner applied as one gather and one dense matrix-vector
+// product.
 Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, cudaStream_t st);
 
 // Trailing update used by the factorisation (exposed for tests/benches):

@@ -6,9 +6,11 @@
 // one thread issues the tcgen05.mma chain (kind::tf32 on the FP32 data, or
 // kind::f16 on BF16 copies) accumulating in TMEM, and four warps read the
 // accumulator with tcgen05.ld and subtract it from C along its rows (float4,
-// staged through shared memory).  C's rows must be 16-byte aligned (C and
-// ldc multiples of 4 floats), as the callers' TMA operands already require.  Every wait is bounded:
-// on a timeout the CTA flags the error word, frees its TMEM and returns.
+// staged through shared memory; C's loads are issued ahead, the first slice's
+// before the MMAs, each next slice's before the current one is written).
+// C's rows must be 16-byte aligned (C and ldc multiples of 4 floats), as the
+// callers' TMA operands already require.  Every wait is bounded: on a timeout
+// the CTA flags the error word, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -30,6 +32,19 @@ constexpr int kRowBytes = 128;  // one swizzle row: 32 FP32 / 64 BF16 elements o
 __host__ __device__ constexpr uint32_t make_idesc(uint32_t ab_format) {
   return (1u << 4) | (ab_format << 7) | (ab_format << 10) | ((uint32_t)(kBN >> 3) << 17) |
          ((uint32_t)(kBM >> 4) << 24);
+}
+
+// Loads one thread's share of a 32-column slice of C: rows row0 + 4 p
+// (p < 8), the float4 at column col.  Rows past M and float4s that reach past
+// N are left for the scalar tail path of the epilogue.
+__device__ __forceinline__ void load_c_slice(const float* C, int ldc, int M, int N, int row0, int col,
+                                             float4 (&cv)[8]) {
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    const int row = row0 + p * 4;
+    cv[p] = (row < M && col + 3 < N) ? *reinterpret_cast<const float4*>(C + (long long)row * ldc + col)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
 }
 
 template <bool kBF16>
@@ -64,6 +79,14 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+
+  // The epilogue's read of C does not depend on the MMAs: every thread issues
+  // its loads of the first 32-column slice now, so that they overlap the
+  // operand copies and the MMA chain (the loads of slice j + 1 overlap the
+  // update of slice j below).
+  const int sub = lane >> 3, q4 = (lane & 7) * 4;
+  float4 cv[8];
+  load_c_slice(C, ldc, M, N, m0 + warp * 32 + sub, n0 + q4, cv);
 
   if (threadIdx.x == 0) {
     const uint32_t bytes = (uint32_t)kchunks * (kBM + kBN) * kRowBytes;
@@ -117,7 +140,7 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
     // that the read-modify-write of C runs along rows: 8 lanes per row, a
     // float4 each, 4 rows per instruction.
     float* stage = reinterpret_cast<float*>(sA) + warp * 32 * 33;
-    const int sub = lane >> 3, q4 = (lane & 7) * 4;
+#pragma unroll
     for (int j = 0; j < kBN / 32; ++j) {
       uint32_t r[32];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32);
@@ -130,6 +153,8 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
             "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
             "=r"(r[30]), "=r"(r[31])
           : "r"(taddr));
+      float4 nx[8];
+      if (j + 1 < kBN / 32) load_c_slice(C, ldc, M, N, m0 + warp * 32 + sub, n0 + (j + 1) * 32 + q4, nx);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
       for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = __uint_as_float(r[c]);  // row = lane, column c
@@ -143,7 +168,7 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
         if (row < M) {
           float* c4 = C + (long long)row * ldc + col;
           if (col + 3 < N) {
-            float4 v = *reinterpret_cast<const float4*>(c4);
+            float4 v = cv[p];
             v.x -= srow[0];
             v.y -= srow[1];
             v.z -= srow[2];
@@ -156,6 +181,10 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(const __grid_constant
         }
       }
       __syncwarp();
+      if (j + 1 < kBN / 32) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) cv[p] = nx[p];
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
