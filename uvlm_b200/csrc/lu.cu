@@ -473,10 +473,27 @@ __device__ __forceinline__ void tsp_publish(T* uc, int c0, int k, const T (&v)[k
   }
 }
 
-// The elimination of step c = c0 + k against the pivot row uc (column c0 + j
-// at uc[j]): l = v[k] / uc[k] into *lk, v[j] -= l uc[j] for the live columns
-// right of c, chunk by chunk.  A zero pivot leaves the row as it is and
-// returns v[k] as its multiplier.
+// v[j] -= l uc[j] (column c0 + j of the pivot row) for the live columns
+// j >= lo, chunk by chunk (chunks past column 63 hold dead entries of the
+// shifted row and are skipped).
+template <class T>
+__device__ __forceinline__ void tsp_axpy(T (&v)[kLuNB], T l, const T* uc, int c0, int lo) {
+#pragma unroll
+  for (int jc = 0; jc < 8; ++jc) {
+    if (8 * jc + 7 < lo) continue;
+    if (c0 + 8 * jc < kLuNB) {
+      T t8[8];
+      tsp_ld8<T>(uc + 8 * jc, t8);
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (8 * jc + t >= lo) v[8 * jc + t] -= l * t8[t];
+    }
+  }
+}
+
+// The elimination of step c = c0 + k against the pivot row uc: l = v[k] /
+// uc[k] into *lk, then v[j] -= l uc[j] for j > k.  A zero pivot leaves the
+// row as it is and returns v[k] as its multiplier.
 template <class T>
 __device__ __forceinline__ void tsp_eliminate(T (&v)[kLuNB], const T* uc, int c0, int k, T* lk) {
   const T piv = uc[k];
@@ -486,17 +503,7 @@ __device__ __forceinline__ void tsp_eliminate(T (&v)[kLuNB], const T* uc, int c0
   }
   const T l = v[k] / piv;
   *lk = l;
-#pragma unroll
-  for (int jc = 0; jc < 8; ++jc) {
-    if (8 * jc + 7 < k + 1) continue;
-    if (c0 + 8 * jc < kLuNB) {
-      T t8[8];
-      tsp_ld8<T>(uc + 8 * jc, t8);
-#pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if (8 * jc + t >= k + 1) v[8 * jc + t] -= l * t8[t];
-    }
-  }
+  tsp_axpy<T>(v, l, uc, c0, k + 1);
 }
 
 template <class T>
@@ -512,9 +519,11 @@ __device__ __forceinline__ void tsp_shift8(T (&v)[kLuNB]) {
 // multiplier in Lrow[thread][c].  Per column: the per-warp keys (of the
 // step's parity: a slow reader of step c may still read them while a fast
 // warp writes those of step c + 1) and a barrier; the block key; the owner
-// publishes its row and a barrier; the others eliminate.  The operations on
-// each row are those of a column-by-column factorisation, in the same order.
-// Every thread of the CTA calls it.
+// publishes its row and a barrier; the others eliminate.  (Deferring all but
+// the next column's update past the next argmax barrier measured 7-11 %
+// slower per step.)  The operations on each row are those of a
+// column-by-column factorisation, in the same order.  Every thread of the
+// CTA calls it.
 template <class T>
 __device__ int tsp_factor(T (&v)[kLuNB], bool alive, int myid, int R, T* Top, T* Lrow, TspScratch& sc,
                           int* out) {
@@ -755,12 +764,34 @@ __global__ void laswp_kernel(T* A, int lda, int n, int k0, int kb, const int* __
 
 // U12 = L11^-1 A12 (unit lower L11), one thread per column.  Optionally also
 // writes U12 transposed into ut ([col - (k0+kb)][k], leading dim ldut).
+// Columns per CTA of the TRSM (one column per thread; L11 staged once per
+// CTA).  32-column CTAs, which spread a panel's columns over more SMs, took
+// twice as long: each stages the whole L11 with a quarter of the threads.
+constexpr int kTrsmThreads = 128;
+
 template <class T>
-__global__ void __launch_bounds__(128) trsm_kernel(T* A, int lda, int n, int k0, int kb, T* ut, int ldut) {
+__global__ void __launch_bounds__(kTrsmThreads) trsm_kernel(T* A, int lda, int n, int k0, int kb, T* ut, int ldut) {
   __shared__ T L[kLuNB][kLuNB + 1];
-  for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
-    const int r = q / kb, c = q % kb;
-    L[r][c] = A[(long long)(k0 + r) * lda + k0 + c];
+  if (kb == kLuNB) {
+    // all of a thread's loads of L11 issued before any is stored (one round
+    // trip, not one per element)
+    constexpr int kPer = kLuNB * kLuNB / kTrsmThreads;
+    T t[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int q = threadIdx.x + i * kTrsmThreads;
+      t[i] = A[(long long)(k0 + q / kLuNB) * lda + k0 + q % kLuNB];
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int q = threadIdx.x + i * kTrsmThreads;
+      L[q / kLuNB][q % kLuNB] = t[i];
+    }
+  } else {
+    for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) {
+      const int r = q / kb, c = q % kb;
+      L[r][c] = A[(long long)(k0 + r) * lda + k0 + c];
+    }
   }
   __syncthreads();
   const int col = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
@@ -778,9 +809,20 @@ __global__ void __launch_bounds__(128) trsm_kernel(T* A, int lda, int n, int k0,
     if (r < kb) A[(long long)(k0 + r) * lda + col] = x[r];
   if (ut) {
     T* o = ut + (long long)(col - k0 - kb) * ldut;
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (kb == kLuNB && ldut % 4 == 0) {
+        // whole rows of the transposed copy: 16-byte stores
 #pragma unroll
-    for (int r = 0; r < kLuNB; ++r)
-      if (r < kb) o[r] = x[r];
+        for (int r = 0; r < kLuNB; r += 4) *reinterpret_cast<float4*>(o + r) = make_float4(x[r], x[r + 1], x[r + 2], x[r + 3]);
+        done = true;
+      }
+    }
+    if (!done) {
+#pragma unroll
+      for (int r = 0; r < kLuNB; ++r)
+        if (r < kb) o[r] = x[r];
+    }
   }
 }
 
@@ -1156,7 +1198,7 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
     const int rest = n - k0 - kb;
     if (rest > 0) {
       T* ut = (upd != kLuUpdateSimt) ? reinterpret_cast<T*>(w->ut) : nullptr;
-      trsm_kernel<T><<<ceil_div(rest, 128), 128, 0, st>>>(A, n, n, k0, kb, ut, kLuNB);
+      trsm_kernel<T><<<ceil_div(rest, kTrsmThreads), kTrsmThreads, 0, st>>>(A, n, n, k0, kb, ut, kLuNB);
       UVLM_LAUNCH_CHECK();
       T* C = A + (long long)(k0 + kb) * n + (k0 + kb);
       const T* L21 = A + (long long)(k0 + kb) * n + k0;
