@@ -365,7 +365,9 @@ bool launch_panel_cluster(T* A, int n, int k0, int kb, int P, int* ipiv, int* er
 // U part in shared memory; every other live row stores its multiplier in its
 // shared-memory row of L (Lrow) and eliminates against the pivot row.  Two
 // block barriers per column: a published row from one lane (one warp) costs
-// less than every warp's candidate row before a single barrier.
+// less than every warp's candidate row before a single barrier.  Two lanes per
+// row (16 warps, half rows, each lane reading half of the pivot row) measured
+// 5 % (FP32) and 12 % (FP64) slower per panel than one lane per row.
 constexpr int kTspRows = 256;  // rows per CTA = threads per CTA
 constexpr int kTspMaxCtas = 16;
 constexpr int kTspMaxRows = kTspRows * kTspMaxCtas;
@@ -880,10 +882,11 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(T* C, int ldc, const T
 // FP64 trailing update C -= A B of the plain form's LU (K = the panel width):
 // 128 x 128 output tiles, 256 threads each holding an 8 x 8 register block
 // (rows ty*4 + i and 64 + ty*4 + i, columns tx*4 + j and 64 + tx*4 + j), K
-// in steps of 16 through a three-stage cp.async pipeline.  Each product is
-// accumulated over k in order with FMAs and subtracted from C once, as in
-// gemm_update_kernel, so both kernels give the same bits.  The 16-byte copies
-// need 16-byte aligned rows: even leading dimensions and aligned bases.
+// in steps of 16 through a three-stage cp.async pipeline.  Each entry of C
+// has its products subtracted one by one in k order (FMA), so the rounding
+// differs from gemm_update_kernel's (which sums the products, then subtracts
+// once) at the level of FP64 rounding.  The 16-byte copies need 16-byte
+// aligned rows: even leading dimensions and aligned bases.
 constexpr int kG64BM = 128, kG64BN = 128, kG64BK = 16, kG64Stages = 3;
 constexpr int kG64ALd = kG64BK + 2;  // 144-byte rows of the A tile: the 4-row strides fall on other banks
 constexpr int kG64StageA = kG64BM * kG64ALd;
@@ -931,11 +934,30 @@ __global__ void __launch_bounds__(256, 1) gemm_update_f64_kernel(double* C, int 
     }
   };
 
+  // the accumulators start as this thread's 8 x 8 block of C (loaded while
+  // the operand pipeline fills) and the products are subtracted one by one,
+  // so the tile's C traffic overlaps its loads instead of following the MMAs
   double acc[8][8];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 8; ++i) {
+    const int r = row0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int h = 0; h < 2; ++h) {
+      const int c = col0 + h * 64 + tx * 4;
+      const double* cp = C + (long long)r * ldc + c;
+      if (r < m && c + 3 < nc) {
+        const double2 v0 = *reinterpret_cast<const double2*>(cp);
+        const double2 v1 = *reinterpret_cast<const double2*>(cp + 2);
+        acc[i][h * 4 + 0] = v0.x;
+        acc[i][h * 4 + 1] = v0.y;
+        acc[i][h * 4 + 2] = v1.x;
+        acc[i][h * 4 + 3] = v1.y;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][h * 4 + j] = (r < m && c + j < nc) ? cp[j] : 0.0;
+      }
+    }
+  }
 
 #pragma unroll
   for (int s = 0; s < kG64Stages - 1; ++s) {
@@ -949,7 +971,7 @@ __global__ void __launch_bounds__(256, 1) gemm_update_f64_kernel(double* C, int 
     asm volatile("cp.async.commit_group;" ::: "memory");
     const double* a = sA + (t % kG64Stages) * kG64StageA;
     const double* b = sB + (t % kG64Stages) * kG64StageB;
-#pragma unroll
+#pragma unroll 8
     for (int kk = 0; kk < kG64BK; ++kk) {
       double av[8], bv[8];
 #pragma unroll
@@ -966,7 +988,7 @@ __global__ void __launch_bounds__(256, 1) gemm_update_f64_kernel(double* C, int 
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -980,18 +1002,12 @@ __global__ void __launch_bounds__(256, 1) gemm_update_f64_kernel(double* C, int 
       const int c = col0 + h * 64 + tx * 4;
       double* cp = C + (long long)r * ldc + c;
       if (c + 3 < nc) {
-        double2 v0 = *reinterpret_cast<double2*>(cp);
-        double2 v1 = *reinterpret_cast<double2*>(cp + 2);
-        v0.x -= acc[i][h * 4 + 0];
-        v0.y -= acc[i][h * 4 + 1];
-        v1.x -= acc[i][h * 4 + 2];
-        v1.y -= acc[i][h * 4 + 3];
-        *reinterpret_cast<double2*>(cp) = v0;
-        *reinterpret_cast<double2*>(cp + 2) = v1;
+        *reinterpret_cast<double2*>(cp) = make_double2(acc[i][h * 4 + 0], acc[i][h * 4 + 1]);
+        *reinterpret_cast<double2*>(cp + 2) = make_double2(acc[i][h * 4 + 2], acc[i][h * 4 + 3]);
       } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          if (c + j < nc) cp[j] -= acc[i][h * 4 + j];
+          if (c + j < nc) cp[j] = acc[i][h * 4 + j];
       }
     }
   }
