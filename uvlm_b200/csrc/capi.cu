@@ -108,7 +108,8 @@ struct uvlm_ctx {
   // fp64_h2_t1_b128_m3, each autotuned on that stage's first large evaluation
   // unless the configuration pins one
   int stage_variant[3][2] = {{16, 9}, {16, 9}, {16, 9}};
-  bool stage_tuned[3][2] = {};
+  bool stage_pinned[3][2] = {};        // the configuration chose the tile
+  double stage_tuned_pairs[3][2] = {};  // pairs of the evaluation the tile was tuned on (0: not yet)
   // learned warm start: network (borrowed), per-step features, collected data
   uvlm_mlp* mlp = nullptr;
   double* d_rhs_prev = nullptr;
@@ -297,7 +298,9 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBody
   work_nbody += pairs;
   const int pi = prec == kNBodyFP64 ? 1 : 0;
   int& chosen = stage_variant[stage][pi];
-  if (!stage_tuned[stage][pi] && nblocks > 0 && pairs >= 2e9) {
+  // tune on the first evaluation with >= 2e9 pairs and again whenever the
+  // stage has grown by half since (a growing wake changes the far-strip share)
+  if (!stage_pinned[stage][pi] && nblocks > 0 && pairs >= 2e9 && pairs >= 1.5 * stage_tuned_pairs[stage][pi]) {
     // Tile autotune on the stage's first large evaluation: time every
     // compiled variant of this precision on the real sources and targets,
     // keep the fastest (the default unless another is more than 3% faster).
@@ -324,7 +327,7 @@ Error uvlm_ctx::eval(const SourceBlock* blocks, int nblocks, long long nt, NBody
       }
     }
     chosen = best;
-    stage_tuned[stage][pi] = true;
+    stage_tuned_pairs[stage][pi] = pairs;
   }
   if (nblocks == 0) {
     UVLM_CUDA_TRY(cudaMemsetAsync(d_vx, 0, sizeof(double) * nt, st));
@@ -812,7 +815,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
     const int pi = nbody_variant_prec(k.nbody_variant) == kNBodyFP64 ? 1 : 0;
     for (int st = 0; st < 3; ++st) {
       c->stage_variant[st][pi] = k.nbody_variant;
-      c->stage_tuned[st][pi] = true;
+      c->stage_pinned[st][pi] = true;
     }
   }
   *out = c;
