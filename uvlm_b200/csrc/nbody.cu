@@ -828,7 +828,7 @@ template <class T, class Rec, int H, int TPT, int BLOCK, bool PAD, int PK = 0, b
 __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, long long s_end,
                                             const Rec* __restrict__ rec, Rec* buf0, Rec* buf1, float4* loc,
                                             float* red, const Tgt<T> (&tg)[TPT], double (&accd)[TPT][3],
-                                            const RecD* __restrict__ rec64 = nullptr) {
+                                            const RecD* __restrict__ rec64 = nullptr, long long s_stride = 1) {
   if (s_begin >= s_end) return;
   StripInfo si = decode_strip<H>(B, s_begin);
   if constexpr (PAD && PK == 2)
@@ -837,13 +837,14 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
     stage_strip_padded<Rec, H>(buf0, rec, si);
   else
     stage_strip<Rec>(buf0, rec, si);
-  for (long long s = s_begin; s < s_end; ++s) {
-    Rec* cur = ((s - s_begin) & 1) ? buf1 : buf0;
-    Rec* nxt = ((s - s_begin) & 1) ? buf0 : buf1;
+  long long it = 0;
+  for (long long s = s_begin; s < s_end; s += s_stride, ++it) {
+    Rec* cur = (it & 1) ? buf1 : buf0;
+    Rec* nxt = (it & 1) ? buf0 : buf1;
     StripInfo sn;
-    const bool has_next = s + 1 < s_end;
+    const bool has_next = s + s_stride < s_end;
     if (has_next) {
-      sn = decode_strip<H>(B, s + 1);
+      sn = decode_strip<H>(B, s + s_stride);
       if constexpr (PAD && PK == 2)
         stage_strip_rows<Rec, H>(nxt, rec, sn);
       else if constexpr (PAD)
@@ -928,7 +929,7 @@ __device__ __forceinline__ void eval_strips(const Blocks& B, long long s_begin, 
 }
 
 template <class T, class Rec, int H, int TPT, int BLOCK, int MINB, bool PAD, int PK, bool NEAR64 = false>
-__global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips, long long strips_per_split,
+__global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long n_strips,
                                                        const double* __restrict__ tx, const double* __restrict__ ty,
                                                        const double* __restrict__ tz, long long n_targets,
                                                        const Rec* __restrict__ rec, double* __restrict__ partial,
@@ -946,10 +947,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) nbody_kernel(Blocks B, long long 
   load_targets<T, TPT, BLOCK>(tx, ty, tz, 0, tile0, n_targets, tg);
 #pragma unroll
   for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
-  const long long s_begin = (long long)blockIdx.y * strips_per_split;
-  const long long s_end = min(n_strips, s_begin + strips_per_split);
-  eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK, NEAR64>(B, s_begin, s_end, rec, buf0, buf1, loc, red, tg, accd,
-                                                      rec64);
+  // split y takes the strips y, y + splits, y + 2 splits, ...: the strips
+  // near a target tile (the newest wake rows, next to the wing) are spread
+  // over the splits instead of all landing in split 0, which evens out the
+  // costlier near-field work
+  eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK, NEAR64>(B, (long long)blockIdx.y, n_strips, rec, buf0, buf1, loc, red,
+                                                      tg, accd, rec64, (long long)gridDim.y);
   double* px = partial + (long long)blockIdx.y * 3 * n_targets;
 #pragma unroll
   for (int q = 0; q < TPT; ++q) {
@@ -1190,8 +1193,8 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   constexpr bool kCanNear64 = PK == 2 && sizeof(T) == 4 && TPT == 2;
   const RecD* rec64 = (kCanNear64 && work->near64) ? reinterpret_cast<const RecD*>(work->records64) : nullptr;
   if (kCanNear64 && work->near64 && !rec64) return fail(kErrInvalid, "FP64 near field without FP64 records");
-  void (*kern)(Blocks, long long, long long, const double*, const double*, const double*, long long, const Rec*,
-               double*, const RecD*);
+  void (*kern)(Blocks, long long, const double*, const double*, const double*, long long, const Rec*, double*,
+               const RecD*);
   if constexpr (kCanNear64)
     kern = rec64 ? nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK, true>
                  : nbody_kernel<T, Rec, H, TPT, BLOCK, MINB, true, PK, false>;
@@ -1231,7 +1234,7 @@ Error launch_variant(const Blocks& B, long long n_strips, const double* tx, cons
   const long long need = splits * 3 * n_targets;
   if (work->partial_cap < need) return fail(kErrCapacity, "nbody partial buffer too small");
   dim3 grid((unsigned)tiles, (unsigned)splits);
-  kern<<<grid, BLOCK, smem, st>>>(B, n_strips, sps, tx, ty, tz, n_targets, rec, work->partial, rec64);
+  kern<<<grid, BLOCK, smem, st>>>(B, n_strips, tx, ty, tz, n_targets, rec, work->partial, rec64);
   UVLM_LAUNCH_CHECK();
   const int rb = 256;
   const int rg = (int)std::min<long long>((n_targets + rb - 1) / rb, (long long)num_sms * 8);
