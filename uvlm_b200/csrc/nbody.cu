@@ -1064,9 +1064,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_nbody_kernel(const NBodyBat
     load_targets<T, TPT, BLOCK>(tx, ty, tz, P.tgt_off, tile0, P.n_tgt, tg);
 #pragma unroll
     for (int q = 0; q < TPT; ++q) accd[q][0] = accd[q][1] = accd[q][2] = 0.0;
-    const long long s_begin = split * kBatchStripsPerItem;
-    const long long s_end = min(P.n_strips, s_begin + kBatchStripsPerItem);
-    eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK>(P.B, s_begin, s_end, rec, buf0, buf1, loc, red, tg, accd);
+    // interleaved source strips (split s: strips s, s + splits, ...), as in
+    // nbody_kernel: a tile's near strips spread over its items
+    eval_strips<T, Rec, H, TPT, BLOCK, PAD, PK>(P.B, split, P.n_strips, rec, buf0, buf1, loc, red, tg, accd, nullptr,
+                                                P.splits);
     double* px = partial + P.part_off + split * 3 * P.n_tgt;
 #pragma unroll
     for (int q = 0; q < TPT; ++q) {
