@@ -499,8 +499,6 @@ def run_ours(args, rank, world, local_rank):
     t_64, _ = timed_steps(sim64, step0, args.steps, flush, torch, s_64)
     # the same steps without the network (warm start 2 g_n - g_{n-1}), timed alike
     t_ex = timed_steps(simex, step0, args.steps, flush, torch, s_ex)[0] if simex else None
-    if simex:
-        simex.close()
     st = simmx.stats()
     total_mx = float(np.sum(t_mx))
     if world > 1:
@@ -511,6 +509,27 @@ def run_ours(args, rank, world, local_rank):
     value = world * args.steps / (total_mx * 1e-3)
     plain = args.steps / (float(np.sum(t_64)) * 1e-3)
     step0 += args.steps
+
+    # the warm start's own stage: the solve (with the guess) timed per step with
+    # CUDA events, learned network against the extrapolation, the same steps
+    warm_stage = None
+    if simex:
+        def solve_stage(sim):
+            sim.set_stage_timing(True)
+            v, it = [], []
+            for i in range(args.steps):
+                sim.step(step0 + i, DT)
+                s_ = sim.stats()
+                v.append(float(s_.stage_ms[3] + s_.stage_ms[6]))
+                it.append(int(s_.gmres_iters))
+            sim.set_stage_timing(False)
+            return float(np.mean(v)), float(np.mean(it))
+        (ms_l, it_l), (ms_e, it_e) = solve_stage(simmx), solve_stage(simex)
+        warm_stage = {"learned_solve_ms": ms_l, "extrapolate_solve_ms": ms_e, "learned_gmres_iters": it_l,
+                      "extrapolate_gmres_iters": it_e, "stage_speedup": ms_e / ms_l,
+                      "note": "solve stage incl. the guess, CUDA events, mean over the steps after the timed ones"}
+        simex.close()
+        step0 += args.steps
 
     # --- stage timing + roofline of the N-body advection kernel --------------
     simmx.set_stage_timing(True)
@@ -608,6 +627,7 @@ def run_ours(args, rank, world, local_rank):
             "mixed_extrapolate_steps_per_s": (args.steps / (float(np.sum(t_ex)) * 1e-3)) if t_ex is not None else None,
             "learned_warm_start_speedup": ((value / world) / (args.steps / (float(np.sum(t_ex)) * 1e-3))
                                            if t_ex is not None else None),
+            "learned_warm_start_solve_stage": warm_stage,
             "cl_rel_err": cl_err, "cd_rel_err": cd_err,
             "cl_err_reference": f"plain FP64 GPU form, same {WAKE_ROWS} steps",
             "accuracy": accuracy, "warm_start_ablation": warm_ablation,
