@@ -538,9 +538,13 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
                                                                 const double* gamma_hist, const long long* d_step,
                                                                 int max_sweeps, double tol, int stale,
                                                                 int* has_factor, unsigned long long* refac,
-                                                                int* sweeps_out, double* res_out, int* status) {
+                                                                int* sweeps_out, double* res_out, int* status,
+                                                                const int* __restrict__ order) {
   extern __shared__ double sm[];
-  const BCase& b = cs[blockIdx.x];
+  // CTA i takes the i-th largest case: with more cases than SMs the largest
+  // start first instead of forming the launch's last wave
+  const int ci = order[blockIdx.x];
+  const BCase& b = cs[ci];
   const int N = b.N;
   double* x = sm;
   double* r = sm + N;
@@ -601,7 +605,7 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
       __syncthreads();
     };
     bool done = false;
-    if (stale && has_factor[blockIdx.x]) {
+    if (stale && has_factor[ci]) {
       // refine from the extrapolation 2 G(s-1) - G(s-2) (from G(s-1) before step 2)
       const bool extrap = *d_step >= 2;
       for (int i = threadIdx.x; i < N; i += kSolveThreads)
@@ -623,7 +627,7 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
       __syncthreads();
       cta_lu_panel_smem<T>(LU, N, piv, status, panel);
       if (threadIdx.x == 0) {
-        has_factor[blockIdx.x] = 1;
+        has_factor[ci] = 1;
         atomicAdd(refac, 1ull);
       }
       for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
@@ -652,8 +656,8 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
   }
   if (!finite) status[2] = 1;
   if (threadIdx.x == 0) {
-    sweeps_out[blockIdx.x] = sweeps;
-    res_out[blockIdx.x] = rel;
+    sweeps_out[ci] = sweeps;
+    res_out[ci] = rel;
   }
 }
 
@@ -868,6 +872,7 @@ struct uvlm_batch {
   long long* d_totals = nullptr;
   int* d_status = nullptr;
   int* d_sweeps = nullptr;
+  int* d_solve_order = nullptr;          // cases by decreasing N (the solve's CTA order)
   int* d_has_factor = nullptr;           // per case: FP32 factors held (stale reuse)
   unsigned long long* d_refac = nullptr;  // factorisations so far
   double* d_res = nullptr;
@@ -1032,6 +1037,7 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   UVLM_TRY(balloc(&d_totals, 4));
   UVLM_TRY(balloc(&d_status, 4));
   UVLM_TRY(balloc(&d_sweeps, n));
+  UVLM_TRY(balloc(&d_solve_order, n));
   UVLM_TRY(balloc(&d_has_factor, n));
   UVLM_TRY(balloc(&d_refac, 1));
   UVLM_TRY(balloc(&d_res, n));
@@ -1040,6 +1046,12 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
   std::vector<long long> flat;
   for (int k = 0; k < 7; ++k) flat.insert(flat.end(), pre[k].begin(), pre[k].end());
   UVLM_CUDA_TRY(cudaMemcpy(d_cases, hc.data(), sizeof(BCase) * n, cudaMemcpyHostToDevice));
+  {
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return hc[a].N > hc[b].N; });
+    UVLM_CUDA_TRY(cudaMemcpy(d_solve_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  }
   UVLM_CUDA_TRY(cudaMemcpy(d_pre, flat.data(), sizeof(long long) * flat.size(), cudaMemcpyHostToDevice));
   UVLM_CUDA_TRY(cudaMemcpy(d_tiles, tiles.data(), sizeof(AsmTile) * tiles.size(), cudaMemcpyHostToDevice));
   UVLM_CUDA_TRY(cudaMemcpy(d_pos_init, nodes.data(), sizeof(double) * nodes.size(), cudaMemcpyHostToDevice));
@@ -1163,11 +1175,11 @@ Error uvlm_batch::enqueue_step() {
   if (mixed())
     b_solve_kernel<float><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
                                                           d_gamma_hist, d_step, cfg.refine_max_iter, cfg.refine_tol, cfg.stale_factors,
-                                                          d_has_factor, d_refac, d_sweeps, d_res, d_status);
+                                                          d_has_factor, d_refac, d_sweeps, d_res, d_status, d_solve_order);
   else
     b_solve_kernel<double><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
                                                            d_gamma_hist, d_step, 0, 0.0,
-                                                           0, d_has_factor, d_refac, d_sweeps, d_res, d_status);
+                                                           0, d_has_factor, d_refac, d_sweeps, d_res, d_status, d_solve_order);
   UVLM_LAUNCH_CHECK();
   // loads: line velocities from the bound sheet (new circulation) and the wake
   b_line_prep_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, d_step, d_pos, d_pos_init, d_lx, d_ly, d_lz, d_line_uls);
@@ -1210,7 +1222,7 @@ void uvlm_batch::release() {
                   d_normal,
                   d_area, d_uls, d_rhs, d_lx, d_ly, d_lz, d_line_uls, d_wpos, d_wpos2, d_k1, d_wgamma, d_wtx,
                   d_wty, d_wtz, d_vx, d_vy, d_vz, d_A64, d_F32, d_piv, d_tiles, d_rec, d_partial, d_in, d_plan,
-                  d_totals, d_status, d_sweeps, d_res, d_loads, d_has_factor, d_refac};
+                  d_totals, d_status, d_sweeps, d_res, d_loads, d_has_factor, d_refac, d_solve_order};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (st) cudaStreamDestroy(st);
