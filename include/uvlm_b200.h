@@ -101,7 +101,15 @@ typedef struct {
                                 far-field test leaves to the near-field walker (source strips close to
                                 the targets) are evaluated in FP64 from FP64 records and accumulated in
                                 FP64; 0: none; uvlm_config_default sets UVLM_STAGE_RHS */
+  int32_t lu_pivoting;       /* mixed form, the factors of the GMRES preconditioner: UVLM_PIVOT_PANEL
+                                (pivots chosen over every row of a 64-column panel) or UVLM_PIVOT_LOCAL
+                                (over the panel's top 256 rows only, the default: a cheaper panel for
+                                diagonally heavy influence matrices; GMRES with FP64 residuals and the
+                                plain fresh-LU fallback keep the answer whatever the pivots) */
 } uvlm_config;
+
+#define UVLM_PIVOT_PANEL 0
+#define UVLM_PIVOT_LOCAL 1
 
 /* N-body stages of a MainLoop (uvlm_config.nbody_fp64_stages). */
 #define UVLM_STAGE_RHS 1    /* wake normal wash at the collocation points (CalcRhs) */

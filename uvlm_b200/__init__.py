@@ -134,13 +134,16 @@ class SimpleSimulator:
                   in FP64 (FP64 records, FP64 accumulation): True for every
                   stage, or any of "rhs", "loads", "advect"; None (default)
                   takes the library's default, the RHS stage
+      lu_pivoting mixed form, the preconditioner's factors: "panel" (pivots
+                  over every row of each 64-column panel) or "local" (over
+                  the panel's top 256 rows); None takes the library's default
     """
 
     def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
                  lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
                  gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
                  assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True,
-                 preconditioner: str = "inverse", fp64_stages=(), near_fp64=None):
+                 preconditioner: str = "inverse", fp64_stages=(), near_fp64=None, lu_pivoting: str | None = None):
         cfg = Config()
         lib().uvlm_config_default(C.byref(cfg))
         cfg.precision = PRECISION[precision]
@@ -166,6 +169,8 @@ class SimpleSimulator:
             near_fp64 = tuple(stages)
         if near_fp64 is not None:
             cfg.nbody_near_fp64 = sum(stages[s] for s in set(near_fp64 or ()))
+        if lu_pivoting is not None:
+            cfg.lu_pivoting = {"panel": 0, "local": 1}[lu_pivoting]
         self._cfg = cfg
         h = C.c_void_p()
         check(lib().uvlm_create(C.byref(cfg), C.byref(h)))

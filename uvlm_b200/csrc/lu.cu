@@ -572,7 +572,7 @@ __device__ int tsp_factor(T (&v)[kLuNB], bool alive, int myid, int R, T* Top, T*
 
 template <class T>
 __global__ void __launch_bounds__(kTspRows, 1) lu_panel_tsp_kernel(T* A, int lda, int n, int k0, int* ipiv,
-                                                                   int* err) {
+                                                                   int* err, int local) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -585,8 +585,9 @@ __global__ void __launch_bounds__(kTspRows, 1) lu_panel_tsp_kernel(T* A, int lda
   const int nloc = max(0, min(kTspRows, m - rb));
   T v[kLuNB];
 
-  // ---- phase 1: this CTA's rows
-  {
+  // ---- phase 1: this CTA's rows (with local pivoting, only the first CTA's:
+  // the pivots are chosen among the panel's top 256 rows)
+  if (!local || bid == 0) {
     const bool alive = tid < nloc;
     if (alive) tsp_load_row<T>(A, (long long)(k0 + rb + tid) * lda + k0, v);
     const int k = tsp_factor<T>(v, alive, rb + tid, nloc, Top, Lrow, sc, sc.list);
@@ -595,7 +596,7 @@ __global__ void __launch_bounds__(kTspRows, 1) lu_panel_tsp_kernel(T* A, int lda
 
   // ---- phase 2: 4-ary tournament tree over the cluster; the merges factor
   // the candidates' original rows
-  for (int step = 1; step < P; step *= 4) {
+  for (int step = 1; step < (local ? 1 : P); step *= 4) {
     cl.sync();  // the candidate lists of this level are final
     if ((bid % (4 * step)) == 0 && bid + step < P) {
       if (tid == 0)
@@ -703,7 +704,7 @@ __global__ void __launch_bounds__(kTspRows, 1) lu_panel_tsp_kernel(T* A, int lda
 // than 64 columns, too many rows for one cluster, or the cluster cannot be
 // formed).
 template <class T>
-bool launch_panel_tsp(T* A, int n, int k0, int kb, int* ipiv, int* err, cudaStream_t st) {
+bool launch_panel_tsp(T* A, int n, int k0, int kb, int* ipiv, int* err, bool local, cudaStream_t st) {
   const int m = n - k0;
   const int P = ceil_div(m, kTspRows);
   if (P > kTspMaxCtas || kb != kLuNB || m < kLuNB) return false;
@@ -738,7 +739,7 @@ bool launch_panel_tsp(T* A, int n, int k0, int kb, int* ipiv, int* err, cudaStre
     cudaGetLastError();
     return false;
   }
-  if (cudaLaunchKernelEx(&cfg, kern, A, n, n, k0, ipiv, err) != cudaSuccess) {
+  if (cudaLaunchKernelEx(&cfg, kern, A, n, n, k0, ipiv, err, local ? 1 : 0) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -1201,7 +1202,7 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
     int nn = n, kk0 = k0, kkb = kb, rr = rpc;
     // tournament pivoting in one cluster; else the column-by-column cluster
     // panel; else the cooperative kernel
-    if (!(w->tournament && launch_panel_tsp<T>(A, n, k0, kb, ipiv, err, st)) &&
+    if (!(w->tournament && launch_panel_tsp<T>(A, n, k0, kb, ipiv, err, w->local_pivot, st)) &&
         !launch_panel_cluster<T>(A, n, k0, kb, P, ipiv, err, st)) {
       void* args[] = {&A, &lda, &nn, &kk0, &kkb, &ipiv, &cv, &cr, &cd, &dd, &bar, &err, &rr};
       UVLM_CUDA_TRY(cudaLaunchCooperativeKernel((void*)panel, dim3(P), dim3(kPanelRows), args, smem, st));

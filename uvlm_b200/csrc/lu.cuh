@@ -57,6 +57,8 @@ struct LuWork {
   int elem_size = 8;
   int num_sms = 148;
   bool tournament = true;     // panel pivots by a tournament (one cluster per panel) where it fits
+  bool local_pivot = false;   // tournament panel: pivots only among each panel's top 256 rows (a
+                              // preconditioner's factors; L may then exceed 1 in magnitude)
 };
 
 constexpr int kLuMaxCtas = 148;
