@@ -1052,16 +1052,24 @@ __global__ void diag_inverse_kernel(const T* LU, int n, T* dinv_l, T* dinv_u) {
 
 // perm[k] = row of b that lands in row k after the LAPACK-style swap sequence.
 __global__ void ipiv_to_perm_kernel(const int* ipiv, int n, int* perm) {
+  // sp: the permutation, si: the pivot sequence (both staged by every thread;
+  // the swaps themselves are one sequential chain in shared memory)
   extern __shared__ int sp[];
-  if (threadIdx.x != 0) return;
-  for (int k = 0; k < n; ++k) sp[k] = k;
-  for (int k = 0; k < n; ++k) {
-    const int p = ipiv[k];
-    const int t = sp[k];
-    sp[k] = sp[p];
-    sp[p] = t;
+  int* si = sp + n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    sp[k] = k;
+    si[k] = ipiv[k];
   }
-  for (int k = 0; k < n; ++k) perm[k] = sp[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < n; ++k) {
+      const int p = si[k];
+      const int t = sp[k];
+      sp[k] = sp[p];
+      sp[p] = t;
+    }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) perm[k] = sp[k];
 }
 
 constexpr int kTriBatch = 8;  // block rows a CTA can consume in one pass
@@ -1241,7 +1249,11 @@ Error lu_factor_impl(T* A, int n, LuUpdate upd, LuWork* w, cudaStream_t st) {
                                                      reinterpret_cast<T*>(w->dinv_u));
   UVLM_LAUNCH_CHECK();
   // permutation vector stored after ipiv
-  ipiv_to_perm_kernel<<<1, 32, sizeof(int) * n, st>>>(w->ipiv, n, w->ipiv + n);
+  const size_t perm_smem = 2 * sizeof(int) * (size_t)n;
+  if (perm_smem > 48 * 1024)
+    UVLM_CUDA_TRY(cudaFuncSetAttribute(ipiv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)perm_smem));
+  ipiv_to_perm_kernel<<<1, 256, perm_smem, st>>>(w->ipiv, n, w->ipiv + n);
   UVLM_LAUNCH_CHECK();
   return ok();
 }
@@ -1358,30 +1370,71 @@ __global__ void split_a3_kernel(const float* __restrict__ A, int lda, int m, flo
   }
 }
 
-// B3[j][0:64] = hi, [64:128] = hi, [128:192] = lo of X[r0 + k][j], j < ncols:
-// block row r0 of X (row-major, leading dimension n) transposed, 32 x 32
-// tiles through shared memory.
-__global__ void __launch_bounds__(256) split_b3_kernel(const float* __restrict__ X, int n, int ncols, int r0,
-                                                       float* __restrict__ B3) {
-  __shared__ float t[32][33];
-  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int r = ty; r < 32; r += 8) {
-    const int j = j0 + tx;
-    t[r][tx] = j < ncols ? X[(long long)(r0 + k0 + r) * n + j] : 0.f;
+
+namespace {
+// apply_block_kernel and the B operand of the split-TF32 update in one pass,
+// for a whole 64-row block: X[r0 .. r0+64) = D X[r0 .. r0+64) on the columns
+// below ncols, written back, and its transposed split-TF32 copy
+// B3[j][0:64] = hi, [64:128] = hi, [128:192] = lo of X[r0 + k][j] from the
+// same values.  A CTA owns 32 columns: D and the X tile
+// in shared memory, thread (k, group) forms the 8 products of row k for the
+// group's 8 columns, then the tile goes out along rows of X and along k of B3.
+__global__ void __launch_bounds__(256) apply_split_kernel(const float* __restrict__ D, float* X, int n, int r0,
+                                                          int ncols, float* __restrict__ B3) {
+  __shared__ float Ds[kTriB][kTriB + 1];
+  __shared__ __align__(16) float Ts[kTriB][32];
+  __shared__ float Ys[kTriB][33];
+  const int j0 = blockIdx.x * 32;
+  const int tid = threadIdx.x;
+  {
+    float dv[kTriB * kTriB / 256], tv[kTriB * 32 / 256];
+#pragma unroll
+    for (int u = 0; u < kTriB * kTriB / 256; ++u) dv[u] = D[tid + 256 * u];
+#pragma unroll
+    for (int u = 0; u < kTriB * 32 / 256; ++u) {
+      const int q = tid + 256 * u, i = q >> 5, j = q & 31;
+      tv[u] = j0 + j < ncols ? X[(long long)(r0 + i) * n + j0 + j] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kTriB * kTriB / 256; ++u) {
+      const int q = tid + 256 * u;
+      Ds[q / kTriB][q % kTriB] = dv[u];
+    }
+#pragma unroll
+    for (int u = 0; u < kTriB * 32 / 256; ++u) {
+      const int q = tid + 256 * u;
+      Ts[q >> 5][q & 31] = tv[u];
+    }
   }
   __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    const int j = j0 + r;
-    if (j < ncols) {
-      const float b = t[tx][r], h = tf32_hi(b);
-      float* o = B3 + (long long)j * 3 * kTriB + k0 + tx;
+  const int k = tid & 63, g = tid >> 6;  // row k, columns 8 g .. 8 g + 7
+  float acc[8] = {};
+  for (int s = 0; s < kTriB; ++s) {
+    const float a = Ds[k][s];
+    const float4 b0 = *reinterpret_cast<const float4*>(&Ts[s][8 * g]);
+    const float4 b1 = *reinterpret_cast<const float4*>(&Ts[s][8 * g + 4]);
+    acc[0] += a * b0.x, acc[1] += a * b0.y, acc[2] += a * b0.z, acc[3] += a * b0.w;
+    acc[4] += a * b1.x, acc[5] += a * b1.y, acc[6] += a * b1.z, acc[7] += a * b1.w;
+  }
+#pragma unroll
+  for (int e = 0; e < 8; ++e) Ys[k][8 * g + e] = acc[e];
+  __syncthreads();
+  for (int q = tid; q < kTriB * 32; q += 256) {
+    const int i = q >> 5, j = q & 31;
+    if (j0 + j < ncols) X[(long long)(r0 + i) * n + j0 + j] = Ys[i][j];
+  }
+  for (int q = tid; q < kTriB * 32; q += 256) {
+    const int j = q >> 6, kk = q & 63;
+    if (j0 + j < ncols) {
+      const float b = Ys[kk][j], h = tf32_hi(b);
+      float* o = B3 + (long long)(j0 + j) * 3 * kTriB + kk;
       o[0] = h;
       o[kTriB] = h;
       o[2 * kTriB] = b - h;
     }
   }
 }
+}  // namespace
 
 Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, cudaStream_t st) {
   if (n <= 0) return ok();
@@ -1396,15 +1449,20 @@ Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, 
   // in: split-TF32 on the tensor cores when the operands are TMA-aligned
   // (n % 4 == 0, whole 64-row blocks), else SIMT.
   const bool tc = upd != kLuUpdateSimt && n % 4 == 0 && w->a3 != nullptr && w->b3 != nullptr;
-  auto update = [&](float* C, const float* A, int m, int ncols, int r0, int nb) -> Error {
-    if (m <= 0 || ncols <= 0) return ok();
-    if (tc && nb == kTriB) {
-      split_a3_kernel<<<std::min<long long>(ceil_div((long long)m * kTriB, 256), 4096), 256, 0, st>>>(A, n, m, w->a3);
+  // X_I = D X_I (block row I, columns below ncols), then C -= A X_I; on the
+  // tensor-core path the first two steps are one kernel that also writes X_I's
+  // split-TF32 copy
+  auto step = [&](const float* D, float* C, const float* A, int m, int ncols, int r0, int nb) -> Error {
+    if (tc && nb == kTriB && m > 0) {
+      apply_split_kernel<<<ceil_div(ncols, 32), 256, 0, st>>>(D, X, n, r0, ncols, w->b3);
       UVLM_LAUNCH_CHECK();
-      split_b3_kernel<<<dim3(ceil_div(ncols, 32), kTriB / 32), 256, 0, st>>>(X, n, ncols, r0, w->b3);
+      split_a3_kernel<<<std::min<long long>(ceil_div((long long)m * kTriB, 256), 4096), 256, 0, st>>>(A, n, m, w->a3);
       UVLM_LAUNCH_CHECK();
       return gemm_update_tc(C, n, w->a3, 3 * kTriB, w->b3, 3 * kTriB, m, ncols, 3 * kTriB, kLuUpdateTF32, w, st);
     }
+    apply_block_kernel<<<ceil_div(ncols, 64), 256, 0, st>>>(D, X, n, r0, nb, ncols);
+    UVLM_LAUNCH_CHECK();
+    if (m <= 0) return ok();
     return gemm_update_f32_simt(C, n, A, n, X + (long long)r0 * n, n, m, ncols, nb, st);
   };
   // X = L^-1 (L unit lower triangular, so X is too: block row I is non-zero
@@ -1412,17 +1470,13 @@ Error lu_inverse_f32(const float* LU, int n, LuUpdate upd, LuWork* w, float* X, 
   // X_>I -= L_>I,I X_I on those columns
   for (int I = 0; I < nblk; ++I) {
     const int r0 = I * kTriB, nb = std::min(kTriB, n - r0), r1 = r0 + nb;
-    apply_block_kernel<<<ceil_div(r1, 64), 256, 0, st>>>(dl + (long long)I * kTriB * kTriB, X, n, r0, nb, r1);
-    UVLM_LAUNCH_CHECK();
-    UVLM_TRY(update(X + (long long)r1 * n, LU + (long long)r1 * n + r0, n - r1, r1, r0, nb));
+    UVLM_TRY(step(dl + (long long)I * kTriB * kTriB, X + (long long)r1 * n, LU + (long long)r1 * n + r0, n - r1, r1,
+                  r0, nb));
   }
   // X = U^-1 X (dense): X_I = Uinv_II X_I, then X_<I -= U_<I,I X_I
-  const int cg = ceil_div(n, 64);
   for (int I = nblk - 1; I >= 0; --I) {
     const int r0 = I * kTriB, nb = std::min(kTriB, n - r0);
-    apply_block_kernel<<<cg, 256, 0, st>>>(du + (long long)I * kTriB * kTriB, X, n, r0, nb, n);
-    UVLM_LAUNCH_CHECK();
-    UVLM_TRY(update(X, LU + r0, r0, n, r0, nb));
+    UVLM_TRY(step(du + (long long)I * kTriB * kTriB, X, LU + r0, r0, n, r0, nb));
   }
   return ok();
 }
