@@ -106,6 +106,10 @@ typedef struct {
                                 (over the panel's top 256 rows only, the default: a cheaper panel for
                                 diagonally heavy influence matrices; GMRES with FP64 residuals and the
                                 plain fresh-LU fallback keep the answer whatever the pivots) */
+  int32_t gmres_refresh_iter; /* mixed form, GMRES solver: a step whose GMRES took at least this many
+                                 iterations has the preconditioner refactored from the next step's
+                                 matrix (0: only when gmres_max_iter is exceeded, the fallback); the
+                                 default 16 refreshes aging factors before they reach the fallback */
 } uvlm_config;
 
 #define UVLM_PIVOT_PANEL 0

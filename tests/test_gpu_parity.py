@@ -342,6 +342,38 @@ def test_mixed_local_and_panel_pivoting_agree():
     np.testing.assert_allclose(out["local"][0], out["panel"][0], rtol=0, atol=1e-10 * scale)
 
 
+def test_mixed_preconditioner_refresh_keeps_the_answer():
+    """gmres_refresh_iter = 1 refactors the preconditioner after every step that
+    iterated (the step after reports refactored, path 0), 0 only on the
+    fallback: both give the same loads to the GMRES tolerance."""
+    import uvlm_b200 as M
+
+    dt = 2 * math.pi / 40
+    out = {}
+    for ref in (0, 1):
+        sim = M.SimpleSimulator(precision="mixed", warm_start="extrapolate", gmres_refresh_iter=ref, max_wake_rows=40)
+        m = M.Morphing().set_plug(0.2, 1.0).set_twist(math.radians(10), 1.0, math.pi / 2)
+        sim.AddWing(M.RectGenerator(), m, 1.0, 4.0, 8, 16)
+        sim.set_forward_flight([-1.0, 0.0, 0.0])
+        sim.begin()
+        rows, stats = [], []
+        for s_ in range(10):
+            rows.append(sim.step(s_, dt))
+            st = sim.stats()
+            stats.append((int(st.refactored), int(st.solve_path), int(st.gmres_iters)))
+        sim.close()
+        out[ref] = (np.array(rows), stats)
+    assert sum(r for r, _, _ in out[0][1]) == 1  # step 0 only
+    refreshed = 0
+    for (r_prev, _, it_prev), (r, path, _) in zip(out[1][1][1:], out[1][1][2:]):
+        if r_prev == 0 and it_prev >= 1:  # a stale-factor step that iterated
+            assert r == 1 and path == 0
+            refreshed += 1
+    assert refreshed >= 1
+    scale = np.max(np.abs(out[0][0][:, 1:]))
+    np.testing.assert_allclose(out[1][0], out[0][0], rtol=0, atol=1e-10 * scale)
+
+
 def test_dense_solve_singular_reports():
     M = U()
     A = np.ones((4, 4))

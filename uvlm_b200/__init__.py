@@ -137,13 +137,17 @@ class SimpleSimulator:
       lu_pivoting mixed form, the preconditioner's factors: "panel" (pivots
                   over every row of each 64-column panel) or "local" (over
                   the panel's top 256 rows); None takes the library's default
+      gmres_refresh_iter  mixed form: refactor the preconditioner after a step
+                  whose GMRES took at least this many iterations (0: only on
+                  the fallback); None takes the library's default (16)
     """
 
     def __init__(self, precision: str = "fp64", solver: str | None = None, warm_start: str = "previous",
                  lu_precision: str = "tf32", max_wake_rows: int = 1024, erase_wake_after: int = 0,
                  gmres_tol: float = 1e-12, gmres_max_iter: int = 20, gmres_restart: int = 20, device: int = 0,
                  assembly_fp64: bool | None = None, nbody_variant: int = -1, compute_loads: bool = True,
-                 preconditioner: str = "inverse", fp64_stages=(), near_fp64=None, lu_pivoting: str | None = None):
+                 preconditioner: str = "inverse", fp64_stages=(), near_fp64=None, lu_pivoting: str | None = None,
+                 gmres_refresh_iter: int | None = None):
         cfg = Config()
         lib().uvlm_config_default(C.byref(cfg))
         cfg.precision = PRECISION[precision]
@@ -171,6 +175,8 @@ class SimpleSimulator:
             cfg.nbody_near_fp64 = sum(stages[s] for s in set(near_fp64 or ()))
         if lu_pivoting is not None:
             cfg.lu_pivoting = {"panel": 0, "local": 1}[lu_pivoting]
+        if gmres_refresh_iter is not None:
+            cfg.gmres_refresh_iter = int(gmres_refresh_iter)
         self._cfg = cfg
         h = C.c_void_p()
         check(lib().uvlm_create(C.byref(cfg), C.byref(h)))

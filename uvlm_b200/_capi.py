@@ -32,7 +32,7 @@ class Config(C.Structure):
         ("gmres_restart", C.c_int32), ("gmres_max_iter", C.c_int32), ("gmres_tol", C.c_double),
         ("device", C.c_int32), ("compute_loads", C.c_int32), ("assembly_fp64", C.c_int32),
         ("nbody_variant", C.c_int32), ("preconditioner", C.c_int32), ("nbody_fp64_stages", C.c_int32),
-        ("nbody_near_fp64", C.c_int32), ("lu_pivoting", C.c_int32),
+        ("nbody_near_fp64", C.c_int32), ("lu_pivoting", C.c_int32), ("gmres_refresh_iter", C.c_int32),
     ]
 
 

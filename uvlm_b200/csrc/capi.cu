@@ -103,6 +103,7 @@ struct uvlm_ctx {
   LuWork lu;
   GmresWork gm;
   bool have_factors = false;
+  bool refresh_next = false;  // refactor at the next solve (GMRES reached gmres_refresh_iter)
   // N-body tile variant per stage (kStageRhs, kStageLoads, kStageAdvect) and
   // precision ([0] FP32, [1] FP64); defaults fp32_h3_t2_b128_x2f and
   // fp64_h2_t1_b128_m3, each autotuned on that stage's first large evaluation
@@ -396,7 +397,10 @@ Error uvlm_ctx::solve(long long step) {
     work_lu += 2.0 / 3.0 * (double)N * N * N;
     return ok();
   };
-  const bool fresh = cfg.solver == UVLM_SOLVER_LU || !have_factors;
+  // a fresh factorisation every step (the LU solver), on the first step, or
+  // when the previous step's GMRES needed gmres_refresh_iter iterations or more
+  const bool fresh = cfg.solver == UVLM_SOLVER_LU || !have_factors || refresh_next;
+  refresh_next = false;
   if (fresh) UVLM_TRY(factor());
   // initial guess: d_gamma holds g_n (the previous solution); the linear
   // extrapolation 2 g_n - g_{n-1} uses the history kept in d_gamma_hist
@@ -455,6 +459,9 @@ Error uvlm_ctx::solve(long long step) {
   }
   last.residual = r.relres;
   if (!r.converged) return fail(kErrNonFinite, "GMRES did not converge after a fresh factorisation");
+  // aging factors: refactor from the next step's matrix before GMRES reaches its cap (the fallback
+  // costs a fresh FP64 LU on top of the refactorisation)
+  if (!fresh && cfg.gmres_refresh_iter > 0 && r.iters >= cfg.gmres_refresh_iter) refresh_next = true;
   return ok();
 }
 
@@ -751,6 +758,7 @@ void uvlm_config_default(uvlm_config* c) {
   // there, so the factors (and every GMRES iterate) are the same as with the
   // panel-wide tournament, for 0.65x the factorisation time
   c->lu_pivoting = UVLM_PIVOT_LOCAL;
+  c->gmres_refresh_iter = 16;
 }
 
 const char* uvlm_status_string(int s) {
@@ -787,7 +795,7 @@ int uvlm_create(const uvlm_config* cfg, uvlm_ctx** out) {
       !(k.gmres_tol > 0) || k.preconditioner < 0 || k.preconditioner > 1 || k.nbody_fp64_stages < 0 ||
       k.nbody_fp64_stages > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT) || k.nbody_near_fp64 < 0 ||
       k.nbody_near_fp64 > (UVLM_STAGE_RHS | UVLM_STAGE_LOADS | UVLM_STAGE_ADVECT) ||
-      (k.lu_pivoting != UVLM_PIVOT_PANEL && k.lu_pivoting != UVLM_PIVOT_LOCAL)) {
+      (k.lu_pivoting != UVLM_PIVOT_PANEL && k.lu_pivoting != UVLM_PIVOT_LOCAL) || k.gmres_refresh_iter < 0) {
     delete c;
     return set_global(fail(kErrInvalid, "invalid configuration"));
   }
