@@ -664,8 +664,9 @@ def run_ours(args, rank, world, local_rank):
                                   "frac": asm_tflops / pk64.value,
                                   "per_unit": f"{FLOP_PER_PAIR} FLOP per (collocation point, unique wing segment) pair",
                                   "units_per_step": asm_pairs, "stage_ms": stage_ms[1],
-                                  "note": "the kernel evaluates each ring's 4 segments (about 2x the unique "
-                                          "segments), which is not credited"},
+                                  "note": "each unique segment once per collocation point (a ring's 4 "
+                                          "segments combined from its own and its neighbours'); the FP64 "
+                                          "reciprocal square roots and divides are instruction sequences"},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 8 * (1 + 2 * wl.num + wl.num * ROWS * COLS),
                     "note": "wall clock per uvlm_step + circulation download; per-step inputs are scalars"},

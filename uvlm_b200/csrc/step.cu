@@ -59,72 +59,79 @@ __global__ void panel_geometry_kernel(const uvlm_kinematics* __restrict__ kin, W
 }
 
 // ---------------------------------------------------------------- assembly
-// CTA: 128 rings (threads) x a chunk of collocation points staged in shared
-// memory; each thread evaluates its ring's four segments p0->p1->p2->p3->p0
-// (VORING, src/vortex.cpp:145-160) at every staged point.
-constexpr int kAsmRings = 128;
-constexpr int kAsmTargets = 128;
-
-template <class T>
-struct AsmPt {
-  T hx, hy, hz, lx, ly, lz, nx, ny, nz;
-};
+// A[K][L] = VORING(c_K, L, 1) . n_K by unique lattice segments.  Ring (i, j)
+// is p0 -> p1 -> p2 -> p3 -> p0 with p0 = (i, j), p1 = (i, j+1), p2 = (i+1, j+1),
+// p3 = (i+1, j) (src/vortex.cpp:145-160): the spanwise segment S(i, j) =
+// (i, j) -> (i, j+1), the chordwise H(i, j+1) = (i, j+1) -> (i+1, j+1), then
+// S(i+1, j) and H(i, j) backwards.  Neighbouring rings share those segments
+// with opposite signs, so one lane per (collocation point K, node column j of
+// wing n) walks the node rows i = 0..R, forms the nodes (i, j) and (i, j+1)
+// once per row and the segments S(i, j) and H(i-1, j) once, takes H(i-1, j+1)
+// from the next lane, and writes ring (i-1, j) = S(i-1, j) + H(i-1, j+1) -
+// S(i, j) - H(i-1, j): two segment evaluations per (point, ring) pair instead
+// of four, two nodes instead of four.  Lanes run over (K, node column) with 31
+// new positions per warp, so lane 31 only supplies its chordwise segment to
+// lane 30; node column C of a wing (no ring of its own) does the same for
+// column C - 1.  The segment arithmetic is the ring form's (bs_math.cuh); a
+// backward segment is the negated forward one, equal to rounding.
+constexpr int kAsmBlock = 128;
+constexpr int kAsmPerWarp = 31;
 
 template <class T, class OutT>
-__global__ void __launch_bounds__(kAsmRings) assemble_kernel(WingShape ws, const double* __restrict__ pos,
-                                                              const double* __restrict__ cx, const double* __restrict__ cy,
-                                                              const double* __restrict__ cz,
-                                                              const double* __restrict__ normal, int chunk, OutT* A) {
-  __shared__ AsmPt<T> pts[kAsmTargets];
+__global__ void __launch_bounds__(kAsmBlock) assemble_kernel(WingShape ws, const double* __restrict__ pos,
+                                                             const double* __restrict__ cx, const double* __restrict__ cy,
+                                                             const double* __restrict__ cz,
+                                                             const double* __restrict__ normal, OutT* A) {
+  const int C1 = ws.C + 1;
+  const int NC = ws.num * C1;
   const int N = ws.num * ws.R * ws.C;
-  const int L = blockIdx.x * kAsmRings + threadIdx.x;
-  const bool valid = L < N;
-  const int Lc = valid ? L : N - 1;
-  const int per = ws.R * ws.C;
-  const int n = Lc / per, i = (Lc % per) / ws.C, j = Lc % ws.C;
-  const long long idx[4] = {ws.node(n, i, j), ws.node(n, i, j + 1), ws.node(n, i + 1, j + 1), ws.node(n, i + 1, j)};
-  T ph[4][3], pl[4][3];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const double v = pos[3 * idx[q] + d];
-      ph[q][d] = (T)v;
-      pl[q][d] = (T)(v - (double)ph[q][d]);
-    }
+  const long long P = (long long)N * NC;
+  const int lane = threadIdx.x & 31;
+  const long long p0 = ((long long)blockIdx.x * (kAsmBlock / 32) + (threadIdx.x >> 5)) * kAsmPerWarp;
+  if (p0 >= P) return;  // the whole warp
+  const long long p = min(p0 + lane, P - 1);
+  const int K = (int)(p / NC);
+  const int jn = (int)(p - (long long)K * NC);
+  const int n = jn / C1, j = jn - n * C1;
+  const bool owner = lane < kAsmPerWarp && p0 + lane < P && j < ws.C;
+  const int j1 = min(j + 1, ws.C);
+  const double X = cx[K], Y = cy[K], Z = cz[K];
+  const T hx = (T)X, hy = (T)Y, hz = (T)Z;
+  const T lx = (T)(X - (double)hx), ly = (T)(Y - (double)hy), lz = (T)(Z - (double)hz);
+  const T nx = (T)normal[3 * K], ny = (T)normal[3 * K + 1], nz = (T)normal[3 * K + 2];
   const T g = (T)(1.0 / (4.0 * kPi));
-  const int K0 = blockIdx.y * chunk;
-  const int K1 = min(N, K0 + chunk);
-  for (int kb = K0; kb < K1; kb += kAsmTargets) {
-    const int cnt = min(kAsmTargets, K1 - kb);
-    __syncthreads();
-    if (threadIdx.x < cnt) {
-      const int K = kb + threadIdx.x;
-      AsmPt<T> p;
-      const double x = cx[K], y = cy[K], z = cz[K];
-      p.hx = (T)x; p.hy = (T)y; p.hz = (T)z;
-      p.lx = (T)(x - (double)p.hx); p.ly = (T)(y - (double)p.hy); p.lz = (T)(z - (double)p.hz);
-      p.nx = (T)normal[3 * K]; p.ny = (T)normal[3 * K + 1]; p.nz = (T)normal[3 * K + 2];
-      pts[threadIdx.x] = p;
+  // x - p from the hi/lo parts of both (FP64: lo = 0, the plain difference)
+  auto node_at = [&](int i, int jj) {
+    const double* q = pos + 3 * ws.node(n, i, jj);
+    const double qx = q[0], qy = q[1], qz = q[2];
+    const T px = (T)qx, py = (T)qy, pz = (T)qz;
+    return make_node<T>((hx - px) + (lx - (T)(qx - (double)px)), (hy - py) + (ly - (T)(qy - (double)py)),
+                        (hz - pz) + (lz - (T)(qz - (double)pz)));
+  };
+  Node<T> a = node_at(0, j), b = node_at(0, j1);
+  T sx = 0, sy = 0, sz = 0;  // S(i-1, j)
+  segment<T>(a, b, g, sx, sy, sz);
+  OutT* row = A + (long long)K * N + ws.ring(n, 0, j);
+  for (int i = 1; i <= ws.R; ++i) {
+    const Node<T> a2 = node_at(i, j), b2 = node_at(i, j1);
+    T hvx = 0, hvy = 0, hvz = 0;  // H(i-1, j)
+    segment<T>(a, a2, g, hvx, hvy, hvz);
+    const T hnx = __shfl_down_sync(0xffffffffu, hvx, 1);  // H(i-1, j+1)
+    const T hny = __shfl_down_sync(0xffffffffu, hvy, 1);
+    const T hnz = __shfl_down_sync(0xffffffffu, hvz, 1);
+    T s2x = 0, s2y = 0, s2z = 0;  // S(i, j)
+    segment<T>(a2, b2, g, s2x, s2y, s2z);
+    if (owner) {
+      const T vx = ((sx + hnx) - s2x) - hvx;
+      const T vy = ((sy + hny) - s2y) - hvy;
+      const T vz = ((sz + hnz) - s2z) - hvz;
+      row[(long long)(i - 1) * ws.C] = (OutT)(vx * nx + vy * ny + vz * nz);
     }
-    __syncthreads();
-    for (int t = 0; t < cnt; ++t) {
-      const AsmPt<T> p = pts[t];
-      Node<T> nd[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const T x = (p.hx - ph[q][0]) + (p.lx - pl[q][0]);
-        const T y = (p.hy - ph[q][1]) + (p.ly - pl[q][1]);
-        const T z = (p.hz - ph[q][2]) + (p.lz - pl[q][2]);
-        nd[q] = make_node<T>(x, y, z);
-      }
-      T vx = 0, vy = 0, vz = 0;
-      segment<T>(nd[0], nd[1], g, vx, vy, vz);
-      segment<T>(nd[1], nd[2], g, vx, vy, vz);
-      segment<T>(nd[2], nd[3], g, vx, vy, vz);
-      segment<T>(nd[3], nd[0], g, vx, vy, vz);
-      if (valid) A[(long long)(kb + t) * N + L] = (OutT)(vx * p.nx + vy * p.ny + vz * p.nz);
-    }
+    a = a2;
+    b = b2;
+    sx = s2x;
+    sy = s2y;
+    sz = s2z;
   }
 }
 
@@ -390,22 +397,20 @@ Error launch_panel_geometry(const uvlm_kinematics* d_kin, WingShape ws, const do
 
 Error launch_assemble(WingShape ws, const double* pos, const double* cx, const double* cy, const double* cz,
                       const double* normal, bool fp32, void* A, bool out_f32, cudaStream_t st) {
-  const int N = ws.num * ws.R * ws.C;
-  const int gx = ceil_div(N, kAsmRings);
-  // split the collocation points so that the grid has a few waves
-  int chunk = kAsmTargets * std::max(1, ceil_div(N, kAsmTargets * std::max(1, 1184 / std::max(gx, 1))));
-  const int gy = ceil_div(N, chunk);
-  dim3 grid(gx, gy);
+  const long long N = (long long)ws.num * ws.R * ws.C;
+  const long long lanes = N * ws.num * (ws.C + 1);
+  const long long warps = (lanes + kAsmPerWarp - 1) / kAsmPerWarp;
+  const unsigned grid = (unsigned)((warps + kAsmBlock / 32 - 1) / (kAsmBlock / 32));
   if (fp32) {
     if (out_f32)
-      assemble_kernel<float, float><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (float*)A);
+      assemble_kernel<float, float><<<grid, kAsmBlock, 0, st>>>(ws, pos, cx, cy, cz, normal, (float*)A);
     else
-      assemble_kernel<float, double><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (double*)A);
+      assemble_kernel<float, double><<<grid, kAsmBlock, 0, st>>>(ws, pos, cx, cy, cz, normal, (double*)A);
   } else {
     if (out_f32)
-      assemble_kernel<double, float><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (float*)A);
+      assemble_kernel<double, float><<<grid, kAsmBlock, 0, st>>>(ws, pos, cx, cy, cz, normal, (float*)A);
     else
-      assemble_kernel<double, double><<<grid, kAsmRings, 0, st>>>(ws, pos, cx, cy, cz, normal, chunk, (double*)A);
+      assemble_kernel<double, double><<<grid, kAsmBlock, 0, st>>>(ws, pos, cx, cy, cz, normal, (double*)A);
   }
   UVLM_LAUNCH_CHECK();
   return ok();
