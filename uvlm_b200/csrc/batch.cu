@@ -142,62 +142,74 @@ __global__ void b_geometry_kernel(const BCase* __restrict__ cs, BPrefix P, int n
 }
 
 // ---------------------------------------------------------------- assembly
-// Tile = (case, 128 rings, a range of collocation points); thread = ring L,
-// its four segments p0->p1->p2->p3->p0 (VORING, src/vortex.cpp:145-160)
-// evaluated at every staged point, FP64.
+// FP64 influence matrix of every case by unique lattice segments, as the
+// single-case assembly: one lane per (collocation point K, node column j)
+// walks the node rows and writes ring (i-1, j) = S(i-1, j) + H(i-1, j+1) -
+// S(i, j) - H(i-1, j) (VORING's p0 -> p1 -> p2 -> p3 -> p0, src/vortex.cpp:145-160),
+// H(i-1, j+1) from the next lane; warps advance 31 positions.  Tile = (case,
+// a range [p0, p1) of its (K, node column) positions, K-major).
 struct AsmTile {
-  int c, L0, K0, K1;
+  int c;
+  long long p0, p1;
 };
-constexpr int kBAsmRings = 128;
+constexpr int kBAsmThreads = 128;
+constexpr int kBAsmPerWarp = 31;
+constexpr int kBAsmTilePositions = kBAsmPerWarp * (kBAsmThreads / 32) * 8;
 
-__global__ void __launch_bounds__(kBAsmRings) b_assemble_kernel(const BCase* __restrict__ cs,
-                                                                const AsmTile* __restrict__ tiles,
-                                                                const double* __restrict__ pos,
-                                                                const double* __restrict__ cx,
-                                                                const double* __restrict__ cy,
-                                                                const double* __restrict__ cz,
-                                                                const double* __restrict__ normal, double* A) {
-  __shared__ double pts[kBAsmRings][6];
+__global__ void __launch_bounds__(kBAsmThreads) b_assemble_kernel(const BCase* __restrict__ cs,
+                                                                  const AsmTile* __restrict__ tiles,
+                                                                  const double* __restrict__ pos,
+                                                                  const double* __restrict__ cx,
+                                                                  const double* __restrict__ cy,
+                                                                  const double* __restrict__ cz,
+                                                                  const double* __restrict__ normal, double* A) {
   const AsmTile T = tiles[blockIdx.x];
   const BCase& b = cs[T.c];
   const WingShape ws = shape_of(b);
-  const int L = T.L0 + threadIdx.x;
-  const bool valid = L < b.N;
-  const int Lc = valid ? L : b.N - 1;
-  const int i = Lc / b.C, j = Lc % b.C;
+  const int C1 = b.C + 1;
+  const long long P = (long long)b.N * C1;
+  const int lane = threadIdx.x & 31;
   const double* ps = pos + 3 * b.node_off;
-  const long long idx[4] = {ws.node(0, i, j), ws.node(0, i, j + 1), ws.node(0, i + 1, j + 1), ws.node(0, i + 1, j)};
-  double p[4][3];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) p[q][d] = ps[3 * idx[q] + d];
   const double g = 1.0 / (4.0 * kPi);
   double* Ac = A + b.mat_off;
-  for (int kb = T.K0; kb < T.K1; kb += kBAsmRings) {
-    const int cnt = min(kBAsmRings, T.K1 - kb);
-    __syncthreads();
-    if (threadIdx.x < cnt) {
-      const long long K = b.ring_off + kb + threadIdx.x;
-      pts[threadIdx.x][0] = cx[K];
-      pts[threadIdx.x][1] = cy[K];
-      pts[threadIdx.x][2] = cz[K];
-      pts[threadIdx.x][3] = normal[3 * K];
-      pts[threadIdx.x][4] = normal[3 * K + 1];
-      pts[threadIdx.x][5] = normal[3 * K + 2];
-    }
-    __syncthreads();
-    for (int t = 0; t < cnt; ++t) {
-      Node<double> nd[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        nd[q] = make_node<double>(pts[t][0] - p[q][0], pts[t][1] - p[q][1], pts[t][2] - p[q][2]);
-      double vx = 0, vy = 0, vz = 0;
-      segment<double>(nd[0], nd[1], g, vx, vy, vz);
-      segment<double>(nd[1], nd[2], g, vx, vy, vz);
-      segment<double>(nd[2], nd[3], g, vx, vy, vz);
-      segment<double>(nd[3], nd[0], g, vx, vy, vz);
-      if (valid) Ac[(long long)(kb + t) * b.N + L] = vx * pts[t][3] + vy * pts[t][4] + vz * pts[t][5];
+  for (long long base = T.p0 + (long long)(threadIdx.x >> 5) * kBAsmPerWarp; base < T.p1;
+       base += (long long)kBAsmPerWarp * (kBAsmThreads / 32)) {
+    // the halo lane may read the position after the tile (or the case's last again)
+    const long long p = min(base + lane, P - 1);
+    const int K = (int)(p / C1), j = (int)(p - (long long)K * C1);
+    const bool owner = lane < kBAsmPerWarp && base + lane < T.p1 && j < b.C;
+    const int j1 = min(j + 1, b.C);
+    const long long Kg = b.ring_off + K;
+    const double X = cx[Kg], Y = cy[Kg], Z = cz[Kg];
+    const double nx = normal[3 * Kg], ny = normal[3 * Kg + 1], nz = normal[3 * Kg + 2];
+    auto node_at = [&](int i, int jj) {
+      const double* q = ps + 3 * ws.node(0, i, jj);
+      return make_node<double>(X - q[0], Y - q[1], Z - q[2]);
+    };
+    Node<double> na = node_at(0, j), nb = node_at(0, j1);
+    double sx = 0, sy = 0, sz = 0;  // S(i-1, j)
+    segment<double>(na, nb, g, sx, sy, sz);
+    double* row = Ac + (long long)K * b.N + j;
+    for (int i = 1; i <= b.R; ++i) {
+      const Node<double> na2 = node_at(i, j), nb2 = node_at(i, j1);
+      double hx = 0, hy = 0, hz = 0;  // H(i-1, j)
+      segment<double>(na, na2, g, hx, hy, hz);
+      const double hnx = __shfl_down_sync(0xffffffffu, hx, 1);  // H(i-1, j+1)
+      const double hny = __shfl_down_sync(0xffffffffu, hy, 1);
+      const double hnz = __shfl_down_sync(0xffffffffu, hz, 1);
+      double s2x = 0, s2y = 0, s2z = 0;  // S(i, j)
+      segment<double>(na2, nb2, g, s2x, s2y, s2z);
+      if (owner) {
+        const double vx = ((sx + hnx) - s2x) - hx;
+        const double vy = ((sy + hny) - s2y) - hy;
+        const double vz = ((sz + hnz) - s2z) - hz;
+        row[(long long)(i - 1) * b.C] = vx * nx + vy * ny + vz * nz;
+      }
+      na = na2;
+      nb = nb2;
+      sx = s2x;
+      sy = s2y;
+      sz = s2z;
     }
   }
 }
@@ -954,9 +966,10 @@ Error uvlm_batch::alloc(const uvlm_batch_case* cases) {
     w.chebyshev_span = u.chebyshev_span;
     auto v = whole_wing_nodes(w);
     nodes.insert(nodes.end(), v.begin(), v.end());
-    // assembly tiles: 128 rings x up to 512 collocation points
-    for (int L0 = 0; L0 < b.N; L0 += kBAsmRings)
-      for (int K0 = 0; K0 < b.N; K0 += 512) tiles.push_back(AsmTile{c, L0, K0, std::min(b.N, K0 + 512)});
+    // assembly tiles: runs of (collocation point, node column) positions
+    const long long positions = (long long)b.N * (b.C + 1);
+    for (long long p0 = 0; p0 < positions; p0 += kBAsmTilePositions)
+      tiles.push_back(AsmTile{c, p0, std::min(positions, p0 + kBAsmTilePositions)});
   }
   for (int k = 0; k < 7; ++k) pre[k][n] = off[k];
   tot_nodes = off[0];
@@ -1163,7 +1176,7 @@ Error uvlm_batch::enqueue_step() {
   b_geometry_kernel<<<grid, 256, 0, st>>>(d_cases, P, n, d_step, d_pos, d_pos_init, d_cx, d_cy, d_cz, d_normal,
                                           d_area, d_uls);
   UVLM_LAUNCH_CHECK();
-  b_assemble_kernel<<<n_tiles, kBAsmRings, 0, st>>>(d_cases, d_tiles, d_pos, d_cx, d_cy, d_cz, d_normal, d_A64);
+  b_assemble_kernel<<<n_tiles, kBAsmThreads, 0, st>>>(d_cases, d_tiles, d_pos, d_cx, d_cy, d_cz, d_normal, d_A64);
   UVLM_LAUNCH_CHECK();
   // RHS: wake normal wash at the collocation points
   UVLM_TRY(records(0, d_wpos));
