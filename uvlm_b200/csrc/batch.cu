@@ -479,22 +479,45 @@ __device__ void cta_lu_solve(const T* LU, int N, const int* piv, double* x) {
       }
     }
   __syncthreads();
+  // Full 32-column blocks take unrolled loops (the same operations in the
+  // same order): the loads of a row segment, which do not depend on the
+  // substitution chain, then issue together instead of a few at a time.
   for (int J0 = 0; J0 < N; J0 += 32) {
     const int nb = min(32, N - J0);
     if (threadIdx.x < 32) {
       const int q = threadIdx.x;
       double v = q < nb ? x[J0 + q] : 0.0;
-      for (int l = 0; l < nb; ++l) {
-        const double xl = __shfl_sync(0xffffffffu, v, l);
-        if (q > l && q < nb) v -= (double)LU[(long long)(J0 + q) * N + J0 + l] * xl;
+      if (nb == 32) {
+        const T* a = LU + (long long)(J0 + q) * N + J0;
+#pragma unroll
+        for (int l = 0; l < 32; ++l) {
+          const double xl = __shfl_sync(0xffffffffu, v, l);
+          if (q > l) v -= (double)a[l] * xl;
+        }
+      } else {
+        for (int l = 0; l < nb; ++l) {
+          const double xl = __shfl_sync(0xffffffffu, v, l);
+          if (q > l && q < nb) v -= (double)LU[(long long)(J0 + q) * N + J0 + l] * xl;
+        }
       }
       if (q < nb) x[J0 + q] = v;
     }
     __syncthreads();
-    for (int i = J0 + nb + threadIdx.x; i < N; i += blockDim.x) {
-      double s = x[i];
-      for (int l = 0; l < nb; ++l) s -= (double)LU[(long long)i * N + J0 + l] * x[J0 + l];
-      x[i] = s;
+    if (nb == 32) {
+#pragma unroll 2
+      for (int i = J0 + 32 + threadIdx.x; i < N; i += blockDim.x) {
+        const T* a = LU + (long long)i * N + J0;
+        double s = x[i];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) s -= (double)a[l] * x[J0 + l];
+        x[i] = s;
+      }
+    } else {
+      for (int i = J0 + nb + threadIdx.x; i < N; i += blockDim.x) {
+        double s = x[i];
+        for (int l = 0; l < nb; ++l) s -= (double)LU[(long long)i * N + J0 + l] * x[J0 + l];
+        x[i] = s;
+      }
     }
     __syncthreads();
   }
@@ -503,18 +526,39 @@ __device__ void cta_lu_solve(const T* LU, int N, const int* piv, double* x) {
     if (threadIdx.x < 32) {
       const int q = threadIdx.x;
       double v = q < nb ? x[J0 + q] : 0.0;
-      for (int l = nb - 1; l >= 0; --l) {
-        if (q == l) v /= (double)LU[(long long)(J0 + l) * N + J0 + l];
-        const double xl = __shfl_sync(0xffffffffu, v, l);
-        if (q < l) v -= (double)LU[(long long)(J0 + q) * N + J0 + l] * xl;
+      if (nb == 32) {
+        const T* a = LU + (long long)(J0 + q) * N + J0;
+#pragma unroll
+        for (int l = 31; l >= 0; --l) {
+          if (q == l) v /= (double)a[l];
+          const double xl = __shfl_sync(0xffffffffu, v, l);
+          if (q < l) v -= (double)a[l] * xl;
+        }
+      } else {
+        for (int l = nb - 1; l >= 0; --l) {
+          if (q == l) v /= (double)LU[(long long)(J0 + l) * N + J0 + l];
+          const double xl = __shfl_sync(0xffffffffu, v, l);
+          if (q < l) v -= (double)LU[(long long)(J0 + q) * N + J0 + l] * xl;
+        }
       }
       if (q < nb) x[J0 + q] = v;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < J0; i += blockDim.x) {
-      double s = x[i];
-      for (int l = 0; l < nb; ++l) s -= (double)LU[(long long)i * N + J0 + l] * x[J0 + l];
-      x[i] = s;
+    if (nb == 32) {
+#pragma unroll 2
+      for (int i = threadIdx.x; i < J0; i += blockDim.x) {
+        const T* a = LU + (long long)i * N + J0;
+        double s = x[i];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) s -= (double)a[l] * x[J0 + l];
+        x[i] = s;
+      }
+    } else {
+      for (int i = threadIdx.x; i < J0; i += blockDim.x) {
+        double s = x[i];
+        for (int l = 0; l < nb; ++l) s -= (double)LU[(long long)i * N + J0 + l] * x[J0 + l];
+        x[i] = s;
+      }
     }
     __syncthreads();
   }
@@ -584,7 +628,7 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
         const double* a2 = v2 ? a0 + 2LL * kW * N : a0;
         const double* a3 = v3 ? a0 + 3LL * kW * N : a0;
         double c0 = 0, c1 = 0, c2 = 0, c3 = 0;
-#pragma unroll 4
+#pragma unroll 8
         for (int j = lane; j < N; j += 32) {
           const double xj = x[j];
           c0 += a0[j] * xj;
