@@ -287,7 +287,13 @@ __global__ void b_rhs_kernel(const BCase* __restrict__ cs, BPrefix P, int n, con
 }
 
 // ------------------------------------------------------------- dense solve
-constexpr int kSolveThreads = 256;
+// Threads of the per-case solve CTA: the FP32-factor form (refinement sweeps,
+// latency-bound streaming on the largest cases) takes 16 warps; the FP64
+// form, which factors every step, 8 (its panel code keeps its registers).
+template <class T>
+struct SolveCfg {
+  static constexpr int kThreads = sizeof(T) == 4 ? 512 : 256;
+};
 
 // Panel width of the shared-memory LU: 32 FP32 / 16 FP64 columns, so that
 // the whole panel of the largest case (1024 rows) stays in shared memory.
@@ -314,15 +320,17 @@ inline size_t panel_smem_bytes(int max_N, int elem) {
 template <class T>
 __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
   constexpr int NB = PanelCfg<T>::NB, LD = PanelCfg<T>::LD;
-  __shared__ double s_val[kSolveThreads / 32];
-  __shared__ int s_idx[kSolveThreads / 32];
+  constexpr int NT = SolveCfg<T>::kThreads;
+  constexpr int TR = NT / 16 * 4;  // rows of an A22 tile (16 threads x 4 columns across, 4 rows each)
+  __shared__ double s_val[NT / 32];
+  __shared__ int s_idx[NT / 32];
   __shared__ int s_piv[NB];
   __shared__ T Bs[NB][64];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int k0 = 0; k0 < N; k0 += NB) {
     const int kb = min(NB, N - k0);
     const int m = N - k0;
-    for (int q = tid; q < m * NB; q += kSolveThreads) {
+    for (int q = tid; q < m * NB; q += NT) {
       const int r = q / NB, c = q % NB;
       P[r * LD + c] = c < kb ? A[(long long)(k0 + r) * N + k0 + c] : (T)0;
     }
@@ -330,7 +338,7 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
     for (int jj = 0; jj < kb; ++jj) {
       double best = -1.0;
       int bi = jj;
-      for (int i = jj + tid; i < m; i += kSolveThreads) {
+      for (int i = jj + tid; i < m; i += NT) {
         const double v = fabs((double)P[i * LD + jj]);
         if (v > best) {
           best = v;
@@ -353,7 +361,7 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
       if (tid == 0) {
         double bv = s_val[0];
         int ii = s_idx[0];
-        for (int w = 1; w < kSolveThreads / 32; ++w)
+        for (int w = 1; w < NT / 32; ++w)
           if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < ii)) {
             bv = s_val[w];
             ii = s_idx[w];
@@ -371,7 +379,7 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
       }
       __syncthreads();
       const T d = P[jj * LD + jj];
-      for (int i = jj + 1 + tid; i < m; i += kSolveThreads) {
+      for (int i = jj + 1 + tid; i < m; i += NT) {
         T* row = P + i * LD;
         const T l = row[jj] / d;
         row[jj] = l;
@@ -380,7 +388,7 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
       __syncthreads();
     }
     // panel back to global memory
-    for (int q = tid; q < m * NB; q += kSolveThreads) {
+    for (int q = tid; q < m * NB; q += NT) {
       const int r = q / NB, c = q % NB;
       if (c < kb) A[(long long)(k0 + r) * N + k0 + c] = P[r * LD + c];
     }
@@ -390,7 +398,7 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
       if (p != jj) {
         T* ra = A + (long long)(k0 + jj) * N;
         T* rb = A + (long long)(k0 + p) * N;
-        for (int c = tid; c < N - kb; c += kSolveThreads) {
+        for (int c = tid; c < N - kb; c += NT) {
           const int col = c < k0 ? c : c + kb;
           const T t = ra[col];
           ra[col] = rb[col];
@@ -402,7 +410,7 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
     const int c0 = k0 + kb;
     if (c0 >= N) break;
     // U12 = L11^-1 A12: column per thread, the column in registers
-    for (int c = c0 + tid; c < N; c += kSolveThreads) {
+    for (int c = c0 + tid; c < N; c += NT) {
       T u[NB];
 #pragma unroll
       for (int i = 0; i < NB; ++i) u[i] = i < kb ? A[(long long)(k0 + i) * N + c] : (T)0;
@@ -418,13 +426,13 @@ __device__ void cta_lu_panel_smem(T* A, int N, int* piv, int* status, T* P) {
         if (i < kb) A[(long long)(k0 + i) * N + c] = u[i];
     }
     __syncthreads();
-    // A22 -= L21 U12 in 64 x 64 tiles, L21 = panel rows kb.. (shared memory)
+    // A22 -= L21 U12 in TR x 64 tiles, L21 = panel rows kb.. (shared memory)
     const int mt = N - c0;
-    const int tiles = (mt + 63) / 64;
+    const int rtiles = (mt + TR - 1) / TR, ctiles = (mt + 63) / 64;
     const int tx = tid & 15, ty = tid >> 4;
-    for (int t = 0; t < tiles * tiles; ++t) {
-      const int r0 = (t / tiles) * 64, q0 = c0 + (t % tiles) * 64;  // r0 counts from row c0
-      for (int q = tid; q < NB * 64; q += kSolveThreads) {
+    for (int t = 0; t < rtiles * ctiles; ++t) {
+      const int r0 = (t / ctiles) * TR, q0 = c0 + (t % ctiles) * 64;  // r0 counts from row c0
+      for (int q = tid; q < NB * 64; q += NT) {
         const int l = q / 64, cc = q % 64;
         Bs[l][cc] = (q0 + cc < N && l < kb) ? A[(long long)(k0 + l) * N + q0 + cc] : (T)0;
       }
@@ -564,14 +572,15 @@ __device__ void cta_lu_solve(const T* LU, int N, const int* piv, double* x) {
   }
 }
 
+template <int NT>
 __device__ double cta_sum(double v) {
-  __shared__ double sh[kSolveThreads / 32];
+  __shared__ double sh[NT / 32];
   for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
   __syncthreads();
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
   double t = 0;
-  for (int w = 0; w < kSolveThreads / 32; ++w) t += sh[w];
+  for (int w = 0; w < NT / 32; ++w) t += sh[w];
   return t;
 }
 
@@ -589,13 +598,14 @@ constexpr double kStaleContraction = 0.5;
 // than kStaleContraction, is the FP32 copy of the current A factored again
 // (each case decides for itself; refac counts the factorisations).
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __restrict__ cs, double* A64, float* F32,
+__global__ void __launch_bounds__(SolveCfg<T>::kThreads) b_solve_kernel(const BCase* __restrict__ cs, double* A64, float* F32,
                                                                 int* piv_all, const double* rhs, double* gamma,
                                                                 const double* gamma_hist, const long long* d_step,
                                                                 int max_sweeps, double tol, int stale,
                                                                 int* has_factor, unsigned long long* refac,
                                                                 int* sweeps_out, double* res_out, int* status,
                                                                 const int* __restrict__ order) {
+  constexpr int NT = SolveCfg<T>::kThreads;
   extern __shared__ double sm[];
   // CTA i takes the i-th largest case: with more cases than SMs the largest
   // start first instead of forming the launch's last wave
@@ -613,14 +623,14 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
   if constexpr (sizeof(T) == 4) {
     T* LU = F32 + b.mat_off;
     double bn = 0;
-    for (int i = threadIdx.x; i < N; i += kSolveThreads) bn += bb[i] * bb[i];
-    bn = sqrt(cta_sum(bn));
+    for (int i = threadIdx.x; i < N; i += NT) bn += bb[i] * bb[i];
+    bn = sqrt(cta_sum<NT>(bn));
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     // r = b - A x (FP64), returns ||r|| / ||b|| (same value in every thread)
     auto residual = [&]() -> double {
       // four rows per warp at a time, so that enough loads of A are in
       // flight for one SM to stream the matrix
-      constexpr int kW = kSolveThreads / 32;
+      constexpr int kW = NT / 32;
       for (int i0 = wid; i0 < N; i0 += 4 * kW) {
         const double* a0 = A + (long long)i0 * N;
         const bool v1 = i0 + kW < N, v2 = i0 + 2 * kW < N, v3 = i0 + 3 * kW < N;
@@ -651,20 +661,20 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
       }
       __syncthreads();
       double rn = 0;
-      for (int i = threadIdx.x; i < N; i += kSolveThreads) rn += r[i] * r[i];
-      rn = sqrt(cta_sum(rn));
+      for (int i = threadIdx.x; i < N; i += NT) rn += r[i] * r[i];
+      rn = sqrt(cta_sum<NT>(rn));
       return bn > 0 ? rn / bn : 0.0;
     };
     auto sweep = [&]() {
       cta_lu_solve<T>(LU, N, piv, r);
-      for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] += r[i];
+      for (int i = threadIdx.x; i < N; i += NT) x[i] += r[i];
       __syncthreads();
     };
     bool done = false;
     if (stale && has_factor[ci]) {
       // refine from the extrapolation 2 G(s-1) - G(s-2) (from G(s-1) before step 2)
       const bool extrap = *d_step >= 2;
-      for (int i = threadIdx.x; i < N; i += kSolveThreads)
+      for (int i = threadIdx.x; i < N; i += NT)
         x[i] = extrap ? 2.0 * gamma[b.ring_off + i] - gamma_hist[b.ring_off + i] : gamma[b.ring_off + i];
       __syncthreads();
       rel = residual();
@@ -679,14 +689,14 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
       done = rel <= tol;
     }
     if (!done) {
-      for (long long q = threadIdx.x; q < (long long)N * N; q += kSolveThreads) LU[q] = (float)A[q];
+      for (long long q = threadIdx.x; q < (long long)N * N; q += NT) LU[q] = (float)A[q];
       __syncthreads();
       cta_lu_panel_smem<T>(LU, N, piv, status, panel);
       if (threadIdx.x == 0) {
         has_factor[ci] = 1;
         atomicAdd(refac, 1ull);
       }
-      for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
+      for (int i = threadIdx.x; i < N; i += NT) x[i] = bb[i];
       __syncthreads();
       cta_lu_solve<T>(LU, N, piv, x);
       sweeps = 0;
@@ -701,12 +711,12 @@ __global__ void __launch_bounds__(kSolveThreads) b_solve_kernel(const BCase* __r
   } else {
     cta_lu_panel_smem<T>(A, N, piv, status, panel);
     if (threadIdx.x == 0) atomicAdd(refac, 1ull);
-    for (int i = threadIdx.x; i < N; i += kSolveThreads) x[i] = bb[i];
+    for (int i = threadIdx.x; i < N; i += NT) x[i] = bb[i];
     __syncthreads();
     cta_lu_solve<T>(A, N, piv, x);
   }
   bool finite = true;
-  for (int i = threadIdx.x; i < N; i += kSolveThreads) {
+  for (int i = threadIdx.x; i < N; i += NT) {
     gamma[b.ring_off + i] = x[i];
     if (!isfinite(x[i])) finite = false;
   }
@@ -1230,11 +1240,11 @@ Error uvlm_batch::enqueue_step() {
   // solve
   const size_t smem = sizeof(double) * 2 * (size_t)max_N + panel_smem_bytes(max_N, mixed() ? 4 : 8);
   if (mixed())
-    b_solve_kernel<float><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
+    b_solve_kernel<float><<<n, SolveCfg<float>::kThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
                                                           d_gamma_hist, d_step, cfg.refine_max_iter, cfg.refine_tol, cfg.stale_factors,
                                                           d_has_factor, d_refac, d_sweeps, d_res, d_status, d_solve_order);
   else
-    b_solve_kernel<double><<<n, kSolveThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
+    b_solve_kernel<double><<<n, SolveCfg<double>::kThreads, smem, st>>>(d_cases, d_A64, d_F32, d_piv, d_rhs, d_gamma,
                                                            d_gamma_hist, d_step, 0, 0.0,
                                                            0, d_has_factor, d_refac, d_sweeps, d_res, d_status, d_solve_order);
   UVLM_LAUNCH_CHECK();
