@@ -467,48 +467,53 @@ Error uvlm_ctx::solve(long long step) {
 
 Error uvlm_ctx::advect(double dt) {
   const WakeLayout L = wl();
-  const long long nt = (long long)num * (wake_nodes - 1) * (C + 1);
   SourceBlock blocks[2];
   int nbk = 0;
   const NBodyPrec prec = stage_prec(UVLM_STAGE_ADVECT);
   nb.near64 = stage_near64(UVLM_STAGE_ADVECT);
-  auto velocity_at = [&](const double* pos_buf, bool rebuild) -> Error {
+  // velocities at the wake rows first_row.. (sources: bound and wake sheets at pos_buf)
+  auto velocity_at = [&](const double* pos_buf, bool rebuild, int first_row) -> Error {
     if (rebuild) UVLM_TRY(build_sources(true, pos_buf, prec, blocks, &nbk));
-    if (nt > 0) {
-      UVLM_TRY(launch_gather_wake(L, pos_buf, d_tx, d_ty, d_tz, st));
-      UVLM_TRY(eval(blocks, nbk, nt, prec, kStageAdvect));
+    const long long n_rows = std::max(0, wake_nodes - first_row);
+    const long long n_tgt = (long long)num * n_rows * (C + 1);
+    if (n_tgt > 0) {
+      UVLM_TRY(launch_gather_wake(L, pos_buf, d_tx, d_ty, d_tz, st, first_row));
+      UVLM_TRY(eval(blocks, nbk, n_tgt, prec, kStageAdvect));
     }
     return ok();
   };
   const int ign = cfg.rk_ignore_rows;
+  // RK2's second evaluation only feeds the rows past ignore_rows (the others take the Euler step,
+  // src/advect.cpp:71-79): its targets start there
+  const int rk2_row0 = std::max(1, ign + 1);
   const bool loads_built = cfg.compute_loads != 0;
   switch (cfg.advection) {
     case UVLM_ADVECT_EULER:
-      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(velocity_at(d_wpos, true, 1));
       UVLM_TRY(launch_advect(kAdvEuler, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
                              ign, st));
       break;
     case UVLM_ADVECT_RK2:
-      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(velocity_at(d_wpos, true, 1));
       UVLM_TRY(launch_advect(kAdvRK2K1, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
                              ign, st));
-      UVLM_TRY(velocity_at(d_wpos2, true));
+      UVLM_TRY(velocity_at(d_wpos2, true, rk2_row0));
       UVLM_TRY(launch_advect(kAdvRK2Upd, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff,
-                             dt, ign, st));
+                             dt, ign, st, rk2_row0));
       break;
     case UVLM_ADVECT_RK4:
-      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(velocity_at(d_wpos, true, 1));
       UVLM_TRY(launch_advect(kAdvRK4K1, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
                              ign, st));
-      UVLM_TRY(velocity_at(d_wpos2, true));
+      UVLM_TRY(velocity_at(d_wpos2, true, 1));
       UVLM_TRY(launch_advect(kAdvRK4K2, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
                              ign, st));
-      UVLM_TRY(velocity_at(d_wpos2, true));
+      UVLM_TRY(velocity_at(d_wpos2, true, 1));
       UVLM_TRY(launch_advect(kAdvRK4Upd, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff,
                              dt, ign, st));
       break;
     case UVLM_ADVECT_AB2:
-      UVLM_TRY(velocity_at(d_wpos, true));
+      UVLM_TRY(velocity_at(d_wpos, true, 1));
       UVLM_TRY(launch_advect(kAdvAB2, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, has_vprev, d_vx, d_vy, d_vz, ff,
                              dt, ign, st));
       has_vprev = true;

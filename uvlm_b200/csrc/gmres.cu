@@ -180,7 +180,6 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
     std::fill(gv.begin(), gv.end(), 0.0);
     gv[0] = beta;
     int j = 0;
-    bool done = false;
     for (; j < m && total < max_iter; ++j) {
       double* Vj = g->V + (size_t)j * n;
       double* Zj = g->Z + (size_t)j * n;
@@ -229,7 +228,6 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
       if (!std::isfinite(gv[j + 1])) return fail(kErrNonFinite, "non-finite GMRES iteration");
       if (std::fabs(gv[j + 1]) <= tol * bnorm || !(hnext > 0)) {
         ++j;
-        done = true;
         break;
       }
     }
@@ -242,7 +240,6 @@ Error gmres_solve(const float* A32, const double* A64, int n, const float* LU, L
     UVLM_CUDA_TRY(cudaMemcpyAsync(g->y, yv.data(), sizeof(double) * j, cudaMemcpyHostToDevice, st));
     update_kernel<<<grid_n(n), 256, 0, st>>>(g->Z, n, j, g->y, x);
     UVLM_LAUNCH_CHECK();
-    (void)done;
   }
   res->iters = total;
   return ok();

@@ -266,14 +266,16 @@ __global__ void __launch_bounds__(BS) loads_kernel(WingShape ws, const double* p
   }
 }
 
-__global__ void gather_wake_kernel(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz) {
+// Wake nodes of rows first_row.. of every wake sheet as SoA targets.
+__global__ void gather_wake_kernel(WakeLayout wl, const double* pos, int first_row, double* tx, double* ty,
+                                   double* tz) {
   const int C1 = wl.C + 1;
-  const int rows = wl.node_rows - 1;
+  const int rows = wl.node_rows - first_row;
   const long long total = (long long)wl.num * rows * C1;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
     const int j = (int)(k % C1);
     const long long nr = k / C1;
-    const int i = (int)(nr % rows) + 1, n = (int)(nr / rows);
+    const int i = (int)(nr % rows) + first_row, n = (int)(nr / rows);
     const double* p = pos + 3 * wl.node(n, i, j);
     tx[k] = p[0];
     ty[k] = p[1];
@@ -281,9 +283,11 @@ __global__ void gather_wake_kernel(WakeLayout wl, const double* pos, double* tx,
   }
 }
 
+// vx/vy/vz hold the induced velocities of the wake rows vrow0.. (the gather's
+// first_row); rows above vrow0 take -ff alone where the mode reads them.
 __global__ void advect_kernel(int mode, WakeLayout wl, double* x, double* pos2, double* k1, double* k2, double* k3,
                               double* vprev, int has_vprev, const double* vx, const double* vy, const double* vz,
-                              d3 ff, double dt, int ignore) {
+                              d3 ff, double dt, int ignore, int vrow0) {
   const int C1 = wl.C + 1;
   const long long total = (long long)wl.num * wl.node_rows * C1;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
@@ -293,8 +297,8 @@ __global__ void advect_kernel(int mode, WakeLayout wl, double* x, double* pos2, 
     const long long P = 3 * wl.node(n, i, j);
     const d3 mff = mk(-ff.x, -ff.y, -ff.z);
     d3 u = mff;
-    if (i >= 1) {
-      const long long ti = ((long long)n * (wl.node_rows - 1) + (i - 1)) * C1 + j;
+    if (i >= vrow0) {
+      const long long ti = ((long long)n * (wl.node_rows - vrow0) + (i - vrow0)) * C1 + j;
       u = add(mff, mk(vx[ti], vy[ti], vz[ti]));
     }
     const d3 xp = ld3(x + P);
@@ -460,21 +464,22 @@ Error launch_loads(WingShape ws, const double* pos, const double* gamma, const d
   return ok();
 }
 
-Error launch_gather_wake(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz, cudaStream_t st) {
-  if (wl.node_rows < 2) return ok();
-  gather_wake_kernel<<<grid_for((long long)wl.num * (wl.node_rows - 1) * (wl.C + 1)), 256, 0, st>>>(wl, pos, tx, ty,
-                                                                                                   tz);
+Error launch_gather_wake(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz, cudaStream_t st,
+                         int first_row) {
+  if (first_row < 1 || wl.node_rows <= first_row) return ok();
+  gather_wake_kernel<<<grid_for((long long)wl.num * (wl.node_rows - first_row) * (wl.C + 1)), 256, 0, st>>>(
+      wl, pos, first_row, tx, ty, tz);
   UVLM_LAUNCH_CHECK();
   return ok();
 }
 
 Error launch_advect(AdvectMode mode, WakeLayout wl, double* x, double* pos2, double* k1, double* k2, double* k3,
                     double* vprev, bool has_vprev, const double* vx, const double* vy, const double* vz,
-                    const double ff[3], double dt, int ignore_rows, cudaStream_t st) {
+                    const double ff[3], double dt, int ignore_rows, cudaStream_t st, int vrow0) {
   if (wl.node_rows < 1) return ok();
   advect_kernel<<<grid_for((long long)wl.num * wl.node_rows * (wl.C + 1)), 256, 0, st>>>(
       (int)mode, wl, x, pos2, k1, k2, k3, vprev, has_vprev ? 1 : 0, vx, vy, vz, mk(ff[0], ff[1], ff[2]), dt,
-      ignore_rows);
+      ignore_rows, vrow0);
   UVLM_LAUNCH_CHECK();
   return ok();
 }

@@ -64,8 +64,10 @@ Error launch_loads(WingShape ws, const double* pos, const double* gamma, const d
                    const double* normal, const double* area, const double* vx, const double* vy, const double* vz,
                    const double* line_uls, const double ff[3], const double* chord_span, double t, double dt,
                    double* row, cudaStream_t st);
-// wake node rows 1..node_rows-1 of pos into SoA targets
-Error launch_gather_wake(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz, cudaStream_t st);
+// wake node rows first_row..node_rows-1 of pos into SoA targets (row 0, the
+// trailing edge, moves with -ff alone)
+Error launch_gather_wake(WakeLayout wl, const double* pos, double* tx, double* ty, double* tz, cudaStream_t st,
+                         int first_row = 1);
 
 enum AdvectMode {
   kAdvEuler = 0,
@@ -76,10 +78,12 @@ enum AdvectMode {
   kAdvRK4Upd = 5,   // k3 = u; x = x + (k1 + 2k2 + 2k3 + k3) dt/6 (rows > ignore) else x + k1 dt
   kAdvAB2 = 6,      // v = u; x = x + (3v - v_prev) dt/2 (rows >= 1, with history) else x + v dt
 };
-// u = -ff + vel (rows >= 1, vel indexed like launch_gather_wake) or -ff (row 0)
+// u = -ff + vel (rows >= vrow0, vel indexed like launch_gather_wake with
+// first_row = vrow0) or -ff (rows above vrow0; for kAdvRK2Upd with vrow0 =
+// ignore_rows + 1 those rows take the Euler step and do not read u)
 Error launch_advect(AdvectMode mode, WakeLayout wl, double* x, double* pos2, double* k1, double* k2, double* k3,
                     double* vprev, bool has_vprev, const double* vx, const double* vy, const double* vz,
-                    const double ff[3], double dt, int ignore_rows, cudaStream_t st);
+                    const double ff[3], double dt, int ignore_rows, cudaStream_t st, int vrow0 = 1);
 // in-place relocation of the live wake rows (compaction of the prepend buffer)
 Error launch_move_rows(double* buf, int num, int PR, int row_elems, int from, int to, int rows, double* tmp,
                        cudaStream_t st);
