@@ -115,6 +115,32 @@ def test_invalid_advection_name_is_rejected_without_device():
     assert "euler" in str(ei.value)
 
 
+@pytest.mark.parametrize("field,value,message", [
+    ("precision", 7, "unknown precision"),
+    ("advection", 4, "invalid configuration"),
+    ("max_wake_rows", 0, "invalid configuration"),
+    ("gmres_tol", 0.0, "invalid configuration"),
+    ("preconditioner", 2, "invalid configuration"),
+    ("nbody_fp64_stages", 8, "invalid configuration"),
+    ("nbody_near_fp64", -1, "invalid configuration"),
+    ("lu_pivoting", 2, "invalid configuration"),
+    ("gmres_refresh_iter", -1, "invalid configuration"),
+])
+def test_invalid_configuration_is_rejected_before_the_device(field, value, message):
+    """uvlm_create checks the configuration before it looks for a device, so a
+    bad field reads UVLM_ERR_INVALID on any machine (and no context is made)."""
+    from uvlm_b200 import _capi
+
+    L = _capi.lib()
+    cfg = _capi.Config()
+    L.uvlm_config_default(C.byref(cfg))
+    setattr(cfg, field, value)
+    out = C.c_void_p(1)
+    assert L.uvlm_create(C.byref(cfg), C.byref(out)) == 1
+    assert out.value is None
+    assert message in L.uvlm_global_last_error().decode()
+
+
 def test_oracle_is_not_linked_into_the_product():
     from uvlm_b200 import _capi
 
