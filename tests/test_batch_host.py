@@ -3,6 +3,7 @@ case sharding over ranks (world size 2, gloo on CPU; no GPU)."""
 import os
 
 import numpy as np
+import pytest
 
 
 def test_draw_cases_ranges_and_seed():
@@ -89,3 +90,53 @@ def test_gather_case_rows_single_process_needs_every_case():
     np.testing.assert_array_equal(gather_case_rows(rows, [1, 0], 2), rows[:, ::-1])
     with pytest.raises(ValueError):
         gather_case_rows(rows, [0, 1], 3)
+
+
+def _batch_create(cfg_changes=None, case_changes=None, n=1):
+    import ctypes as C
+
+    from uvlm_b200 import _capi
+
+    L = _capi.lib()
+    cfg = _capi.BatchConfig()
+    L.uvlm_batch_config_default(C.byref(cfg))
+    for k, v in (cfg_changes or {}).items():
+        setattr(cfg, k, v)
+    cases = (_capi.BatchCase * n)()
+    for c in cases:
+        c.chord, c.span, c.rows, c.cols, c.dt = 1.0, 4.0, 4, 8, 0.1
+        c.forward_flight[0] = -1.0
+        for k, v in (case_changes or {}).items():
+            setattr(c, k, v)
+    out = C.c_void_p(1)
+    rc = L.uvlm_batch_create(C.byref(cfg), cases, n, C.byref(out))
+    return rc, out.value, L.uvlm_global_last_error().decode()
+
+
+
+@pytest.mark.parametrize("field,value", [
+    ("precision", 5), ("advection", 2), ("max_steps", 0), ("refine_max_iter", -1), ("refine_tol", 0.0),
+    ("nbody_tile", -2), ("nbody_tile", 3),
+])
+def test_batch_invalid_configuration_is_rejected_before_the_device(field, value):
+    """uvlm_batch_create checks its configuration and every case before it
+    looks for a device: UVLM_ERR_INVALID on any machine, no handle."""
+    rc, h, msg = _batch_create({field: value})
+    assert rc == 1 and h is None
+    assert "invalid configuration" in msg
+
+
+@pytest.mark.parametrize("field,value", [
+    ("rows", 0), ("rows", 65), ("cols", 7), ("cols", 66), ("cols", 0), ("chord", 0.0), ("span", -1.0), ("dt", 0.0),
+])
+def test_batch_invalid_case_is_rejected_before_the_device(field, value):
+    rc, h, msg = _batch_create(case_changes={field: value}, n=3)
+    assert rc == 1 and h is None
+    assert "every case needs" in msg
+
+
+def test_batch_case_size_limit():
+    # 32 x 40 = 1280 rings per case is above the one-CTA solve's 1024
+    rc, h, msg = _batch_create(case_changes={"rows": 32, "cols": 40})
+    assert rc == 1 and h is None
+    assert "rows * cols <= 1024" in msg
