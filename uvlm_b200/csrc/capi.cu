@@ -483,8 +483,9 @@ Error uvlm_ctx::advect(double dt) {
     return ok();
   };
   const int ign = cfg.rk_ignore_rows;
-  // RK2's second evaluation only feeds the rows past ignore_rows (the others take the Euler step,
-  // src/advect.cpp:71-79): its targets start there
+  // The last evaluation of RK2 and of RK4 only feeds the rows past ignore_rows (the others take the
+  // Euler step, src/advect.cpp:71-79, :167-178): its targets start there.  The earlier RK4
+  // evaluations move the whole intermediate wake (the sources of the next one) and take every row.
   const int rk2_row0 = std::max(1, ign + 1);
   const bool loads_built = cfg.compute_loads != 0;
   switch (cfg.advection) {
@@ -508,9 +509,9 @@ Error uvlm_ctx::advect(double dt) {
       UVLM_TRY(velocity_at(d_wpos2, true, 1));
       UVLM_TRY(launch_advect(kAdvRK4K2, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff, dt,
                              ign, st));
-      UVLM_TRY(velocity_at(d_wpos2, true, 1));
+      UVLM_TRY(velocity_at(d_wpos2, true, rk2_row0));
       UVLM_TRY(launch_advect(kAdvRK4Upd, L, d_wpos, d_wpos2, d_k1, d_k2, d_k3, d_vprev, false, d_vx, d_vy, d_vz, ff,
-                             dt, ign, st));
+                             dt, ign, st, rk2_row0));
       break;
     case UVLM_ADVECT_AB2:
       UVLM_TRY(velocity_at(d_wpos, true, 1));

@@ -79,8 +79,8 @@ enum AdvectMode {
   kAdvAB2 = 6,      // v = u; x = x + (3v - v_prev) dt/2 (rows >= 1, with history) else x + v dt
 };
 // u = -ff + vel (rows >= vrow0, vel indexed like launch_gather_wake with
-// first_row = vrow0) or -ff (rows above vrow0; for kAdvRK2Upd with vrow0 =
-// ignore_rows + 1 those rows take the Euler step and do not read u)
+// first_row = vrow0) or -ff (rows above vrow0; for kAdvRK2Upd and kAdvRK4Upd
+// with vrow0 = ignore_rows + 1 those rows take the Euler step and do not read u)
 Error launch_advect(AdvectMode mode, WakeLayout wl, double* x, double* pos2, double* k1, double* k2, double* k3,
                     double* vprev, bool has_vprev, const double* vx, const double* vy, const double* vz,
                     const double ff[3], double dt, int ignore_rows, cudaStream_t st, int vrow0 = 1);
