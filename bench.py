@@ -139,13 +139,17 @@ class Workload:
         sim.set_advection(self.advection)
         return sim
 
-    def advect_pairs(self):
+    def advect_pairs(self, ignore_rows=5):
         """(target, unique segment) pairs of the advection stage at the held
-        wake: W + 1 ring rows before the erase, node rows 1..W+1 as targets."""
-        R, Cc, W = self.rows, self.cols, self.wake_rows + 1
+        wake: the bound sheets and W ring rows of wake as sources, the wake
+        node rows 1..W+1 as targets of each evaluation, except the last one of
+        RK2 and RK4, whose targets are the rows past ignore_rows (the others
+        take the Euler step)."""
+        R, Cc, W = self.rows, self.cols, self.wake_rows
         segs = self.num * ((R + 1) * Cc + R * (Cc + 1) + (W + 1) * Cc + W * (Cc + 1))
-        evals = {"euler": 1, "RK2": 2, "RK4": 3, "AB2": 1}[self.advection]
-        return evals * self.num * W * (Cc + 1) * segs
+        full = {"euler": 1, "RK2": 1, "RK4": 2, "AB2": 1}[self.advection]
+        rows = full * (W + 1) + (max(0, W + 1 - ignore_rows) if self.advection in ("RK2", "RK4") else 0)
+        return self.num * rows * (Cc + 1) * segs
 
 
 def _heave_pitch():
@@ -203,28 +207,85 @@ def make_sim(precision, wl=None, **kw):
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during a timed region.
 
-    def __init__(self, gpu_index):
+    NVML (the nvidia_ml_py bindings; read-only queries) every 10 ms where it
+    loads, else nvidia-smi every 200 ms (a short region then gets one or two
+    samples).  `nvml` replaces the bindings module (tests)."""
+
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, gpu_index, nvml=None):
         self.gpu = gpu_index
-        self.samples = []
+        self.samples = []  # (sm MHz, max sm MHz, active reason names)
         self._stop = threading.Event()
         self._t = None
+        self._nvml = nvml
+        self._nvml_open = None
+        self.source = None
 
-    def start(self):
-        def run():
-            q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-            while not self._stop.is_set():
+    def _nvml_reader(self):
+        mod = self._nvml
+        if mod is None:
+            try:
+                import pynvml as mod
+            except Exception:
+                return None
+        try:
+            mod.nvmlInit()
+            self._nvml_open = mod
+            h = mod.nvmlDeviceGetHandleByIndex(self.gpu)
+            # the clocks-event query of newer drivers, else its older name
+            get_reasons = mod.nvmlDeviceGetCurrentClocksThrottleReasons
+            newer = getattr(mod, "nvmlDeviceGetCurrentClocksEventReasons", None)
+            if newer is not None:
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([x.strip() for x in out.split(",")])
+                    newer(h)
+                    get_reasons = newer
                 except Exception:
                     pass
-                self._stop.wait(0.2)
+            bits = (getattr(mod, "nvmlClocksThrottleReasonHwSlowdown", 0x8),
+                    getattr(mod, "nvmlClocksThrottleReasonHwThermalSlowdown", 0x40),
+                    getattr(mod, "nvmlClocksThrottleReasonSwThermalSlowdown", 0x20),
+                    getattr(mod, "nvmlClocksThrottleReasonSwPowerCap", 0x4))
+            mx = float(mod.nvmlDeviceGetMaxClockInfo(h, mod.NVML_CLOCK_SM))
+
+            def read():
+                mask = int(get_reasons(h))
+                return (float(mod.nvmlDeviceGetClockInfo(h, mod.NVML_CLOCK_SM)), mx,
+                        tuple(n for n, b in zip(self.NAMES, bits) if mask & b))
+
+            read()
+            return read
+        except Exception:
+            return None
+
+    def _smi_read(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=5).stdout.strip()
+        if not out:
+            return None
+        f = [x.strip() for x in out.split(",")]
+        num = lambda x: float(x) if x.replace(".", "").isdigit() else None  # noqa: E731
+        return (num(f[0]), num(f[1]), tuple(n for i, n in enumerate(self.NAMES) if f[2 + i] == "Active"))
+
+    def start(self):
+        read = self._nvml_reader()
+        self.source = "nvml" if read else "nvidia-smi"
+        period = 0.01 if read else 0.2
+        read = read or self._smi_read
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    smp = read()
+                    if smp:
+                        self.samples.append(smp)
+                except Exception:
+                    pass
+                self._stop.wait(period)
 
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
@@ -233,14 +294,19 @@ class Clocks:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
+        if self._nvml_open is not None:
+            try:
+                self._nvml_open.nvmlShutdown()
+            except Exception:
+                pass
+            self._nvml_open = None
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].strip() == "Active"})
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "source": self.source}
+        sm = [x[0] for x in self.samples if x[0] is not None]
+        mx = [x[1] for x in self.samples if x[1] is not None]
+        reasons = sorted({n for x in self.samples for n in x[2]})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples), "source": self.source}
 
 
 def oracle_sample(wl, state, stride, lu_n, threads):
